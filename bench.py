@@ -1,0 +1,347 @@
+"""TRSM benchmark: one JSON line on rank 0.
+
+Headline workload: dtrsm side=L, uplo=L, transA=N, diag=N, m=16384, n=4096, alpha=1, lda=ldb=m
+(the precision-form problem size) in the plain FP64 form.  A is the condition-band recipe
+(band k=0) with a NaN upper triangle; B ~ U(-1,1).  One step = restore the right-hand side
+(a device copy of 512 MiB, inside the timed region) + one rocblas_dtrsm through the C ABI.
+A (2 GiB) and B (512 MiB) are larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: a single solve does not shard (SURVEY: replicas only), so N ranks each run their
+own independent solve; `value` is the sum over ranks of m*n*k flops / the max-over-ranks time.
+`--impl reference` times the host CBLAS trsm (OpenBLAS bundled with scipy, the library the
+reference's ref_trsm wraps) on all host cores on a bounded column sample of the same problem.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M, N = 16384, 4096
+FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
+WORKLOAD = "dtrsm L/L/N/N m=16384 n=4096 lda=ldb=16384 alpha=1 (condition band k=0), plain FP64"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 dense peak on this GPU: cuBLAS DGEMM 8192^3 (torch.matmul), best of 5."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_cblas_sample(A_host, B_host, ncols, threads):
+    """Time host cblas_dtrsm on the first `ncols` right-hand sides; returns (TFLOP/s, s, X)."""
+    import oracle
+
+    oracle.cblas_set_threads(threads)
+    Bs = np.asfortranarray(B_host[:, :ncols])
+    # the host BLAS may read the unused triangle in blocked kernels: give it zeros there
+    t0 = time.perf_counter()
+    oracle.cblas_trsm_inplace("L", "L", "N", "N", 1.0, A_host, Bs)
+    dt = time.perf_counter() - t0
+    return float(M) * M * ncols / dt / 1e12, dt, Bs
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    import oracle
+
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    m = M
+    # host copy of the same recipe (numpy stream): lower triangle, zeros above for the CBLAS
+    A, B = oracle.condition_band_problem(0, m, 64, 0)
+    A = np.asfortranarray(np.tril(np.nan_to_num(A, nan=0.0)))
+    ncols = 64
+    for _ in range(args.warmup):
+        cpu_cblas_sample(A, B, ncols, threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt, _ = cpu_cblas_sample(A, B, ncols, threads)
+        times.append(dt)
+    tot = sum(times)
+    val = float(m) * m * ncols * args.steps / tot / 1e12
+    del rng
+    line = {
+        "metric": "dtrsm TFLOP/s", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "m": M, "n": N},
+        "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+                         "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) on "
+                                   f"{ncols} of the {N} right-hand sides per step, full m={M}"},
+        "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    import rocblas_b200 as rb
+    from rocblas_b200 import workloads
+
+    rank, world, local = _env_rank()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    rb.build()
+    L = rb.lib()
+
+    At, B0 = workloads.condition_band_lower_torch(M, N, 0, seed=1234 + rank, device=dev)
+    Bt = B0.clone()
+    stream = torch.cuda.current_stream(dev)
+    h = rb.Handle()
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    # reserve the invA workspace up front (128 * m doubles)
+    assert L.rocblas_set_device_memory_size(h.value, 128 * M * 8) == 0
+    one = ctypes.c_double(1.0)
+    one_p = ctypes.cast(ctypes.byref(one), ctypes.c_void_p)
+
+    def solve(Bbuf, Abuf=At):
+        st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
+                             rb.diagonal_non_unit, M, N, one_p, ctypes.c_void_p(Abuf.data_ptr()), M,
+                             ctypes.c_void_p(Bbuf.data_ptr()), M)
+        if st != 0:
+            raise rb.RocblasError("rocblas_dtrsm", st)
+
+    def step():
+        Bt.copy_(B0)
+        solve(Bt)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    sampler = ClockSampler(dev.index if dev.index is not None else 0)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = L.rocblas_b200_kernel_launch_count()
+    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_m = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev_s[i].record(stream)
+        Bt.copy_(B0)
+        ev_m[i].record(stream)
+        solve(Bt)
+        ev_e[i].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    launches = L.rocblas_b200_kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    solve_ms = [ev_m[i].elapsed_time(ev_e[i]) for i in range(args.steps)]
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = FLOPS * world / (ms_per_step * 1e-3) / 1e12
+
+    # ---- e2e: host buffers through the C ABI, copies inside the timed region -----------
+    e2e = None
+    if rank == 0:
+        A_host = torch.empty_like(At, device="cpu").pin_memory()
+        B_host = torch.empty_like(B0, device="cpu").pin_memory()
+        A_host.copy_(At)
+        B_host.copy_(B0)
+        Ad = torch.empty_like(At)
+        Bd = torch.empty_like(B0)
+
+        def e2e_step():
+            Ad.copy_(A_host, non_blocking=True)
+            Bd.copy_(B_host, non_blocking=True)
+            solve(Bd, Ad)
+            B_host.copy_(Bd, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        B_host.copy_(B0)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ksteps = max(2, min(args.steps, 5))
+        s0.record(stream)
+        for _ in range(ksteps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = s0.elapsed_time(s1) / ksteps
+        e2e = {"value": FLOPS / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(At.numel() * 8 + B0.numel() * 8),
+               "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms}
+        del Ad, Bd, A_host, B_host
+
+    # ---- error against the FP64 host oracle on a column sample + CPU baseline --------------
+    extra = {}
+    if rank == 0:
+        import oracle
+
+        peak = fp64_peak_tflops(torch, dev)
+        solve_med = statistics.median(solve_ms)
+        achieved = FLOPS / (solve_med * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "kernel": "whole rocblas_dtrsm call (DMMA GEMM tiles + trtri + invA leaves)",
+                    "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
+                                   "MEASURED_PEAKS.json has no FP64 figure"}
+        # final X of the last timed step is in Bt; A on the host (upper triangle -> 0)
+        X = Bt.cpu().numpy().T  # (m, n) view of column-major storage
+        A_host = np.asfortranarray(np.nan_to_num(At.cpu().numpy().T, nan=0.0))
+        B_host = np.asfortranarray(B0.cpu().numpy().T)
+        threads = os.cpu_count() or 1
+        ncols = 64
+        cpu_tflops, cpu_s, Xc = cpu_cblas_sample(A_host, B_host, ncols, threads)
+        cols = list(range(8))
+        Xq = oracle.trsm("L", "L", "N", "N", 1.0, A_host, np.asfortranarray(B_host[:, cols]), precision="q")
+        err_q = oracle.normwise_forward_error(X[:, cols], Xq)
+        err_c = oracle.normwise_forward_error(X[:, :ncols], Xc)
+        err_c_vs_q = oracle.normwise_forward_error(Xc[:, cols], Xq)
+        extra = {
+            "roofline": roofline,
+            "cpu_baseline": {"value": cpu_tflops, "unit": "TFLOP/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) "
+                                       f"on {ncols} of the {N} right-hand sides, full m={M}, "
+                                       f"{cpu_s:.2f} s"},
+            "error": {"vs_fp64_cblas_normwise": err_c, "vs_float128_oracle_normwise": err_q,
+                      "fp64_cblas_vs_float128": err_c_vs_q,
+                      "sample": f"columns 0..{ncols - 1} (cblas) / 0..7 (float128 oracle)"},
+            "solve_ms_median": solve_med,
+        }
+
+    if rank == 0:
+        line = {
+            "metric": "dtrsm TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "m": M, "n": N, "form": "plain FP64",
+                       "l2": "inputs larger than L2 (A 2 GiB, B 512 MiB); no flush",
+                       "step": "device copy of B (512 MiB) + rocblas_dtrsm",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,356 @@
+/*
+ * rocblas.h -- the drop-in C ABI of the B200 TRSM library (librocblas_b200.so).
+ *
+ * This header declares the subset of the rocBLAS C API that the level-3 triangular-solve
+ * path uses: handle / stream / pointer-mode / device-memory functions, rocblas_{s,d}trsm
+ * and its _batched, _strided_batched and _ex forms, and rocblas_{s,d}trtri (which builds
+ * the invA that the _ex forms accept).  Types, enum values, status codes and argument
+ * meaning are those of the reference so that existing callers relink unchanged;
+ * hipStream_t becomes cudaStream_t.  Each declaration cites the reference declaration it
+ * replaces (paths inside the rocBLAS source tree).
+ *
+ * Conventions (as in the reference):
+ *   - column-major storage, leading dimensions in elements;
+ *   - A, B, invA and device-mode alpha are device pointers; B is overwritten with X;
+ *   - every call is asynchronous on the handle's stream (return != completion);
+ *   - no function throws; failures are reported as rocblas_status.
+ */
+#ifndef ROCBLAS_B200_ROCBLAS_H
+#define ROCBLAS_B200_ROCBLAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+#include <cuda_runtime_api.h>
+
+#if defined(__GNUC__)
+#define ROCBLAS_EXPORT __attribute__((visibility("default")))
+#else
+#define ROCBLAS_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- types: library/include/internal/rocblas-types.h:60-245 ---------------------------- */
+typedef struct _rocblas_handle* rocblas_handle; /* rocblas-types.h:64 */
+typedef int32_t rocblas_int;                    /* rocblas-types.h:80 (LP64 API) */
+typedef int64_t rocblas_stride;                 /* rocblas-types.h:84 */
+typedef float   rocblas_float;
+typedef double  rocblas_double;
+
+typedef enum rocblas_operation_ /* rocblas-types.h:123-129 */
+{
+    rocblas_operation_none                = 111,
+    rocblas_operation_transpose           = 112,
+    rocblas_operation_conjugate_transpose = 113
+} rocblas_operation;
+
+typedef enum rocblas_fill_ /* rocblas-types.h:134-139 */
+{
+    rocblas_fill_upper = 121,
+    rocblas_fill_lower = 122,
+    rocblas_fill_full  = 123
+} rocblas_fill;
+
+typedef enum rocblas_diagonal_ /* rocblas-types.h:144-148 */
+{
+    rocblas_diagonal_non_unit = 131,
+    rocblas_diagonal_unit     = 132
+} rocblas_diagonal;
+
+typedef enum rocblas_side_ /* rocblas-types.h:151-157 */
+{
+    rocblas_side_left  = 141,
+    rocblas_side_right = 142,
+    rocblas_side_both  = 143
+} rocblas_side;
+
+typedef enum rocblas_datatype_ /* rocblas-types.h:164-184 */
+{
+    rocblas_datatype_f16_r   = 150,
+    rocblas_datatype_f32_r   = 151,
+    rocblas_datatype_f64_r   = 152,
+    rocblas_datatype_f16_c   = 153,
+    rocblas_datatype_f32_c   = 154,
+    rocblas_datatype_f64_c   = 155,
+    rocblas_datatype_i8_r    = 160,
+    rocblas_datatype_u8_r    = 161,
+    rocblas_datatype_i32_r   = 162,
+    rocblas_datatype_u32_r   = 163,
+    rocblas_datatype_i8_c    = 164,
+    rocblas_datatype_u8_c    = 165,
+    rocblas_datatype_i32_c   = 166,
+    rocblas_datatype_u32_c   = 167,
+    rocblas_datatype_bf16_r  = 168,
+    rocblas_datatype_bf16_c  = 169,
+    rocblas_datatype_f8_r    = 170,
+    rocblas_datatype_bf8_r   = 171,
+    rocblas_datatype_invalid = 255
+} rocblas_datatype;
+
+typedef enum rocblas_status_ /* rocblas-types.h:203-223 */
+{
+    rocblas_status_success             = 0,
+    rocblas_status_invalid_handle      = 1,
+    rocblas_status_not_implemented     = 2,
+    rocblas_status_invalid_pointer     = 3,
+    rocblas_status_invalid_size        = 4,
+    rocblas_status_memory_error        = 5,
+    rocblas_status_internal_error      = 6,
+    rocblas_status_perf_degraded       = 7,
+    rocblas_status_size_query_mismatch = 8,
+    rocblas_status_size_increased      = 9,
+    rocblas_status_size_unchanged      = 10,
+    rocblas_status_invalid_value       = 11,
+    rocblas_status_continue            = 12,
+    rocblas_status_check_numerics_fail = 13,
+    rocblas_status_excluded_from_build = 14,
+    rocblas_status_arch_mismatch       = 15
+} rocblas_status;
+
+typedef enum rocblas_pointer_mode_ /* rocblas-types.h:228-234 */
+{
+    rocblas_pointer_mode_host   = 0,
+    rocblas_pointer_mode_device = 1
+} rocblas_pointer_mode;
+
+/* ---- handle / stream / pointer mode: library/include/internal/rocblas-auxiliary.h:40-61 --- */
+ROCBLAS_EXPORT rocblas_status rocblas_create_handle(rocblas_handle* handle);
+ROCBLAS_EXPORT rocblas_status rocblas_destroy_handle(rocblas_handle handle);
+ROCBLAS_EXPORT rocblas_status rocblas_set_stream(rocblas_handle handle, cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_get_stream(rocblas_handle handle, cudaStream_t* stream);
+ROCBLAS_EXPORT rocblas_status rocblas_set_pointer_mode(rocblas_handle       handle,
+                                                       rocblas_pointer_mode pointer_mode);
+ROCBLAS_EXPORT rocblas_status rocblas_get_pointer_mode(rocblas_handle        handle,
+                                                       rocblas_pointer_mode* pointer_mode);
+/* rocblas-auxiliary.h:97 */
+ROCBLAS_EXPORT rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr);
+
+/* ---- device memory: library/include/internal/rocblas-functions.h:25027-25122 ---------- */
+ROCBLAS_EXPORT rocblas_status rocblas_start_device_memory_size_query(rocblas_handle handle);
+ROCBLAS_EXPORT rocblas_status rocblas_stop_device_memory_size_query(rocblas_handle handle,
+                                                                    size_t*        size);
+ROCBLAS_EXPORT bool           rocblas_is_device_memory_size_query(rocblas_handle handle);
+ROCBLAS_EXPORT rocblas_status rocblas_get_device_memory_size(rocblas_handle handle, size_t* size);
+ROCBLAS_EXPORT rocblas_status rocblas_set_device_memory_size(rocblas_handle handle, size_t size);
+ROCBLAS_EXPORT rocblas_status rocblas_set_workspace(rocblas_handle handle, void* addr, size_t size);
+ROCBLAS_EXPORT bool           rocblas_is_managing_device_memory(rocblas_handle handle);
+ROCBLAS_EXPORT bool           rocblas_is_user_managing_device_memory(rocblas_handle handle);
+
+/* ---- trsm: rocblas-functions.h:19388-19412 -------------------------------------------- */
+ROCBLAS_EXPORT rocblas_status rocblas_strsm(rocblas_handle    handle,
+                                            rocblas_side      side,
+                                            rocblas_fill      uplo,
+                                            rocblas_operation transA,
+                                            rocblas_diagonal  diag,
+                                            rocblas_int       m,
+                                            rocblas_int       n,
+                                            const float*      alpha,
+                                            const float*      A,
+                                            rocblas_int       lda,
+                                            float*            B,
+                                            rocblas_int       ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm(rocblas_handle    handle,
+                                            rocblas_side      side,
+                                            rocblas_fill      uplo,
+                                            rocblas_operation transA,
+                                            rocblas_diagonal  diag,
+                                            rocblas_int       m,
+                                            rocblas_int       n,
+                                            const double*     alpha,
+                                            const double*     A,
+                                            rocblas_int       lda,
+                                            double*           B,
+                                            rocblas_int       ldb);
+
+/* ---- trsm_batched: rocblas-functions.h:19574-19601 (A, B: device arrays of device
+ *      pointers) ----------------------------------------------------------------------- */
+ROCBLAS_EXPORT rocblas_status rocblas_strsm_batched(rocblas_handle     handle,
+                                                    rocblas_side       side,
+                                                    rocblas_fill       uplo,
+                                                    rocblas_operation  transA,
+                                                    rocblas_diagonal   diag,
+                                                    rocblas_int        m,
+                                                    rocblas_int        n,
+                                                    const float*       alpha,
+                                                    const float* const A[],
+                                                    rocblas_int        lda,
+                                                    float* const       B[],
+                                                    rocblas_int        ldb,
+                                                    rocblas_int        batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm_batched(rocblas_handle      handle,
+                                                    rocblas_side        side,
+                                                    rocblas_fill        uplo,
+                                                    rocblas_operation   transA,
+                                                    rocblas_diagonal    diag,
+                                                    rocblas_int         m,
+                                                    rocblas_int         n,
+                                                    const double*       alpha,
+                                                    const double* const A[],
+                                                    rocblas_int         lda,
+                                                    double* const       B[],
+                                                    rocblas_int         ldb,
+                                                    rocblas_int         batch_count);
+
+/* ---- trsm_strided_batched: rocblas-functions.h:19774-19805 ---------------------------- */
+ROCBLAS_EXPORT rocblas_status rocblas_strsm_strided_batched(rocblas_handle    handle,
+                                                            rocblas_side      side,
+                                                            rocblas_fill      uplo,
+                                                            rocblas_operation transA,
+                                                            rocblas_diagonal  diag,
+                                                            rocblas_int       m,
+                                                            rocblas_int       n,
+                                                            const float*      alpha,
+                                                            const float*      A,
+                                                            rocblas_int       lda,
+                                                            rocblas_stride    stride_a,
+                                                            float*            B,
+                                                            rocblas_int       ldb,
+                                                            rocblas_stride    stride_b,
+                                                            rocblas_int       batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm_strided_batched(rocblas_handle    handle,
+                                                            rocblas_side      side,
+                                                            rocblas_fill      uplo,
+                                                            rocblas_operation transA,
+                                                            rocblas_diagonal  diag,
+                                                            rocblas_int       m,
+                                                            rocblas_int       n,
+                                                            const double*     alpha,
+                                                            const double*     A,
+                                                            rocblas_int       lda,
+                                                            rocblas_stride    stride_a,
+                                                            double*           B,
+                                                            rocblas_int       ldb,
+                                                            rocblas_stride    stride_b,
+                                                            rocblas_int       batch_count);
+
+/* ---- trsm_ex family: rocblas-functions.h:23223-23238, 23404-23420, 23563-23581.
+ *      invA: packed 128 x 128 inverses of the diagonal blocks of A (ld 128, stride
+ *      128*128) followed by the k % 128 remainder block; invA_size in elements.
+ *      compute_type f32_r / f64_r; complex types return rocblas_status_not_implemented. */
+ROCBLAS_EXPORT rocblas_status rocblas_trsm_ex(rocblas_handle    handle,
+                                              rocblas_side      side,
+                                              rocblas_fill      uplo,
+                                              rocblas_operation transA,
+                                              rocblas_diagonal  diag,
+                                              rocblas_int       m,
+                                              rocblas_int       n,
+                                              const void*       alpha,
+                                              const void*       A,
+                                              rocblas_int       lda,
+                                              void*             B,
+                                              rocblas_int       ldb,
+                                              const void*       invA,
+                                              rocblas_int       invA_size,
+                                              rocblas_datatype  compute_type);
+
+ROCBLAS_EXPORT rocblas_status rocblas_trsm_batched_ex(rocblas_handle    handle,
+                                                      rocblas_side      side,
+                                                      rocblas_fill      uplo,
+                                                      rocblas_operation transA,
+                                                      rocblas_diagonal  diag,
+                                                      rocblas_int       m,
+                                                      rocblas_int       n,
+                                                      const void*       alpha,
+                                                      const void*       A,
+                                                      rocblas_int       lda,
+                                                      void*             B,
+                                                      rocblas_int       ldb,
+                                                      rocblas_int       batch_count,
+                                                      const void*       invA,
+                                                      rocblas_int       invA_size,
+                                                      rocblas_datatype  compute_type);
+
+ROCBLAS_EXPORT rocblas_status rocblas_trsm_strided_batched_ex(rocblas_handle    handle,
+                                                              rocblas_side      side,
+                                                              rocblas_fill      uplo,
+                                                              rocblas_operation transA,
+                                                              rocblas_diagonal  diag,
+                                                              rocblas_int       m,
+                                                              rocblas_int       n,
+                                                              const void*       alpha,
+                                                              const void*       A,
+                                                              rocblas_int       lda,
+                                                              rocblas_stride    stride_A,
+                                                              void*             B,
+                                                              rocblas_int       ldb,
+                                                              rocblas_stride    stride_B,
+                                                              rocblas_int       batch_count,
+                                                              const void*       invA,
+                                                              rocblas_int       invA_size,
+                                                              rocblas_stride    stride_invA,
+                                                              rocblas_datatype  compute_type);
+
+/* ---- trtri: rocblas-functions.h:19081-19098, 19159-19177, 19249-19272 ----------------- */
+ROCBLAS_EXPORT rocblas_status rocblas_strtri(rocblas_handle   handle,
+                                             rocblas_fill     uplo,
+                                             rocblas_diagonal diag,
+                                             rocblas_int      n,
+                                             const float*     A,
+                                             rocblas_int      lda,
+                                             float*           invA,
+                                             rocblas_int      ldinvA);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrtri(rocblas_handle   handle,
+                                             rocblas_fill     uplo,
+                                             rocblas_diagonal diag,
+                                             rocblas_int      n,
+                                             const double*    A,
+                                             rocblas_int      lda,
+                                             double*          invA,
+                                             rocblas_int      ldinvA);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strtri_batched(rocblas_handle     handle,
+                                                     rocblas_fill       uplo,
+                                                     rocblas_diagonal   diag,
+                                                     rocblas_int        n,
+                                                     const float* const A[],
+                                                     rocblas_int        lda,
+                                                     float* const       invA[],
+                                                     rocblas_int        ldinvA,
+                                                     rocblas_int        batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrtri_batched(rocblas_handle      handle,
+                                                     rocblas_fill        uplo,
+                                                     rocblas_diagonal    diag,
+                                                     rocblas_int         n,
+                                                     const double* const A[],
+                                                     rocblas_int         lda,
+                                                     double* const       invA[],
+                                                     rocblas_int         ldinvA,
+                                                     rocblas_int         batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strtri_strided_batched(rocblas_handle   handle,
+                                                             rocblas_fill     uplo,
+                                                             rocblas_diagonal diag,
+                                                             rocblas_int      n,
+                                                             const float*     A,
+                                                             rocblas_int      lda,
+                                                             rocblas_stride   stride_a,
+                                                             float*           invA,
+                                                             rocblas_int      ldinvA,
+                                                             rocblas_stride   stride_invA,
+                                                             rocblas_int      batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrtri_strided_batched(rocblas_handle   handle,
+                                                             rocblas_fill     uplo,
+                                                             rocblas_diagonal diag,
+                                                             rocblas_int      n,
+                                                             const double*    A,
+                                                             rocblas_int      lda,
+                                                             rocblas_stride   stride_a,
+                                                             double*          invA,
+                                                             rocblas_int      ldinvA,
+                                                             rocblas_stride   stride_invA,
+                                                             rocblas_int      batch_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROCBLAS_B200_ROCBLAS_H */

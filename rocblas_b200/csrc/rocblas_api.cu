@@ -1,0 +1,833 @@
+// The C ABI of librocblas_b200.so: handle functions, trsm / trsm_ex / trtri in their plain,
+// _batched and _strided_batched forms.  Every entry point is `extern "C"`, catches every
+// exception (as the reference's IMPL wrappers do, library/src/blas3/rocblas_trsm_imp.hpp:
+// 285-314) and validates its arguments in the reference's order before touching the GPU.
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <new>
+#include <type_traits>
+
+#include "../../include/rocblas_b200_ext.h"
+#include "trsm_driver.cuh"
+
+using namespace rb200;
+
+// =========================================================================================
+// handle
+// =========================================================================================
+void* _rocblas_handle::borrow(size_t bytes)
+{
+    bytes = roundup(bytes);
+    if(bytes == 0)
+        return mem; // may be nullptr; callers that need 0 bytes never dereference it
+    if(owner != MemOwner::managed)
+        return bytes <= mem_size ? mem : nullptr;
+    if(bytes <= mem_size && mem)
+        return mem;
+    // grow: wait for work that may still use the old buffer, then reallocate
+    if(mem)
+    {
+        cudaStreamSynchronize(stream);
+        cudaFree(mem);
+        mem      = nullptr;
+        mem_size = 0;
+    }
+    if(cudaMalloc(&mem, bytes) != cudaSuccess)
+    {
+        cudaGetLastError();
+        mem = nullptr;
+        return nullptr;
+    }
+    mem_size = bytes;
+    return mem;
+}
+
+rocblas_status _rocblas_handle::free_mem()
+{
+    if(mem && owner != MemOwner::user_owned)
+    {
+        cudaStreamSynchronize(stream);
+        cudaFree(mem);
+    }
+    mem      = nullptr;
+    mem_size = 0;
+    owner    = MemOwner::managed;
+    return rocblas_status_success;
+}
+
+namespace
+{
+// Device capability of the handle's device: 0 ok, otherwise a rocblas_status to return.
+rocblas_status device_ready(rocblas_handle h)
+{
+    if(h->device < 0)
+        return rocblas_status_internal_error; // no CUDA device was visible at create time
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if(cur != h->device)
+        cudaSetDevice(h->device);
+    return rocblas_status_success;
+}
+
+rocblas_status launch_status()
+{
+    cudaError_t e = cudaGetLastError();
+    if(e == cudaSuccess)
+        return rocblas_status_success;
+    if(e == cudaErrorMemoryAllocation)
+        return rocblas_status_memory_error;
+    if(e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDeviceFunction)
+        return rocblas_status_arch_mismatch;
+    return rocblas_status_internal_error;
+}
+
+rocblas_status exception_status()
+{
+    try
+    {
+        throw;
+    }
+    catch(const std::bad_alloc&)
+    {
+        return rocblas_status_memory_error;
+    }
+    catch(...)
+    {
+        return rocblas_status_internal_error;
+    }
+}
+
+template <typename T>
+__global__ void zero_fill_kernel(BatchPtr<T> B, int64_t ldb, int m, int n, int batch_base)
+{
+    T*        b = B.get(batch_base + blockIdx.z);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if(i < m)
+        b[i + (int64_t)j * ldb] = T(0);
+}
+
+// set_block_unit with val 0 (library/src/blas3/rocblas_trsm_kernels.hpp:213-265)
+template <typename T>
+void zero_fill(BatchPtr<T> B, int64_t ldb, int m, int n, int batch, cudaStream_t s)
+{
+    for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+        for(int j0 = 0; j0 < n; j0 += kMaxGridYZ)
+        {
+            dim3 grid((unsigned)ceil_div(m, 256), (unsigned)std::min(kMaxGridYZ, n - j0),
+                      (unsigned)std::min(kMaxGridYZ, batch - b0));
+            zero_fill_kernel<T><<<grid, 256, 0, s>>>(B.shifted((int64_t)j0 * ldb), ldb, m,
+                                                     std::min(kMaxGridYZ, n - j0), b0);
+            count_launch();
+        }
+}
+
+// rocblas_trsm_arg_check (library/src/blas3/rocblas_trsm.hpp:30-82)
+template <typename T>
+rocblas_status trsm_arg_check(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                              rocblas_operation trans, rocblas_diagonal diag, int64_t m,
+                              int64_t n, const T* alpha, const void* A, int64_t lda,
+                              const void* B, int64_t ldb, int64_t batch)
+{
+    if(side != rocblas_side_left && side != rocblas_side_right)
+        return rocblas_status_invalid_value;
+    if(uplo != rocblas_fill_lower && uplo != rocblas_fill_upper)
+        return rocblas_status_invalid_value;
+    if(trans != rocblas_operation_none && trans != rocblas_operation_transpose
+       && trans != rocblas_operation_conjugate_transpose)
+        return rocblas_status_invalid_value;
+    if(diag != rocblas_diagonal_non_unit && diag != rocblas_diagonal_unit)
+        return rocblas_status_invalid_value;
+    const int64_t k = side == rocblas_side_left ? m : n;
+    if(batch < 0 || m < 0 || n < 0 || lda < k || ldb < m)
+        return rocblas_status_invalid_size;
+    if(!m || !n || !batch)
+        return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
+    if(!h->size_query)
+    {
+        if(!B || !alpha || (h->pointer_mode == rocblas_pointer_mode_host && *alpha != T(0) && !A))
+            return rocblas_status_invalid_pointer;
+    }
+    return rocblas_status_continue;
+}
+
+// The body shared by all trsm entry points (rocblas_trsm_ex_impl,
+// library/src/blas3/rocblas_trsm_imp.hpp:55-272 and its batched / strided twins).
+template <typename T>
+rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                         rocblas_operation trans, rocblas_diagonal diag, int m, int n,
+                         const T* alpha, const void* Aptr, BatchPtr<T> A, int lda,
+                         const void* Bptr, BatchPtr<T> B, int ldb, int batch,
+                         const void* invA_ptr, BatchPtr<T> invA, int64_t invA_size)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st
+        = trsm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr, ldb, batch);
+    if(st != rocblas_status_continue)
+        return st;
+
+    if(h->pointer_mode == rocblas_pointer_mode_host && alpha && *alpha == T(0))
+    {
+        if(h->size_query)
+            return rocblas_status_size_unchanged;
+        if((st = device_ready(h)) != rocblas_status_success)
+            return st;
+        zero_fill<T>(B, ldb, m, n, batch, h->stream);
+        return launch_status();
+    }
+
+    TrsmProblem<T> pr{};
+    pr.side_left = side == rocblas_side_left;
+    pr.upper     = uplo == rocblas_fill_upper;
+    pr.trans     = trans != rocblas_operation_none;
+    pr.unit      = diag == rocblas_diagonal_unit;
+    pr.m = m;
+    pr.n = n;
+    pr.batch = batch;
+    pr.A = A;
+    pr.lda = lda;
+    pr.B = B;
+    pr.ldb = ldb;
+    pr.stream   = h->stream;
+    pr.sm_count = h->sm_count;
+
+    const int64_t k = pr.k();
+    // a supplied invA smaller than 128 * k elements is ignored (rocblas_trsm_kernels.hpp:3832-3836)
+    rocblas_status perf = rocblas_status_success;
+    bool           have_invA = invA_ptr != nullptr;
+    if(have_invA && invA_size / kInvNB < k)
+    {
+        have_invA = false;
+        perf      = rocblas_status_perf_degraded;
+        static bool warned = false;
+        if(!warned)
+        {
+            warned = true;
+            fprintf(stderr, "WARNING: TRSM invA_size argument is too small; invA argument is being "
+                            "ignored; TRSM performance is degraded\n");
+        }
+    }
+
+    const size_t ws_bytes = trsm_workspace_bytes<T>(pr, have_invA);
+    if(h->size_query)
+        return ws_bytes ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+
+    if(h->pointer_mode == rocblas_pointer_mode_host)
+        pr.alpha.val = *alpha;
+    else
+        pr.alpha.ptr = alpha;
+
+    void* ws = nullptr;
+    if(ws_bytes)
+    {
+        ws = h->borrow(ws_bytes);
+        if(!ws)
+        {
+            // backup: recursive solve with block-solver leaves needs no workspace
+            perf = rocblas_status_perf_degraded;
+            static bool warned = false;
+            if(!warned)
+            {
+                warned = true;
+                fprintf(stderr, "WARNING: Device memory allocation size is too small for TRSM; TRSM "
+                                "performance is degraded\n");
+            }
+        }
+    }
+    if(have_invA)
+        pr.invA = invA;
+    trsm_run<T>(pr, ws, have_invA);
+    st = launch_status();
+    return st != rocblas_status_success ? st : perf;
+}
+
+template <typename T>
+BatchPtr<T> strided(const T* p, int64_t stride)
+{
+    BatchPtr<T> b;
+    b.base   = const_cast<T*>(p);
+    b.stride = stride;
+    return b;
+}
+
+template <typename T>
+BatchPtr<T> arrayed(const void* arr)
+{
+    BatchPtr<T> b;
+    b.arr = arr;
+    return b;
+}
+
+// ---- trtri ---------------------------------------------------------------------------------
+// rocblas_trtri_arg_check (library/src/blas3/rocblas_trtri.hpp:30-64)
+rocblas_status trtri_arg_check(rocblas_fill uplo, rocblas_diagonal diag, int64_t n,
+                               const void* A, int64_t lda, const void* invA, int64_t ldinvA,
+                               int64_t batch)
+{
+    if(uplo != rocblas_fill_lower && uplo != rocblas_fill_upper)
+        return rocblas_status_invalid_value;
+    if(diag != rocblas_diagonal_non_unit && diag != rocblas_diagonal_unit)
+        return rocblas_status_invalid_value;
+    if(batch < 0 || n < 0 || lda < n || ldinvA < n)
+        return rocblas_status_invalid_size;
+    if(!n || !batch)
+        return rocblas_status_success;
+    if(!A || !invA)
+        return rocblas_status_invalid_pointer;
+    return rocblas_status_continue;
+}
+
+template <typename T>
+size_t trtri_workspace_bytes(int n, int batch)
+{
+    if(n <= kInvNB)
+        return 0;
+    const int64_t half = ceil_div(ceil_div(n, kInvNB), 2) * kInvNB;
+    return sizeof(T) * (size_t)half * (size_t)half * (size_t)batch;
+}
+
+// inv(A) for n > 128: diagonal blocks by the fused kernel, then recursive merges
+//   lower: X21 = -X22 (A21 X11),   upper: X12 = -X11 (A12 X22)
+// (the role of rocblas_trtri_large, library/src/blas3/rocblas_trtri.hpp:732-1100).
+template <typename T>
+struct TrtriRec
+{
+    int          n, upper;
+    BatchPtr<T>  A, X, Tmp;
+    int64_t      lda, ldx, ldt;
+    int          batch;
+    cudaStream_t s;
+
+    int row_of(int b) const { return std::min(b * kInvNB, n); }
+
+    void gemm(int M, int N, int K, BatchPtr<T> P, int64_t ldp, int triP, BatchPtr<T> Q,
+              int64_t ldq, int triQ, BatchPtr<T> C, int64_t ldc, T a) const
+    {
+        GemmParams<T> g{};
+        g.M = M; g.N = N; g.K = K;
+        g.P = P; g.ldp = ldp; g.transP = 0; g.triP = triP;
+        g.Q = Q; g.ldq = ldq; g.transQ = 0; g.triQ = triQ;
+        g.C = C; g.ldc = ldc;
+        g.a_imm = a; g.a_user = 0; g.b_imm = T(0); g.b_user = 0;
+        g.zero_guard = 0;
+        launch_gemm<T>(g, batch, s);
+    }
+
+    void run(int b0, int b1) const
+    {
+        if(b1 - b0 <= 1)
+            return;
+        const int bm = (b0 + b1) / 2;
+        run(b0, bm);
+        run(bm, b1);
+        const int r0 = row_of(b0), rm = row_of(bm), r1 = row_of(b1);
+        const int tri = upper ? kTriUpper : kTriLower;
+        auto at = [](BatchPtr<T> p, int64_t ld, int i, int j) { return p.shifted(i + (int64_t)j * ld); };
+        if(!upper)
+        {
+            const int M = r1 - rm, N = rm - r0;
+            gemm(M, N, N, at(A, lda, rm, r0), lda, kTriNone, at(X, ldx, r0, r0), ldx, tri, Tmp, M, T(1));
+            gemm(M, N, M, at(X, ldx, rm, rm), ldx, tri, Tmp, M, kTriNone, at(X, ldx, rm, r0), ldx, T(-1));
+        }
+        else
+        {
+            const int M = rm - r0, N = r1 - rm;
+            gemm(M, N, N, at(A, lda, r0, rm), lda, kTriNone, at(X, ldx, rm, rm), ldx, tri, Tmp, M, T(1));
+            gemm(M, N, M, at(X, ldx, r0, r0), ldx, tri, Tmp, M, kTriNone, at(X, ldx, r0, rm), ldx, T(-1));
+        }
+    }
+};
+
+template <typename T>
+rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag, int n,
+                          const void* Aptr, BatchPtr<T> A, int lda, const void* Xptr,
+                          BatchPtr<T> X, int ldinv, int batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    const size_t ws_bytes = trtri_workspace_bytes<T>(n, std::max(batch, 0));
+    if(h->size_query)
+    {
+        if(!n || !ws_bytes)
+            return rocblas_status_size_unchanged;
+        return h->set_optimal_size(ws_bytes);
+    }
+    rocblas_status st = trtri_arg_check(uplo, diag, n, Aptr, lda, Xptr, ldinv, batch);
+    if(st != rocblas_status_continue)
+        return st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    void* ws = nullptr;
+    if(ws_bytes && !(ws = h->borrow(ws_bytes)))
+        return rocblas_status_memory_error;
+
+    TrtriParams<T> t{};
+    t.k = n;
+    t.nb = kInvNB;
+    t.A = A;
+    t.lda = lda;
+    t.inv = X;
+    t.ldinv = ldinv;
+    t.inv_block_stride = (int64_t)kInvNB * ldinv + kInvNB;
+    t.upper = uplo == rocblas_fill_upper;
+    t.unit = diag == rocblas_diagonal_unit;
+    launch_trtri<T>(t, (int)ceil_div(n, kInvNB), batch, h->stream);
+    if(n > kInvNB)
+    {
+        TrtriRec<T> r;
+        r.n = n;
+        r.upper = t.upper;
+        r.A = A;
+        r.X = X;
+        r.lda = lda;
+        r.ldx = ldinv;
+        const int64_t half = ceil_div(ceil_div(n, kInvNB), 2) * kInvNB;
+        r.Tmp = strided<T>(reinterpret_cast<T*>(ws), half * half);
+        r.ldt = 0;
+        r.batch = batch;
+        r.s = h->stream;
+        r.run(0, (int)ceil_div(n, kInvNB));
+    }
+    return launch_status();
+}
+
+} // namespace
+
+// =========================================================================================
+// exported functions
+// =========================================================================================
+extern "C" {
+
+uint64_t rocblas_b200_kernel_launch_count(void)
+{
+    return g_kernel_launches.load(std::memory_order_relaxed);
+}
+
+rocblas_status rocblas_create_handle(rocblas_handle* handle)
+try
+{
+    if(!handle)
+        return rocblas_status_invalid_pointer;
+    auto* h = new _rocblas_handle();
+    int   dev = -1;
+    if(cudaGetDevice(&dev) == cudaSuccess)
+    {
+        cudaDeviceProp prop;
+        if(cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+        {
+            h->device   = dev;
+            h->sm_count = prop.multiProcessorCount;
+        }
+    }
+    cudaGetLastError();
+    *handle = h;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_destroy_handle(rocblas_handle handle)
+try
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->free_mem();
+    delete handle;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_stream(rocblas_handle handle, cudaStream_t stream)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->stream = stream;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_get_stream(rocblas_handle handle, cudaStream_t* stream)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!stream)
+        return rocblas_status_invalid_pointer;
+    *stream = handle->stream;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_pointer_mode(rocblas_handle handle, rocblas_pointer_mode mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(mode != rocblas_pointer_mode_host && mode != rocblas_pointer_mode_device)
+        return rocblas_status_invalid_value;
+    handle->pointer_mode = mode;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_get_pointer_mode(rocblas_handle handle, rocblas_pointer_mode* mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!mode)
+        return rocblas_status_invalid_pointer;
+    *mode = handle->pointer_mode;
+    return rocblas_status_success;
+}
+
+rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr)
+{
+    cudaPointerAttributes attr;
+    if(cudaPointerGetAttributes(&attr, ptr) == cudaSuccess && attr.type == cudaMemoryTypeDevice)
+        return rocblas_pointer_mode_device;
+    cudaGetLastError();
+    return rocblas_pointer_mode_host;
+}
+
+rocblas_status rocblas_start_device_memory_size_query(rocblas_handle handle)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(handle->size_query)
+        return rocblas_status_size_query_mismatch;
+    handle->size_query = true;
+    handle->query_size = 0;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_stop_device_memory_size_query(rocblas_handle handle, size_t* size)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!handle->size_query)
+        return rocblas_status_size_query_mismatch;
+    if(!size)
+        return rocblas_status_invalid_pointer;
+    *size              = handle->query_size;
+    handle->size_query = false;
+    return rocblas_status_success;
+}
+
+bool rocblas_is_device_memory_size_query(rocblas_handle handle)
+{
+    return handle && handle->size_query;
+}
+
+rocblas_status rocblas_get_device_memory_size(rocblas_handle handle, size_t* size)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!size)
+        return rocblas_status_invalid_pointer;
+    *size = handle->mem_size;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_device_memory_size(rocblas_handle handle, size_t size)
+try
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->free_mem();
+    if(!size)
+        return rocblas_status_success;
+    if(handle->device < 0)
+        return rocblas_status_memory_error;
+    size = _rocblas_handle::roundup(size);
+    if(cudaMalloc(&handle->mem, size) != cudaSuccess)
+    {
+        cudaGetLastError();
+        handle->mem = nullptr;
+        return rocblas_status_memory_error;
+    }
+    handle->mem_size = size;
+    handle->owner    = MemOwner::user_managed;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_workspace(rocblas_handle handle, void* addr, size_t size)
+try
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->free_mem();
+    if(size && addr)
+    {
+        handle->owner    = MemOwner::user_owned;
+        handle->mem      = addr;
+        handle->mem_size = size;
+    }
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+bool rocblas_is_managing_device_memory(rocblas_handle handle)
+{
+    return handle && handle->owner == MemOwner::managed;
+}
+
+bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
+{
+    return handle && handle->owner == MemOwner::user_managed;
+}
+
+// ---- trsm ------------------------------------------------------------------------------------
+#define TRSM_PLAIN(NAME, T)                                                                       \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
+                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
+                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda, T* B,        \
+                        rocblas_int ldb)                                                         \
+    try                                                                                          \
+    {                                                                                            \
+        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, 0), lda,   \
+                            B, strided<T>(B, 0), ldb, 1, nullptr, BatchPtr<T>{}, 0);             \
+    }                                                                                            \
+    catch(...)                                                                                   \
+    {                                                                                            \
+        return exception_status();                                                               \
+    }
+
+TRSM_PLAIN(rocblas_strsm, float)
+TRSM_PLAIN(rocblas_dtrsm, double)
+
+#define TRSM_BATCHED(NAME, T)                                                                     \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
+                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
+                        rocblas_int n, const T* alpha, const T* const A[], rocblas_int lda,      \
+                        T* const B[], rocblas_int ldb, rocblas_int batch_count)                  \
+    try                                                                                          \
+    {                                                                                            \
+        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, arrayed<T>(A), lda, B,   \
+                            arrayed<T>(B), ldb, batch_count, nullptr, BatchPtr<T>{}, 0);         \
+    }                                                                                            \
+    catch(...)                                                                                   \
+    {                                                                                            \
+        return exception_status();                                                               \
+    }
+
+TRSM_BATCHED(rocblas_strsm_batched, float)
+TRSM_BATCHED(rocblas_dtrsm_batched, double)
+
+#define TRSM_STRIDED(NAME, T)                                                                     \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
+                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
+                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda,              \
+                        rocblas_stride stride_a, T* B, rocblas_int ldb, rocblas_stride stride_b, \
+                        rocblas_int batch_count)                                                 \
+    try                                                                                          \
+    {                                                                                            \
+        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, stride_a), \
+                            lda, B, strided<T>(B, stride_b), ldb, batch_count, nullptr,          \
+                            BatchPtr<T>{}, 0);                                                   \
+    }                                                                                            \
+    catch(...)                                                                                   \
+    {                                                                                            \
+        return exception_status();                                                               \
+    }
+
+TRSM_STRIDED(rocblas_strsm_strided_batched, float)
+TRSM_STRIDED(rocblas_dtrsm_strided_batched, double)
+
+// rocblas_trsm_ex type switch (library/src/blas3/rocblas_trsm.cpp:28-73)
+rocblas_status rocblas_trsm_ex(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                               rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,
+                               rocblas_int n, const void* alpha, const void* A, rocblas_int lda,
+                               void* B, rocblas_int ldb, const void* invA, rocblas_int invA_size,
+                               rocblas_datatype compute_type)
+try
+{
+    switch(compute_type)
+    {
+    case rocblas_datatype_f32_r:
+        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+                                strided<float>((const float*)A, 0), lda, B,
+                                strided<float>((float*)B, 0), ldb, 1, invA,
+                                strided<float>((const float*)invA, 0), invA_size);
+    case rocblas_datatype_f64_r:
+        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+                                 strided<double>((const double*)A, 0), lda, B,
+                                 strided<double>((double*)B, 0), ldb, 1, invA,
+                                 strided<double>((const double*)invA, 0), invA_size);
+    case rocblas_datatype_f32_c:
+    case rocblas_datatype_f64_c:
+        // complex trsm is outside this library's scope
+        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+    default:
+        return rocblas_status_not_implemented;
+    }
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_trsm_batched_ex(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                       rocblas_operation trans, rocblas_diagonal diag,
+                                       rocblas_int m, rocblas_int n, const void* alpha,
+                                       const void* A, rocblas_int lda, void* B, rocblas_int ldb,
+                                       rocblas_int batch_count, const void* invA,
+                                       rocblas_int invA_size, rocblas_datatype compute_type)
+try
+{
+    switch(compute_type)
+    {
+    case rocblas_datatype_f32_r:
+        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+                                arrayed<float>(A), lda, B, arrayed<float>(B), ldb, batch_count,
+                                invA, arrayed<float>(invA), invA_size);
+    case rocblas_datatype_f64_r:
+        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+                                 arrayed<double>(A), lda, B, arrayed<double>(B), ldb, batch_count,
+                                 invA, arrayed<double>(invA), invA_size);
+    case rocblas_datatype_f32_c:
+    case rocblas_datatype_f64_c:
+        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+    default:
+        return rocblas_status_not_implemented;
+    }
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_trsm_strided_batched_ex(rocblas_handle h, rocblas_side side,
+                                               rocblas_fill uplo, rocblas_operation trans,
+                                               rocblas_diagonal diag, rocblas_int m,
+                                               rocblas_int n, const void* alpha, const void* A,
+                                               rocblas_int lda, rocblas_stride stride_A, void* B,
+                                               rocblas_int ldb, rocblas_stride stride_B,
+                                               rocblas_int batch_count, const void* invA,
+                                               rocblas_int invA_size, rocblas_stride stride_invA,
+                                               rocblas_datatype compute_type)
+try
+{
+    switch(compute_type)
+    {
+    case rocblas_datatype_f32_r:
+        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+                                strided<float>((const float*)A, stride_A), lda, B,
+                                strided<float>((float*)B, stride_B), ldb, batch_count, invA,
+                                strided<float>((const float*)invA, stride_invA), invA_size);
+    case rocblas_datatype_f64_r:
+        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+                                 strided<double>((const double*)A, stride_A), lda, B,
+                                 strided<double>((double*)B, stride_B), ldb, batch_count, invA,
+                                 strided<double>((const double*)invA, stride_invA), invA_size);
+    case rocblas_datatype_f32_c:
+    case rocblas_datatype_f64_c:
+        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+    default:
+        return rocblas_status_not_implemented;
+    }
+}
+catch(...)
+{
+    return exception_status();
+}
+
+// ---- trtri ------------------------------------------------------------------------------------
+rocblas_status rocblas_strtri(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag,
+                              rocblas_int n, const float* A, rocblas_int lda, float* invA,
+                              rocblas_int ldinvA)
+try
+{
+    return trtri_impl<float>(h, uplo, diag, n, A, strided<float>(A, 0), lda, invA,
+                             strided<float>(invA, 0), ldinvA, 1);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_dtrtri(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag,
+                              rocblas_int n, const double* A, rocblas_int lda, double* invA,
+                              rocblas_int ldinvA)
+try
+{
+    return trtri_impl<double>(h, uplo, diag, n, A, strided<double>(A, 0), lda, invA,
+                              strided<double>(invA, 0), ldinvA, 1);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_strtri_batched(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag,
+                                      rocblas_int n, const float* const A[], rocblas_int lda,
+                                      float* const invA[], rocblas_int ldinvA,
+                                      rocblas_int batch_count)
+try
+{
+    return trtri_impl<float>(h, uplo, diag, n, A, arrayed<float>(A), lda, invA,
+                             arrayed<float>(invA), ldinvA, batch_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_dtrtri_batched(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag,
+                                      rocblas_int n, const double* const A[], rocblas_int lda,
+                                      double* const invA[], rocblas_int ldinvA,
+                                      rocblas_int batch_count)
+try
+{
+    return trtri_impl<double>(h, uplo, diag, n, A, arrayed<double>(A), lda, invA,
+                              arrayed<double>(invA), ldinvA, batch_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_strtri_strided_batched(rocblas_handle h, rocblas_fill uplo,
+                                              rocblas_diagonal diag, rocblas_int n,
+                                              const float* A, rocblas_int lda,
+                                              rocblas_stride stride_a, float* invA,
+                                              rocblas_int ldinvA, rocblas_stride stride_invA,
+                                              rocblas_int batch_count)
+try
+{
+    return trtri_impl<float>(h, uplo, diag, n, A, strided<float>(A, stride_a), lda, invA,
+                             strided<float>(invA, stride_invA), ldinvA, batch_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_dtrtri_strided_batched(rocblas_handle h, rocblas_fill uplo,
+                                              rocblas_diagonal diag, rocblas_int n,
+                                              const double* A, rocblas_int lda,
+                                              rocblas_stride stride_a, double* invA,
+                                              rocblas_int ldinvA, rocblas_stride stride_invA,
+                                              rocblas_int batch_count)
+try
+{
+    return trtri_impl<double>(h, uplo, diag, n, A, strided<double>(A, stride_a), lda, invA,
+                              strided<double>(invA, stride_invA), ldinvA, batch_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+} // extern "C"

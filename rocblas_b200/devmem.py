@@ -1,0 +1,152 @@
+"""Device-memory helpers for callers that hold column-major matrices as numpy arrays.
+
+A column-major ``ld x ncols`` matrix is kept on the GPU as a C-contiguous torch tensor of
+shape ``(ncols, ld)``: element (i, j) sits at ``j * ld + i``, exactly the layout the C ABI
+expects.  PyTorch only provides device memory and streams here; every computation goes
+through librocblas_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import (
+    DIAG, SIDE, TRANS, UPLO, check, datatype_f32_r, datatype_f64_r, lib, pointer_mode_device,
+    pointer_mode_host, status_perf_degraded, status_success,
+)
+
+
+def to_device(a: np.ndarray, device="cuda") -> torch.Tensor:
+    """Fortran-ordered (ld x ncols) numpy array -> (ncols x ld) device tensor, same bytes."""
+    a = np.asfortranarray(a)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).to(device)
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    """(ncols x ld) device tensor -> Fortran-ordered (ld x ncols) numpy array."""
+    return np.asfortranarray(t.detach().cpu().numpy().T)
+
+
+def empty(ld, ncols, dtype, device="cuda", fill=float("nan")) -> torch.Tensor:
+    return torch.full((ncols, ld), fill, dtype=dtype, device=device)
+
+
+def _code(table, v):
+    return v if isinstance(v, int) else table[v]
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+def _is_double(t):
+    return t.dtype == torch.float64
+
+
+def trsm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, alpha_on_device=False,
+         allow=(status_success,)):
+    """rocblas_?trsm on device tensors; alpha is a Python float (host pointer mode) or, with
+    alpha_on_device, placed in device memory and passed in device pointer mode."""
+    dbl = _is_double(B)
+    fn = lib().rocblas_dtrsm if dbl else lib().rocblas_strsm
+    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
+            _code(DIAG, diag), m, n, aptr, _ptr(A), lda, _ptr(B), ldb)
+    _restore(handle, alpha_on_device)
+    return check("rocblas_trsm", st, allow)
+
+
+def trsm_ex(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, invA, invA_size,
+            alpha_on_device=False, allow=(status_success,)):
+    dbl = _is_double(B)
+    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    st = lib().rocblas_trsm_ex(handle.value, _code(SIDE, side), _code(UPLO, uplo),
+                               _code(TRANS, trans), _code(DIAG, diag), m, n, aptr, _ptr(A), lda,
+                               _ptr(B), ldb, _ptr(invA), invA_size,
+                               datatype_f64_r if dbl else datatype_f32_r)
+    _restore(handle, alpha_on_device)
+    return check("rocblas_trsm_ex", st, allow)
+
+
+def trsm_strided_batched(handle, side, uplo, trans, diag, m, n, alpha, A, lda, stride_a, B, ldb,
+                         stride_b, batch, alpha_on_device=False, allow=(status_success,)):
+    dbl = _is_double(B)
+    fn = lib().rocblas_dtrsm_strided_batched if dbl else lib().rocblas_strsm_strided_batched
+    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
+            _code(DIAG, diag), m, n, aptr, _ptr(A), lda, stride_a, _ptr(B), ldb, stride_b, batch)
+    _restore(handle, alpha_on_device)
+    return check("rocblas_trsm_strided_batched", st, allow)
+
+
+def trsm_batched(handle, side, uplo, trans, diag, m, n, alpha, A_list, lda, B_list, ldb,
+                 alpha_on_device=False, allow=(status_success,)):
+    """A_list / B_list: lists of device tensors; their addresses are gathered into device
+    arrays of device pointers, as the _batched API takes them."""
+    dbl = _is_double(B_list[0])
+    fn = lib().rocblas_dtrsm_batched if dbl else lib().rocblas_strsm_batched
+    dev = B_list[0].device
+    Ap = torch.tensor([a.data_ptr() for a in A_list], dtype=torch.int64, device=dev)
+    Bp = torch.tensor([b.data_ptr() for b in B_list], dtype=torch.int64, device=dev)
+    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, dev)
+    st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
+            _code(DIAG, diag), m, n, aptr, _ptr(Ap), lda, _ptr(Bp), ldb, len(B_list))
+    _restore(handle, alpha_on_device)
+    torch.cuda.synchronize(dev)
+    return check("rocblas_trsm_batched", st, allow)
+
+
+def trtri(handle, uplo, diag, n, A, lda, invA, ldinv, allow=(status_success,)):
+    dbl = _is_double(A)
+    fn = lib().rocblas_dtrtri if dbl else lib().rocblas_strtri
+    st = fn(handle.value, _code(UPLO, uplo), _code(DIAG, diag), n, _ptr(A), lda, _ptr(invA), ldinv)
+    return check("rocblas_trtri", st, allow)
+
+
+def trtri_strided_batched(handle, uplo, diag, n, A, lda, stride_a, invA, ldinv, stride_inv, batch,
+                          a_offset=0, inv_offset=0, allow=(status_success,)):
+    dbl = _is_double(A)
+    fn = lib().rocblas_dtrtri_strided_batched if dbl else lib().rocblas_strtri_strided_batched
+    es = A.element_size()
+    st = fn(handle.value, _code(UPLO, uplo), _code(DIAG, diag), n,
+            ctypes.c_void_p(A.data_ptr() + a_offset * es), lda, stride_a,
+            ctypes.c_void_p(invA.data_ptr() + inv_offset * es), ldinv, stride_inv, batch)
+    return check("rocblas_trtri_strided_batched", st, allow)
+
+
+def _alpha(handle, alpha, dbl, on_device, device):
+    if on_device:
+        t = torch.tensor([alpha], dtype=torch.float64 if dbl else torch.float32, device=device)
+        lib().rocblas_set_pointer_mode(handle.value, pointer_mode_device)
+        return t, ctypes.c_void_p(t.data_ptr())
+    c = ctypes.c_double(alpha) if dbl else ctypes.c_float(alpha)
+    return c, ctypes.cast(ctypes.byref(c), ctypes.c_void_p)
+
+
+def _restore(handle, on_device):
+    if on_device:
+        # the kernels read alpha asynchronously: keep its storage alive until they ran
+        torch.cuda.synchronize()
+        lib().rocblas_set_pointer_mode(handle.value, pointer_mode_host)
+
+
+def build_invA(handle, uplo, diag, A, lda, k, nb=128):
+    """invA for rocblas_trsm_ex, built the way rocblas-test builds it
+    (clients/include/blas_ex/testing_trsm_ex.hpp:329-336, 408-436): trtri_strided_batched
+    over the k // nb full blocks (stride nb*lda + nb in A, nb*nb in invA), then the
+    remainder block with batch 1."""
+    invA = torch.zeros(nb * k, dtype=A.dtype, device=A.device)
+    nfull, rem = divmod(k, nb)
+    if nfull:
+        trtri_strided_batched(handle, uplo, diag, nb, A, lda, nb * lda + nb, invA, nb, nb * nb, nfull)
+    if rem:
+        trtri_strided_batched(handle, uplo, diag, rem, A, lda, 0, invA, nb, 0, 1,
+                              a_offset=nfull * nb * lda + nfull * nb, inv_offset=nfull * nb * nb)
+    return invA
+
+
+__all__ = ["to_device", "to_host", "empty", "trsm", "trsm_ex", "trsm_strided_batched",
+           "trsm_batched", "trtri", "trtri_strided_batched", "build_invA", "status_perf_degraded",
+           "pointer_mode_host", "pointer_mode_device"]

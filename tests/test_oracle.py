@@ -1,0 +1,99 @@
+"""Pin the CPU oracle before trusting it (CPU only).
+
+The reference has no golden trsm vectors; its tests compare against the host CBLAS
+(ref_trsm -> cblas_?trsm) and against the X the right-hand side was built from.  These
+tests check the C restatement in oracle/ against both, through the committed fixtures
+made by tests/golden/make_golden.py and live against the host CBLAS.
+"""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+COMBOS = list(itertools.product("LR", "UL", "NT", "NU"))
+
+
+def _cases(npz):
+    keys = sorted({k.rsplit("_", 1)[0] for k in npz.files})
+    return keys
+
+
+@pytest.mark.parametrize("dt", ["d", "s"])
+def test_oracle_matches_cblas_golden(dt):
+    z = np.load(os.path.join(GOLDEN, f"cblas_{dt}.npz"))
+    keys = _cases(z)
+    assert len(keys) == 16 * 4
+    eps = np.finfo(np.float64 if dt == "d" else np.float32).eps
+    for key in keys:
+        combo, shape = key.split("_")
+        side, uplo, trans, diag = combo
+        m, n = map(int, shape.split("x"))
+        A, B, X, alpha = z[key + "_A"], z[key + "_B"], z[key + "_X"], float(z[key + "_alpha"])
+        got = oracle.trsm(side, uplo, trans, diag, alpha, A, np.asfortranarray(B[:m]))
+        assert not np.isnan(got).any(), key
+        err = oracle.matrix_norm_1(X, got)
+        assert err <= oracle.trsm_tolerance(got.dtype, max(m, n)), (key, err)
+        # much tighter in practice: the two differ only in operation order
+        assert err <= 64 * eps, (key, err)
+
+
+@pytest.mark.parametrize("dt", ["d", "s"])
+def test_oracle_recovers_protocol_x(dt):
+    """rocblas-test's own check: forward error and residual within 40 eps M."""
+    z = np.load(os.path.join(GOLDEN, f"protocol_{dt}.npz"))
+    for key in _cases(z):
+        side, uplo, trans, diag = key
+        A, B, X, alpha = z[key + "_A"], z[key + "_B"], z[key + "_X"], float(z[key + "_alpha"])
+        m, n = B.shape
+        got = oracle.trsm(side, uplo, trans, diag, alpha, A, B)
+        tol = oracle.trsm_tolerance(got.dtype, m)
+        assert oracle.matrix_norm_1(X, got) <= tol, key
+        res = oracle.trmm(side, uplo, trans, diag, 1.0 / alpha, A, got)
+        assert oracle.matrix_norm_1(B, res) <= tol, key
+
+
+def test_quad_oracle_tighter_than_double():
+    A, B = oracle.condition_band_problem(3, 300, 7, 4)
+    Xq = oracle.trsm("L", "L", "N", "N", 1.0, A, B, precision="q")
+    Xd = oracle.trsm("L", "L", "N", "N", 1.0, A, B, precision="d")
+    Xc = oracle.cblas_trsm("L", "L", "N", "N", 1.0, A, B)
+    e_d = oracle.normwise_forward_error(Xd, Xq)
+    e_c = oracle.normwise_forward_error(Xc, Xq)
+    assert e_d < 1e-9 and e_c < 1e-9
+    # the quad residual is at the double rounding level of X
+    assert oracle.normwise_backward_error("L", "L", "N", "N", 1.0, A, Xq, B) < 1e-16
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", COMBOS)
+def test_oracle_vs_live_cblas(side, uplo, trans, diag):
+    m, n = 70, 45
+    k = m if side == "L" else n
+    A, B = oracle.nan_triangle_problem(11, side, uplo, trans, diag, m, n, k, m, np.float64)
+    X = oracle.trsm(side, uplo, trans, diag, -1.5, A, B)
+    Xc = oracle.cblas_trsm(side, uplo, trans, diag, -1.5, A, B)
+    assert oracle.matrix_norm_1(Xc, X) < 1e-14
+
+
+def test_alpha_zero_and_trtri():
+    A, B = oracle.nan_triangle_problem(5, "L", "U", "N", "N", 9, 4, 9, 9, np.float64)
+    assert np.all(oracle.trsm("L", "U", "N", "N", 0.0, A, B) == 0)
+    inv = oracle.trtri("U", "N", A)
+    T = oracle.clean_triangle(A, 9, "U", "N")
+    assert np.allclose(inv @ T, np.eye(9), atol=1e-13)
+    assert np.all(np.tril(inv, -1) == 0)
+    # zero diagonal entries are treated as 1 (rocblas_trtri.hpp:138-141)
+    Z = np.eye(3)
+    Z[1, 1] = 0.0
+    assert oracle.trtri("L", "N", Z)[1, 1] == 1.0
+
+
+def test_matrix_norm_1_is_cumulative():
+    """The reference never resets its per-column sums: the metric is sum|e| / sum|x|."""
+    gold = np.array([[1.0, 100.0], [1.0, 100.0]], order="F")
+    x = gold.copy(order="F")
+    x[0, 0] = 2.0
+    assert abs(oracle.matrix_norm_1(gold, x) - 1.0 / 202.0) < 1e-15
