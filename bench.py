@@ -32,7 +32,10 @@ sys.path.insert(0, ROOT)
 
 M, N = 16384, 4096
 FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
-WORKLOAD = "dtrsm L/L/N/N m=16384 n=4096 lda=ldb=16384 alpha=1 (condition band k=0), plain FP64"
+
+
+def workload_name():
+    return f"dtrsm L/L/N/N m={M} n={N} lda=ldb={M} alpha=1 (condition band k=0), plain FP64"
 
 
 def _env_rank():
@@ -118,7 +121,7 @@ def cpu_cblas_sample(A_host, B_host, ncols, threads):
     import oracle
 
     oracle.cblas_set_threads(threads)
-    Bs = np.asfortranarray(B_host[:, :ncols])
+    Bs = np.array(B_host[:, :ncols], order="F", copy=True)  # the solve overwrites it
     # the host BLAS may read the unused triangle in blocked kernels: give it zeros there
     t0 = time.perf_counter()
     oracle.cblas_trsm_inplace("L", "L", "N", "N", 1.0, A_host, Bs)
@@ -136,9 +139,9 @@ def run_reference(args):
     rng = np.random.default_rng(0)
     m = M
     # host copy of the same recipe (numpy stream): lower triangle, zeros above for the CBLAS
-    A, B = oracle.condition_band_problem(0, m, 64, 0)
+    ncols = min(N, 512)
+    A, B = oracle.condition_band_problem(0, m, ncols, 0)
     A = np.asfortranarray(np.tril(np.nan_to_num(A, nan=0.0)))
-    ncols = 64
     for _ in range(args.warmup):
         cpu_cblas_sample(A, B, ncols, threads)
     times = []
@@ -153,7 +156,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "m": M, "n": N},
+        "config": {"workload": workload_name(), "m": M, "n": N},
         "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
                          "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) on "
                                    f"{ncols} of the {N} right-hand sides per step, full m={M}"},
@@ -290,7 +293,7 @@ def run_ours(args):
         A_host = np.asfortranarray(np.nan_to_num(At.cpu().numpy().T, nan=0.0))
         B_host = np.asfortranarray(B0.cpu().numpy().T)
         threads = os.cpu_count() or 1
-        ncols = 64
+        ncols = min(N, 512)
         cpu_tflops, cpu_s, Xc = cpu_cblas_sample(A_host, B_host, ncols, threads)
         cols = list(range(8))
         Xq = oracle.trsm("L", "L", "N", "N", 1.0, A_host, np.asfortranarray(B_host[:, cols]), precision="q")
@@ -316,7 +319,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "m": M, "n": N, "form": "plain FP64",
+            "config": {"workload": workload_name(), "m": M, "n": N, "form": "plain FP64",
                        "l2": "inputs larger than L2 (A 2 GiB, B 512 MiB); no flush",
                        "step": "device copy of B (512 MiB) + rocblas_dtrsm",
                        "parallelism": f"replicas x{world}"},
@@ -336,7 +339,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--m", type=int, default=M, help="problem size (profiling runs use smaller)")
+    ap.add_argument("--n", type=int, default=N)
     args = ap.parse_args()
+    global M, N, FLOPS
+    M, N = args.m, args.n
+    FLOPS = float(M) * M * N
     if args.impl == "reference":
         run_reference(args)
     else:

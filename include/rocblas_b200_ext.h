@@ -17,6 +17,48 @@ extern "C" {
  * many of the launches in that region were this library's own kernels. */
 ROCBLAS_EXPORT uint64_t rocblas_b200_kernel_launch_count(void);
 
+/* ---- variable-size batched trsm -------------------------------------------------------
+ * One entry of a variable-size batch: solve op(A) X = alpha B (side left) or
+ * X op(A) = alpha B (side right) for this entry's own sizes, leading dimensions and flags
+ * (same meaning and validity rules as rocblas_?trsm).  The array of descriptors lives in
+ * device memory; A and B are device pointers of the element type of the call. */
+typedef struct rocblas_b200_trsm_problem
+{
+    const void*       A;
+    void*             B;
+    rocblas_int       m;
+    rocblas_int       n;
+    rocblas_int       lda;
+    rocblas_int       ldb;
+    rocblas_side      side;
+    rocblas_fill      uplo;
+    rocblas_operation transA;
+    rocblas_diagonal  diag;
+} rocblas_b200_trsm_problem;
+
+/* Solve `count` independent systems described by `problems` (device array) with one
+ * alpha (host or device pointer per the handle's pointer mode) in one persistent kernel.
+ * No reference counterpart: rocblas_?trsm_batched needs one m, n for the whole batch, so a
+ * reference caller makes one call per system.
+ *   max_k: an upper bound of k (m for side left, n for side right) over the batch; at most
+ *          512.  Larger bounds return rocblas_status_invalid_size.
+ *   invalid_count: optional device pointer; receives the number of descriptors that broke
+ *          the trsm argument rules or exceeded max_k (those entries are skipped, their B is
+ *          not written).
+ * Workspace: 4 * (count + 1) + 16 bytes from the handle (size query supported). */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_vbatched(rocblas_handle                   handle,
+                                                          const double*                    alpha,
+                                                          const rocblas_b200_trsm_problem* problems,
+                                                          rocblas_int                      count,
+                                                          rocblas_int                      max_k,
+                                                          rocblas_int* invalid_count);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle                   handle,
+                                                          const float*                     alpha,
+                                                          const rocblas_b200_trsm_problem* problems,
+                                                          rocblas_int                      count,
+                                                          rocblas_int                      max_k,
+                                                          rocblas_int* invalid_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,6 +137,8 @@ SIGNATURES = {
     "rocblas_dtrtri_strided_batched": (_i, _TRTRI_SB),
     # include/rocblas_b200_ext.h
     "rocblas_b200_kernel_launch_count": (ctypes.c_uint64, []),
+    "rocblas_b200_dtrsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
+    "rocblas_b200_strsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
 }
 
 _lib = None

@@ -10,6 +10,7 @@
 
 #include "../../include/rocblas_b200_ext.h"
 #include "trsm_driver.cuh"
+#include "vbatched.cuh"
 
 using namespace rb200;
 
@@ -396,6 +397,68 @@ rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal 
     return launch_status();
 }
 
+template <typename T>
+__global__ void vb_copy_invalid_kernel(const VbState* st, rocblas_int* out)
+{
+    *out = st->invalid;
+}
+
+static_assert(sizeof(VbProblem) == sizeof(rocblas_b200_trsm_problem), "descriptor layout");
+
+template <typename T>
+rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
+                                  const rocblas_b200_trsm_problem* problems, int count,
+                                  int max_k, rocblas_int* invalid_count)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(count < 0 || max_k < 0 || max_k > kBlockSolveMaxK)
+        return rocblas_status_invalid_size;
+    const size_t ws_bytes = sizeof(VbState) + sizeof(int) * ((size_t)count + 1);
+    if(h->size_query)
+        return count ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+    if(!count)
+        return rocblas_status_success;
+    if(!alpha || !problems)
+        return rocblas_status_invalid_pointer;
+    rocblas_status st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    void* ws = h->borrow(ws_bytes);
+    if(!ws)
+        return rocblas_status_memory_error;
+    VbState* state   = reinterpret_cast<VbState*>(ws);
+    int*     offsets = reinterpret_cast<int*>(state + 1);
+    cudaMemsetAsync(state, 0, sizeof(VbState), h->stream);
+    const VbProblem* probs = reinterpret_cast<const VbProblem*>(problems);
+    vb_prepass_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, offsets, state);
+    count_launch();
+
+    VbParams<T> p;
+    p.probs   = probs;
+    p.count   = count;
+    p.offsets = offsets;
+    p.st      = state;
+    if(h->pointer_mode == rocblas_pointer_mode_host)
+        p.alpha.val = *alpha;
+    else
+        p.alpha.ptr = alpha;
+    const size_t smem = block_solve_smem_bytes<T>(std::max(max_k, 1));
+    cudaFuncSetAttribute((const void*)vb_persistent_kernel<T>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<T>, kBsThreads, smem);
+    per_sm = std::max(per_sm, 1);
+    vb_persistent_kernel<T><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
+    count_launch();
+    if(invalid_count)
+    {
+        vb_copy_invalid_kernel<T><<<1, 1, 0, h->stream>>>(state, invalid_count);
+        count_launch();
+    }
+    return launch_status();
+}
+
 } // namespace
 
 // =========================================================================================
@@ -737,6 +800,33 @@ try
     default:
         return rocblas_status_not_implemented;
     }
+}
+catch(...)
+{
+    return exception_status();
+}
+
+// ---- variable-size batched (rocblas_b200_ext.h) --------------------------------------------
+rocblas_status rocblas_b200_dtrsm_vbatched(rocblas_handle h, const double* alpha,
+                                           const rocblas_b200_trsm_problem* problems,
+                                           rocblas_int count, rocblas_int max_k,
+                                           rocblas_int* invalid_count)
+try
+{
+    return trsm_vbatched_impl<double>(h, alpha, problems, count, max_k, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle h, const float* alpha,
+                                           const rocblas_b200_trsm_problem* problems,
+                                           rocblas_int count, rocblas_int max_k,
+                                           rocblas_int* invalid_count)
+try
+{
+    return trsm_vbatched_impl<float>(h, alpha, problems, count, max_k, invalid_count);
 }
 catch(...)
 {

@@ -1,0 +1,161 @@
+// Variable-size batched TRSM: thousands of independent systems of different (m, n),
+// side, uplo, transA and diag in one persistent kernel.
+//
+// The reference has no variable-size batch API (rocblas_trsm_batched requires one m, n for
+// every entry, library/src/blas3/rocblas_trsm_batched_imp.hpp:57-300), so a caller with
+// uneven systems makes one call per system.  Here one launch pair covers the whole batch:
+//   1. a single-CTA prepass validates every problem descriptor, counts its work items
+//      (strips of 32 right-hand sides) and writes the exclusive prefix sum of those counts;
+//   2. a persistent kernel (grid = SMs x resident CTAs) pulls work-item indices from a
+//      device-side queue head (one atomicAdd per item), maps an item to its (problem,
+//      strip) by binary search over the prefix sum, and runs the one-CTA strip solver
+//      (block_solve.cuh) on it.  There is no inter-CTA waiting, so no wait can hang.
+// Both launches are stream-ordered and capturable in a CUDA graph.
+#pragma once
+#include "block_solve.cuh"
+
+namespace rb200
+{
+
+// Problem descriptor, same layout as rocblas_b200_trsm_problem in rocblas_b200_ext.h.
+struct VbProblem
+{
+    const void* A;
+    void*       B;
+    int         m, n, lda, ldb;
+    int         side, uplo, trans, diag;
+};
+
+struct VbState
+{
+    int counter; // queue head
+    int invalid; // number of rejected descriptors
+    int pad[2];
+};
+
+constexpr int kVbPrepThreads = 1024;
+
+__device__ __forceinline__ bool vb_valid(const VbProblem& p, int max_k)
+{
+    if(p.side != kLeft && p.side != kRight)
+        return false;
+    if(p.uplo != kLower && p.uplo != kUpper)
+        return false;
+    if(p.trans != kOpN && p.trans != kOpT && p.trans != kOpC)
+        return false;
+    if(p.diag != kNonUnit && p.diag != kUnit)
+        return false;
+    const int k = p.side == kLeft ? p.m : p.n;
+    if(p.m < 0 || p.n < 0 || p.lda < k || p.ldb < p.m || k > max_k)
+        return false;
+    if((p.m > 0 && p.n > 0) && (!p.A || !p.B))
+        return false;
+    return true;
+}
+
+__device__ __forceinline__ int vb_items(const VbProblem& p)
+{
+    const int ncols = p.side == kLeft ? p.n : p.m;
+    const int k     = p.side == kLeft ? p.m : p.n;
+    if(k == 0 || ncols == 0)
+        return 0;
+    return (ncols + kBsW - 1) / kBsW;
+}
+
+// offsets[i] = number of work items of problems 0..i-1; offsets[count] = total.
+__global__ void __launch_bounds__(kVbPrepThreads)
+    vb_prepass_kernel(const VbProblem* probs, int count, int max_k, int* offsets, VbState* st)
+{
+    __shared__ int part[kVbPrepThreads];
+    const int tid   = threadIdx.x;
+    const int chunk = (count + kVbPrepThreads - 1) / kVbPrepThreads;
+    const int lo = min(count, tid * chunk), hi = min(count, lo + chunk);
+    int       sum = 0, bad = 0;
+    for(int i = lo; i < hi; ++i)
+    {
+        const VbProblem p = probs[i];
+        if(vb_valid(p, max_k))
+            sum += vb_items(p);
+        else
+            ++bad;
+    }
+    part[tid] = sum;
+    __syncthreads();
+    // inclusive scan of the per-thread sums (Hillis-Steele)
+    for(int off = 1; off < kVbPrepThreads; off <<= 1)
+    {
+        const int v = tid >= off ? part[tid - off] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int run = part[tid] - sum; // exclusive prefix of this thread's chunk
+    for(int i = lo; i < hi; ++i)
+    {
+        offsets[i]        = run;
+        const VbProblem p = probs[i];
+        if(vb_valid(p, max_k))
+            run += vb_items(p);
+    }
+    if(tid == kVbPrepThreads - 1)
+    {
+        offsets[count] = part[tid];
+        st->counter    = 0;
+    }
+    if(bad)
+        atomicAdd(&st->invalid, bad);
+}
+
+template <typename T>
+struct VbParams
+{
+    const VbProblem* probs;
+    int              count;
+    const int*       offsets;
+    VbState*         st;
+    Scalar<T>        alpha;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kBsThreads) vb_persistent_kernel(VbParams<T> p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item;
+    const int total = p.offsets[p.count];
+    const T   alpha = p.alpha.get();
+    for(;;)
+    {
+        if(threadIdx.x == 0)
+            s_item = atomicAdd(&p.st->counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if(item >= total)
+            break;
+        // problem index: last i with offsets[i] <= item (empty problems share offsets)
+        int lo = 0, hi = p.count - 1;
+        while(lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if(p.offsets[mid] <= item)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const VbProblem q = p.probs[lo];
+        const int strip = item - p.offsets[lo];
+        const int left  = q.side == kLeft;
+        const int k     = left ? q.m : q.n;
+        const int ncols = left ? q.n : q.m;
+        const int trans = q.trans != kOpN;
+        const int tM    = trans != (left ? 0 : 1);
+        const int oplow = (q.uplo == kLower) != (trans != 0);
+        const int mlow  = left ? oplow : !oplow;
+        block_solve_strip<T>(reinterpret_cast<const T*>(q.A), q.lda, reinterpret_cast<T*>(q.B),
+                             q.ldb, k, left, tM, !mlow, q.diag == kUnit, alpha, strip * kBsW,
+                             ncols, smem_raw);
+        __syncthreads();
+    }
+}
+
+} // namespace rb200

@@ -69,7 +69,7 @@ def _sizes_for(side, sizes):
     out = []
     for (m, n, lda, ldb) in sizes:
         k = m if side == "L" else n
-        out.append((m, n, max(lda, k), ldb))
+        out.append((m, n, max(lda, k), max(ldb, m)))
     return out
 
 
