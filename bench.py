@@ -334,6 +334,7 @@ def run_ours(args):
 
 
 def main():
+    global M, N, FLOPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -342,7 +343,6 @@ def main():
     ap.add_argument("--m", type=int, default=M, help="problem size (profiling runs use smaller)")
     ap.add_argument("--n", type=int, default=N)
     args = ap.parse_args()
-    global M, N, FLOPS
     M, N = args.m, args.n
     FLOPS = float(M) * M * N
     if args.impl == "reference":
