@@ -59,6 +59,55 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle        
                                                           rocblas_int                      max_k,
                                                           rocblas_int* invalid_count);
 
+/* ---- FP64 GEMM from integer slices on the tensor cores ------------------------------------
+ * C := alpha op(A) op(B) + beta C in FP64 (column-major), computed as exact int8 x int8 ->
+ * int32 products of `slices` 7-bit slices of every row of op(A) and every column of op(B)
+ * (each scaled by a power of two), combined in FP64.  slices = 7 reproduces FP64 dot
+ * products to about 2^-49 relative to K max|row| max|col|; fewer slices are faster and
+ * less accurate (about 2^(-7 slices)).  Inputs must be finite.  alpha and beta are host
+ * pointers (host pointer mode only; device mode returns rocblas_status_not_implemented).
+ * The reference has no counterpart; it is the engine of the precision form of the trsm.
+ * Workspace from the handle (size query supported). */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle    handle,
+                                                        rocblas_operation transA,
+                                                        rocblas_operation transB,
+                                                        rocblas_int       m,
+                                                        rocblas_int       n,
+                                                        rocblas_int       k,
+                                                        const double*     alpha,
+                                                        const double*     A,
+                                                        rocblas_int       lda,
+                                                        const double*     B,
+                                                        rocblas_int       ldb,
+                                                        const double*     beta,
+                                                        double*           C,
+                                                        rocblas_int       ldc,
+                                                        rocblas_int       slices);
+
+/* ---- precision form of dtrsm ----------------------------------------------------------------
+ * Same contract as rocblas_dtrsm.  The blocked solve keeps the diagonal blocks in FP64
+ * (inverted 128 x 128 blocks applied with FP64 tensor-core MMA) and runs every trailing
+ * update on the integer-slice tensor-core GEMM above with `slices` slices (1..7).
+ * Workspace: the invA blocks plus the slices of the largest update (size query supported). */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
+                                                       rocblas_side      side,
+                                                       rocblas_fill      uplo,
+                                                       rocblas_operation transA,
+                                                       rocblas_diagonal  diag,
+                                                       rocblas_int       m,
+                                                       rocblas_int       n,
+                                                       const double*     alpha,
+                                                       const double*     A,
+                                                       rocblas_int       lda,
+                                                       double*           B,
+                                                       rocblas_int       ldb,
+                                                       rocblas_int       slices);
+
+/* Synchronises the handle's stream and returns (and clears) the error word that kernels
+ * with bounded waits set when a wait ran out: 0 = none.  A nonzero value means results of
+ * calls since the last check are not valid. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_get_device_error(rocblas_handle handle, rocblas_int* code);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,9 @@ struct _rocblas_handle
     bool     size_query    = false;
     size_t   query_size    = 0;
 
+    // device word where kernels with bounded waits record a timeout (lazily allocated)
+    int* err_dev = nullptr;
+
     // rounding of every workspace request (handle.hpp:56-61)
     static size_t roundup(size_t s) { return (s + 63) / 64 * 64; }
 

@@ -9,6 +9,7 @@
 #include <type_traits>
 
 #include "../../include/rocblas_b200_ext.h"
+#include "sliced_driver.cuh"
 #include "trsm_driver.cuh"
 #include "vbatched.cuh"
 
@@ -459,6 +460,142 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
     return launch_status();
 }
 
+int* ensure_err(rocblas_handle h)
+{
+    if(!h->err_dev)
+    {
+        if(cudaMalloc(&h->err_dev, 256) != cudaSuccess)
+        {
+            cudaGetLastError();
+            h->err_dev = nullptr;
+            return nullptr;
+        }
+        cudaMemset(h->err_dev, 0, 256);
+    }
+    return h->err_dev;
+}
+
+rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_operation tb, int m,
+                                int n, int k, const double* alpha, const double* A, int lda,
+                                const double* B, int ldb, const double* beta, double* C, int ldc,
+                                int slices)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    auto okop = [](rocblas_operation t) {
+        return t == rocblas_operation_none || t == rocblas_operation_transpose
+               || t == rocblas_operation_conjugate_transpose;
+    };
+    if(!okop(ta) || !okop(tb) || slices < 1 || slices > kOzMaxS)
+        return rocblas_status_invalid_value;
+    const bool nA = ta == rocblas_operation_none, nB = tb == rocblas_operation_none;
+    if(m < 0 || n < 0 || k < 0 || lda < (nA ? m : k) || ldb < (nB ? k : n) || ldc < m)
+        return rocblas_status_invalid_size;
+    if(!m || !n)
+        return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
+    const size_t ws_bytes = sliced_gemm_workspace_bytes(m, n, k, slices);
+    if(h->size_query)
+        return h->set_optimal_size(ws_bytes);
+    if(!alpha || !beta || !C || (k && (!A || !B)))
+        return rocblas_status_invalid_pointer;
+    if(h->pointer_mode != rocblas_pointer_mode_host)
+        return rocblas_status_not_implemented;
+    rocblas_status st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    int* err = ensure_err(h);
+    void* ws = h->borrow(ws_bytes);
+    if(!ws || !err)
+        return rocblas_status_memory_error;
+    SlicedGemm g{};
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.S = slices;
+    g.P = nA ? SliceOperand{A, 1, lda} : SliceOperand{A, lda, 1};
+    g.Q = nB ? SliceOperand{B, ldb, 1} : SliceOperand{B, 1, ldb};
+    g.C = C;
+    g.ldc = ldc;
+    g.a = *alpha;
+    g.b_imm = *beta;
+    if(!run_sliced_gemm(g, ws, err, h->stream))
+        return rocblas_status_arch_mismatch;
+    return launch_status();
+}
+
+rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                               rocblas_operation trans, rocblas_diagonal diag, int m, int n,
+                               const double* alpha, const double* A, int lda, double* B, int ldb,
+                               int slices)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st
+        = trsm_arg_check<double>(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, 1);
+    if(st != rocblas_status_continue)
+        return st;
+    if(slices < 1 || slices > kOzMaxS)
+        return rocblas_status_invalid_value;
+    if(h->pointer_mode == rocblas_pointer_mode_host && alpha && *alpha == 0.0)
+    {
+        if(h->size_query)
+            return rocblas_status_size_unchanged;
+        if((st = device_ready(h)) != rocblas_status_success)
+            return st;
+        zero_fill<double>(strided<double>(B, 0), ldb, m, n, 1, h->stream);
+        return launch_status();
+    }
+    TrsmProblem<double> pr{};
+    pr.side_left = side == rocblas_side_left;
+    pr.upper     = uplo == rocblas_fill_upper;
+    pr.trans     = trans != rocblas_operation_none;
+    pr.unit      = diag == rocblas_diagonal_unit;
+    pr.m = m;
+    pr.n = n;
+    pr.batch = 1;
+    pr.A = strided<double>(A, 0);
+    pr.lda = lda;
+    pr.B = strided<double>(B, 0);
+    pr.ldb = ldb;
+    pr.stream   = h->stream;
+    pr.sm_count = h->sm_count;
+    const int64_t k = pr.k();
+    const bool recursive = choose_algo(pr) == Algo::recursive;
+    const size_t inv_bytes = recursive ? align256((size_t)kInvNB * k * sizeof(double)) : 0;
+    const size_t sl_bytes  = recursive ? mixed_slice_workspace_bytes(pr, slices) : 0;
+    const size_t ws_bytes  = inv_bytes + sl_bytes;
+    if(h->size_query)
+        return ws_bytes ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    if(h->pointer_mode == rocblas_pointer_mode_host)
+        pr.alpha.val = *alpha;
+    else
+        pr.alpha.ptr = alpha;
+    if(!recursive)
+    {
+        trsm_run<double>(pr, nullptr, false);
+        return launch_status();
+    }
+    int*  err = ensure_err(h);
+    void* ws  = h->borrow(ws_bytes);
+    if(!ws || !err)
+        return rocblas_status_memory_error;
+    BatchPtr<double> inv;
+    inv.base   = reinterpret_cast<double*>(ws);
+    inv.stride = (int64_t)kInvNB * k;
+    build_invA<double>(pr, inv);
+    pr.invA = inv;
+    MixedRecursive rec{{pr, (int)k, (int)ceil_div(k, kInvNB)}};
+    rec.S        = slices;
+    rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
+    rec.err_dev  = err;
+    rec.solve_mixed(0, rec.nblk, 1);
+    if(!rec.ok)
+        return rocblas_status_arch_mismatch;
+    return launch_status();
+}
+
 } // namespace
 
 // =========================================================================================
@@ -502,6 +639,8 @@ try
     if(!handle)
         return rocblas_status_invalid_handle;
     handle->free_mem();
+    if(handle->err_dev)
+        cudaFree(handle->err_dev);
     delete handle;
     return rocblas_status_success;
 }
@@ -827,6 +966,59 @@ rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle h, const float* alpha,
 try
 {
     return trsm_vbatched_impl<float>(h, alpha, problems, count, max_k, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+// ---- sliced GEMM / precision form (rocblas_b200_ext.h) -----------------------------------------
+rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle h, rocblas_operation transA,
+                                         rocblas_operation transB, rocblas_int m, rocblas_int n,
+                                         rocblas_int k, const double* alpha, const double* A,
+                                         rocblas_int lda, const double* B, rocblas_int ldb,
+                                         const double* beta, double* C, rocblas_int ldc,
+                                         rocblas_int slices)
+try
+{
+    return gemm_sliced_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                        rocblas_operation transA, rocblas_diagonal diag,
+                                        rocblas_int m, rocblas_int n, const double* alpha,
+                                        const double* A, rocblas_int lda, double* B,
+                                        rocblas_int ldb, rocblas_int slices)
+try
+{
+    return trsm_mixed_impl(h, side, uplo, transA, diag, m, n, alpha, A, lda, B, ldb, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_get_device_error(rocblas_handle h, rocblas_int* code)
+try
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(!code)
+        return rocblas_status_invalid_pointer;
+    *code = 0;
+    if(!h->err_dev)
+        return rocblas_status_success;
+    if(cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return rocblas_status_internal_error;
+    int v = 0;
+    cudaMemcpy(&v, h->err_dev, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemset(h->err_dev, 0, sizeof(int));
+    *code = v;
+    return launch_status();
 }
 catch(...)
 {

@@ -1,0 +1,271 @@
+// Host side of the sliced (integer-slice, tensor-core) FP64 GEMM and of the precision form
+// of the TRSM that uses it for its trailing updates.
+#pragma once
+#include <cuda.h>
+#include <mutex>
+
+#include "ozaki_gemm.cuh"
+#include "trsm_driver.cuh"
+
+namespace rb200
+{
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda link)
+static EncodeTiledFn encode_tiled_fn()
+{
+    static EncodeTiledFn  fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void*                            p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess
+           && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// Element (o, k) of an operand at ptr[o * so + k * sk].
+struct SliceOperand
+{
+    const double* ptr;
+    int64_t       so, sk;
+    SliceOperand  shifted_k(int64_t k0) const { return {ptr + k0 * sk, so, sk}; }
+};
+
+static inline int64_t round_up(int64_t a, int64_t b)
+{
+    return (a + b - 1) / b * b;
+}
+
+static inline size_t align256(size_t b)
+{
+    return (b + 255) & ~size_t(255);
+}
+
+// Workspace for one sliced GEMM of M x N x K with S slices.
+static size_t sliced_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int S)
+{
+    const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), kOzKMax), kOzBK);
+    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kOzBN);
+    return align256((size_t)S * Mp * Kp) + align256((size_t)S * Np * Kp) + align256(4 * Mp)
+           + align256(4 * Np);
+}
+
+struct SlicedGemm
+{
+    // C := b * C + a * P Q  (b = b_user ? *ualpha : b_imm; ualpha == 0 with zero_guard => C := 0)
+    int64_t       M, N, K;
+    int           S;
+    SliceOperand  P, Q;
+    double*       C;
+    int64_t       ldc;
+    double        a;
+    double        b_imm;
+    const double* ualpha_dev; // device-mode alpha of the caller (or nullptr)
+    double        ualpha_host;
+    int           b_user;
+    int           zero_guard;
+};
+
+static void launch_exponents(SliceOperand X, int O, int K, int* exps, cudaStream_t s)
+{
+    if(X.so == 1)
+    {
+        oz_exponent_rows_kernel<<<(unsigned)ceil_div(O, 256), 256, 0, s>>>(X.ptr, X.sk, O, K, exps);
+    }
+    else
+    {
+        const int64_t threads = (int64_t)O * 32;
+        oz_exponent_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps);
+    }
+    count_launch();
+}
+
+static void launch_slices(SliceOperand X, int O, int K, const int* exps, int S, int8_t* dst, int O_pad,
+                          int K_pad, cudaStream_t s)
+{
+    dim3 grid((unsigned)(K_pad / kOzSliceTile), (unsigned)(O_pad / kOzSliceTile));
+    oz_slice_kernel<<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    count_launch();
+}
+
+static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t rows, int box_rows)
+{
+    EncodeTiledFn enc = encode_tiled_fn();
+    if(!enc)
+        return false;
+    cuuint64_t dims[2]    = {(cuuint64_t)K_pad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)K_pad};
+    cuuint32_t box[2]     = {(cuuint32_t)kOzBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2]    = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+           == CUDA_SUCCESS;
+}
+
+// Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
+// Returns false if the tensor-map encoder is unavailable.
+static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream_t s)
+{
+    if(g.M <= 0 || g.N <= 0)
+        return true;
+    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kOzBN);
+    const int     S  = g.S;
+    const int     stage_bytes = S * (kOzTileA + kOzTileB);
+    const int     stages      = std::min(8, kOzSmemBudget / stage_bytes);
+    const size_t  smem        = (size_t)stages * stage_bytes + 1024;
+    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    const int64_t K = std::max<int64_t>(g.K, 0);
+    for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kOzKMax)
+    {
+        const int64_t kc = std::min<int64_t>(kOzKMax, K - k0);
+        const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kOzBK);
+        unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+        int8_t* sP = reinterpret_cast<int8_t*>(w);
+        w += align256((size_t)S * Mp * Kp);
+        int8_t* sQ = reinterpret_cast<int8_t*>(w);
+        w += align256((size_t)S * Np * Kp);
+        int* eP = reinterpret_cast<int*>(w);
+        w += align256(4 * Mp);
+        int* eQ = reinterpret_cast<int*>(w);
+
+        const SliceOperand P = g.P.shifted_k(k0), Q = g.Q.shifted_k(k0);
+        if(kc > 0)
+        {
+            launch_exponents(P, (int)g.M, (int)kc, eP, s);
+            launch_exponents(Q, (int)g.N, (int)kc, eQ, s);
+        }
+        else
+        {
+            cudaMemsetAsync(eP, 0, 4 * Mp, s);
+            cudaMemsetAsync(eQ, 0, 4 * Np, s);
+        }
+        launch_slices(P, (int)g.M, (int)kc, eP, S, sP, (int)Mp, (int)Kp, s);
+        launch_slices(Q, (int)g.N, (int)kc, eQ, S, sQ, (int)Np, (int)Kp, s);
+
+        CUtensorMap mapP, mapQ;
+        if(!make_slice_map(&mapP, sP, Kp, (int64_t)S * Mp, kOzBM)
+           || !make_slice_map(&mapQ, sQ, Kp, (int64_t)S * Np, kOzBN))
+            return false;
+        OzParams p{};
+        p.M = (int)g.M;
+        p.N = (int)g.N;
+        p.K = (int)std::max<int64_t>(kc, 1);
+        p.S = S;
+        p.M_pad = (int)Mp;
+        p.N_pad = (int)Np;
+        p.exp_rows = eP;
+        p.exp_cols = eQ;
+        p.C = g.C;
+        p.ldc = g.ldc;
+        p.alpha = g.a;
+        const bool first = k0 == 0;
+        p.beta  = first ? (g.b_user ? g.ualpha_host : g.b_imm) : 1.0;
+        p.beta_ptr = (first && g.b_user) ? g.ualpha_dev : nullptr;
+        p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
+        p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
+        p.stages = stages;
+        p.error = err_dev;
+        dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / kOzBN));
+        ozaki_gemm_kernel<<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
+        count_launch();
+    }
+    return true;
+}
+
+// ---- precision form of the TRSM ---------------------------------------------------------------
+// The blocked recursive solve of trsm_driver.cuh with its trailing updates on the sliced
+// tensor-core GEMM; the diagonal blocks stay in FP64 (fused trtri + DMMA invA leaves).
+struct MixedRecursive : Recursive<double>
+{
+    int   S;
+    void* slice_ws;
+    int*  err_dev;
+    bool  ok = true;
+
+    void update_sliced(int c_lo, int c_hi, int x_lo, int x_hi, int first)
+    {
+        const TrsmProblem<double>& q = pr;
+        const double* A = q.A.base + q.A.offset;
+        double*       B = q.B.base + q.B.offset;
+        SlicedGemm g{};
+        if(q.side_left)
+        {
+            g.M = c_hi - c_lo;
+            g.N = q.n;
+            g.K = x_hi - x_lo;
+            g.P = !q.trans ? SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda}
+                           : SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1};
+            g.Q = SliceOperand{B + x_lo, q.ldb, 1};
+            g.C = B + c_lo;
+        }
+        else
+        {
+            g.M = q.m;
+            g.N = c_hi - c_lo;
+            g.K = x_hi - x_lo;
+            g.P = SliceOperand{B + (int64_t)x_lo * q.ldb, 1, q.ldb};
+            g.Q = !q.trans ? SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1}
+                           : SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda};
+            g.C = B + (int64_t)c_lo * q.ldb;
+        }
+        g.S = S;
+        g.ldc = q.ldb;
+        g.a = -1.0;
+        g.b_imm = 1.0;
+        g.b_user = first;
+        g.ualpha_dev = q.alpha.ptr;
+        g.ualpha_host = q.alpha.val;
+        g.zero_guard = 1;
+        ok = ok && run_sliced_gemm(g, slice_ws, err_dev, q.stream);
+    }
+
+    void solve_mixed(int b0, int b1, int first)
+    {
+        if(b1 - b0 == 1)
+        {
+            leaf(b0, first);
+            return;
+        }
+        const int  bm = (b0 + b1) / 2;
+        const int  r0 = row_of(b0), rm = row_of(bm), r1 = row_of(b1);
+        const bool forward = pr.side_left ? pr.oplower() : !pr.oplower();
+        if(forward)
+        {
+            solve_mixed(b0, bm, first);
+            update_sliced(rm, r1, r0, rm, first);
+            solve_mixed(bm, b1, 0);
+        }
+        else
+        {
+            solve_mixed(bm, b1, first);
+            update_sliced(r0, rm, rm, r1, first);
+            solve_mixed(b0, bm, 0);
+        }
+    }
+};
+
+// Largest sliced update of the recursion (the top node's off-diagonal block).
+static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S)
+{
+    const int64_t k = pr.k();
+    if(k <= kInvNB)
+        return 0;
+    const int64_t nblk = ceil_div(k, kInvNB);
+    const int64_t bm   = nblk / 2;
+    const int64_t r_m  = std::min<int64_t>(bm * kInvNB, k);
+    const int64_t big  = std::max(r_m, k - r_m);
+    return pr.side_left ? sliced_gemm_workspace_bytes(big, pr.n, big, S)
+                        : sliced_gemm_workspace_bytes(pr.m, big, big, S);
+}
+
+} // namespace rb200
