@@ -61,6 +61,7 @@ struct OzParams
     const double* ualpha_ptr;  // if set and *ualpha_ptr == 0: C := 0 (a trsm with alpha == 0)
     int      ualpha_zero;      // host-side form of the same condition
     int      stages;
+    int      tmem_cols;        // power of two >= S * 64
     int*     error;            // set to a nonzero code if a wait timed out
 };
 
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base_sh)),
-                     "r"(512));
+                     "r"(p.tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -286,14 +287,15 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         const int quarter = warp & 3;                 // TMEM lane group this warp may access
         const int row     = quarter * 32 + lane;
         const int gr      = m0 + row;
-        bool ok = mbar_wait_bounded(&acc_bar, 0);
+        // warp-uniform outcome: the tcgen05.ld below needs the whole warp
+        bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&acc_bar, 0));
         if(!ok)
         {
             atomicExch(p.error, 3);
             atomicExch(&abort_flag, 1);
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        if(ok && !*(volatile int*)&abort_flag)
+        if(__all_sync(0xffffffffu, ok && !*(volatile int*)&abort_flag))
         {
             const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
             const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
@@ -352,7 +354,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     if(warp == 1)
     {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(p.tmem_cols));
     }
 }
 

@@ -174,6 +174,7 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
         p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
         p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
         p.stages = stages;
+        p.tmem_cols = S * kOzBN <= 64 ? 64 : S * kOzBN <= 128 ? 128 : S * kOzBN <= 256 ? 256 : 512;
         p.error = err_dev;
         dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / kOzBN));
         ozaki_gemm_kernel<<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
