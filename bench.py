@@ -1,10 +1,13 @@
 """TRSM benchmark: one JSON line on rank 0.
 
-Headline workload: dtrsm side=L, uplo=L, transA=N, diag=N, m=16384, n=4096, alpha=1, lda=ldb=m
-(the precision-form problem size) in the plain FP64 form.  A is the condition-band recipe
-(band k=0) with a NaN upper triangle; B ~ U(-1,1).  One step = restore the right-hand side
-(a device copy of 512 MiB, inside the timed region) + one rocblas_dtrsm through the C ABI.
-A (2 GiB) and B (512 MiB) are larger than the 126 MB L2, so no flush is needed between steps.
+Headline workload: dtrsm side=L, uplo=L, transA=N, diag=N, m=16384, n=4096, alpha=1, lda=ldb=m,
+solved by the precision form (rocblas_b200_dtrsm_mixed: trailing updates from int8 slices on
+the tcgen05 tensor cores, FP64 diagonal blocks) and, beside it, by the plain FP64 form
+(rocblas_dtrsm).  A is the condition-band recipe (band k=0) with a NaN upper triangle;
+B ~ U(-1,1).  One step = restore the right-hand side (a device copy of 512 MiB, inside the timed
+region) + one solve through the C ABI.  A (2 GiB) and B (512 MiB) are larger than the 126 MB L2,
+so no flush is needed between steps.  Errors are reported per condition band k in {0,2,4,6}
+against the float128 oracle and the host FP64 CBLAS.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -35,7 +38,7 @@ FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
 
 
 def workload_name():
-    return f"dtrsm L/L/N/N m={M} n={N} lda=ldb={M} alpha=1 (condition band k=0), plain FP64"
+    return f"dtrsm L/L/N/N m={M} n={N} lda=ldb={M} alpha=1 (condition band k=0)"
 
 
 def _env_rank():
@@ -184,64 +187,78 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     rb.build()
     L = rb.lib()
+    S = args.slices
 
     At, B0 = workloads.condition_band_lower_torch(M, N, 0, seed=1234 + rank, device=dev)
     Bt = B0.clone()
     stream = torch.cuda.current_stream(dev)
     h = rb.Handle()
     h.set_stream(ctypes.c_void_p(stream.cuda_stream))
-    # reserve the invA workspace up front (128 * m doubles)
-    assert L.rocblas_set_device_memory_size(h.value, 128 * M * 8) == 0
     one = ctypes.c_double(1.0)
     one_p = ctypes.cast(ctypes.byref(one), ctypes.c_void_p)
+    args_common = (rb.side_left, rb.fill_lower, rb.operation_none, rb.diagonal_non_unit, M, N, one_p)
 
-    def solve(Bbuf, Abuf=At):
-        st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
-                             rb.diagonal_non_unit, M, N, one_p, ctypes.c_void_p(Abuf.data_ptr()), M,
+    def solve_plain(Bbuf, Abuf):
+        st = L.rocblas_dtrsm(h.value, *args_common, ctypes.c_void_p(Abuf.data_ptr()), M,
                              ctypes.c_void_p(Bbuf.data_ptr()), M)
         if st != 0:
             raise rb.RocblasError("rocblas_dtrsm", st)
 
-    def step():
-        Bt.copy_(B0)
-        solve(Bt)
+    def solve_mixed(Bbuf, Abuf):
+        st = L.rocblas_b200_dtrsm_mixed(h.value, *args_common, ctypes.c_void_p(Abuf.data_ptr()), M,
+                                        ctypes.c_void_p(Bbuf.data_ptr()), M, S)
+        if st != 0:
+            raise rb.RocblasError("rocblas_b200_dtrsm_mixed", st)
 
-    for _ in range(max(args.warmup, 0)):
-        step()
-    torch.cuda.synchronize(dev)
+    # workspace by the size-query protocol, reserved before timing (no allocation inside)
+    assert L.rocblas_start_device_memory_size_query(h.value) == 0
+    L.rocblas_dtrsm(h.value, *args_common, None, M, None, M)
+    L.rocblas_b200_dtrsm_mixed(h.value, *args_common, None, M, None, M, S)
+    ws = ctypes.c_size_t(0)
+    assert L.rocblas_stop_device_memory_size_query(h.value, ctypes.byref(ws)) == 0
+    assert L.rocblas_set_device_memory_size(h.value, ws.value) == 0
 
+    def timed(solve, steps, warmup):
+        for _ in range(max(warmup, 0)):
+            Bt.copy_(B0)
+            solve(Bt, At)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        l0 = L.rocblas_b200_kernel_launch_count()
+        ev_m = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(steps):
+            Bt.copy_(B0)
+            ev_m[i].record(stream)
+            solve(Bt, At)
+            ev_e[i].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        launches = L.rocblas_b200_kernel_launch_count() - l0
+        total = t0.elapsed_time(t1)
+        if dist:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total, [ev_m[i].elapsed_time(ev_e[i]) for i in range(steps)], launches
+
+    # ---- timed region: the precision form (headline), then the plain FP64 form ---------------
     sampler = ClockSampler(dev.index if dev.index is not None else 0)
     sampler.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    launches0 = L.rocblas_b200_kernel_launch_count()
-    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev_m = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for i in range(args.steps):
-        ev_s[i].record(stream)
-        Bt.copy_(B0)
-        ev_m[i].record(stream)
-        solve(Bt)
-        ev_e[i].record(stream)
-    t_end.record(stream)
-    torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    launches = L.rocblas_b200_kernel_launch_count() - launches0
+    total_ms, solve_ms, launches = timed(solve_mixed, args.steps, args.warmup)
     clocks = sampler.stop()
-    total_ms = t_start.elapsed_time(t_end)
-    solve_ms = [ev_m[i].elapsed_time(ev_e[i]) for i in range(args.steps)]
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
     value = FLOPS * world / (ms_per_step * 1e-3) / 1e12
+    X_mixed_band0 = Bt.clone()
+    p_total, p_solve, p_launches = timed(solve_plain, args.steps, args.warmup)
+    X_plain_band0 = Bt.clone()
+    plain_value = FLOPS * world / (p_total / args.steps * 1e-3) / 1e12
 
     # ---- e2e: host buffers through the C ABI, copies inside the timed region -----------
     e2e = None
@@ -256,7 +273,7 @@ def run_ours(args):
         def e2e_step():
             Ad.copy_(A_host, non_blocking=True)
             Bd.copy_(B_host, non_blocking=True)
-            solve(Bd, Ad)
+            solve_mixed(Bd, Ad)
             B_host.copy_(Bd, non_blocking=True)
 
         e2e_step()
@@ -272,56 +289,86 @@ def run_ours(args):
         e2e_ms = s0.elapsed_time(s1) / ksteps
         e2e = {"value": FLOPS / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(At.numel() * 8 + B0.numel() * 8),
-               "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms}
+               "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms,
+               "form": f"precision form, {S} slices"}
         del Ad, Bd, A_host, B_host
 
-    # ---- error against the FP64 host oracle on a column sample + CPU baseline --------------
+    # ---- errors per condition band against the float128 / FP64 host oracles, CPU baseline -------
     extra = {}
     if rank == 0:
         import oracle
 
         peak = fp64_peak_tflops(torch, dev)
-        solve_med = statistics.median(solve_ms)
-        achieved = FLOPS / (solve_med * 1e-3) / 1e12
+        med_mixed = statistics.median(solve_ms)
+        med_plain = statistics.median(p_solve)
+        threads = os.cpu_count() or 1
+        cols = list(range(8))
+        bands = {}
+        cpu = None
+        for kb in (0, 2, 4, 6):
+            if kb == 0:
+                Ab, Bb, Xm, Xp = At, B0, X_mixed_band0, X_plain_band0
+            else:
+                Ab, Bb = workloads.condition_band_lower_torch(M, N, kb, seed=99 + kb, device=dev)
+                Xm, Xp = Bb.clone(), Bb.clone()
+                solve_mixed(Xm, Ab)
+                solve_plain(Xp, Ab)
+                torch.cuda.synchronize(dev)
+            A_host = np.asfortranarray(np.nan_to_num(Ab.cpu().numpy().T, nan=0.0))
+            B_host = np.asfortranarray(Bb.cpu().numpy().T)
+            Xq = oracle.trsm("L", "L", "N", "N", 1.0, A_host, np.asfortranarray(B_host[:, cols]),
+                             precision="q")
+            Xm_h = Xm.cpu().numpy().T
+            Xp_h = Xp.cpu().numpy().T
+            if kb == 0:
+                ncols = min(N, 512)
+                cpu_tflops, cpu_s, Xc = cpu_cblas_sample(A_host, B_host, ncols, threads)
+                cpu = (cpu_tflops, cpu_s, ncols)
+                Xc8 = Xc[:, cols]
+            else:
+                _, _, Xc8 = cpu_cblas_sample(A_host, B_host, len(cols), threads)
+            bands[f"k{kb}"] = {
+                "precision_form_vs_float128": oracle.normwise_forward_error(Xm_h[:, cols], Xq),
+                "plain_fp64_vs_float128": oracle.normwise_forward_error(Xp_h[:, cols], Xq),
+                "fp64_cblas_vs_float128": oracle.normwise_forward_error(Xc8, Xq),
+                "precision_form_vs_fp64_cblas": oracle.normwise_forward_error(Xm_h[:, cols], Xc8),
+                "refinement_iterations": 0,
+            }
+            del A_host, B_host
+        achieved = FLOPS / (med_mixed * 1e-3) / 1e12
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None,
-                    "kernel": "whole rocblas_dtrsm call (DMMA GEMM tiles + trtri + invA leaves)",
-                    "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
-                                   "MEASURED_PEAKS.json has no FP64 figure"}
-        # final X of the last timed step is in Bt; A on the host (upper triangle -> 0)
-        X = Bt.cpu().numpy().T  # (m, n) view of column-major storage
-        A_host = np.asfortranarray(np.nan_to_num(At.cpu().numpy().T, nan=0.0))
-        B_host = np.asfortranarray(B0.cpu().numpy().T)
-        threads = os.cpu_count() or 1
-        ncols = min(N, 512)
-        cpu_tflops, cpu_s, Xc = cpu_cblas_sample(A_host, B_host, ncols, threads)
-        cols = list(range(8))
-        Xq = oracle.trsm("L", "L", "N", "N", 1.0, A_host, np.asfortranarray(B_host[:, cols]), precision="q")
-        err_q = oracle.normwise_forward_error(X[:, cols], Xq)
-        err_c = oracle.normwise_forward_error(X[:, :ncols], Xc)
-        err_c_vs_q = oracle.normwise_forward_error(Xc[:, cols], Xq)
+                    "kernel": f"whole rocblas_b200_dtrsm_mixed call ({S}-slice int8 tcgen05 updates, "
+                              "FP64 DMMA diagonal blocks), m*n*k FP64-equivalent flops",
+                    "peak_source": "FP64 denominator: cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured "
+                                   "in this run; MEASURED_PEAKS.json has no FP64 figure"}
         extra = {
             "roofline": roofline,
-            "cpu_baseline": {"value": cpu_tflops, "unit": "TFLOP/s", "cores": threads,
-                             "kind": "reference",
+            "plain_fp64": {"value": plain_value, "unit": "TFLOP/s", "ms_per_step": p_total / args.steps,
+                           "solve_ms_median": med_plain, "frac_of_fp64_peak": plain_value / peak,
+                           "gpu_launches": int(p_launches)},
+            "precision_vs_plain": value / plain_value,
+            "cpu_baseline": {"value": cpu[0], "unit": "TFLOP/s", "cores": threads, "kind": "reference",
                              "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) "
-                                       f"on {ncols} of the {N} right-hand sides, full m={M}, "
-                                       f"{cpu_s:.2f} s"},
-            "error": {"vs_fp64_cblas_normwise": err_c, "vs_float128_oracle_normwise": err_q,
-                      "fp64_cblas_vs_float128": err_c_vs_q,
-                      "sample": f"columns 0..{ncols - 1} (cblas) / 0..7 (float128 oracle)"},
-            "solve_ms_median": solve_med,
+                                       f"on {cpu[2]} of the {N} right-hand sides, full m={M}, "
+                                       f"{cpu[1]:.2f} s"},
+            "error_bands": bands,
+            "error_sample": "normwise ||X - X*||_F / ||X*||_F on right-hand sides 0..7; X* = float128 "
+                            "oracle; bands: diagonal 10^(-k i/m)",
+            "solve_ms_median": med_mixed,
         }
 
     if rank == 0:
         line = {
-            "metric": "dtrsm TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "metric": "dtrsm TFLOP/s (precision form, FP64 accuracy)", "value": value,
+            "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": workload_name(), "m": M, "n": N, "form": "plain FP64",
+            "config": {"workload": workload_name(), "m": M, "n": N,
+                       "form": f"precision form: int8-slice tensor-core updates ({S} slices), FP64 diagonal blocks",
                        "l2": "inputs larger than L2 (A 2 GiB, B 512 MiB); no flush",
-                       "step": "device copy of B (512 MiB) + rocblas_dtrsm",
+                       "step": "device copy of B (512 MiB) + one solve",
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
         }
@@ -342,6 +389,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--m", type=int, default=M, help="problem size (profiling runs use smaller)")
     ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--slices", type=int, default=7, help="slices of the precision form")
     args = ap.parse_args()
     M, N = args.m, args.n
     FLOPS = float(M) * M * N
