@@ -1,0 +1,282 @@
+// FP64 GEMM tiles on the DMMA tensor path with a cp.async multistage pipeline.
+//
+//     C := a * op(P) * op(Q) + b * C        (same contract as gemm_tile.cuh, GemmParams<double>)
+//
+// B200's FP64 tensor instruction is mma.sync m8n8k4 (the tcgen05 tensor cores have no f64
+// kind), so these tiles feed DMMA from shared memory filled by 8-byte cp.async copies
+// (any leading dimension, zero-fill for out-of-range and masked-triangle elements) in a
+// 3..4-stage ring.  Each operand is staged in the orientation that keeps both the copies and
+// the fragment reads free of bank conflicts:
+//   operand rows contiguous in memory (kc = false): smem [k][o], pitch O + 4 doubles;
+//   operand k contiguous in memory   (kc = true) : smem [o][k], pitch 16 + 4 doubles.
+// Tile shapes range from 128 x 128 (8 warps, warp tile 64 x 32) down to 128 x 32 / 32 x 128
+// (4 warps, warp tile 32 x 32) so that small trailing updates and the invA leaves still fill
+// the 148 SMs.
+#pragma once
+#include "gemm_tile.cuh"
+
+namespace rb200
+{
+
+constexpr int kDBK = 16;
+
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem, bool valid)
+{
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    const int      n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
+struct DmmaCfg
+{
+    static constexpr int kWarpsM  = BM / WM;
+    static constexpr int kWarpsN  = BN / WN;
+    static constexpr int kThreads = kWarpsM * kWarpsN * 32;
+    static constexpr int kPitchA  = KCP ? (kDBK + 4) : (BM + 4);
+    static constexpr int kPitchB  = KCQ ? (kDBK + 4) : (BN + 4);
+    static constexpr int kStageA  = KCP ? BM * kPitchA : kDBK * kPitchA; // doubles
+    static constexpr int kStageB  = KCQ ? BN * kPitchB : kDBK * kPitchB;
+    static constexpr int kStage   = kStageA + kStageB;
+    static constexpr size_t kSmem = (size_t)STAGES * kStage * sizeof(double);
+};
+
+// Loads one BK-deep stage of an operand tile of `O` rows (o0..o0+O-1 of the logical operand)
+// with cp.async.  Logical (o, k) is stored at ptr[r + c*ld], (r, c) = kc ? (k, o) : (o, k).
+template <int O, int NT, bool KC>
+__device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, int64_t ld, int tri,
+                                                int o0, int k0, int Olim, int Klim, int tid)
+{
+    constexpr int PER = O * kDBK / NT;
+    static_assert(PER * NT == O * kDBK, "tile / thread mismatch");
+#pragma unroll
+    for(int i = 0; i < PER; ++i)
+    {
+        const int e = tid + i * NT;
+        int       o, kk;
+        if(KC)
+        {
+            kk = e % kDBK;
+            o  = e / kDBK;
+        }
+        else
+        {
+            o  = e % O;
+            kk = e / O;
+        }
+        const int     go = o0 + o, gk = k0 + kk;
+        const int64_t r = KC ? gk : go, c = KC ? go : gk;
+        const bool    valid = go < Olim && gk < Klim && tri_keep(tri, r, c);
+        const double* src   = valid ? ptr + r + c * ld : ptr;
+        double*       dst   = KC ? s + o * (kDBK + 4) + kk : s + kk * (O + 4) + o;
+        cp_async_8(dst, src, valid);
+    }
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads)
+    gemm_dmma_kernel(GemmParams<double> p)
+{
+    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>;
+    constexpr int NT = Cfg::kThreads;
+    constexpr int TM = WM / 8, TN = WN / 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* smem = reinterpret_cast<double*>(smem_raw);
+
+    const int tid   = threadIdx.x;
+    const int lane  = tid & 31, warp = tid >> 5;
+    const int wm    = warp % Cfg::kWarpsM, wn = warp / Cfg::kWarpsM;
+    const int m0    = blockIdx.x * BM;
+    const int n0    = blockIdx.y * BN;
+    const int batch = p.batch_base + blockIdx.z;
+
+    double*      C  = p.C.get(batch);
+    const double ua = (p.zero_guard || p.a_user || p.b_user) ? p.ualpha.get() : 1.0;
+    const bool   zero_out = p.zero_guard && ua == 0.0;
+    const double a  = p.a_user ? ua : p.a_imm;
+    const double b  = p.b_user ? ua : p.b_imm;
+
+    double acc[TM][TN][2];
+#pragma unroll
+    for(int i = 0; i < TM; ++i)
+#pragma unroll
+        for(int j = 0; j < TN; ++j)
+            acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    if(!zero_out)
+    {
+        const double* P  = p.P.get(batch);
+        const double* Q  = p.Q.get(batch);
+        const int     nk = (p.K + kDBK - 1) / kDBK;
+        auto load = [&](int stage, int kt) {
+            double* sA = smem + stage * Cfg::kStage;
+            double* sB = sA + Cfg::kStageA;
+            dmma_load_stage<BM, NT, KCP>(sA, P, p.ldp, p.triP, m0, kt * kDBK, p.M, p.K, tid);
+            dmma_load_stage<BN, NT, KCQ>(sB, Q, p.ldq, p.triQ, n0, kt * kDBK, p.N, p.K, tid);
+        };
+#pragma unroll
+        for(int s = 0; s < STAGES - 1; ++s)
+        {
+            if(s < nk)
+                load(s, s);
+            cp_async_commit();
+        }
+        const int lr = lane >> 2, lk = lane & 3;
+        for(int kt = 0; kt < nk; ++kt)
+        {
+            cp_async_wait<STAGES - 2>();
+            __syncthreads();
+            const double* sA = smem + (kt % STAGES) * Cfg::kStage;
+            const double* sB = sA + Cfg::kStageA;
+#pragma unroll
+            for(int ks = 0; ks < kDBK / 4; ++ks)
+            {
+                const int k = ks * 4 + lk;
+                double    fa[TM], fb[TN];
+#pragma unroll
+                for(int i = 0; i < TM; ++i)
+                {
+                    const int o = wm * WM + i * 8 + lr;
+                    fa[i]       = KCP ? sA[o * Cfg::kPitchA + k] : sA[k * Cfg::kPitchA + o];
+                }
+#pragma unroll
+                for(int j = 0; j < TN; ++j)
+                {
+                    const int o = wn * WN + j * 8 + lr;
+                    fb[j]       = KCQ ? sB[o * Cfg::kPitchB + k] : sB[k * Cfg::kPitchB + o];
+                }
+#pragma unroll
+                for(int i = 0; i < TM; ++i)
+#pragma unroll
+                    for(int j = 0; j < TN; ++j)
+                        dmma_8x8x4(acc[i][j], fa[i], fb[j]);
+            }
+            const int nxt = kt + STAGES - 1;
+            if(nxt < nk)
+                load(nxt % STAGES, nxt);
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+    }
+
+    const int64_t ldc = p.ldc;
+#pragma unroll
+    for(int i = 0; i < TM; ++i)
+#pragma unroll
+        for(int j = 0; j < TN; ++j)
+#pragma unroll
+            for(int e = 0; e < 2; ++e)
+            {
+                const int gr = m0 + wm * WM + i * 8 + (lane >> 2);
+                const int gc = n0 + wn * WN + j * 8 + (lane & 3) * 2 + e;
+                if(gr < p.M && gc < p.N)
+                {
+                    double* cp = C + gr + (int64_t)gc * ldc;
+                    double  out;
+                    if(zero_out)
+                        out = 0.0;
+                    else if(b == 0.0)
+                        out = a * acc[i][j][e];
+                    else
+                        out = fma(a, acc[i][j][e], b * (*cp));
+                    *cp = out;
+                }
+            }
+}
+
+// ---- launch --------------------------------------------------------------------------------
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
+static void launch_dmma_cfg(const GemmParams<double>& p0, int batch, cudaStream_t s)
+{
+    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>;
+    auto kern = gemm_dmma_kernel<BM, BN, WM, WN, STAGES, KCP, KCQ>;
+    cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
+    for(int b0 = 0; b0 < batch; b0 += 65535)
+    {
+        GemmParams<double> p = p0;
+        p.batch_base = b0;
+        dim3 grid((unsigned)ceil_div(p.M, BM), (unsigned)ceil_div(p.N, BN),
+                  (unsigned)std::min(65535, batch - b0));
+        kern<<<grid, Cfg::kThreads, Cfg::kSmem, s>>>(p);
+    }
+}
+
+enum class DmmaTile
+{
+    t128x128,
+    t128x64,
+    t64x128,
+    t64x64,
+    t128x32,
+    t32x128
+};
+
+template <bool KCP, bool KCQ>
+static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch, cudaStream_t s)
+{
+    switch(t)
+    {
+    case DmmaTile::t128x128: launch_dmma_cfg<128, 128, 64, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t128x64:  launch_dmma_cfg<128, 64, 32, 32, 3, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t64x128:  launch_dmma_cfg<64, 128, 32, 32, 3, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t64x64:   launch_dmma_cfg<64, 64, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t128x32:  launch_dmma_cfg<128, 32, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t32x128:  launch_dmma_cfg<32, 128, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
+    }
+}
+
+// Tile choice: the largest tile that still gives every SM work.  `full_m` / `full_n` force a
+// tile that spans all M rows (N columns), which the in-place invA application needs.
+static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, bool full_m, bool full_n)
+{
+    auto tiles = [&](int bm, int bn) { return ceil_div(M, bm) * ceil_div(N, bn) * batch; };
+    if(full_m)
+    {
+        if(tiles(128, 128) >= sms)
+            return DmmaTile::t128x128;
+        if(tiles(128, 64) >= sms)
+            return DmmaTile::t128x64;
+        return DmmaTile::t128x32;
+    }
+    if(full_n)
+    {
+        if(tiles(128, 128) >= sms)
+            return DmmaTile::t128x128;
+        if(tiles(64, 128) >= sms)
+            return DmmaTile::t64x128;
+        return DmmaTile::t32x128;
+    }
+    if(tiles(128, 128) >= 2 * sms)
+        return DmmaTile::t128x128;
+    if(M >= N ? tiles(128, 64) >= sms : tiles(64, 128) >= sms)
+        return M >= N ? DmmaTile::t128x64 : DmmaTile::t64x128;
+    return DmmaTile::t64x64;
+}
+
+static void launch_gemm_dmma(const GemmParams<double>& p, int batch, cudaStream_t s, int sms,
+                             bool full_m, bool full_n)
+{
+    if(p.M <= 0 || p.N <= 0)
+        return;
+    const DmmaTile t   = choose_dmma_tile(p.M, p.N, batch, sms, full_m, full_n);
+    const bool     kcP = p.transP != 0, kcQ = p.transQ == 0;
+    if(kcP && kcQ)
+        launch_dmma_tile<true, true>(t, p, batch, s);
+    else if(kcP)
+        launch_dmma_tile<true, false>(t, p, batch, s);
+    else if(kcQ)
+        launch_dmma_tile<false, true>(t, p, batch, s);
+    else
+        launch_dmma_tile<false, false>(t, p, batch, s);
+}
+
+} // namespace rb200

@@ -21,8 +21,10 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <type_traits>
 
 #include "block_solve.cuh"
+#include "gemm_dmma.cuh"
 #include "gemm_tile.cuh"
 #include "handle.hpp"
 #include "trtri_block.cuh"
@@ -67,11 +69,21 @@ static void ensure_smem_attr(const void* fn, size_t bytes)
 }
 
 // ----------------------------------------------------------------------------------------
+// GEMM dispatch: FP64 on the DMMA multistage tiles, FP32 on the FFMA tiles.  full_m / full_n:
+// the tile must span all M rows / N columns (in-place application of an inverted block).
 template <typename T>
-static void launch_gemm(const GemmParams<T>& p0, int batch, cudaStream_t s)
+static void launch_gemm(const GemmParams<T>& p0, int batch, cudaStream_t s, int sms = 148,
+                        bool full_m = false, bool full_n = false)
 {
     if(p0.M <= 0 || p0.N <= 0)
         return;
+    if constexpr(std::is_same<T, double>::value)
+    {
+        launch_gemm_dmma(p0, batch, s, sms, full_m, full_n);
+        for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+            count_launch();
+        return;
+    }
     const size_t smem = gemm_smem_bytes<T>();
     ensure_smem_attr<T>((const void*)gemm_tile_kernel<T>, smem);
     for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
@@ -194,7 +206,7 @@ struct Recursive
         g.a_imm = T(1); g.a_user = first;
         g.b_imm = T(0); g.b_user = 0;
         g.ualpha = pr.alpha; g.zero_guard = 1;
-        launch_gemm<T>(g, pr.batch, pr.stream);
+        launch_gemm<T>(g, pr.batch, pr.stream, pr.sm_count, pr.side_left != 0, pr.side_left == 0);
     }
 
     // C := beta * C - opA(rows i0.., cols j0..) * X  (side L)   or
@@ -219,7 +231,7 @@ struct Recursive
         g.a_imm = T(-1); g.a_user = 0;
         g.b_imm = T(1); g.b_user = first;
         g.ualpha = pr.alpha; g.zero_guard = 1;
-        launch_gemm<T>(g, pr.batch, pr.stream);
+        launch_gemm<T>(g, pr.batch, pr.stream, pr.sm_count);
     }
 
     void solve(int b0, int b1, int first) const

@@ -1,0 +1,282 @@
+"""Continuous-batching TRSM server on one GPU.
+
+Requests (dtype, m, n, a resident-A key or a fresh A) arrive over time.  The server:
+
+* admits a request once its device memory (B, a fresh A, workspace share) fits in the HBM
+  budget, in arrival order; a request that cannot fit yet waits without blocking the loop;
+* keeps resident A matrices and their inverted 128 x 128 diagonal blocks (invA, the
+  rocblas_trsm_ex format) on the device and reuses them for every request on that A;
+* collects small systems (k <= 512) for up to `window_us` and solves each collection with
+  one variable-size batched launch (rocblas_b200_?trsm_vbatched); large systems go to
+  rocblas_?trsm_ex (resident invA) or rocblas_?trsm (fresh A) as soon as they are admitted;
+* runs launches on a pool of streams, each with its own rocblas handle, so work admitted
+  while other work is on the GPU overlaps with it;
+* completes a request when its launch's event has fired, frees its budget and records its
+  latency (completion - arrival, host clock).
+
+The kernels a request runs depend only on that request (its sizes and route), never on what
+else is in flight, so a result is bitwise the same alone and in the mix.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from . import (
+    DIAG, SIDE, TRANS, UPLO, Handle, check, datatype_f32_r, datatype_f64_r, lib, status_success,
+)
+from .workloads import condition_band_lower_torch
+
+SMALL_K = 512  # systems up to this order go through the variable-size batch
+TORCH_DT = {"d": torch.float64, "s": torch.float32}
+ESIZE = {"d": 8, "s": 4}
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float              # seconds after the start of the run
+    dtype: str                  # "d" or "s"
+    m: int
+    n: int
+    a_key: Optional[int]        # resident A, or None for a fresh A
+    seed: int
+    kband: int = 0              # condition band of a fresh A
+    # filled in by the server
+    B: Optional[torch.Tensor] = None
+    A: Optional[torch.Tensor] = None
+    admitted: float = -1.0
+    done: float = -1.0
+    bytes: int = 0
+
+
+@dataclass
+class Resident:
+    key: int
+    m: int
+    A: Dict[str, torch.Tensor] = field(default_factory=dict)      # per dtype, (m, m) col-major
+    invA: Dict[str, torch.Tensor] = field(default_factory=dict)   # per dtype, 128 * m elements
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+class TrsmServer:
+    def __init__(self, device="cuda", hbm_budget=120 << 30, n_streams=4, window_us=200.0,
+                 max_batch=4096):
+        self.dev = torch.device(device)
+        self.budget = int(hbm_budget)
+        self.used = 0
+        self.window = window_us * 1e-6
+        self.max_batch = max_batch
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
+        self.handles = []
+        for s in self.streams:
+            h = Handle()
+            h.set_stream(ctypes.c_void_p(s.cuda_stream))
+            self.handles.append(h)
+        self.rr = 0
+        self.residents: Dict[int, Resident] = {}
+        self.inflight = collections.deque()  # (event, [requests], keepalive)
+        self.one = {"d": ctypes.c_double(1.0), "s": ctypes.c_float(1.0)}
+
+    # ---- resident matrices ------------------------------------------------------------
+    def add_resident(self, key, m, kband, seed, dtypes=("d", "s")):
+        """Build a resident lower-triangular A (condition-band recipe) and its invA."""
+        At, _ = condition_band_lower_torch(m, 1, kband, seed, device=self.dev)
+        r = Resident(key, m)
+        for dt in dtypes:
+            A = At.to(TORCH_DT[dt]).contiguous()
+            inv = torch.zeros(128 * m, dtype=TORCH_DT[dt], device=self.dev)
+            self._build_invA(A, m, inv, dt)
+            r.A[dt], r.invA[dt] = A, inv
+            self.used += A.numel() * ESIZE[dt] + inv.numel() * ESIZE[dt]
+        torch.cuda.synchronize(self.dev)
+        self.residents[key] = r
+        return r
+
+    def _build_invA(self, A, m, inv, dt):
+        L = lib()
+        fn = L.rocblas_dtrtri_strided_batched if dt == "d" else L.rocblas_strtri_strided_batched
+        h = self.handles[0]
+        nfull, rem = divmod(m, 128)
+        es = ESIZE[dt]
+        if nfull:
+            check("trtri", fn(h.value, UPLO["L"], DIAG["N"], 128, _p(A), m, 128 * m + 128, _p(inv), 128,
+                              128 * 128, nfull))
+        if rem:
+            off_a = nfull * 128 * m + nfull * 128
+            check("trtri", fn(h.value, UPLO["L"], DIAG["N"], rem, ctypes.c_void_p(A.data_ptr() + off_a * es),
+                              m, 0, ctypes.c_void_p(inv.data_ptr() + nfull * 128 * 128 * es), 128, 0, 1))
+
+    # ---- per-request memory ------------------------------------------------------------
+    def _request_bytes(self, q: Request):
+        es = ESIZE[q.dtype]
+        b = q.m * q.n * es
+        if q.a_key is None:
+            b += q.m * q.m * es
+        if q.m > SMALL_K:
+            b += 128 * q.m * es  # workspace share (invA of a fresh A)
+        return b
+
+    def _materialise(self, q: Request, stream):
+        """Create B (and a fresh A) for an admitted request on `stream`."""
+        with torch.cuda.stream(stream):
+            g = torch.Generator(device=self.dev)
+            g.manual_seed(q.seed)
+            q.B = (torch.rand(q.n, q.m, generator=g, device=self.dev, dtype=torch.float64) * 2 - 1).to(
+                TORCH_DT[q.dtype])
+            if q.a_key is None:
+                At, _ = condition_band_lower_torch(q.m, 1, q.kband, q.seed, device=self.dev)
+                q.A = At.to(TORCH_DT[q.dtype])
+
+    # ---- launches ----------------------------------------------------------------------
+    def _next(self):
+        i = self.rr
+        self.rr = (self.rr + 1) % len(self.streams)
+        return self.streams[i], self.handles[i]
+
+    def _alpha(self, dt):
+        return ctypes.cast(ctypes.byref(self.one[dt]), ctypes.c_void_p)
+
+    def _launch_large(self, q: Request):
+        stream, h = self._next()
+        self._materialise(q, stream)
+        L = lib()
+        args = (h.value, SIDE["L"], UPLO["L"], TRANS["N"], DIAG["N"], q.m, q.n, self._alpha(q.dtype))
+        if q.a_key is not None:
+            r = self.residents[q.a_key]
+            st = L.rocblas_trsm_ex(*args, _p(r.A[q.dtype]), q.m, _p(q.B), q.m, _p(r.invA[q.dtype]),
+                                   128 * q.m, datatype_f64_r if q.dtype == "d" else datatype_f32_r)
+        else:
+            fn = L.rocblas_dtrsm if q.dtype == "d" else L.rocblas_strsm
+            st = fn(*args, _p(q.A), q.m, _p(q.B), q.m)
+        check("trsm (server)", st)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.inflight.append((ev, [q], None))
+
+    def _launch_small(self, group: List[Request], dt):
+        stream, h = self._next()
+        for q in group:
+            self._materialise(q, stream)
+        rec = np.zeros(len(group), dtype=np.dtype([
+            ("A", np.uint64), ("B", np.uint64), ("m", np.int32), ("n", np.int32), ("lda", np.int32),
+            ("ldb", np.int32), ("side", np.int32), ("uplo", np.int32), ("trans", np.int32),
+            ("diag", np.int32)]))
+        max_k = 1
+        for i, q in enumerate(group):
+            A = self.residents[q.a_key].A[dt] if q.a_key is not None else q.A
+            rec[i] = (A.data_ptr(), q.B.data_ptr(), q.m, q.n, q.m, q.m, SIDE["L"], UPLO["L"], TRANS["N"],
+                      DIAG["N"])
+            max_k = max(max_k, q.m)
+        host = torch.from_numpy(rec.view(np.uint8)).pin_memory()
+        with torch.cuda.stream(stream):
+            desc = host.to(self.dev, non_blocking=True)
+        fn = lib().rocblas_b200_dtrsm_vbatched if dt == "d" else lib().rocblas_b200_strsm_vbatched
+        check("vbatched (server)", fn(h.value, self._alpha(dt), _p(desc), len(group), max_k, None))
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.inflight.append((ev, list(group), (host, desc)))
+
+    # ---- the loop ----------------------------------------------------------------------
+    def run(self, requests: List[Request], keep_results=False):
+        """Serve `requests` (sorted by arrival).  Returns per-request latencies in seconds."""
+        reqs = sorted(requests, key=lambda q: q.arrival)
+        for q in reqs:
+            q.bytes = self._request_bytes(q)
+            if q.bytes > self.budget - self.used:
+                raise ValueError(f"request {q.rid} needs {q.bytes} B, more than the free budget")
+        pending = collections.deque()
+        small = {"d": collections.deque(), "s": collections.deque()}
+        i = 0
+        t0 = time.perf_counter()
+        done = 0
+        total = len(reqs)
+        while done < total:
+            now = time.perf_counter() - t0
+            # arrivals
+            while i < total and reqs[i].arrival <= now:
+                pending.append(reqs[i])
+                i += 1
+            # admission in arrival order, within the HBM budget
+            while pending and pending[0].bytes <= self.budget - self.used:
+                q = pending.popleft()
+                self.used += q.bytes
+                q.admitted = now
+                if q.m <= SMALL_K:
+                    small[q.dtype].append(q)
+                else:
+                    self._launch_large(q)
+            # small systems: launch a collection when the window closes or it is full
+            for dt, dq in small.items():
+                while dq and (len(dq) >= self.max_batch or now - dq[0].admitted >= self.window
+                              or (i >= total and not pending)):
+                    group = [dq.popleft() for _ in range(min(len(dq), self.max_batch))]
+                    self._launch_small(group, dt)
+            # completions
+            progressed = False
+            while self.inflight and self.inflight[0][0].query():
+                ev, group, _ = self.inflight.popleft()
+                tdone = time.perf_counter() - t0
+                for q in group:
+                    q.done = tdone
+                    self.used -= q.bytes
+                    if not keep_results:
+                        q.B = None
+                    q.A = None
+                    done += 1
+                progressed = True
+            # later events may complete before the head (different streams)
+            if not progressed and len(self.inflight) > 1:
+                rest = collections.deque()
+                tdone = None
+                for item in self.inflight:
+                    if item[0].query():
+                        tdone = tdone if tdone is not None else time.perf_counter() - t0
+                        for q in item[1]:
+                            q.done = tdone
+                            self.used -= q.bytes
+                            if not keep_results:
+                                q.B = None
+                            q.A = None
+                            done += 1
+                    else:
+                        rest.append(item)
+                self.inflight = rest
+        torch.cuda.synchronize(self.dev)
+        return np.array([q.done - q.arrival for q in reqs])
+
+    def close(self):
+        for h in self.handles:
+            h.close()
+
+
+def make_requests(n_requests, rate, seed, resident_sizes, reuse=0.6, fp64=0.7, m_range=(64, 8192),
+                  n_range=(1, 512)):
+    """Poisson arrivals at `rate` per second; m, n log-uniform; dtype 70/30; a fraction
+    `reuse` of the requests use one of the resident matrices (whose size sets m)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    out = []
+    keys = list(resident_sizes.keys())
+    for r in range(n_requests):
+        dt = "d" if rng.random() < fp64 else "s"
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        if rng.random() < reuse and keys:
+            key = keys[int(rng.integers(0, len(keys)))]
+            m = resident_sizes[key]
+            out.append(Request(r, float(t[r]), dt, m, n, key, int(rng.integers(1 << 30))))
+        else:
+            m = int(round(math.exp(rng.uniform(math.log(m_range[0]), math.log(m_range[1])))))
+            out.append(Request(r, float(t[r]), dt, m, n, None, int(rng.integers(1 << 30)),
+                               kband=int(rng.choice([0, 2, 4]))))
+    return out

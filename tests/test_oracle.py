@@ -97,3 +97,21 @@ def test_matrix_norm_1_is_cumulative():
     x = gold.copy(order="F")
     x[0, 0] = 2.0
     assert abs(oracle.matrix_norm_1(gold, x) - 1.0 / 202.0) < 1e-15
+
+
+def test_workload_generators_shapes_and_nan_triangle():
+    import torch
+
+    from rocblas_b200 import workloads
+
+    At, Bt = workloads.condition_band_lower_torch(64, 5, 4, seed=3, device="cpu")
+    A = At.numpy().T
+    assert A.shape == (64, 64) and Bt.shape == (5, 64)
+    assert np.isnan(A[np.triu_indices(64, 1)]).all()
+    assert not np.isnan(np.tril(A)).any()
+    d = np.diag(A)
+    assert d[0] > 1.0 and d[-1] < 1.1e-4 * 1.0001 * 1.1 and np.all(d > 0)
+    # off-diagonals of row i are scaled by d_i
+    assert np.all(np.abs(A[40, :40]) <= d[40] * 6.0 / np.sqrt(64))
+    assert float(Bt.abs().max()) <= 1.0
+    del torch

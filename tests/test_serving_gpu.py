@@ -1,0 +1,80 @@
+"""Serving loop: continuous batching under an HBM budget, resident A / invA reuse, and
+results that are bitwise the same alone and in the mix."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import oracle  # noqa: E402
+from rocblas_b200 import serving  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+RESIDENT = {0: 200, 1: 700, 2: 1300, 3: 64, 4: 513, 5: 96}
+
+
+def _server(budget=8 << 30, streams=3):
+    srv = serving.TrsmServer(hbm_budget=budget, n_streams=streams, window_us=100.0)
+    for key, m in RESIDENT.items():
+        srv.add_resident(key, m, kband=key % 3 * 2, seed=10 + key)
+    return srv
+
+
+def _requests(n, rate, seed):
+    reqs = serving.make_requests(n, rate, seed, RESIDENT, m_range=(16, 1500), n_range=(1, 96))
+    return reqs
+
+
+def test_serving_mix_equals_alone_and_is_correct():
+    srv = _server()
+    reqs = _requests(400, 20000.0, 3)
+    lat = srv.run(reqs, keep_results=True)
+    assert np.all(lat > 0)
+    mixed = {q.rid: q.B.clone() for q in reqs}
+    # correctness of a sample against the oracle
+    for q in reqs[:40]:
+        if q.a_key is not None:
+            A = srv.residents[q.a_key].A[q.dtype]
+        else:
+            from rocblas_b200.workloads import condition_band_lower_torch
+            At, _ = condition_band_lower_torch(q.m, 1, q.kband, q.seed, device="cuda")
+            A = At.to(serving.TORCH_DT[q.dtype])
+        g = torch.Generator(device="cuda")
+        g.manual_seed(q.seed)
+        B = (torch.rand(q.n, q.m, generator=g, device="cuda", dtype=torch.float64) * 2 - 1).to(
+            serving.TORCH_DT[q.dtype])
+        Ah = np.asfortranarray(A.cpu().numpy().T)
+        Bh = np.asfortranarray(B.cpu().numpy().T)
+        X = oracle.trsm("L", "L", "N", "N", 1.0, Ah, Bh)
+        got = mixed[q.rid].cpu().numpy().T
+        err = oracle.normwise_forward_error(got, X)
+        assert err < (1e-11 if q.dtype == "d" else 2e-3), (q.rid, q.m, q.n, q.dtype, err)
+    srv.close()
+    # the same requests one at a time through a fresh server: bitwise identical
+    alone_srv = _server()
+    for q in reqs[:60]:
+        q2 = serving.Request(q.rid, 0.0, q.dtype, q.m, q.n, q.a_key, q.seed, q.kband)
+        alone_srv.run([q2], keep_results=True)
+        assert torch.equal(q2.B, mixed[q.rid]), (q.rid, q.m, q.n, q.dtype)
+    alone_srv.close()
+
+
+def test_serving_admission_respects_budget():
+    srv = _server()
+    base = srv.used
+    reqs = _requests(200, 50000.0, 5)
+    biggest = max(srv._request_bytes(q) for q in reqs)
+    srv.budget = base + biggest + 1024  # room for about one request at a time
+    peak = [0]
+    orig = srv._launch_large
+
+    def spy(q):
+        peak[0] = max(peak[0], srv.used)
+        return orig(q)
+
+    srv._launch_large = spy
+    lat = srv.run(reqs)
+    assert np.all(lat > 0)
+    assert peak[0] <= srv.budget
+    assert srv.used == base
+    srv.close()
