@@ -46,6 +46,7 @@ constexpr int kOzTileA   = kOzBM * kOzBK; // bytes per slice tile
 constexpr int kOzTileB   = kOzBN * kOzBK;
 constexpr int kOzKMax    = 16384;         // longest exact int32 accumulation run (S <= 7)
 constexpr int kOzSmemBudget = 220 * 1024;
+constexpr int kOzExpNone    = -(1 << 30); // exponent of an all-zero row / column
 
 struct OzParams
 {
@@ -299,7 +300,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         {
             const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
             const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
-            const int    er   = gr < p.M ? p.exp_rows[gr] : 0;
+            int er = gr < p.M ? p.exp_rows[gr] : 0;
+            if(er == kOzExpNone)
+                er = 0;
             const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll 1
             for(int half = 0; half < kOzBN / 32; ++half)
@@ -325,7 +328,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         if(gc < p.N)
                         {
                             double* cp = p.C + gr + (int64_t)gc * p.ldc;
-                            const double pq = ldexp(h[j], er + p.exp_cols[gc] - 14);
+                            const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
+                            const double pq = ldexp(h[j], er + ec - 14);
                             double out;
                             if(zero)
                                 out = 0.0;
@@ -360,35 +364,47 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 }
 
 // ---- slicing ----------------------------------------------------------------------------
-// Operand element (o, k) lives at src[o * so + k * sk].  exps[o] = 1 + exponent of max_k |x|
-// (0 for an all-zero row), so that |x| * 2^-exps[o] < 1.
+// Operand element (o, k) lives at src[o * so + k * sk].  exps[o] = 1 + exponent of max_k |x|,
+// so that |x| * 2^-exps[o] < 1; rows that are all zero keep kOzExpNone and are sliced as 0.
+// exps must be preset to kOzExpNone; partial maxima over K chunks are merged with atomicMax
+// (the exponent is monotone in the maximum).
+constexpr int kOzExpChunk = 256;
+
+__device__ __forceinline__ void oz_merge_exp(int* exps, int o, double mx)
+{
+    if(mx > 0.0)
+        atomicMax(&exps[o], ilogb(mx) + 1);
+}
+
+// one warp per row o and K chunk; lanes stride over k (rows whose k is contiguous)
 __global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, int O, int K, int* exps)
 {
-    // one warp per row o; lanes stride over k
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int k0 = blockIdx.y * kOzExpChunk;
     if(w >= O)
         return;
     double mx = 0.0;
-    for(int k = lane; k < K; k += 32)
+    for(int k = k0 + lane; k < min(K, k0 + kOzExpChunk); k += 32)
         mx = fmax(mx, fabs(src[(int64_t)w * so + (int64_t)k * sk]));
 #pragma unroll
     for(int off = 16; off; off >>= 1)
         mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     if(lane == 0)
-        exps[w] = mx > 0.0 ? ilogb(mx) + 1 : 0;
+        oz_merge_exp(exps, w, mx);
 }
 
-// Same, one thread per row, for operands whose rows are adjacent in memory (so == 1):
-// consecutive threads read consecutive addresses.
+// one thread per row o and K chunk, for operands whose rows are adjacent in memory
+// (so == 1): consecutive threads read consecutive addresses
 __global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, int K, int* exps)
 {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = blockIdx.y * kOzExpChunk;
     if(o >= O)
         return;
     double mx = 0.0;
-    for(int k = 0; k < K; ++k)
+    for(int k = k0; k < min(K, k0 + kOzExpChunk); ++k)
         mx = fmax(mx, fabs(src[o + (int64_t)k * sk]));
-    exps[o] = mx > 0.0 ? ilogb(mx) + 1 : 0;
+    oz_merge_exp(exps, o, mx);
 }
 
 // Slices: dst[s][o][k] (int8, row pitch K_pad, slice stride O_pad * K_pad).  Rows o >= O and
@@ -417,7 +433,9 @@ __global__ void __launch_bounds__(256)
     const int o  = o0 + oo;
     if(o >= O_pad)
         return;
-    const int e = (o < O) ? exps[o] : 0;
+    int e = (o < O) ? exps[o] : 0;
+    if(e == kOzExpNone)
+        e = 0; // all-zero row: every slice is 0
     uint32_t  words[kOzMaxS][4];
 #pragma unroll
     for(int s = 0; s < kOzMaxS; ++s)

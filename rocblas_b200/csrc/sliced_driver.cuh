@@ -74,16 +74,27 @@ struct SlicedGemm
     int           zero_guard;
 };
 
+__global__ void oz_fill_kernel(int* p, int n, int v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n)
+        p[i] = v;
+}
+
 static void launch_exponents(SliceOperand X, int O, int K, int* exps, cudaStream_t s)
 {
+    oz_fill_kernel<<<(unsigned)ceil_div(O, 256), 256, 0, s>>>(exps, O, kOzExpNone);
+    count_launch();
+    const unsigned kchunks = (unsigned)std::max<int64_t>(1, ceil_div(K, kOzExpChunk));
     if(X.so == 1)
     {
-        oz_exponent_rows_kernel<<<(unsigned)ceil_div(O, 256), 256, 0, s>>>(X.ptr, X.sk, O, K, exps);
+        dim3 grid((unsigned)ceil_div(O, 128), kchunks);
+        oz_exponent_rows_kernel<<<grid, 128, 0, s>>>(X.ptr, X.sk, O, K, exps);
     }
     else
     {
-        const int64_t threads = (int64_t)O * 32;
-        oz_exponent_kernel<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps);
+        dim3 grid((unsigned)ceil_div((int64_t)O * 32, 256), kchunks);
+        oz_exponent_kernel<<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps);
     }
     count_launch();
 }
@@ -193,8 +204,17 @@ struct MixedRecursive : Recursive<double>
     int*  err_dev;
     bool  ok = true;
 
+    // Updates with a short inner dimension stay on the FP64 DMMA tiles: slicing costs about
+    // as much as a K <= kSlicedMinK product and the short GEMMs gain nothing on the slices.
+    static constexpr int kSlicedMinK = 1024;
+
     void update_sliced(int c_lo, int c_hi, int x_lo, int x_hi, int first)
     {
+        if(x_hi - x_lo < kSlicedMinK)
+        {
+            update(c_lo, c_hi, x_lo, x_hi, first);
+            return;
+        }
         const TrsmProblem<double>& q = pr;
         const double* A = q.A.base + q.A.offset;
         double*       B = q.B.base + q.B.offset;
