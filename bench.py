@@ -168,6 +168,147 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
+    """Config C3: `count` uneven systems (m log-uniform [16, 512], n uniform [1, 64], side and
+    uplo uniform, transA N, diag N) through rocblas_b200_?trsm_vbatched, FP64 and FP32; plus
+    the uniform strided batch (4096 x m=128, n=32) through rocblas_?trsm_strided_batched.
+    Solves/s and algorithmic GB/s against the HBM roofline."""
+    rng = np.random.default_rng(seed)
+    ms = np.exp(rng.uniform(np.log(16), np.log(512), size=count)).astype(np.int64)
+    ns = rng.integers(1, 65, size=count)
+    sides = rng.choice([141, 142], size=count)
+    uplos = rng.choice([121, 122], size=count)
+    ks = np.where(sides == 141, ms, ns)
+    order = np.argsort(ks, kind="stable")  # group equal k so that A is generated per k
+    out = {}
+    for dt, tdt, es in (("d", torch.float64, 8), ("s", torch.float32, 4)):
+        a_off = np.zeros(count, dtype=np.int64)
+        b_off = np.zeros(count, dtype=np.int64)
+        a_tot = b_tot = 0
+        for i in order:
+            a_off[i] = a_tot
+            a_tot += int(ks[i]) ** 2
+        for i in range(count):
+            b_off[i] = b_tot
+            b_tot += int(ms[i] * ns[i])
+        Aar = torch.empty(a_tot, dtype=tdt, device=dev)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        # per distinct k: off-diagonal U(-1,1)/k, diagonal 1 + U(0,1) (the drop-in recipe)
+        uk, first = np.unique(ks[order], return_index=True)
+        for j, k in enumerate(uk):
+            lo = first[j]
+            hi = first[j + 1] if j + 1 < len(uk) else count
+            cnt = hi - lo
+            base = int(a_off[order[lo]])
+            blk = (torch.rand(cnt, int(k), int(k), generator=g, device=dev, dtype=torch.float64) * 2 - 1) / k
+            idx = torch.arange(int(k), device=dev)
+            blk[:, idx, idx] = 1.0 + torch.rand(cnt, int(k), generator=g, device=dev, dtype=torch.float64)
+            Aar[base: base + cnt * int(k) * int(k)] = blk.reshape(-1).to(tdt)
+        B0 = (torch.rand(b_tot, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
+        Bar = B0.clone()
+        rec = np.zeros(count, dtype=np.dtype([
+            ("A", np.uint64), ("B", np.uint64), ("m", np.int32), ("n", np.int32), ("lda", np.int32),
+            ("ldb", np.int32), ("side", np.int32), ("uplo", np.int32), ("trans", np.int32),
+            ("diag", np.int32)]))
+        rec["A"] = Aar.data_ptr() + a_off * es
+        rec["B"] = Bar.data_ptr() + b_off * es
+        rec["m"], rec["n"], rec["lda"], rec["ldb"] = ms, ns, ks, ms
+        rec["side"], rec["uplo"], rec["trans"], rec["diag"] = sides, uplos, 111, 131
+        desc = torch.from_numpy(rec.view(np.uint8).copy()).to(dev)
+        alpha = ctypes.c_double(1.0) if dt == "d" else ctypes.c_float(1.0)
+        ap = ctypes.cast(ctypes.byref(alpha), ctypes.c_void_p)
+        fn = L.rocblas_b200_dtrsm_vbatched if dt == "d" else L.rocblas_b200_strsm_vbatched
+
+        def run():
+            st = fn(h.value, ap, ctypes.c_void_p(desc.data_ptr()), count, 512, None)
+            assert st == 0, st
+
+        for _ in range(3):
+            Bar.copy_(B0)
+            run()
+        torch.cuda.synchronize(dev)
+        times = []
+        for _ in range(10):
+            Bar.copy_(B0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        t = statistics.median(times) * 1e-3
+        flops = float(np.sum(ms * ns * ks))
+        nbytes = float(np.sum(es * (ks * (ks + 1) / 2 + 2 * ms * ns)))
+        out[f"vbatched_{dt}"] = {"systems": count, "solves_per_s": count / t, "ms": t * 1e3,
+                                 "tflops": flops / t / 1e12, "algorithmic_GBps": nbytes / t / 1e9,
+                                 "hbm_frac": nbytes / t / 1e9 / hbm_gbs}
+        del Aar, Bar, B0, desc
+        # uniform strided batch: 4096 x (m=128, n=32), side L lower
+        bc, m, n = 4096, 128, 32
+        As = torch.rand(bc, m, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        As /= m
+        idx = torch.arange(m, device=dev)
+        As[:, idx, idx] = 1.0 + torch.rand(bc, m, generator=g, device=dev, dtype=torch.float64)
+        As = As.to(tdt).contiguous()
+        Bs0 = (torch.rand(bc, n, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
+        Bs = Bs0.clone()
+        sfn = L.rocblas_dtrsm_strided_batched if dt == "d" else L.rocblas_strsm_strided_batched
+
+        def run_sb():
+            st = sfn(h.value, 141, 122, 111, 131, m, n, ap, ctypes.c_void_p(As.data_ptr()), m, m * m,
+                     ctypes.c_void_p(Bs.data_ptr()), m, m * n, bc)
+            assert st == 0, st
+
+        for _ in range(3):
+            Bs.copy_(Bs0)
+            run_sb()
+        torch.cuda.synchronize(dev)
+        times = []
+        for _ in range(10):
+            Bs.copy_(Bs0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run_sb()
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        t = statistics.median(times) * 1e-3
+        nbytes = bc * es * (m * (m + 1) / 2 + 2 * m * n)
+        out[f"strided_batched_{dt}"] = {"batch": bc, "m": m, "n": n, "solves_per_s": bc / t, "ms": t * 1e3,
+                                        "tflops": bc * m * m * n / t / 1e12,
+                                        "algorithmic_GBps": nbytes / t / 1e9,
+                                        "hbm_frac": nbytes / t / 1e9 / hbm_gbs}
+        del As, Bs, Bs0
+    return out
+
+
+def bench_serving(torch, dev, n_requests, rate, seed=7):
+    """Config C4: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
+    60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
+    budget.  Returns p50 / p99 latency and solves/s."""
+    from rocblas_b200 import serving
+
+    rng = np.random.default_rng(seed)
+    srv = serving.TrsmServer(device=dev, hbm_budget=120 << 30, n_streams=4, window_us=200.0)
+    sizes = {}
+    for key in range(256):
+        m = int(round(np.exp(rng.uniform(np.log(64), np.log(8192)))))
+        srv.add_resident(key, m, kband=int(rng.choice([0, 2, 4])), seed=1000 + key)
+        sizes[key] = m
+    reqs = serving.make_requests(n_requests, rate, seed, sizes)
+    flops = float(sum(q.m * q.m * q.n for q in reqs))
+    t0 = time.perf_counter()
+    lat = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    srv.close()
+    return {"requests": n_requests, "arrival_rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "solves_per_s": n_requests / wall,
+            "tflops": flops / wall / 1e12, "wall_s": wall, "resident_matrices": 256,
+            "fp64_fraction": float(np.mean([q.dtype == "d" for q in reqs])),
+            "reuse_fraction": float(np.mean([q.a_key is not None for q in reqs]))}
+
+
 def run_ours(args):
     import torch
 
@@ -358,6 +499,16 @@ def run_ours(args):
             "solve_ms_median": med_mixed,
         }
 
+    if rank == 0 and not args.no_extras:
+        hbm = 6455.3
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm = float(json.load(f)["hbm_gbs"])
+        except (OSError, KeyError, ValueError):
+            pass
+        extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
+        extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
+
     if rank == 0:
         line = {
             "metric": "dtrsm TFLOP/s (precision form, FP64 accuracy)", "value": value,
@@ -390,6 +541,9 @@ def main():
     ap.add_argument("--m", type=int, default=M, help="problem size (profiling runs use smaller)")
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--slices", type=int, default=7, help="slices of the precision form")
+    ap.add_argument("--serving-requests", type=int, default=200000)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and serving sections (profiling runs)")
     args = ap.parse_args()
     M, N = args.m, args.n
     FLOPS = float(M) * M * N

@@ -87,7 +87,8 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle    handle
 /* ---- precision form of dtrsm ----------------------------------------------------------------
  * Same contract as rocblas_dtrsm.  The blocked solve keeps the diagonal blocks in FP64
  * (inverted 128 x 128 blocks applied with FP64 tensor-core MMA) and runs every trailing
- * update on the integer-slice tensor-core GEMM above with `slices` slices (1..7).
+ * update with K >= sliced_min_k on the integer-slice tensor-core GEMM above with `slices`
+ * slices (1..8; 0 = the tuning table's mixed_slices); shorter updates stay on FP64 DMMA.
  * Workspace: the invA blocks plus the slices of the largest update (size query supported). */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
                                                        rocblas_side      side,
@@ -102,6 +103,16 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
                                                        double*           B,
                                                        rocblas_int       ldb,
                                                        rocblas_int       slices);
+
+/* ---- tuning table -----------------------------------------------------------------------
+ * Thresholds of the algorithm and tile choices (no reference counterpart beyond its
+ * compiled-in block-size tables).  Loaded once from $ROCBLAS_B200_TUNING or tuning.cfg next
+ * to the library ("key value" lines, written by rocblas_b200/autotune.py); these two calls
+ * read or change one entry in the running process.  Keys: block_max_k, block_always_k,
+ * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices.  Unknown keys or
+ * out-of-range values return rocblas_status_invalid_value. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_set_tuning(const char* key, rocblas_int value);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_get_tuning(const char* key, rocblas_int* value);
 
 /* Synchronises the handle's stream and returns (and clears) the error word that kernels
  * with bounded waits set when a wait ran out: 0 = none.  A nonzero value means results of

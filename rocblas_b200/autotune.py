@@ -1,0 +1,164 @@
+"""Autotuner for the thresholds in the library's tuning table (csrc/tuning.hpp).
+
+It times the candidate values of each entry on the GPU through the C ABI, keeps the fastest
+(or, for the slice count of the precision form, the cheapest count that meets the accuracy
+target in every condition band), and writes
+
+  rocblas_b200/tuning.cfg   "key value" lines, read by the library at first use
+  rocblas_b200/tuning.json  the measurements behind every choice
+
+Run:  python -m rocblas_b200.autotune [--quick]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import time
+
+import torch
+
+from . import HERE, Handle, lib
+from .workloads import condition_band_lower_torch
+
+
+
+def set_tuning(key, value):
+    st = lib().rocblas_b200_set_tuning(key.encode(), int(value))
+    if st != 0:
+        raise ValueError(f"tuning {key}={value} rejected ({st})")
+
+
+def get_tuning(key):
+    v = ctypes.c_int(0)
+    assert lib().rocblas_b200_get_tuning(key.encode(), ctypes.byref(v)) == 0
+    return v.value
+
+
+class Bench:
+    def __init__(self):
+        self.h = Handle()
+        self.stream = torch.cuda.current_stream()
+        self.h.set_stream(ctypes.c_void_p(self.stream.cuda_stream))
+        self.one = ctypes.c_double(1.0)
+        self.onef = ctypes.c_float(1.0)
+
+    def time(self, fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        return best
+
+    def dtrsm(self, At, Bt, m, n, mixed_slices=None):
+        L = lib()
+        a = ctypes.cast(ctypes.byref(self.one), ctypes.c_void_p)
+        args = (self.h.value, 141, 122, 111, 131, m, n, a, ctypes.c_void_p(At.data_ptr()), m,
+                ctypes.c_void_p(Bt.data_ptr()), m)
+        if mixed_slices is None:
+            st = L.rocblas_dtrsm(*args)
+        else:
+            st = L.rocblas_b200_dtrsm_mixed(*args, mixed_slices)
+        assert st == 0, st
+
+
+def tune(quick=False, out_dir=HERE):
+    torch.cuda.init()
+    b = Bench()
+    report = {"device": torch.cuda.get_device_name(), "when": time.strftime("%Y-%m-%dT%H:%M:%S"),
+              "entries": {}}
+    big = (8192, 2048) if quick else (16384, 4096)
+
+    # ---- dmma_big_tile_pct: plain dtrsm over a few shapes ------------------------------------
+    shapes = [big, (4096, 512), (2048, 2048), (8192, 256)]
+    cands = [100, 150, 200, 300, 400]
+    res = {}
+    data = {s: condition_band_lower_torch(s[0], s[1], 0, seed=5, device="cuda") for s in shapes}
+    for c in cands:
+        set_tuning("dmma_big_tile_pct", c)
+        tot = 0.0
+        for (m, n), (At, B0) in data.items():
+            Bt = B0.clone()
+            tot += b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n)))
+        res[c] = tot
+    best = min(res, key=res.get)
+    set_tuning("dmma_big_tile_pct", best)
+    report["entries"]["dmma_big_tile_pct"] = {"chosen": best, "ms_sum_over_shapes": res,
+                                              "shapes": shapes}
+
+    # ---- sliced_min_k: precision form at the large shape ----------------------------------
+    m, n = big
+    At, B0 = data[big]
+    res = {}
+    for c in [512, 1024, 2048, 4096]:
+        set_tuning("sliced_min_k", c)
+        Bt = B0.clone()
+        res[c] = b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=7)))
+    best = min(res, key=res.get)
+    set_tuning("sliced_min_k", best)
+    report["entries"]["sliced_min_k"] = {"chosen": best, "ms": res, "shape": big}
+    del data
+
+    # ---- block solver vs recursive for k in (128, 512] ------------------------------------
+    res = {}
+    for pct in [25, 50, 100, 200, 400]:
+        set_tuning("block_min_strips_pct", pct)
+        tot = 0.0
+        for (k, n) in [(192, 32), (256, 256), (384, 64), (512, 1024), (300, 4096)]:
+            At, B0 = condition_band_lower_torch(k, n, 0, seed=k, device="cuda")
+            Bt = B0.clone()
+            tot += b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, k, n)))
+        res[pct] = tot
+    best = min(res, key=res.get)
+    set_tuning("block_min_strips_pct", best)
+    report["entries"]["block_min_strips_pct"] = {"chosen": best, "ms_sum": res}
+
+    # ---- slice count of the precision form: cheapest count meeting 1e-12 in every band ----
+    # error measured against the plain FP64 solve of the same system (itself ~1e-15 from
+    # the exact solution on these bands)
+    mm, nn = (2048, 64) if quick else (4096, 64)
+    chosen = 8
+    errs = {}
+    for S in (5, 6, 7, 8):
+        worst = 0.0
+        for kb in (0, 2, 4, 6):
+            At, B0 = condition_band_lower_torch(mm, nn, kb, seed=40 + kb, device="cuda")
+            Xm, Xp = B0.clone(), B0.clone()
+            b.dtrsm(At, Xm, mm, nn, mixed_slices=S)
+            b.dtrsm(At, Xp, mm, nn)
+            torch.cuda.synchronize()
+            worst = max(worst, float(torch.linalg.norm(Xm - Xp) / torch.linalg.norm(Xp)))
+        errs[S] = worst
+    for S in (5, 6, 7, 8):
+        if errs[S] <= 1e-13:  # a 10x margin under the 1e-12 target at the tuning size
+            chosen = S
+            break
+    set_tuning("mixed_slices", chosen)
+    report["entries"]["mixed_slices"] = {"chosen": chosen, "worst_band_error": errs,
+                                         "target": "1e-12 with a 10x margin", "shape": [mm, nn]}
+
+    keys = ["block_max_k", "block_always_k", "block_min_strips_pct", "sliced_min_k",
+            "dmma_big_tile_pct", "mixed_slices"]
+    with open(os.path.join(out_dir, "tuning.cfg"), "w") as f:
+        f.write("# written by rocblas_b200/autotune.py on " + report["device"] + "\n")
+        for k in keys:
+            f.write(f"{k} {get_tuning(k)}\n")
+    with open(os.path.join(out_dir, "tuning.json"), "w") as f:
+        json.dump(report, f, indent=1, default=str)
+    b.h.close()
+    return report
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--out", default=HERE, help="directory for tuning.cfg / tuning.json")
+    a = ap.parse_args()
+    print(json.dumps(tune(a.quick, a.out), indent=1, default=str))

@@ -14,6 +14,7 @@
 // the 148 SMs.
 #pragma once
 #include "gemm_tile.cuh"
+#include "tuning.hpp"
 
 namespace rb200
 {
@@ -255,7 +256,7 @@ static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, b
             return DmmaTile::t64x128;
         return DmmaTile::t32x128;
     }
-    if(tiles(128, 128) >= 2 * sms)
+    if(tiles(128, 128) * 100 >= (int64_t)sms * tuning().dmma_big_tile_pct)
         return DmmaTile::t128x128;
     if(M >= N ? tiles(128, 64) >= sms : tiles(64, 128) >= sms)
         return M >= N ? DmmaTile::t128x64 : DmmaTile::t64x128;

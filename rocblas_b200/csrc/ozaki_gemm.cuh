@@ -19,11 +19,12 @@
 // bits, S = 8 gives 56 bits (beyond FP64 rounding of a K-term dot product).
 //
 // Kernel layout (one CTA per 128 x 64 output tile, 192 threads):
-//   warp 0   TMA producer: per 64-deep K step it loads all S slices of the P tile
-//            (128 x 64 int8, SWIZZLE_64B) and of the Q tile (64 x 64) into one stage;
+//   warp 0   TMA producer: per 32-deep K step it loads all S slices of the P tile
+//            (128 x 32 int8, SWIZZLE_32B) and of the Q tile (64 x 32) into one stage of a
+//            4..5-stage ring (a stage is S * 6 KB);
 //   warp 1   TMEM owner and MMA issuer: S <= 8 accumulators of 128 x 64 int32 (S*64 <= 512
 //            TMEM columns);
-//            per stage it issues the S(S+1)/2 slice-pair MMAs (M=128, N=64, K=32, twice);
+//            per stage it issues the S(S+1)/2 slice-pair MMAs (M=128, N=64, K=32);
 //   warps 2-5 epilogue: tcgen05.ld of the S accumulators (lanes = rows), Horner combination in
 //            FP64 registers, scaling by the row/column exponents, beta * C + alpha * (...).
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its
@@ -39,7 +40,7 @@ namespace rb200
 
 constexpr int kOzBM      = 128;
 constexpr int kOzBN      = 64;
-constexpr int kOzBK      = 64;   // int8 elements per K step (64-byte swizzled rows)
+constexpr int kOzBK      = 32;   // int8 elements per K step (32-byte swizzled rows, one MMA)
 constexpr int kOzMaxS    = 8;
 constexpr int kOzThreads = 192;
 constexpr int kOzTileA   = kOzBM * kOzBK; // bytes per slice tile
@@ -116,15 +117,15 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
                  : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major operand, 64-byte swizzle, 8-row groups 512 B apart.
+// UMMA shared-memory descriptor: K-major operand, 32-byte swizzle, 8-row groups 256 B apart.
 __device__ __forceinline__ uint64_t oz_smem_desc(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);       // start address
     d |= (uint64_t)1 << 16;                       // leading byte offset (unused, 16 B)
-    d |= (uint64_t)(512 >> 4) << 32;              // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)((8 * kOzBK) >> 4) << 32;      // stride byte offset: 8 rows x 32 B
     d |= (uint64_t)1 << 46;                       // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                       // SWIZZLE_64B
+    d |= (uint64_t)6 << 61;                       // SWIZZLE_32B
     return d;
 }
 

@@ -534,6 +534,8 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
         = trsm_arg_check<double>(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, 1);
     if(st != rocblas_status_continue)
         return st;
+    if(slices == 0)
+        slices = tuning().mixed_slices;
     if(slices < 1 || slices > kOzMaxS)
         return rocblas_status_invalid_value;
     if(h->pointer_mode == rocblas_pointer_mode_host && alpha && *alpha == 0.0)
@@ -1000,6 +1002,20 @@ try
 catch(...)
 {
     return exception_status();
+}
+
+rocblas_status rocblas_b200_set_tuning(const char* key, rocblas_int value)
+{
+    if(!key)
+        return rocblas_status_invalid_pointer;
+    return tuning_set(tuning(), key, value) ? rocblas_status_success : rocblas_status_invalid_value;
+}
+
+rocblas_status rocblas_b200_get_tuning(const char* key, rocblas_int* value)
+{
+    if(!key || !value)
+        return rocblas_status_invalid_pointer;
+    return tuning_get(tuning(), key, value) ? rocblas_status_success : rocblas_status_invalid_value;
 }
 
 rocblas_status rocblas_b200_get_device_error(rocblas_handle h, rocblas_int* code)

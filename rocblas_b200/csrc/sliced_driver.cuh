@@ -52,8 +52,9 @@ static inline size_t align256(size_t b)
 // Workspace for one sliced GEMM of M x N x K with S slices.
 static size_t sliced_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int S)
 {
-    const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), kOzKMax), kOzBK);
+    const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), kOzKMax), kOzSliceTile);
     const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kOzBN);
+    static_assert(kOzSliceTile % kOzBK == 0, "slice padding must cover whole K steps");
     return align256((size_t)S * Mp * Kp) + align256((size_t)S * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np);
 }
@@ -117,7 +118,7 @@ static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t 
     cuuint32_t box[2]     = {(cuuint32_t)kOzBK, (cuuint32_t)box_rows};
     cuuint32_t estr[2]    = {1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
            == CUDA_SUCCESS;
 }
@@ -139,7 +140,7 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
     for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kOzKMax)
     {
         const int64_t kc = std::min<int64_t>(kOzKMax, K - k0);
-        const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kOzBK);
+        const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kOzSliceTile);
         unsigned char* w = reinterpret_cast<unsigned char*>(ws);
         int8_t* sP = reinterpret_cast<int8_t*>(w);
         w += align256((size_t)S * Mp * Kp);
@@ -204,13 +205,11 @@ struct MixedRecursive : Recursive<double>
     int*  err_dev;
     bool  ok = true;
 
-    // Updates with a short inner dimension stay on the FP64 DMMA tiles: slicing costs about
-    // as much as a K <= kSlicedMinK product and the short GEMMs gain nothing on the slices.
-    static constexpr int kSlicedMinK = 1024;
-
+    // Updates with a short inner dimension stay on the FP64 DMMA tiles (K < sliced_min_k):
+    // slicing costs about as much as a short product and short GEMMs gain nothing from it.
     void update_sliced(int c_lo, int c_hi, int x_lo, int x_hi, int first)
     {
-        if(x_hi - x_lo < kSlicedMinK)
+        if(x_hi - x_lo < tuning().sliced_min_k)
         {
             update(c_lo, c_hi, x_lo, x_hi, first);
             return;

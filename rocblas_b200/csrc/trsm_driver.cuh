@@ -28,6 +28,7 @@
 #include "gemm_tile.cuh"
 #include "handle.hpp"
 #include "trtri_block.cuh"
+#include "tuning.hpp"
 
 namespace rb200
 {
@@ -287,14 +288,16 @@ enum class Algo
 template <typename T>
 static Algo choose_algo(const TrsmProblem<T>& pr)
 {
-    const int k = pr.k();
-    if(k > kBlockSolveMaxK)
+    const Tuning& t = tuning();
+    const int     k = pr.k();
+    if(k > std::min(t.block_max_k, kBlockSolveMaxK))
         return Algo::recursive;
-    if(k <= 128)
+    if(k <= t.block_always_k)
         return Algo::block;
     const int64_t ncols   = pr.side_left ? pr.n : pr.m;
     const int64_t nstrips = ceil_div(ncols, kBsW) * (int64_t)pr.batch;
-    return nstrips >= pr.sm_count ? Algo::block : Algo::recursive;
+    return nstrips * 100 >= (int64_t)pr.sm_count * t.block_min_strips_pct ? Algo::block
+                                                                         : Algo::recursive;
 }
 
 // Workspace bytes the call wants: invA for the recursive path unless supplied.

@@ -1,0 +1,110 @@
+// Tunable thresholds of the algorithm and tile choices.
+//
+// Defaults are compiled in.  At first use the table is overridden from a text file of
+// "key value" lines: $ROCBLAS_B200_TUNING if set, else tuning.cfg next to the shared library
+// (written by rocblas_b200/autotune.py, which times the candidates on the GPU).  The
+// extension functions rocblas_b200_set_tuning / rocblas_b200_get_tuning change or read an
+// entry at run time.  The reference's counterpart is its hand-made block-size tables
+// (library/src/blas3/rocblas_trsm_kernels.hpp:39-132) and selection heuristics (:1458-1610).
+#pragma once
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <dlfcn.h>
+#include <mutex>
+#include <string>
+
+namespace rb200
+{
+
+struct Tuning
+{
+    int block_max_k          = 512;  // largest k for the one-CTA block solver (<= 512)
+    int block_always_k       = 128;  // block solver at any parallelism up to this k
+    int block_min_strips_pct = 100;  // else block solver if strips * batch >= SMs * pct / 100
+    int sliced_min_k         = 1024; // precision form: sliced updates only for K >= this
+    int dmma_big_tile_pct    = 200;  // 128x128 DMMA tiles if tiles >= SMs * pct / 100
+    int mixed_slices         = 7;    // slices of the precision form when the caller passes 0
+};
+
+struct TuningEntry
+{
+    const char* key;
+    int Tuning::*field;
+    int         lo, hi;
+};
+
+static const TuningEntry kTuningEntries[] = {
+    {"block_max_k", &Tuning::block_max_k, 0, 512},
+    {"block_always_k", &Tuning::block_always_k, 0, 512},
+    {"block_min_strips_pct", &Tuning::block_min_strips_pct, 1, 100000},
+    {"sliced_min_k", &Tuning::sliced_min_k, 1, 1 << 30},
+    {"dmma_big_tile_pct", &Tuning::dmma_big_tile_pct, 1, 100000},
+    {"mixed_slices", &Tuning::mixed_slices, 1, 8},
+};
+
+inline bool tuning_set(Tuning& t, const char* key, int value)
+{
+    for(const auto& e : kTuningEntries)
+        if(!std::strcmp(e.key, key))
+        {
+            if(value < e.lo || value > e.hi)
+                return false;
+            t.*(e.field) = value;
+            return true;
+        }
+    return false;
+}
+
+inline bool tuning_get(const Tuning& t, const char* key, int* value)
+{
+    for(const auto& e : kTuningEntries)
+        if(!std::strcmp(e.key, key))
+        {
+            *value = t.*(e.field);
+            return true;
+        }
+    return false;
+}
+
+inline void tuning_load_file(Tuning& t, const char* path)
+{
+    FILE* f = std::fopen(path, "r");
+    if(!f)
+        return;
+    char line[256];
+    while(std::fgets(line, sizeof(line), f))
+    {
+        char key[128];
+        int  v;
+        if(line[0] == '#')
+            continue;
+        if(std::sscanf(line, "%127s %d", key, &v) == 2)
+            tuning_set(t, key, v);
+    }
+    std::fclose(f);
+}
+
+inline Tuning& tuning()
+{
+    static Tuning         t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if(const char* env = std::getenv("ROCBLAS_B200_TUNING"))
+        {
+            tuning_load_file(t, env);
+            return;
+        }
+        Dl_info info;
+        if(dladdr(reinterpret_cast<void*>(&tuning_load_file), &info) && info.dli_fname)
+        {
+            std::string p(info.dli_fname);
+            const size_t slash = p.rfind('/');
+            p = (slash == std::string::npos ? std::string(".") : p.substr(0, slash)) + "/tuning.cfg";
+            tuning_load_file(t, p.c_str());
+        }
+    });
+    return t;
+}
+
+} // namespace rb200
