@@ -9,9 +9,10 @@
 // the fragment reads free of bank conflicts:
 //   operand rows contiguous in memory (kc = false): smem [k][o], pitch O + 4 doubles;
 //   operand k contiguous in memory   (kc = true) : smem [o][k], pitch 16 + 4 doubles.
-// Tile shapes range from 128 x 128 (8 warps, warp tile 64 x 32) down to 128 x 32 / 32 x 128
-// (4 warps, warp tile 32 x 32) so that small trailing updates and the invA leaves still fill
-// the 148 SMs.
+// Every warp owns a 32 x 32 block of C computed with mma.sync m16n8k8 .f64 (2 x 4 MMAs per
+// 8-deep k step).  Tile shapes range from 128 x 128 (16 warps) over 64 x 128 / 128 x 64
+// (8 warps, two CTAs per SM) down to 128 x 32 / 32 x 128 (4 warps), so that small trailing
+// updates and the invA leaves still fill the 148 SMs.
 #pragma once
 #include "gemm_tile.cuh"
 #include "tuning.hpp"
@@ -35,6 +36,17 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait()
 {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// mma.sync m16n8k8 .f64 (sm_90+ shape; 1024 FMAs per instruction).  Fragments, with
+// g = lane / 4 and t = lane % 4: A (16x8): a0 (g, t), a1 (g+8, t), a2 (g, t+4), a3 (g+8, t+4);
+// B (8x8): b0 (t, g), b1 (t+4, g); C (16x8): c0 (g, 2t), c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1).
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2])
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+                 "{%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
@@ -84,12 +96,13 @@ __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, in
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
-__global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads)
+__global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads,
+                                  DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads <= 256 ? 2 : 1)
     gemm_dmma_kernel(GemmParams<double> p)
 {
     using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>;
     constexpr int NT = Cfg::kThreads;
-    constexpr int TM = WM / 8, TN = WN / 8;
+    constexpr int TM = WM / 16, TN = WN / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* smem = reinterpret_cast<double*>(smem_raw);
 
@@ -106,13 +119,16 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
     const double a  = p.a_user ? ua : p.a_imm;
     const double b  = p.b_user ? ua : p.b_imm;
 
-    double acc[TM][TN][2];
+    double acc[TM][TN][4];
 #pragma unroll
     for(int i = 0; i < TM; ++i)
 #pragma unroll
         for(int j = 0; j < TN; ++j)
-            acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+            for(int e = 0; e < 4; ++e)
+                acc[i][j][e] = 0.0;
 
+    const int g = lane >> 2, t = lane & 3;
     if(!zero_out)
     {
         const double* P  = p.P.get(batch);
@@ -124,6 +140,12 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
             dmma_load_stage<BM, NT, KCP>(sA, P, p.ldp, p.triP, m0, kt * kDBK, p.M, p.K, tid);
             dmma_load_stage<BN, NT, KCQ>(sB, Q, p.ldq, p.triQ, n0, kt * kDBK, p.N, p.K, tid);
         };
+        auto ldA = [&](const double* sA, int m, int k) {
+            return KCP ? sA[m * Cfg::kPitchA + k] : sA[k * Cfg::kPitchA + m];
+        };
+        auto ldB = [&](const double* sB, int n, int k) {
+            return KCQ ? sB[n * Cfg::kPitchB + k] : sB[k * Cfg::kPitchB + n];
+        };
 #pragma unroll
         for(int s = 0; s < STAGES - 1; ++s)
         {
@@ -131,7 +153,6 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
                 load(s, s);
             cp_async_commit();
         }
-        const int lr = lane >> 2, lk = lane & 3;
         for(int kt = 0; kt < nk; ++kt)
         {
             cp_async_wait<STAGES - 2>();
@@ -139,27 +160,31 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
             const double* sA = smem + (kt % STAGES) * Cfg::kStage;
             const double* sB = sA + Cfg::kStageA;
 #pragma unroll
-            for(int ks = 0; ks < kDBK / 4; ++ks)
+            for(int ks = 0; ks < kDBK / 8; ++ks)
             {
-                const int k = ks * 4 + lk;
-                double    fa[TM], fb[TN];
+                const int k = ks * 8 + t;
+                double    fa[TM][4], fb[TN][2];
 #pragma unroll
                 for(int i = 0; i < TM; ++i)
                 {
-                    const int o = wm * WM + i * 8 + lr;
-                    fa[i]       = KCP ? sA[o * Cfg::kPitchA + k] : sA[k * Cfg::kPitchA + o];
+                    const int m = wm * WM + i * 16 + g;
+                    fa[i][0] = ldA(sA, m, k);
+                    fa[i][1] = ldA(sA, m + 8, k);
+                    fa[i][2] = ldA(sA, m, k + 4);
+                    fa[i][3] = ldA(sA, m + 8, k + 4);
                 }
 #pragma unroll
                 for(int j = 0; j < TN; ++j)
                 {
-                    const int o = wn * WN + j * 8 + lr;
-                    fb[j]       = KCQ ? sB[o * Cfg::kPitchB + k] : sB[k * Cfg::kPitchB + o];
+                    const int n = wn * WN + j * 8 + g;
+                    fb[j][0] = ldB(sB, n, k);
+                    fb[j][1] = ldB(sB, n, k + 4);
                 }
 #pragma unroll
                 for(int i = 0; i < TM; ++i)
 #pragma unroll
                     for(int j = 0; j < TN; ++j)
-                        dmma_8x8x4(acc[i][j], fa[i], fb[j]);
+                        dmma_16x8x8(acc[i][j], fa[i], fb[j]);
             }
             const int nxt = kt + STAGES - 1;
             if(nxt < nk)
@@ -175,10 +200,10 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
 #pragma unroll
         for(int j = 0; j < TN; ++j)
 #pragma unroll
-            for(int e = 0; e < 2; ++e)
+            for(int e = 0; e < 4; ++e)
             {
-                const int gr = m0 + wm * WM + i * 8 + (lane >> 2);
-                const int gc = n0 + wn * WN + j * 8 + (lane & 3) * 2 + e;
+                const int gr = m0 + wm * WM + i * 16 + g + (e >> 1) * 8;
+                const int gc = n0 + wn * WN + j * 8 + 2 * t + (e & 1);
                 if(gr < p.M && gc < p.N)
                 {
                     double* cp = C + gr + (int64_t)gc * ldc;
@@ -226,7 +251,7 @@ static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch,
 {
     switch(t)
     {
-    case DmmaTile::t128x128: launch_dmma_cfg<128, 128, 64, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t128x128: launch_dmma_cfg<128, 128, 32, 32, 3, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t128x64:  launch_dmma_cfg<128, 64, 32, 32, 3, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t64x128:  launch_dmma_cfg<64, 128, 32, 32, 3, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t64x64:   launch_dmma_cfg<64, 64, 32, 32, 4, KCP, KCQ>(p, batch, s); break;

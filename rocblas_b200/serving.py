@@ -85,8 +85,16 @@ class TrsmServer:
             self.handles.append(h)
         self.rr = 0
         self.residents: Dict[int, Resident] = {}
-        self.inflight = collections.deque()  # (event, [requests], keepalive)
+        # per stream, launches complete in order: (event, [requests], keepalive)
+        self.inflight = [collections.deque() for _ in self.streams]
+        self.max_inflight = 8 * n_streams  # launch slots; admission waits when they are full
         self.one = {"d": ctypes.c_double(1.0), "s": ctypes.c_float(1.0)}
+        # request payloads are cut from a fixed pool of U(-1,1) values (a stand-in for data that
+        # arrives with the request): a request's B and fresh A depend only on its seed
+        g = torch.Generator(device=self.dev)
+        g.manual_seed(12345)
+        self.pool = {"d": torch.rand(1 << 26, generator=g, device=self.dev, dtype=torch.float64) * 2 - 1}
+        self.pool["s"] = self.pool["d"].to(torch.float32)
 
     # ---- resident matrices ------------------------------------------------------------
     def add_resident(self, key, m, kband, seed, dtypes=("d", "s")):
@@ -127,22 +135,31 @@ class TrsmServer:
             b += 128 * q.m * es  # workspace share (invA of a fresh A)
         return b
 
+    def _cut(self, dt, count, seed):
+        pool = self.pool[dt]
+        off = (seed * 2654435761) % (pool.numel() - count)
+        return pool[off: off + count]
+
     def _materialise(self, q: Request, stream):
-        """Create B (and a fresh A) for an admitted request on `stream`."""
+        """Create B (and a fresh A) for an admitted request on `stream`: B is cut from the
+        pool; a fresh lower-triangular A has off-diagonals U(-1,1)/m and diagonal 1.5 +
+        U(-1,1)/m (the drop-in recipe's conditioning)."""
         with torch.cuda.stream(stream):
-            g = torch.Generator(device=self.dev)
-            g.manual_seed(q.seed)
-            q.B = (torch.rand(q.n, q.m, generator=g, device=self.dev, dtype=torch.float64) * 2 - 1).to(
-                TORCH_DT[q.dtype])
+            q.B = self._cut(q.dtype, q.m * q.n, q.seed).clone()
             if q.a_key is None:
-                At, _ = condition_band_lower_torch(q.m, 1, q.kband, q.seed, device=self.dev)
-                q.A = At.to(TORCH_DT[q.dtype])
+                A = self._cut(q.dtype, q.m * q.m, q.seed + 1) * (1.0 / q.m)
+                A.view(q.m, q.m).diagonal().add_(1.5)
+                q.A = A
 
     # ---- launches ----------------------------------------------------------------------
     def _next(self):
         i = self.rr
         self.rr = (self.rr + 1) % len(self.streams)
+        self._cur = i
         return self.streams[i], self.handles[i]
+
+    def _n_inflight(self):
+        return sum(len(d) for d in self.inflight)
 
     def _alpha(self, dt):
         return ctypes.cast(ctypes.byref(self.one[dt]), ctypes.c_void_p)
@@ -162,7 +179,7 @@ class TrsmServer:
         check("trsm (server)", st)
         ev = torch.cuda.Event()
         ev.record(stream)
-        self.inflight.append((ev, [q], None))
+        self.inflight[self._cur].append((ev, [q], None))
 
     def _launch_small(self, group: List[Request], dt):
         stream, h = self._next()
@@ -185,7 +202,7 @@ class TrsmServer:
         check("vbatched (server)", fn(h.value, self._alpha(dt), _p(desc), len(group), max_k, None))
         ev = torch.cuda.Event()
         ev.record(stream)
-        self.inflight.append((ev, list(group), (host, desc)))
+        self.inflight[self._cur].append((ev, list(group), (host, desc)))
 
     # ---- the loop ----------------------------------------------------------------------
     def run(self, requests: List[Request], keep_results=False):
@@ -207,8 +224,9 @@ class TrsmServer:
             while i < total and reqs[i].arrival <= now:
                 pending.append(reqs[i])
                 i += 1
-            # admission in arrival order, within the HBM budget
-            while pending and pending[0].bytes <= self.budget - self.used:
+            # admission in arrival order, within the HBM budget and the launch slots
+            while (pending and pending[0].bytes <= self.budget - self.used
+                   and self._n_inflight() < self.max_inflight):
                 q = pending.popleft()
                 self.used += q.bytes
                 q.admitted = now
@@ -222,36 +240,18 @@ class TrsmServer:
                               or (i >= total and not pending)):
                     group = [dq.popleft() for _ in range(min(len(dq), self.max_batch))]
                     self._launch_small(group, dt)
-            # completions
-            progressed = False
-            while self.inflight and self.inflight[0][0].query():
-                ev, group, _ = self.inflight.popleft()
-                tdone = time.perf_counter() - t0
-                for q in group:
-                    q.done = tdone
-                    self.used -= q.bytes
-                    if not keep_results:
-                        q.B = None
-                    q.A = None
-                    done += 1
-                progressed = True
-            # later events may complete before the head (different streams)
-            if not progressed and len(self.inflight) > 1:
-                rest = collections.deque()
-                tdone = None
-                for item in self.inflight:
-                    if item[0].query():
-                        tdone = tdone if tdone is not None else time.perf_counter() - t0
-                        for q in item[1]:
-                            q.done = tdone
-                            self.used -= q.bytes
-                            if not keep_results:
-                                q.B = None
-                            q.A = None
-                            done += 1
-                    else:
-                        rest.append(item)
-                self.inflight = rest
+            # completions: each stream's launches finish in order, so only heads are polled
+            for dq in self.inflight:
+                while dq and dq[0][0].query():
+                    ev, group, _ = dq.popleft()
+                    tdone = time.perf_counter() - t0
+                    for q in group:
+                        q.done = tdone
+                        self.used -= q.bytes
+                        if not keep_results:
+                            q.B = None
+                        q.A = None
+                        done += 1
         torch.cuda.synchronize(self.dev)
         return np.array([q.done - q.arrival for q in reqs])
 

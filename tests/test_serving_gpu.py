@@ -34,22 +34,19 @@ def test_serving_mix_equals_alone_and_is_correct():
     # correctness of a sample against the oracle
     for q in reqs[:40]:
         if q.a_key is not None:
-            A = srv.residents[q.a_key].A[q.dtype]
+            A = srv.residents[q.a_key].A[q.dtype].reshape(q.m, q.m)
         else:
-            from rocblas_b200.workloads import condition_band_lower_torch
-            At, _ = condition_band_lower_torch(q.m, 1, q.kband, q.seed, device="cuda")
-            A = At.to(serving.TORCH_DT[q.dtype])
-        g = torch.Generator(device="cuda")
-        g.manual_seed(q.seed)
-        B = (torch.rand(q.n, q.m, generator=g, device="cuda", dtype=torch.float64) * 2 - 1).to(
-            serving.TORCH_DT[q.dtype])
-        Ah = np.asfortranarray(A.cpu().numpy().T)
+            A = (srv._cut(q.dtype, q.m * q.m, q.seed + 1) * (1.0 / q.m)).reshape(q.m, q.m)
+            A.diagonal().add_(1.5)
+        B = srv._cut(q.dtype, q.m * q.n, q.seed).reshape(q.n, q.m)
+        Ah = np.asfortranarray(np.tril(np.nan_to_num(A.cpu().numpy().T)))
         Bh = np.asfortranarray(B.cpu().numpy().T)
         X = oracle.trsm("L", "L", "N", "N", 1.0, Ah, Bh)
         got = mixed[q.rid].cpu().numpy().T
         err = oracle.normwise_forward_error(got, X)
         assert err < (1e-11 if q.dtype == "d" else 2e-3), (q.rid, q.m, q.n, q.dtype, err)
     srv.close()
+    del srv
     # the same requests one at a time through a fresh server: bitwise identical
     alone_srv = _server()
     for q in reqs[:60]:
