@@ -59,6 +59,27 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle        
                                                           rocblas_int                      max_k,
                                                           rocblas_int* invalid_count);
 
+/* ---- the variable-size batch without any allocation ---------------------------------------
+ * No counterpart in the reference.  Same contract and results as
+ * rocblas_b200_dtrsm_vbatched, for callers that must not allocate device memory: code that
+ * records the call into a CUDA graph by stream capture (cudaMalloc is not allowed while a
+ * capture is active), applications that hand all device memory to their own pool and forbid
+ * libraries to allocate, and loops that cannot afford the device-wide synchronisation of a
+ * cudaFree when the handle's workspace would grow.  Its scratch (queue state and prefix sums)
+ * is a fixed device array inside the library, sized for at most 65536 systems (256 KiB +
+ * 16 B, held on every GPU that loads the library until exit); count > 65536 returns
+ * rocblas_status_invalid_size.  It calls no cudaMalloc or cudaFree and takes nothing from the
+ * handle's workspace.  The first call on a device looks up the array's device address (once
+ * per device) and should be made before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (for example on two streams, or two handles at once) race and
+ * must be ordered by the caller. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_vbatched_noalloc(rocblas_handle                   handle,
+                                                                  const double*                    alpha,
+                                                                  const rocblas_b200_trsm_problem* problems,
+                                                                  rocblas_int                      count,
+                                                                  rocblas_int                      max_k,
+                                                                  rocblas_int* invalid_count);
+
 /* ---- FP64 GEMM from integer slices on the tensor cores ------------------------------------
  * C := alpha op(A) op(B) + beta C in FP64 (column-major), computed as exact int8 x int8 ->
  * int32 products of `slices` 7-bit slices of every row of op(A) and every column of op(B)

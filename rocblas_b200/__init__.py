@@ -139,6 +139,7 @@ SIGNATURES = {
     "rocblas_b200_kernel_launch_count": (ctypes.c_uint64, []),
     "rocblas_b200_dtrsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
     "rocblas_b200_strsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
+    "rocblas_b200_dtrsm_vbatched_noalloc": (_i, [_H, _p, _p, _i, _i, _p]),
     "rocblas_b200_dgemm_sliced": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_get_device_error": (_i, [_H, ctypes.POINTER(_i)]),

@@ -460,6 +460,99 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
     return launch_status();
 }
 
+// ---- variable-size batch without any allocation ------------------------------------------
+// Scratch of rocblas_b200_dtrsm_vbatched_noalloc: the queue state and the prefix sums of work
+// items for at most kVbNoAllocMaxCount descriptors, in a fixed device array that every GPU
+// loading the library holds until exit (256 KiB + 16 B).  Host code reaches it only through
+// the address cudaGetSymbolAddress returns for the current device.
+constexpr int kVbNoAllocMaxCount = 65536;
+static __device__ __align__(256) unsigned char
+    g_vb_noalloc_scratch[sizeof(VbState) + sizeof(int) * (kVbNoAllocMaxCount + 1)];
+
+constexpr int kVbNoAllocMaxDevices = 64;
+std::mutex    g_vb_noalloc_mutex;
+void*         g_vb_noalloc_addr[kVbNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `device` (which must be current); looked up once per
+// device.  nullptr if the lookup fails.
+void* vb_noalloc_scratch(int device)
+{
+    if(device < 0 || device >= kVbNoAllocMaxDevices)
+        return nullptr;
+    std::lock_guard<std::mutex> lock(g_vb_noalloc_mutex);
+    if(!g_vb_noalloc_addr[device])
+    {
+        void* ptr = nullptr;
+        if(cudaGetSymbolAddress(&ptr, g_vb_noalloc_scratch) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_vb_noalloc_addr[device] = ptr;
+    }
+    return g_vb_noalloc_addr[device];
+}
+
+rocblas_status trsm_vbatched_noalloc_impl(rocblas_handle h, const double* alpha,
+                                          const rocblas_b200_trsm_problem* problems, int count,
+                                          int max_k, rocblas_int* invalid_count)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(count < 0 || max_k < 0 || max_k > kBlockSolveMaxK)
+        return rocblas_status_invalid_size;
+    if(count > kVbNoAllocMaxCount)
+    {
+        fprintf(stderr,
+                "rocblas_b200_dtrsm_vbatched_noalloc: count %d exceeds the fixed scratch limit of "
+                "%d systems; use rocblas_b200_dtrsm_vbatched\n",
+                count, kVbNoAllocMaxCount);
+        return rocblas_status_invalid_size;
+    }
+    if(h->size_query)
+        return rocblas_status_size_unchanged; // needs no workspace
+    if(!count)
+        return rocblas_status_success;
+    if(!alpha || !problems)
+        return rocblas_status_invalid_pointer;
+    rocblas_status st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    void* scratch = vb_noalloc_scratch(h->device);
+    if(!scratch)
+        return rocblas_status_internal_error;
+    VbState* state   = reinterpret_cast<VbState*>(scratch);
+    int*     offsets = reinterpret_cast<int*>(state + 1);
+    // the queue head and the invalid count must start at zero; the previous call left its values
+    cudaMemsetAsync(state, 0, sizeof(VbState), h->stream);
+    const VbProblem* probs = reinterpret_cast<const VbProblem*>(problems);
+    vb_prepass_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, offsets, state);
+    count_launch();
+    VbParams<double> p;
+    p.probs   = probs;
+    p.count   = count;
+    p.offsets = offsets;
+    p.st      = state;
+    if(h->pointer_mode == rocblas_pointer_mode_host)
+        p.alpha.val = *alpha;
+    else
+        p.alpha.ptr = alpha;
+    const size_t smem = block_solve_smem_bytes<double>(std::max(max_k, 1));
+    cudaFuncSetAttribute((const void*)vb_persistent_kernel<double>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<double>, kBsThreads, smem);
+    per_sm = std::max(per_sm, 1);
+    vb_persistent_kernel<double><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
+    count_launch();
+    if(invalid_count)
+    {
+        vb_copy_invalid_kernel<double><<<1, 1, 0, h->stream>>>(state, invalid_count);
+        count_launch();
+    }
+    return launch_status();
+}
+
 int* ensure_err(rocblas_handle h)
 {
     if(!h->err_dev)
@@ -955,6 +1048,19 @@ rocblas_status rocblas_b200_dtrsm_vbatched(rocblas_handle h, const double* alpha
 try
 {
     return trsm_vbatched_impl<double>(h, alpha, problems, count, max_k, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dtrsm_vbatched_noalloc(rocblas_handle h, const double* alpha,
+                                                   const rocblas_b200_trsm_problem* problems,
+                                                   rocblas_int count, rocblas_int max_k,
+                                                   rocblas_int* invalid_count)
+try
+{
+    return trsm_vbatched_noalloc_impl(h, alpha, problems, count, max_k, invalid_count);
 }
 catch(...)
 {
