@@ -105,6 +105,26 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle    handle
                                                         rocblas_int       ldc,
                                                         rocblas_int       slices);
 
+/* ---- FP64 GEMM on the DMMA tiles of the trsm updates -----------------------------------------
+ * C := alpha op(A) op(B) + beta C (column-major FP64), the engine of rocblas_dtrsm's trailing
+ * updates (mma.sync m16n8k8 .f64 tiles fed by cp.async), exposed as a GEMM.  Same argument
+ * meaning as rocblas_dgemm (rocblas-functions.h), host pointer mode only (device mode returns
+ * rocblas_status_not_implemented); needs no workspace. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm(rocblas_handle    handle,
+                                                 rocblas_operation transA,
+                                                 rocblas_operation transB,
+                                                 rocblas_int       m,
+                                                 rocblas_int       n,
+                                                 rocblas_int       k,
+                                                 const double*     alpha,
+                                                 const double*     A,
+                                                 rocblas_int       lda,
+                                                 const double*     B,
+                                                 rocblas_int       ldb,
+                                                 const double*     beta,
+                                                 double*           C,
+                                                 rocblas_int       ldc);
+
 /* ---- precision form of dtrsm ----------------------------------------------------------------
  * Same contract as rocblas_dtrsm.  The blocked solve keeps the diagonal blocks in FP64
  * (inverted 128 x 128 blocks applied with FP64 tensor-core MMA) and runs every trailing
@@ -130,7 +150,8 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  * compiled-in block-size tables).  Loaded once from $ROCBLAS_B200_TUNING or tuning.cfg next
  * to the library ("key value" lines, written by rocblas_b200/autotune.py); these two calls
  * read or change one entry in the running process.  Keys: block_max_k, block_always_k,
- * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices.  Unknown keys or
+ * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices, dmma_force_tile,
+ * dmma_big_bk.  Unknown keys or
  * out-of-range values return rocblas_status_invalid_value. */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_set_tuning(const char* key, rocblas_int value);
 ROCBLAS_EXPORT rocblas_status rocblas_b200_get_tuning(const char* key, rocblas_int* value);

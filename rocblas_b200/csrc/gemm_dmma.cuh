@@ -49,28 +49,29 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
                  : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK = kDBK>
 struct DmmaCfg
 {
+    static constexpr int kBK      = BK;
     static constexpr int kWarpsM  = BM / WM;
     static constexpr int kWarpsN  = BN / WN;
     static constexpr int kThreads = kWarpsM * kWarpsN * 32;
-    static constexpr int kPitchA  = KCP ? (kDBK + 4) : (BM + 4);
-    static constexpr int kPitchB  = KCQ ? (kDBK + 4) : (BN + 4);
-    static constexpr int kStageA  = KCP ? BM * kPitchA : kDBK * kPitchA; // doubles
-    static constexpr int kStageB  = KCQ ? BN * kPitchB : kDBK * kPitchB;
+    static constexpr int kPitchA  = KCP ? (BK + 4) : (BM + 4);
+    static constexpr int kPitchB  = KCQ ? (BK + 4) : (BN + 4);
+    static constexpr int kStageA  = KCP ? BM * kPitchA : BK * kPitchA; // doubles
+    static constexpr int kStageB  = KCQ ? BN * kPitchB : BK * kPitchB;
     static constexpr int kStage   = kStageA + kStageB;
     static constexpr size_t kSmem = (size_t)STAGES * kStage * sizeof(double);
 };
 
 // Loads one BK-deep stage of an operand tile of `O` rows (o0..o0+O-1 of the logical operand)
 // with cp.async.  Logical (o, k) is stored at ptr[r + c*ld], (r, c) = kc ? (k, o) : (o, k).
-template <int O, int NT, bool KC>
+template <int O, int NT, bool KC, int BK>
 __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, int64_t ld, int tri,
                                                 int o0, int k0, int Olim, int Klim, int tid)
 {
-    constexpr int PER = O * kDBK / NT;
-    static_assert(PER * NT == O * kDBK, "tile / thread mismatch");
+    constexpr int PER = O * BK / NT;
+    static_assert(PER * NT == O * BK, "tile / thread mismatch");
 #pragma unroll
     for(int i = 0; i < PER; ++i)
     {
@@ -78,8 +79,8 @@ __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, in
         int       o, kk;
         if(KC)
         {
-            kk = e % kDBK;
-            o  = e / kDBK;
+            kk = e % BK;
+            o  = e / BK;
         }
         else
         {
@@ -90,17 +91,17 @@ __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, in
         const int64_t r = KC ? gk : go, c = KC ? go : gk;
         const bool    valid = go < Olim && gk < Klim && tri_keep(tri, r, c);
         const double* src   = valid ? ptr + r + c * ld : ptr;
-        double*       dst   = KC ? s + o * (kDBK + 4) + kk : s + kk * (O + 4) + o;
+        double*       dst   = KC ? s + o * (BK + 4) + kk : s + kk * (O + 4) + o;
         cp_async_8(dst, src, valid);
     }
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
-__global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads,
-                                  DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kThreads <= 256 ? 2 : 1)
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK>
+__global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads,
+                                  DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads <= 256 ? 2 : 1)
     gemm_dmma_kernel(GemmParams<double> p)
 {
-    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>;
+    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>;
     constexpr int NT = Cfg::kThreads;
     constexpr int TM = WM / 16, TN = WN / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,12 +134,12 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
     {
         const double* P  = p.P.get(batch);
         const double* Q  = p.Q.get(batch);
-        const int     nk = (p.K + kDBK - 1) / kDBK;
+        const int     nk = (p.K + BK - 1) / BK;
         auto load = [&](int stage, int kt) {
             double* sA = smem + stage * Cfg::kStage;
             double* sB = sA + Cfg::kStageA;
-            dmma_load_stage<BM, NT, KCP>(sA, P, p.ldp, p.triP, m0, kt * kDBK, p.M, p.K, tid);
-            dmma_load_stage<BN, NT, KCQ>(sB, Q, p.ldq, p.triQ, n0, kt * kDBK, p.N, p.K, tid);
+            dmma_load_stage<BM, NT, KCP, BK>(sA, P, p.ldp, p.triP, m0, kt * BK, p.M, p.K, tid);
+            dmma_load_stage<BN, NT, KCQ, BK>(sB, Q, p.ldq, p.triQ, n0, kt * BK, p.N, p.K, tid);
         };
         auto ldA = [&](const double* sA, int m, int k) {
             return KCP ? sA[m * Cfg::kPitchA + k] : sA[k * Cfg::kPitchA + m];
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
             const double* sA = smem + (kt % STAGES) * Cfg::kStage;
             const double* sB = sA + Cfg::kStageA;
 #pragma unroll
-            for(int ks = 0; ks < kDBK / 8; ++ks)
+            for(int ks = 0; ks < BK / 8; ++ks)
             {
                 const int k = ks * 8 + t;
                 double    fa[TM][4], fb[TN][2];
@@ -220,11 +221,11 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>::kTh
 }
 
 // ---- launch --------------------------------------------------------------------------------
-template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ>
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK = kDBK>
 static void launch_dmma_cfg(const GemmParams<double>& p0, int batch, cudaStream_t s)
 {
-    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ>;
-    auto kern = gemm_dmma_kernel<BM, BN, WM, WN, STAGES, KCP, KCQ>;
+    using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>;
+    auto kern = gemm_dmma_kernel<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>;
     cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
     for(int b0 = 0; b0 < batch; b0 += 65535)
     {
@@ -238,12 +239,13 @@ static void launch_dmma_cfg(const GemmParams<double>& p0, int batch, cudaStream_
 
 enum class DmmaTile
 {
-    t128x128,
+    t128x128 = 1,
     t128x64,
     t64x128,
     t64x64,
     t128x32,
-    t32x128
+    t32x128,
+    t128x128k32
 };
 
 template <bool KCP, bool KCQ>
@@ -257,6 +259,7 @@ static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch,
     case DmmaTile::t64x64:   launch_dmma_cfg<64, 64, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t128x32:  launch_dmma_cfg<128, 32, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t32x128:  launch_dmma_cfg<32, 128, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t128x128k32: launch_dmma_cfg<128, 128, 32, 32, 3, KCP, KCQ, 32>(p, batch, s); break;
     }
 }
 
@@ -265,6 +268,18 @@ static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch,
 static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, bool full_m, bool full_n)
 {
     auto tiles = [&](int bm, int bn) { return ceil_div(M, bm) * ceil_div(N, bn) * batch; };
+    const int forced = tuning().dmma_force_tile;
+    if(forced >= 1 && forced <= 7)
+    {
+        const DmmaTile f = (DmmaTile)forced;
+        // a forced tile must still respect the in-place constraint of the invA leaves
+        const bool spans_m = f == DmmaTile::t128x128 || f == DmmaTile::t128x64 || f == DmmaTile::t128x32
+                             || f == DmmaTile::t128x128k32;
+        const bool spans_n = f == DmmaTile::t128x128 || f == DmmaTile::t64x128 || f == DmmaTile::t32x128
+                             || f == DmmaTile::t128x128k32;
+        if((!full_m || spans_m) && (!full_n || spans_n))
+            return f;
+    }
     if(full_m)
     {
         if(tiles(128, 128) >= sms)
@@ -282,7 +297,7 @@ static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, b
         return DmmaTile::t32x128;
     }
     if(tiles(128, 128) * 100 >= (int64_t)sms * tuning().dmma_big_tile_pct)
-        return DmmaTile::t128x128;
+        return tuning().dmma_big_bk == 32 ? DmmaTile::t128x128k32 : DmmaTile::t128x128;
     if(M >= N ? tiles(128, 64) >= sms : tiles(64, 128) >= sms)
         return M >= N ? DmmaTile::t128x64 : DmmaTile::t64x128;
     return DmmaTile::t64x64;

@@ -18,13 +18,15 @@
 // dropped slice pairs (s + t >= S) add about S * 2^-7(S+1) of 2^(e_r+f_c): S = 7 gives 49
 // bits, S = 8 gives 56 bits (beyond FP64 rounding of a K-term dot product).
 //
-// Kernel layout (one CTA per 128 x 64 output tile, 192 threads):
-//   warp 0   TMA producer: per 32-deep K step it loads all S slices of the P tile
-//            (128 x 32 int8, SWIZZLE_32B) and of the Q tile (64 x 32) into one stage of a
-//            4..5-stage ring (a stage is S * 6 KB);
-//   warp 1   TMEM owner and MMA issuer: S <= 8 accumulators of 128 x 64 int32 (S*64 <= 512
-//            TMEM columns);
-//            per stage it issues the S(S+1)/2 slice-pair MMAs (M=128, N=64, K=32);
+// Kernel layout (one CTA per 128 x BN output tile, BN = 128 or 64, 192 threads):
+//   warp 0   TMA producer: per 64-deep K step it loads the slices the pass needs of the P
+//            tile (128 x 64 int8, SWIZZLE_64B) and of the Q tile (BN x 64) into one stage;
+//   warp 1   TMEM owner and MMA issuer: one 128 x BN int32 accumulator per slice-pair group
+//            d = s + t of the pass (at most 512 TMEM columns); per stage it issues the
+//            pass's slice-pair MMAs (M=128, N=BN, K=32, twice).  With S > 4 the groups are
+//            split into two passes (d < 4, then d >= 4; the second adds onto C) so that the
+//            accumulators of a pass fit TMEM with BN = 128, which halves the shared-memory
+//            reads of P per tensor-core operation compared with BN = 64;
 //   warps 2-5 epilogue: tcgen05.ld of the S accumulators (lanes = rows), Horner combination in
 //            FP64 registers, scaling by the row/column exponents, beta * C + alpha * (...).
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its
@@ -39,20 +41,21 @@ namespace rb200
 {
 
 constexpr int kOzBM      = 128;
-constexpr int kOzBN      = 64;
-constexpr int kOzBK      = 32;   // int8 elements per K step (32-byte swizzled rows, one MMA)
+constexpr int kOzBK      = 64;   // int8 elements per K step (64-byte swizzled rows, two MMAs)
 constexpr int kOzMaxS    = 8;
 constexpr int kOzThreads = 192;
-constexpr int kOzTileA   = kOzBM * kOzBK; // bytes per slice tile
-constexpr int kOzTileB   = kOzBN * kOzBK;
-constexpr int kOzKMax    = 16384;         // longest exact int32 accumulation run (S <= 7)
-constexpr int kOzSmemBudget = 220 * 1024;
+constexpr int kOzTileA   = kOzBM * kOzBK; // bytes per slice tile of P
+constexpr int kOzKMax    = 16384;         // longest exact int32 accumulation run (S <= 8)
+constexpr int kOzSmemBudget = 226 * 1024;
+constexpr int kOzNPad    = 128;           // row padding of the Q slice buffers
 constexpr int kOzExpNone    = -(1 << 30); // exponent of an all-zero row / column
 
 struct OzParams
 {
     int      M, N, K;          // logical sizes
-    int      S;                // slices (1..7)
+    int      S;                // slices (1..8)
+    int      d_lo, d_hi;       // slice-pair groups d = s + t computed by this pass
+    int      ns;               // slices staged per operand: min(S, d_hi)
     int      M_pad, N_pad;     // slice-buffer row counts (multiples of 128 / 64)
     const int* exp_rows;       // e_r, M entries
     const int* exp_cols;       // f_c, N entries
@@ -117,25 +120,26 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
                  : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major operand, 32-byte swizzle, 8-row groups 256 B apart.
+// UMMA shared-memory descriptor: K-major operand, 64-byte swizzle, 8-row groups 512 B apart.
 __device__ __forceinline__ uint64_t oz_smem_desc(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);       // start address
     d |= (uint64_t)1 << 16;                       // leading byte offset (unused, 16 B)
-    d |= (uint64_t)((8 * kOzBK) >> 4) << 32;      // stride byte offset: 8 rows x 32 B
+    d |= (uint64_t)((8 * kOzBK) >> 4) << 32;      // stride byte offset: 8 rows x 64 B
     d |= (uint64_t)1 << 46;                       // descriptor version (sm_100)
-    d |= (uint64_t)6 << 61;                       // SWIZZLE_32B
+    d |= (uint64_t)4 << 61;                       // SWIZZLE_64B
     return d;
 }
 
-// Instruction descriptor, kind::i8: s8 x s8 -> s32, K-major A and B, M = 128, N = 64.
+// Instruction descriptor, kind::i8: s8 x s8 -> s32, K-major A and B, M = 128, N = BN.
+template <int BN>
 __host__ __device__ constexpr uint32_t oz_idesc()
 {
     return (2u << 4)                      // D format S32
            | (1u << 7)                    // A format signed int8
            | (1u << 10)                   // B format signed int8
-           | ((uint32_t)(kOzBN >> 3) << 17)
+           | ((uint32_t)(BN >> 3) << 17)
            | ((uint32_t)(kOzBM >> 4) << 24);
 }
 
@@ -169,15 +173,17 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+template <int BN>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapP, const __grid_constant__ CUtensorMap mapQ,
                       OzParams p)
 {
+    constexpr int kOzTileB = BN * kOzBK; // bytes per slice tile of Q
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     // 1 KB alignment for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S         = p.S;
+    const int S         = p.ns; // slices staged per operand in this pass
     const int stage_bytes = S * (kOzTileA + kOzTileB);
     const int NS        = p.stages;
 
@@ -187,7 +193,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     __shared__ int      issued, consumed; // K steps loaded / handed to the tensor cores
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kOzBM, n0 = blockIdx.y * kOzBN;
+    const int m0 = blockIdx.x * kOzBM, n0 = blockIdx.y * BN;
     const int nk = (p.K + kOzBK - 1) / kOzBK;
 
     if(threadIdx.x == 0)
@@ -248,7 +254,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ---------------- MMA issuer ----------------
         if(lane == 0)
         {
-            const uint32_t idesc = oz_idesc();
+            const uint32_t idesc = oz_idesc<BN>();
+            uint32_t touched = 0; // groups whose accumulator holds data
             int i = 0;
             for(; i < nk; ++i)
             {
@@ -265,16 +272,20 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 const uint32_t abase = smem_u32(smem + st * stage_bytes);
                 const uint32_t bbase = abase + S * kOzTileA;
                 for(int s = 0; s < S; ++s)
-                    for(int t = 0; t + s < S; ++t)
+                    for(int t = 0; t < S; ++t)
                     {
-                        const uint32_t dcol = tmem + (uint32_t)((s + t) * kOzBN);
+                        const int d = s + t;
+                        if(d < p.d_lo || d >= p.d_hi)
+                            continue;
+                        const uint32_t dcol = tmem + (uint32_t)((d - p.d_lo) * BN);
 #pragma unroll
                         for(int kk = 0; kk < kOzBK / 32; ++kk)
                         {
                             const uint64_t ad = oz_smem_desc(abase + s * kOzTileA + kk * 32);
                             const uint64_t bd = oz_smem_desc(bbase + t * kOzTileB + kk * 32);
-                            const uint32_t acc = (i > 0 || kk > 0 || s > 0) ? 1u : 0u;
+                            const uint32_t acc = (touched >> (d - p.d_lo)) & 1u;
                             oz_mma(dcol, ad, bd, idesc, acc);
+                            touched |= 1u << (d - p.d_lo);
                         }
                     }
                 oz_commit(&empty_bar[st]);
@@ -306,16 +317,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 er = 0;
             const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll 1
-            for(int half = 0; half < kOzBN / 32; ++half)
+            for(int half = 0; half < BN / 32; ++half)
             {
                 double h[32];
 #pragma unroll
                 for(int j = 0; j < 32; ++j)
                     h[j] = 0.0;
-                for(int d = S - 1; d >= 0; --d)
+                for(int d = p.d_hi - 1; d >= p.d_lo; --d)
                 {
                     uint32_t v[32];
-                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)(d * kOzBN + half * 32), v);
+                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)((d - p.d_lo) * BN + half * 32), v);
 #pragma unroll
                     for(int j = 0; j < 32; ++j)
                         h[j] = fma(h[j], 0x1p-7, (double)(int)v[j]);
@@ -330,7 +341,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         {
                             double* cp = p.C + gr + (int64_t)gc * p.ldc;
                             const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
-                            const double pq = ldexp(h[j], er + ec - 14);
+                            const double pq = ldexp(h[j], er + ec - 14 - 7 * p.d_lo);
                             double out;
                             if(zero)
                                 out = 0.0;

@@ -616,6 +616,52 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
     return launch_status();
 }
 
+// C := alpha op(A) op(B) + beta C on the FP64 DMMA tiles (host pointer mode).
+rocblas_status gemm_dmma_impl(rocblas_handle h, rocblas_operation ta, rocblas_operation tb, int m,
+                              int n, int k, const double* alpha, const double* A, int lda,
+                              const double* B, int ldb, const double* beta, double* C, int ldc)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    auto okop = [](rocblas_operation t) {
+        return t == rocblas_operation_none || t == rocblas_operation_transpose
+               || t == rocblas_operation_conjugate_transpose;
+    };
+    if(!okop(ta) || !okop(tb))
+        return rocblas_status_invalid_value;
+    const bool nA = ta == rocblas_operation_none, nB = tb == rocblas_operation_none;
+    if(m < 0 || n < 0 || k < 0 || lda < (nA ? m : k) || ldb < (nB ? k : n) || ldc < m)
+        return rocblas_status_invalid_size;
+    if(!m || !n)
+        return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
+    if(h->size_query)
+        return rocblas_status_size_unchanged;
+    if(!alpha || !beta || !C || (k && (!A || !B)))
+        return rocblas_status_invalid_pointer;
+    if(h->pointer_mode != rocblas_pointer_mode_host)
+        return rocblas_status_not_implemented;
+    rocblas_status st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    GemmParams<double> g{};
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.P = strided<double>(A, 0);
+    g.ldp = lda;
+    g.transP = nA ? 0 : 1;
+    g.Q = strided<double>(B, 0);
+    g.ldq = ldb;
+    g.transQ = nB ? 0 : 1;
+    g.C = strided<double>(C, 0);
+    g.ldc = ldc;
+    g.a_imm = *alpha;
+    g.b_imm = *beta;
+    g.zero_guard = 0;
+    launch_gemm<double>(g, 1, h->stream, h->sm_count);
+    return launch_status();
+}
+
 rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                                rocblas_operation trans, rocblas_diagonal diag, int m, int n,
                                const double* alpha, const double* A, int lda, double* B, int ldb,
@@ -1090,6 +1136,20 @@ rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle h, rocblas_operation tra
 try
 {
     return gemm_sliced_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dgemm(rocblas_handle h, rocblas_operation transA,
+                                  rocblas_operation transB, rocblas_int m, rocblas_int n,
+                                  rocblas_int k, const double* alpha, const double* A,
+                                  rocblas_int lda, const double* B, rocblas_int ldb,
+                                  const double* beta, double* C, rocblas_int ldc)
+try
+{
+    return gemm_dmma_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 catch(...)
 {

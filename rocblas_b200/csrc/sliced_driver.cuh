@@ -53,7 +53,7 @@ static inline size_t align256(size_t b)
 static size_t sliced_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int S)
 {
     const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), kOzKMax), kOzSliceTile);
-    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kOzBN);
+    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kOzNPad);
     static_assert(kOzSliceTile % kOzBK == 0, "slice padding must cover whole K steps");
     return align256((size_t)S * Mp * Kp) + align256((size_t)S * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np);
@@ -123,19 +123,60 @@ static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t 
            == CUDA_SUCCESS;
 }
 
+// One pass of the slice-pair groups [d_lo, d_hi) with output tiles 128 x BN.
+struct OzPass
+{
+    int d_lo, d_hi, bn, ns, stages;
+};
+
+static int oz_stage_bytes(int ns, int bn)
+{
+    return ns * (kOzTileA + bn * kOzBK);
+}
+
+// Split the S(S+1)/2 slice-pair products into passes whose accumulators fit TMEM (512
+// columns of 128 x BN int32) and whose operand stages fit shared memory at least twice.
+static int plan_oz_passes(int S, OzPass* out)
+{
+    auto make = [](int lo, int hi, int S) {
+        OzPass q{lo, hi, 128, std::min(S, hi), 0};
+        if((hi - lo) * 128 > 512 || 2 * oz_stage_bytes(q.ns, 128) + 1024 > kOzSmemBudget)
+            q.bn = 64;
+        q.stages = std::min(8, (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn));
+        return q;
+    };
+    if(S <= 4)
+    {
+        out[0] = make(0, S, S);
+        return 1;
+    }
+    out[0] = make(0, 4, S);
+    out[1] = make(4, S, S);
+    return 2;
+}
+
+template <int BN>
+static void launch_oz_pass(const CUtensorMap& mapP, const CUtensorMap& mapQ, const OzParams& p,
+                           int64_t Mp, int64_t Np, cudaStream_t s)
+{
+    const size_t smem = (size_t)p.stages * oz_stage_bytes(p.ns, BN) + 1024;
+    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / BN));
+    ozaki_gemm_kernel<BN><<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
+    count_launch();
+}
+
 // Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
 // Returns false if the tensor-map encoder is unavailable.
 static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream_t s)
 {
     if(g.M <= 0 || g.N <= 0)
         return true;
-    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kOzBN);
+    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kOzNPad);
     const int     S  = g.S;
-    const int     stage_bytes = S * (kOzTileA + kOzTileB);
-    const int     stages      = std::min(8, kOzSmemBudget / stage_bytes);
-    const size_t  smem        = (size_t)stages * stage_bytes + 1024;
-    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    OzPass        passes[2];
+    const int     npass = plan_oz_passes(S, passes);
     const int64_t K = std::max<int64_t>(g.K, 0);
     for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kOzKMax)
     {
@@ -164,33 +205,43 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
         launch_slices(P, (int)g.M, (int)kc, eP, S, sP, (int)Mp, (int)Kp, s);
         launch_slices(Q, (int)g.N, (int)kc, eQ, S, sQ, (int)Np, (int)Kp, s);
 
-        CUtensorMap mapP, mapQ;
+        CUtensorMap mapP, mapQ64, mapQ128;
         if(!make_slice_map(&mapP, sP, Kp, (int64_t)S * Mp, kOzBM)
-           || !make_slice_map(&mapQ, sQ, Kp, (int64_t)S * Np, kOzBN))
+           || !make_slice_map(&mapQ64, sQ, Kp, (int64_t)S * Np, 64)
+           || !make_slice_map(&mapQ128, sQ, Kp, (int64_t)S * Np, 128))
             return false;
-        OzParams p{};
-        p.M = (int)g.M;
-        p.N = (int)g.N;
-        p.K = (int)std::max<int64_t>(kc, 1);
-        p.S = S;
-        p.M_pad = (int)Mp;
-        p.N_pad = (int)Np;
-        p.exp_rows = eP;
-        p.exp_cols = eQ;
-        p.C = g.C;
-        p.ldc = g.ldc;
-        p.alpha = g.a;
-        const bool first = k0 == 0;
-        p.beta  = first ? (g.b_user ? g.ualpha_host : g.b_imm) : 1.0;
-        p.beta_ptr = (first && g.b_user) ? g.ualpha_dev : nullptr;
-        p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
-        p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
-        p.stages = stages;
-        p.tmem_cols = S * kOzBN <= 64 ? 64 : S * kOzBN <= 128 ? 128 : S * kOzBN <= 256 ? 256 : 512;
-        p.error = err_dev;
-        dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / kOzBN));
-        ozaki_gemm_kernel<<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
-        count_launch();
+        for(int pi = 0; pi < npass; ++pi)
+        {
+            const OzPass& q = passes[pi];
+            OzParams p{};
+            p.M = (int)g.M;
+            p.N = (int)g.N;
+            p.K = (int)std::max<int64_t>(kc, 1);
+            p.S = S;
+            p.d_lo = q.d_lo;
+            p.d_hi = q.d_hi;
+            p.ns = q.ns;
+            p.M_pad = (int)Mp;
+            p.N_pad = (int)Np;
+            p.exp_rows = eP;
+            p.exp_cols = eQ;
+            p.C = g.C;
+            p.ldc = g.ldc;
+            p.alpha = g.a;
+            const bool first = k0 == 0 && pi == 0;
+            p.beta  = first ? (g.b_user ? g.ualpha_host : g.b_imm) : 1.0;
+            p.beta_ptr = (first && g.b_user) ? g.ualpha_dev : nullptr;
+            p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
+            p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
+            p.stages = q.stages;
+            const int cols = (q.d_hi - q.d_lo) * q.bn;
+            p.tmem_cols = cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : cols <= 256 ? 256 : 512;
+            p.error = err_dev;
+            if(q.bn == 128)
+                launch_oz_pass<128>(mapP, mapQ128, p, Mp, Np, s);
+            else
+                launch_oz_pass<64>(mapP, mapQ64, p, Mp, Np, s);
+        }
     }
     return true;
 }

@@ -25,6 +25,8 @@ struct Tuning
     int sliced_min_k         = 1024; // precision form: sliced updates only for K >= this
     int dmma_big_tile_pct    = 200;  // 128x128 DMMA tiles if tiles >= SMs * pct / 100
     int mixed_slices         = 7;    // slices of the precision form when the caller passes 0
+    int dmma_force_tile      = 0;    // 0: choose; 1..7: force one DMMA tile shape (DmmaTile)
+    int dmma_big_bk          = 16;   // k depth of the 128x128 DMMA stage (16 or 32)
 };
 
 struct TuningEntry
@@ -41,6 +43,8 @@ static const TuningEntry kTuningEntries[] = {
     {"sliced_min_k", &Tuning::sliced_min_k, 1, 1 << 30},
     {"dmma_big_tile_pct", &Tuning::dmma_big_tile_pct, 1, 100000},
     {"mixed_slices", &Tuning::mixed_slices, 1, 8},
+    {"dmma_force_tile", &Tuning::dmma_force_tile, 0, 7},
+    {"dmma_big_bk", &Tuning::dmma_big_bk, 16, 32},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

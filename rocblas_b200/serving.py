@@ -93,7 +93,8 @@ class TrsmServer:
         # arrives with the request): a request's B and fresh A depend only on its seed
         g = torch.Generator(device=self.dev)
         g.manual_seed(12345)
-        self.pool = {"d": torch.rand(1 << 26, generator=g, device=self.dev, dtype=torch.float64) * 2 - 1}
+        self.pool = {"d": torch.rand((1 << 27) + 4096, generator=g, device=self.dev,
+                                     dtype=torch.float64) * 2 - 1}
         self.pool["s"] = self.pool["d"].to(torch.float32)
 
     # ---- resident matrices ------------------------------------------------------------
@@ -137,7 +138,8 @@ class TrsmServer:
 
     def _cut(self, dt, count, seed):
         pool = self.pool[dt]
-        off = (seed * 2654435761) % (pool.numel() - count)
+        span = pool.numel() - count  # > 0: the pool holds the largest A (8192^2) and more
+        off = (seed * 2654435761) % span
         return pool[off: off + count]
 
     def _materialise(self, q: Request, stream):
@@ -145,7 +147,7 @@ class TrsmServer:
         pool; a fresh lower-triangular A has off-diagonals U(-1,1)/m and diagonal 1.5 +
         U(-1,1)/m (the drop-in recipe's conditioning)."""
         with torch.cuda.stream(stream):
-            q.B = self._cut(q.dtype, q.m * q.n, q.seed).clone()
+            q.B = self._cut(q.dtype, q.m * q.n, q.seed).clone().view(q.n, q.m)
             if q.a_key is None:
                 A = self._cut(q.dtype, q.m * q.m, q.seed + 1) * (1.0 / q.m)
                 A.view(q.m, q.m).diagonal().add_(1.5)
