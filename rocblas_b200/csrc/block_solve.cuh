@@ -113,27 +113,80 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
     }
     __syncthreads();
 
-    for(int p = 0; p < k; p += 32)
-    {
-        // ---- 1. diagonal tile of M' --------------------------------------------------------
-        for(int idx = tid; idx < 32 * 32; idx += kBsThreads)
+    // A is read-only, so the loads of the next diagonal tile or update chunk are issued into
+    // registers before the current step computes, and land in shared memory after it.
+    constexpr int kDiagPer  = 32 * 32 / kBsThreads;       // 4 values per thread
+    constexpr int kChunkPer = kBsChunk * 32 / kBsThreads; // 8 values per thread
+    static_assert(kDiagPer <= kChunkPer, "one prefetch buffer serves both steps");
+    T pre[kChunkPer];
+    auto fetch_diag = [&](int p) {
+#pragma unroll
+        for(int u = 0; u < kDiagPer; ++u)
         {
-            int i, j;
+            const int idx = tid + u * kBsThreads;
+            int       i, j;
             if(!tM) { i = idx % 32; j = idx / 32; }
             else    { j = idx % 32; i = idx / 32; }
             T v = T(0);
-            if(j < i && p + i < k)
-                v = mval(p + i, p + j);
-            Ds[i * 33 + j] = v;
-            if(i == j)
+            if(p + i < k)
             {
-                T d = T(1);
-                if(!unit && p + i < k)
-                    d = mval(p + i, p + i);
-                rdiag[i] = T(1) / d;
+                if(j < i)
+                    v = mval(p + i, p + j);
+                else if(i == j)
+                    v = unit ? T(1) : mval(p + i, p + i);
             }
+            else if(i == j)
+                v = T(1); // padding rows solve 0 = 0
+            pre[u] = v;
         }
+    };
+    auto store_diag = [&]() {
+#pragma unroll
+        for(int u = 0; u < kDiagPer; ++u)
+        {
+            const int idx = tid + u * kBsThreads;
+            int       i, j;
+            if(!tM) { i = idx % 32; j = idx / 32; }
+            else    { j = idx % 32; i = idx / 32; }
+            if(i == j)
+                rdiag[i] = T(1) / pre[u];
+            Ds[i * 33 + j] = j < i ? pre[u] : T(0);
+        }
+    };
+    auto fetch_chunk = [&](int p, int i0) {
+#pragma unroll
+        for(int u = 0; u < kChunkPer; ++u)
+        {
+            const int idx = tid + u * kBsThreads;
+            int       r, t;
+            if(!tM) { r = idx % kBsChunk; t = idx / kBsChunk; }
+            else    { t = idx % 32; r = idx / 32; }
+            T v = T(0);
+            if(i0 + r < k && p + t < k)
+                v = mval(i0 + r, p + t);
+            pre[u] = v;
+        }
+    };
+    auto store_chunk = [&]() {
+#pragma unroll
+        for(int u = 0; u < kChunkPer; ++u)
+        {
+            const int idx = tid + u * kBsThreads;
+            int       r, t;
+            if(!tM) { r = idx % kBsChunk; t = idx / kBsChunk; }
+            else    { t = idx % 32; r = idx / 32; }
+            Ps[r * 33 + t] = pre[u];
+        }
+    };
+
+    fetch_diag(0);
+    for(int p = 0; p < k; p += 32)
+    {
+        // ---- 1. diagonal tile of M' (prefetched) -------------------------------------------
+        store_diag();
         __syncthreads();
+        if(p + 32 < k)
+            fetch_chunk(p, p + 32);
 
         // ---- 2. substitution with shuffle broadcast -----------------------------------------
         {
@@ -162,20 +215,15 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
         }
         __syncthreads();
 
-        // ---- 3. update rows p+32 .. k-1 --------------------------------------------------
+        // ---- 3. update rows p+32 .. k-1 (chunks prefetched one step ahead) ----------------
         for(int i0 = p + 32; i0 < k; i0 += kBsChunk)
         {
-            for(int idx = tid; idx < kBsChunk * 32; idx += kBsThreads)
-            {
-                int r, t;
-                if(!tM) { r = idx % kBsChunk; t = idx / kBsChunk; }
-                else    { t = idx % 32; r = idx / 32; }
-                T v = T(0);
-                if(i0 + r < k && p + t < k)
-                    v = mval(i0 + r, p + t);
-                Ps[r * 33 + t] = v;
-            }
+            store_chunk();
             __syncthreads();
+            if(i0 + kBsChunk < k)
+                fetch_chunk(p, i0 + kBsChunk);
+            else
+                fetch_diag(p + 32); // p + 32 < k here
             const int col = lane;
 #pragma unroll
             for(int q = 0; q < kBsChunk / 8; ++q)

@@ -296,10 +296,10 @@ static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, b
             return DmmaTile::t64x128;
         return DmmaTile::t32x128;
     }
+    // 64 x 64 tiles (three CTAs per SM) measured fastest at every size with enough tiles;
+    // the wider tiles remain reachable through dmma_big_tile_pct
     if(tiles(128, 128) * 100 >= (int64_t)sms * tuning().dmma_big_tile_pct)
         return tuning().dmma_big_bk == 32 ? DmmaTile::t128x128k32 : DmmaTile::t128x128;
-    if(M >= N ? tiles(128, 64) >= sms : tiles(64, 128) >= sms)
-        return M >= N ? DmmaTile::t128x64 : DmmaTile::t64x128;
     return DmmaTile::t64x64;
 }
 

@@ -18,16 +18,20 @@
 // dropped slice pairs (s + t >= S) add about S * 2^-7(S+1) of 2^(e_r+f_c): S = 7 gives 49
 // bits, S = 8 gives 56 bits (beyond FP64 rounding of a K-term dot product).
 //
-// Kernel layout (one CTA per 128 x BN output tile, BN = 128 or 64, 192 threads):
-//   warp 0   TMA producer: per 64-deep K step it loads the slices the pass needs of the P
-//            tile (128 x 64 int8, SWIZZLE_64B) and of the Q tile (BN x 64) into one stage;
+// Kernel layout (one CTA per 128 x BN output tile, BN = 64 or 128, 192 threads):
+//   warp 0   TMA producer: per BK-deep K step (BK = 32 or 64 int8, SWIZZLE_32B / _64B rows)
+//            it loads the slices the pass needs of the P tile (128 x BK) and of the Q tile
+//            (BN x BK) into one stage of a ring;
 //   warp 1   TMEM owner and MMA issuer: one 128 x BN int32 accumulator per slice-pair group
-//            d = s + t of the pass (at most 512 TMEM columns); per stage it issues the
-//            pass's slice-pair MMAs (M=128, N=BN, K=32, twice).  With S > 4 the groups are
-//            split into two passes (d < 4, then d >= 4; the second adds onto C) so that the
-//            accumulators of a pass fit TMEM with BN = 128, which halves the shared-memory
-//            reads of P per tensor-core operation compared with BN = 64;
-//   warps 2-5 epilogue: tcgen05.ld of the S accumulators (lanes = rows), Horner combination in
+//            d = s + t of the pass, group d at TMEM column (d - d_lo) * BN.  The Q slices of
+//            a stage sit back to back, so Q slices t0..t0+c-1 form one (c * BN)-row operand and
+//            a single MMA with N = c * BN <= 256 computes the products of P slice s with all
+//            of them into the adjacent accumulators of groups s+t0 .. s+t0+c-1: per K step
+//            and P slice one to two MMAs instead of one per slice pair, and the P tile is read
+//            from shared memory once per MMA instead of once per pair.  With BN = 64 all
+//            S <= 8 groups fit the 512 TMEM columns in one pass; with BN = 128 and S > 4 the
+//            groups are split into two passes (d < 4, then d >= 4; the second adds onto C);
+//   warps 2-5 epilogue: tcgen05.ld of the accumulators (lanes = rows), Horner combination in
 //            FP64 registers, scaling by the row/column exponents, beta * C + alpha * (...).
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its
 // in-flight copies and MMAs (again bounded), frees TMEM and returns.
@@ -41,10 +45,10 @@ namespace rb200
 {
 
 constexpr int kOzBM      = 128;
-constexpr int kOzBK      = 64;   // int8 elements per K step (64-byte swizzled rows, two MMAs)
 constexpr int kOzMaxS    = 8;
 constexpr int kOzThreads = 192;
-constexpr int kOzTileA   = kOzBM * kOzBK; // bytes per slice tile of P
+constexpr int kOzMmaK    = 32;            // int8 K of one tcgen05.mma
+constexpr int kOzMaxN    = 256;           // largest N of one tcgen05.mma with M = 128
 constexpr int kOzKMax    = 16384;         // longest exact int32 accumulation run (S <= 8)
 constexpr int kOzSmemBudget = 226 * 1024;
 constexpr int kOzNPad    = 128;           // row padding of the Q slice buffers
@@ -120,26 +124,28 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
                  : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major operand, 64-byte swizzle, 8-row groups 512 B apart.
+// UMMA shared-memory descriptor: K-major operand with BK-byte rows (BK = 64: SWIZZLE_64B,
+// BK = 32: SWIZZLE_32B), 8-row groups 8 * BK bytes apart.
+template <int BK>
 __device__ __forceinline__ uint64_t oz_smem_desc(uint32_t saddr)
 {
+    static_assert(BK == 32 || BK == 64, "swizzle span of one K step");
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);       // start address
     d |= (uint64_t)1 << 16;                       // leading byte offset (unused, 16 B)
-    d |= (uint64_t)((8 * kOzBK) >> 4) << 32;      // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)((8 * BK) >> 4) << 32;         // stride byte offset: 8 rows x BK bytes
     d |= (uint64_t)1 << 46;                       // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                       // SWIZZLE_64B
+    d |= (uint64_t)(BK == 64 ? 4 : 6) << 61;      // SWIZZLE_64B / SWIZZLE_32B
     return d;
 }
 
-// Instruction descriptor, kind::i8: s8 x s8 -> s32, K-major A and B, M = 128, N = BN.
-template <int BN>
-__host__ __device__ constexpr uint32_t oz_idesc()
+// Instruction descriptor, kind::i8: s8 x s8 -> s32, K-major A and B, M = 128, N = n.
+__host__ __device__ constexpr uint32_t oz_idesc(int n)
 {
     return (2u << 4)                      // D format S32
            | (1u << 7)                    // A format signed int8
            | (1u << 10)                   // B format signed int8
-           | ((uint32_t)(BN >> 3) << 17)
+           | ((uint32_t)(n >> 3) << 17)
            | ((uint32_t)(kOzBM >> 4) << 24);
 }
 
@@ -173,18 +179,20 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN>
+template <int BN, int BK>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapP, const __grid_constant__ CUtensorMap mapQ,
                       OzParams p)
 {
-    constexpr int kOzTileB = BN * kOzBK; // bytes per slice tile of Q
+    constexpr int kTileA = kOzBM * BK; // bytes per slice tile of P
+    constexpr int kTileB = BN * BK;    // bytes per slice tile of Q
+    constexpr int kMerge = kOzMaxN / BN; // Q slices per MMA
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     // 1 KB alignment for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
     const int S         = p.ns; // slices staged per operand in this pass
-    const int stage_bytes = S * (kOzTileA + kOzTileB);
+    const int stage_bytes = S * (kTileA + kTileB);
     const int NS        = p.stages;
 
     __shared__ uint64_t full_bar[8], empty_bar[8], acc_bar;
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kOzBM, n0 = blockIdx.y * BN;
-    const int nk = (p.K + kOzBK - 1) / kOzBK;
+    const int nk = (p.K + BK - 1) / BK;
 
     if(threadIdx.x == 0)
     {
@@ -241,9 +249,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 unsigned char* base = smem + st * stage_bytes;
                 mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
                 for(int s = 0; s < S; ++s)
-                    tma_load_2d(base + s * kOzTileA, &mapP, &full_bar[st], i * kOzBK, s * p.M_pad + m0);
+                    tma_load_2d(base + s * kTileA, &mapP, &full_bar[st], i * BK, s * p.M_pad + m0);
                 for(int t = 0; t < S; ++t)
-                    tma_load_2d(base + S * kOzTileA + t * kOzTileB, &mapQ, &full_bar[st], i * kOzBK,
+                    tma_load_2d(base + S * kTileA + t * kTileB, &mapQ, &full_bar[st], i * BK,
                                 t * p.N_pad + n0);
                 *(volatile int*)&issued = i + 1;
             }
@@ -254,7 +262,6 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ---------------- MMA issuer ----------------
         if(lane == 0)
         {
-            const uint32_t idesc = oz_idesc<BN>();
             uint32_t touched = 0; // groups whose accumulator holds data
             int i = 0;
             for(; i < nk; ++i)
@@ -270,24 +277,31 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 *(volatile int*)&consumed = i + 1;
                 const uint32_t abase = smem_u32(smem + st * stage_bytes);
-                const uint32_t bbase = abase + S * kOzTileA;
+                const uint32_t bbase = abase + S * kTileA;
                 for(int s = 0; s < S; ++s)
-                    for(int t = 0; t < S; ++t)
+                {
+                    // Q slices t with d_lo <= s + t < d_hi, in runs of at most kMerge
+                    const int t_lo = max(0, p.d_lo - s), t_hi = min(S - 1, p.d_hi - 1 - s);
+                    for(int t0 = t_lo; t0 <= t_hi; t0 += kMerge)
                     {
-                        const int d = s + t;
-                        if(d < p.d_lo || d >= p.d_hi)
-                            continue;
-                        const uint32_t dcol = tmem + (uint32_t)((d - p.d_lo) * BN);
+                        const int      c     = min(kMerge, t_hi - t0 + 1);
+                        const int      g0    = s + t0 - p.d_lo; // first group of the run
+                        const uint32_t run   = ((1u << c) - 1u) << g0;
+                        const uint32_t dcol  = tmem + (uint32_t)(g0 * BN);
+                        const uint32_t idesc = oz_idesc(c * BN);
+                        // P slice 0 comes first and covers every group of the pass, so a run
+                        // is either wholly fresh or wholly accumulated
+                        const uint32_t accum = (touched & run) ? 1u : 0u;
 #pragma unroll
-                        for(int kk = 0; kk < kOzBK / 32; ++kk)
+                        for(int kk = 0; kk < BK / kOzMmaK; ++kk)
                         {
-                            const uint64_t ad = oz_smem_desc(abase + s * kOzTileA + kk * 32);
-                            const uint64_t bd = oz_smem_desc(bbase + t * kOzTileB + kk * 32);
-                            const uint32_t acc = (touched >> (d - p.d_lo)) & 1u;
-                            oz_mma(dcol, ad, bd, idesc, acc);
-                            touched |= 1u << (d - p.d_lo);
+                            const uint64_t ad = oz_smem_desc<BK>(abase + s * kTileA + kk * kOzMmaK);
+                            const uint64_t bd = oz_smem_desc<BK>(bbase + t0 * kTileB + kk * kOzMmaK);
+                            oz_mma(dcol, ad, bd, idesc, (kk > 0) ? 1u : accum);
                         }
+                        touched |= run;
                     }
+                }
                 oz_commit(&empty_bar[st]);
             }
             // completion of everything issued so far (also on abort: drains the issued MMAs)

@@ -398,13 +398,26 @@ rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal 
     return launch_status();
 }
 
-template <typename T>
-__global__ void vb_copy_invalid_kernel(const VbState* st, rocblas_int* out)
+__global__ void vb_copy_invalid_kernel(const int* invalid, rocblas_int* out)
 {
-    *out = st->invalid;
+    *out = *invalid;
 }
 
 static_assert(sizeof(VbProblem) == sizeof(rocblas_b200_trsm_problem), "descriptor layout");
+
+// Persistent strip-solver launch over one queue; shared memory sized for systems up to kmax.
+template <typename T>
+void launch_vb_queue(rocblas_handle h, const VbParams<T>& p, int kmax)
+{
+    const size_t smem = block_solve_smem_bytes<T>(std::max(kmax, 1));
+    cudaFuncSetAttribute((const void*)vb_persistent_kernel<T>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<T>, kBsThreads, smem);
+    per_sm = std::max(per_sm, 1);
+    vb_persistent_kernel<T><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
+    count_launch();
+}
 
 template <typename T>
 rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
@@ -415,7 +428,8 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
         return rocblas_status_invalid_handle;
     if(count < 0 || max_k < 0 || max_k > kBlockSolveMaxK)
         return rocblas_status_invalid_size;
-    const size_t ws_bytes = sizeof(VbState) + sizeof(int) * ((size_t)count + 1);
+    const size_t ws_bytes
+        = sizeof(VbClassState) + sizeof(int) * (size_t)kVbClasses * ((size_t)count + 1);
     if(h->size_query)
         return count ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
     if(!count)
@@ -428,33 +442,33 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
     void* ws = h->borrow(ws_bytes);
     if(!ws)
         return rocblas_status_memory_error;
-    VbState* state   = reinterpret_cast<VbState*>(ws);
-    int*     offsets = reinterpret_cast<int*>(state + 1);
-    cudaMemsetAsync(state, 0, sizeof(VbState), h->stream);
+    VbClassState* state   = reinterpret_cast<VbClassState*>(ws);
+    int*          offsets = reinterpret_cast<int*>(state + 1);
+    cudaMemsetAsync(state, 0, sizeof(VbClassState), h->stream);
     const VbProblem* probs = reinterpret_cast<const VbProblem*>(problems);
-    vb_prepass_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, offsets, state);
+    vb_prepass_classes_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, offsets,
+                                                                    state);
     count_launch();
 
     VbParams<T> p;
-    p.probs   = probs;
-    p.count   = count;
-    p.offsets = offsets;
-    p.st      = state;
+    p.probs = probs;
+    p.count = count;
     if(h->pointer_mode == rocblas_pointer_mode_host)
         p.alpha.val = *alpha;
     else
         p.alpha.ptr = alpha;
-    const size_t smem = block_solve_smem_bytes<T>(std::max(max_k, 1));
-    cudaFuncSetAttribute((const void*)vb_persistent_kernel<T>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<T>, kBsThreads, smem);
-    per_sm = std::max(per_sm, 1);
-    vb_persistent_kernel<T><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
-    count_launch();
+    // largest class first, so its long strips start while the small classes fill in behind
+    for(int c = kVbClasses - 1; c >= 0; --c)
+    {
+        if(c > 0 && vb_class_kmax(c - 1) >= max_k)
+            continue; // no valid system reaches this class
+        p.offsets = offsets + (size_t)c * ((size_t)count + 1);
+        p.counter = &state->counter[c];
+        launch_vb_queue<T>(h, p, std::min(vb_class_kmax(c), std::max(max_k, 1)));
+    }
     if(invalid_count)
     {
-        vb_copy_invalid_kernel<T><<<1, 1, 0, h->stream>>>(state, invalid_count);
+        vb_copy_invalid_kernel<<<1, 1, 0, h->stream>>>(&state->invalid, invalid_count);
         count_launch();
     }
     return launch_status();
@@ -532,22 +546,15 @@ rocblas_status trsm_vbatched_noalloc_impl(rocblas_handle h, const double* alpha,
     p.probs   = probs;
     p.count   = count;
     p.offsets = offsets;
-    p.st      = state;
+    p.counter = &state->counter;
     if(h->pointer_mode == rocblas_pointer_mode_host)
         p.alpha.val = *alpha;
     else
         p.alpha.ptr = alpha;
-    const size_t smem = block_solve_smem_bytes<double>(std::max(max_k, 1));
-    cudaFuncSetAttribute((const void*)vb_persistent_kernel<double>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<double>, kBsThreads, smem);
-    per_sm = std::max(per_sm, 1);
-    vb_persistent_kernel<double><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
-    count_launch();
+    launch_vb_queue<double>(h, p, max_k);
     if(invalid_count)
     {
-        vb_copy_invalid_kernel<double><<<1, 1, 0, h->stream>>>(state, invalid_count);
+        vb_copy_invalid_kernel<<<1, 1, 0, h->stream>>>(&state->invalid, invalid_count);
         count_launch();
     }
     return launch_status();

@@ -54,7 +54,7 @@ static size_t sliced_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int S
 {
     const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), kOzKMax), kOzSliceTile);
     const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kOzNPad);
-    static_assert(kOzSliceTile % kOzBK == 0, "slice padding must cover whole K steps");
+    static_assert(kOzSliceTile % 64 == 0, "slice padding must cover whole K steps");
     return align256((size_t)S * Mp * Kp) + align256((size_t)S * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np);
 }
@@ -108,62 +108,71 @@ static void launch_slices(SliceOperand X, int O, int K, const int* exps, int S, 
     count_launch();
 }
 
-static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t rows, int box_rows)
+static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t rows, int box_rows,
+                           int bk)
 {
     EncodeTiledFn enc = encode_tiled_fn();
     if(!enc)
         return false;
     cuuint64_t dims[2]    = {(cuuint64_t)K_pad, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)K_pad};
-    cuuint32_t box[2]     = {(cuuint32_t)kOzBK, (cuuint32_t)box_rows};
+    cuuint32_t box[2]     = {(cuuint32_t)bk, (cuuint32_t)box_rows};
     cuuint32_t estr[2]    = {1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE,
+               bk == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
            == CUDA_SUCCESS;
 }
 
-// One pass of the slice-pair groups [d_lo, d_hi) with output tiles 128 x BN.
+// One pass of the slice-pair groups [d_lo, d_hi) with output tiles 128 x bn and K steps of bk.
 struct OzPass
 {
-    int d_lo, d_hi, bn, ns, stages;
+    int d_lo, d_hi, bn, bk, ns, stages;
 };
 
-static int oz_stage_bytes(int ns, int bn)
+static int oz_stage_bytes(int ns, int bn, int bk)
 {
-    return ns * (kOzTileA + bn * kOzBK);
+    return ns * (kOzBM + bn) * bk;
 }
 
 // Split the S(S+1)/2 slice-pair products into passes whose accumulators fit TMEM (512
 // columns of 128 x BN int32) and whose operand stages fit shared memory at least twice.
+// Output tile width and K depth come from the tuning table (oz_bn, oz_bk).
 static int plan_oz_passes(int S, OzPass* out)
 {
-    auto make = [](int lo, int hi, int S) {
-        OzPass q{lo, hi, 128, std::min(S, hi), 0};
-        if((hi - lo) * 128 > 512 || 2 * oz_stage_bytes(q.ns, 128) + 1024 > kOzSmemBudget)
-            q.bn = 64;
-        q.stages = std::min(8, (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn));
+    const int bn = tuning().oz_bn == 128 ? 128 : 64;
+    const int bk = tuning().oz_bk == 32 ? 32 : 64;
+    auto make = [&](int lo, int hi) {
+        OzPass q{lo, hi, bn, bk, std::min(S, hi), 0};
+        q.stages = (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn, q.bk);
+        if(q.stages < 2 && q.bk == 64)
+        {
+            q.bk     = 32;
+            q.stages = (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn, q.bk);
+        }
+        q.stages = std::min(8, q.stages);
         return q;
     };
-    if(S <= 4)
+    if(S * bn <= 512)
     {
-        out[0] = make(0, S, S);
+        out[0] = make(0, S);
         return 1;
     }
-    out[0] = make(0, 4, S);
-    out[1] = make(4, S, S);
+    out[0] = make(0, 4);
+    out[1] = make(4, S);
     return 2;
 }
 
-template <int BN>
+template <int BN, int BK>
 static void launch_oz_pass(const CUtensorMap& mapP, const CUtensorMap& mapQ, const OzParams& p,
                            int64_t Mp, int64_t Np, cudaStream_t s)
 {
-    const size_t smem = (size_t)p.stages * oz_stage_bytes(p.ns, BN) + 1024;
-    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    const size_t smem = (size_t)p.stages * oz_stage_bytes(p.ns, BN, BK) + 1024;
+    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN, BK>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / BN));
-    ozaki_gemm_kernel<BN><<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
+    ozaki_gemm_kernel<BN, BK><<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
     count_launch();
 }
 
@@ -205,14 +214,13 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
         launch_slices(P, (int)g.M, (int)kc, eP, S, sP, (int)Mp, (int)Kp, s);
         launch_slices(Q, (int)g.N, (int)kc, eQ, S, sQ, (int)Np, (int)Kp, s);
 
-        CUtensorMap mapP, mapQ64, mapQ128;
-        if(!make_slice_map(&mapP, sP, Kp, (int64_t)S * Mp, kOzBM)
-           || !make_slice_map(&mapQ64, sQ, Kp, (int64_t)S * Np, 64)
-           || !make_slice_map(&mapQ128, sQ, Kp, (int64_t)S * Np, 128))
-            return false;
         for(int pi = 0; pi < npass; ++pi)
         {
             const OzPass& q = passes[pi];
+            CUtensorMap   mapP, mapQ;
+            if(!make_slice_map(&mapP, sP, Kp, (int64_t)S * Mp, kOzBM, q.bk)
+               || !make_slice_map(&mapQ, sQ, Kp, (int64_t)S * Np, q.bn, q.bk))
+                return false;
             OzParams p{};
             p.M = (int)g.M;
             p.N = (int)g.N;
@@ -238,9 +246,19 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
             p.tmem_cols = cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : cols <= 256 ? 256 : 512;
             p.error = err_dev;
             if(q.bn == 128)
-                launch_oz_pass<128>(mapP, mapQ128, p, Mp, Np, s);
+            {
+                if(q.bk == 64)
+                    launch_oz_pass<128, 64>(mapP, mapQ, p, Mp, Np, s);
+                else
+                    launch_oz_pass<128, 32>(mapP, mapQ, p, Mp, Np, s);
+            }
             else
-                launch_oz_pass<64>(mapP, mapQ64, p, Mp, Np, s);
+            {
+                if(q.bk == 64)
+                    launch_oz_pass<64, 64>(mapP, mapQ, p, Mp, Np, s);
+                else
+                    launch_oz_pass<64, 32>(mapP, mapQ, p, Mp, Np, s);
+            }
         }
     }
     return true;

@@ -23,10 +23,12 @@ struct Tuning
     int block_always_k       = 128;  // block solver at any parallelism up to this k
     int block_min_strips_pct = 100;  // else block solver if strips * batch >= SMs * pct / 100
     int sliced_min_k         = 1024; // precision form: sliced updates only for K >= this
-    int dmma_big_tile_pct    = 200;  // 128x128 DMMA tiles if tiles >= SMs * pct / 100
+    int dmma_big_tile_pct    = 100000; // 128x128 DMMA tiles if tiles >= SMs * pct / 100
     int mixed_slices         = 7;    // slices of the precision form when the caller passes 0
     int dmma_force_tile      = 0;    // 0: choose; 1..7: force one DMMA tile shape (DmmaTile)
     int dmma_big_bk          = 16;   // k depth of the 128x128 DMMA stage (16 or 32)
+    int oz_bn                = 64;   // sliced GEMM output tile width (64: one pass; 128)
+    int oz_bk                = 64;   // sliced GEMM K step in int8 (32 or 64)
 };
 
 struct TuningEntry
@@ -45,6 +47,8 @@ static const TuningEntry kTuningEntries[] = {
     {"mixed_slices", &Tuning::mixed_slices, 1, 8},
     {"dmma_force_tile", &Tuning::dmma_force_tile, 0, 7},
     {"dmma_big_bk", &Tuning::dmma_big_bk, 16, 32},
+    {"oz_bn", &Tuning::oz_bn, 64, 128},
+    {"oz_bk", &Tuning::oz_bk, 32, 64},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

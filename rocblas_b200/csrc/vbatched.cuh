@@ -1,16 +1,21 @@
 // Variable-size batched TRSM: thousands of independent systems of different (m, n),
-// side, uplo, transA and diag in one persistent kernel.
+// side, uplo, transA and diag in one call.
 //
 // The reference has no variable-size batch API (rocblas_trsm_batched requires one m, n for
 // every entry, library/src/blas3/rocblas_trsm_batched_imp.hpp:57-300), so a caller with
-// uneven systems makes one call per system.  Here one launch pair covers the whole batch:
-//   1. a single-CTA prepass validates every problem descriptor, counts its work items
-//      (strips of 32 right-hand sides) and writes the exclusive prefix sum of those counts;
-//   2. a persistent kernel (grid = SMs x resident CTAs) pulls work-item indices from a
-//      device-side queue head (one atomicAdd per item), maps an item to its (problem,
-//      strip) by binary search over the prefix sum, and runs the one-CTA strip solver
-//      (block_solve.cuh) on it.  There is no inter-CTA waiting, so no wait can hang.
-// Both launches are stream-ordered and capturable in a CUDA graph.
+// uneven systems makes one call per system.  Here one prepass and one persistent launch per
+// size class cover the whole batch:
+//   1. a single-CTA prepass validates every problem descriptor, sorts it into a size class by
+//      its triangle order k (k <= 64, 128, 256, 512), counts its work items (strips of 32
+//      right-hand sides) and writes, per class, the exclusive prefix sum of those counts
+//      (problems of other classes count 0);
+//   2. per class, a persistent kernel (grid = SMs x resident CTAs, shared memory sized for
+//      that class's largest k, so small systems run many CTAs per SM) pulls work-item indices
+//      from the class's device-side queue head (one atomicAdd per item), maps an item to its
+//      (problem, strip) by binary search over the class's prefix sum, and runs the one-CTA
+//      strip solver (block_solve.cuh) on it.  There is no inter-CTA waiting, so no wait can
+//      hang.
+// All launches are stream-ordered and capturable in a CUDA graph.
 #pragma once
 #include "block_solve.cuh"
 
@@ -31,6 +36,29 @@ struct VbState
     int counter; // queue head
     int invalid; // number of rejected descriptors
     int pad[2];
+};
+
+// Size classes of the batch: class c holds the systems with k <= vb_class_kmax(c).
+constexpr int kVbClasses = 4;
+__host__ __device__ constexpr int vb_class_kmax(int c)
+{
+    return 64 << c;
+}
+static_assert(vb_class_kmax(kVbClasses - 1) == kBlockSolveMaxK, "classes cover the strip solver");
+
+__device__ __forceinline__ int vb_class(int k)
+{
+    int c = 0;
+    while(c < kVbClasses - 1 && k > vb_class_kmax(c))
+        ++c;
+    return c;
+}
+
+struct VbClassState
+{
+    int counter[kVbClasses]; // queue head per class
+    int invalid;             // number of rejected descriptors
+    int pad[3];
 };
 
 constexpr int kVbPrepThreads = 1024;
@@ -106,13 +134,75 @@ __global__ void __launch_bounds__(kVbPrepThreads)
         atomicAdd(&st->invalid, bad);
 }
 
+// Per class c: offsets[c * (count + 1) + i] = work items of the class-c problems among
+// 0..i-1; offsets[c * (count + 1) + count] = the class total.
+__global__ void __launch_bounds__(kVbPrepThreads)
+    vb_prepass_classes_kernel(const VbProblem* probs, int count, int max_k, int* offsets,
+                              VbClassState* st)
+{
+    __shared__ int4 part[kVbPrepThreads];
+    const int tid   = threadIdx.x;
+    const int chunk = (count + kVbPrepThreads - 1) / kVbPrepThreads;
+    const int lo = min(count, tid * chunk), hi = min(count, lo + chunk);
+    int       sum[kVbClasses] = {0, 0, 0, 0};
+    int       bad             = 0;
+    static_assert(kVbClasses == 4, "one int4 of partial sums per thread");
+    for(int i = lo; i < hi; ++i)
+    {
+        const VbProblem p = probs[i];
+        if(vb_valid(p, max_k))
+            sum[vb_class(p.side == kLeft ? p.m : p.n)] += vb_items(p);
+        else
+            ++bad;
+    }
+    part[tid] = make_int4(sum[0], sum[1], sum[2], sum[3]);
+    __syncthreads();
+    // inclusive scan of the per-thread sums, four classes at once (Hillis-Steele)
+    for(int off = 1; off < kVbPrepThreads; off <<= 1)
+    {
+        const int4 v = tid >= off ? part[tid - off] : make_int4(0, 0, 0, 0);
+        __syncthreads();
+        int4 w = part[tid];
+        w.x += v.x;
+        w.y += v.y;
+        w.z += v.z;
+        w.w += v.w;
+        part[tid] = w;
+        __syncthreads();
+    }
+    const int4 incl = part[tid];
+    int run[kVbClasses] = {incl.x - sum[0], incl.y - sum[1], incl.z - sum[2], incl.w - sum[3]};
+    const int64_t cstride = (int64_t)count + 1;
+    for(int i = lo; i < hi; ++i)
+    {
+#pragma unroll
+        for(int c = 0; c < kVbClasses; ++c)
+            offsets[c * cstride + i] = run[c];
+        const VbProblem p = probs[i];
+        if(vb_valid(p, max_k))
+            run[vb_class(p.side == kLeft ? p.m : p.n)] += vb_items(p);
+    }
+    if(tid == kVbPrepThreads - 1)
+    {
+        offsets[0 * cstride + count] = incl.x;
+        offsets[1 * cstride + count] = incl.y;
+        offsets[2 * cstride + count] = incl.z;
+        offsets[3 * cstride + count] = incl.w;
+#pragma unroll
+        for(int c = 0; c < kVbClasses; ++c)
+            st->counter[c] = 0;
+    }
+    if(bad)
+        atomicAdd(&st->invalid, bad);
+}
+
 template <typename T>
 struct VbParams
 {
     const VbProblem* probs;
     int              count;
-    const int*       offsets;
-    VbState*         st;
+    const int*       offsets; // count + 1 prefix sums of the work items this launch serves
+    int*             counter; // queue head of this launch
     Scalar<T>        alpha;
 };
 
@@ -126,7 +216,7 @@ __global__ void __launch_bounds__(kBsThreads) vb_persistent_kernel(VbParams<T> p
     for(;;)
     {
         if(threadIdx.x == 0)
-            s_item = atomicAdd(&p.st->counter, 1);
+            s_item = atomicAdd(p.counter, 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
