@@ -49,6 +49,17 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
                  : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+// mma.sync m16n8k16 .f64: the k8 fragments of two consecutive k8 steps side by side,
+// a_{2q+r} = A(g + 8r, t + 4q), b_q = B(t + 4q, g) for q = 0..3, r = 0..1.
+__device__ __forceinline__ void dmma_16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4])
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+                 "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+                 : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+                   "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK = kDBK>
 struct DmmaCfg
 {
@@ -96,7 +107,7 @@ __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, in
     }
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK>
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK, int MK>
 __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads,
                                   DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads <= 256 ? 2 : 1)
     gemm_dmma_kernel(GemmParams<double> p)
@@ -160,6 +171,40 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>:
             __syncthreads();
             const double* sA = smem + (kt % STAGES) * Cfg::kStage;
             const double* sB = sA + Cfg::kStageA;
+            if constexpr(MK == 16)
+            {
+#pragma unroll
+                for(int ks = 0; ks < BK / 16; ++ks)
+                {
+                    const int k = ks * 16 + t;
+                    double    fa[TM][8], fb[TN][4];
+#pragma unroll
+                    for(int i = 0; i < TM; ++i)
+                    {
+                        const int m = wm * WM + i * 16 + g;
+#pragma unroll
+                        for(int q = 0; q < 4; ++q)
+                        {
+                            fa[i][2 * q]     = ldA(sA, m, k + 4 * q);
+                            fa[i][2 * q + 1] = ldA(sA, m + 8, k + 4 * q);
+                        }
+                    }
+#pragma unroll
+                    for(int j = 0; j < TN; ++j)
+                    {
+                        const int n = wn * WN + j * 8 + g;
+#pragma unroll
+                        for(int q = 0; q < 4; ++q)
+                            fb[j][q] = ldB(sB, n, k + 4 * q);
+                    }
+#pragma unroll
+                    for(int i = 0; i < TM; ++i)
+#pragma unroll
+                        for(int j = 0; j < TN; ++j)
+                            dmma_16x8x16(acc[i][j], fa[i], fb[j]);
+                }
+            }
+            else
 #pragma unroll
             for(int ks = 0; ks < BK / 8; ++ks)
             {
@@ -221,11 +266,11 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>:
 }
 
 // ---- launch --------------------------------------------------------------------------------
-template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK = kDBK>
+template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK = kDBK, int MK = 8>
 static void launch_dmma_cfg(const GemmParams<double>& p0, int batch, cudaStream_t s)
 {
     using Cfg = DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>;
-    auto kern = gemm_dmma_kernel<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>;
+    auto kern = gemm_dmma_kernel<BM, BN, WM, WN, STAGES, KCP, KCQ, BK, MK>;
     cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
     for(int b0 = 0; b0 < batch; b0 += 65535)
     {
@@ -245,8 +290,13 @@ enum class DmmaTile
     t64x64,
     t128x32,
     t32x128,
-    t128x128k32
+    t128x128k32,
+    t128x64w64, // 4 warps of 64 x 32
+    t64x128w64, // 4 warps of 32 x 64
+    t64x64w64,  // 2 warps of 64 x 32
+    t64x64k16   // as t64x64 with mma.sync m16n8k16
 };
+constexpr int kDmmaTiles = 11;
 
 template <bool KCP, bool KCQ>
 static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch, cudaStream_t s)
@@ -260,6 +310,10 @@ static void launch_dmma_tile(DmmaTile t, const GemmParams<double>& p, int batch,
     case DmmaTile::t128x32:  launch_dmma_cfg<128, 32, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t32x128:  launch_dmma_cfg<32, 128, 32, 32, 4, KCP, KCQ>(p, batch, s); break;
     case DmmaTile::t128x128k32: launch_dmma_cfg<128, 128, 32, 32, 3, KCP, KCQ, 32>(p, batch, s); break;
+    case DmmaTile::t128x64w64: launch_dmma_cfg<128, 64, 64, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t64x128w64: launch_dmma_cfg<64, 128, 32, 64, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t64x64w64:  launch_dmma_cfg<64, 64, 64, 32, 4, KCP, KCQ>(p, batch, s); break;
+    case DmmaTile::t64x64k16:  launch_dmma_cfg<64, 64, 32, 32, 4, KCP, KCQ, 16, 16>(p, batch, s); break;
     }
 }
 
@@ -269,14 +323,14 @@ static DmmaTile choose_dmma_tile(int64_t M, int64_t N, int64_t batch, int sms, b
 {
     auto tiles = [&](int bm, int bn) { return ceil_div(M, bm) * ceil_div(N, bn) * batch; };
     const int forced = tuning().dmma_force_tile;
-    if(forced >= 1 && forced <= 7)
+    if(forced >= 1 && forced <= kDmmaTiles)
     {
         const DmmaTile f = (DmmaTile)forced;
         // a forced tile must still respect the in-place constraint of the invA leaves
         const bool spans_m = f == DmmaTile::t128x128 || f == DmmaTile::t128x64 || f == DmmaTile::t128x32
-                             || f == DmmaTile::t128x128k32;
+                             || f == DmmaTile::t128x128k32 || f == DmmaTile::t128x64w64;
         const bool spans_n = f == DmmaTile::t128x128 || f == DmmaTile::t64x128 || f == DmmaTile::t32x128
-                             || f == DmmaTile::t128x128k32;
+                             || f == DmmaTile::t128x128k32 || f == DmmaTile::t64x128w64;
         if((!full_m || spans_m) && (!full_n || spans_n))
             return f;
     }

@@ -19,9 +19,12 @@
 // bits, S = 8 gives 56 bits (beyond FP64 rounding of a K-term dot product).
 //
 // Kernel layout (one CTA per 128 x BN output tile, BN = 64 or 128, 192 threads):
-//   warp 0   TMA producer: per BK-deep K step (BK = 32 or 64 int8, SWIZZLE_32B / _64B rows)
-//            it loads the slices the pass needs of the P tile (128 x BK) and of the Q tile
-//            (BN x BK) into one stage of a ring;
+//   warp 0   copy producer: per BK-deep K step (BK = 32 or 64 int8) it brings the slices the
+//            pass needs of the P tile (128 x BK) and of the Q tile (BN x BK) into one stage of
+//            a ring.  The slicing kernel writes every slice as K panels of BK-byte rows that
+//            are already in the tensor cores' swizzled shared-memory order (SWIZZLE_32B /
+//            _64B), so each tile is one contiguous block and one bulk copy
+//            (cp.async.bulk ... complete_tx) per tile replaces a row-by-row tensor copy;
 //   warp 1   TMEM owner and MMA issuer: one 128 x BN int32 accumulator per slice-pair group
 //            d = s + t of the pass, group d at TMEM column (d - d_lo) * BN.  The Q slices of
 //            a stage sit back to back, so Q slices t0..t0+c-1 form one (c * BN)-row operand and
@@ -36,7 +39,6 @@
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its
 // in-flight copies and MMAs (again bounded), frees TMEM and returns.
 #pragma once
-#include <cuda.h>
 #include <cstdint>
 
 #include "common.cuh"
@@ -60,7 +62,10 @@ struct OzParams
     int      S;                // slices (1..8)
     int      d_lo, d_hi;       // slice-pair groups d = s + t computed by this pass
     int      ns;               // slices staged per operand: min(S, d_hi)
-    int      M_pad, N_pad;     // slice-buffer row counts (multiples of 128 / 64)
+    int      M_pad, N_pad;     // slice-buffer row counts (multiples of 128)
+    const int8_t* sliceP;      // S panels sets of P: [s][K / BK][M_pad][BK], swizzled rows
+    const int8_t* sliceQ;      // the same for Q with N_pad rows
+    int      nkc;              // K panels per slice (K_pad / BK)
     const int* exp_rows;       // e_r, M entries
     const int* exp_cols;       // f_c, N entries
     double*  C;                // output (column-major, ldc)
@@ -115,12 +120,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, uint64_t* bar,
-                                            int x, int y)
+// Contiguous global -> shared copy of `bytes` (multiple of 16, both addresses 16-byte
+// aligned) that completes on `bar` (transaction count).
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
-                 "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
 
@@ -179,10 +185,12 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN, int BK>
+// SC > 0: a single pass over all SC slices (d_lo = 0, d_hi = SC) with the slice count known
+// at compile time, so the MMA and copy schedules unroll into straight-line code; SC = 0: the
+// pass and slice count come from p at run time.
+template <int BN, int BK, int SC>
 __global__ void __launch_bounds__(kOzThreads, 1)
-    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapP, const __grid_constant__ CUtensorMap mapQ,
-                      OzParams p)
+    ozaki_gemm_kernel(const __grid_constant__ OzParams p)
 {
     constexpr int kTileA = kOzBM * BK; // bytes per slice tile of P
     constexpr int kTileB = BN * BK;    // bytes per slice tile of Q
@@ -191,7 +199,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     // 1 KB alignment for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S         = p.ns; // slices staged per operand in this pass
+    const int S   = SC > 0 ? SC : p.ns; // slices staged per operand in this pass
+    const int DLO = SC > 0 ? 0 : p.d_lo;
+    const int DHI = SC > 0 ? SC : p.d_hi;
     const int stage_bytes = S * (kTileA + kTileB);
     const int NS        = p.stages;
 
@@ -248,11 +258,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     break;
                 unsigned char* base = smem + st * stage_bytes;
                 mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
+                // slice s, K panel i: rows at ((s * nkc + i) * rows_pad + row) * BK
+                const int8_t* srcP = p.sliceP + ((int64_t)i * p.M_pad + m0) * BK;
+                const int8_t* srcQ = p.sliceQ + ((int64_t)i * p.N_pad + n0) * BK;
+                const int64_t slP = (int64_t)p.nkc * p.M_pad * BK, slQ = (int64_t)p.nkc * p.N_pad * BK;
+#pragma unroll
                 for(int s = 0; s < S; ++s)
-                    tma_load_2d(base + s * kTileA, &mapP, &full_bar[st], i * BK, s * p.M_pad + m0);
+                    bulk_load(base + s * kTileA, srcP + s * slP, kTileA, &full_bar[st]);
+#pragma unroll
                 for(int t = 0; t < S; ++t)
-                    tma_load_2d(base + S * kTileA + t * kTileB, &mapQ, &full_bar[st], i * BK,
-                                t * p.N_pad + n0);
+                    bulk_load(base + S * kTileA + t * kTileB, srcQ + t * slQ, kTileB, &full_bar[st]);
                 *(volatile int*)&issued = i + 1;
             }
         }
@@ -262,7 +277,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         // ---------------- MMA issuer ----------------
         if(lane == 0)
         {
-            uint32_t touched = 0; // groups whose accumulator holds data
+            // descriptors of stage 0's first P and Q tiles; every other tile is a constant
+            // offset (start address field = byte address / 16, no carry out of its 14 bits)
+            const uint64_t desc_a0 = oz_smem_desc<BK>(smem_u32(smem));
+            const uint64_t desc_b0 = oz_smem_desc<BK>(smem_u32(smem) + S * kTileA);
             int i = 0;
             for(; i < nk; ++i)
             {
@@ -276,30 +294,28 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 *(volatile int*)&consumed = i + 1;
-                const uint32_t abase = smem_u32(smem + st * stage_bytes);
-                const uint32_t bbase = abase + S * kTileA;
+                const uint64_t soff = (uint64_t)((st * stage_bytes) >> 4);
+                // P slice 0 comes first in every K step and covers every group of the pass, so
+                // only its first MMA of the first K step starts the accumulators
+                const uint32_t acc0 = i > 0 ? 1u : 0u;
+#pragma unroll
                 for(int s = 0; s < S; ++s)
                 {
                     // Q slices t with d_lo <= s + t < d_hi, in runs of at most kMerge
-                    const int t_lo = max(0, p.d_lo - s), t_hi = min(S - 1, p.d_hi - 1 - s);
+                    const int t_lo = max(0, DLO - s), t_hi = min(S - 1, DHI - 1 - s);
+#pragma unroll
                     for(int t0 = t_lo; t0 <= t_hi; t0 += kMerge)
                     {
                         const int      c     = min(kMerge, t_hi - t0 + 1);
-                        const int      g0    = s + t0 - p.d_lo; // first group of the run
-                        const uint32_t run   = ((1u << c) - 1u) << g0;
-                        const uint32_t dcol  = tmem + (uint32_t)(g0 * BN);
+                        const uint32_t dcol  = tmem + (uint32_t)((s + t0 - DLO) * BN);
                         const uint32_t idesc = oz_idesc(c * BN);
-                        // P slice 0 comes first and covers every group of the pass, so a run
-                        // is either wholly fresh or wholly accumulated
-                        const uint32_t accum = (touched & run) ? 1u : 0u;
 #pragma unroll
                         for(int kk = 0; kk < BK / kOzMmaK; ++kk)
                         {
-                            const uint64_t ad = oz_smem_desc<BK>(abase + s * kTileA + kk * kOzMmaK);
-                            const uint64_t bd = oz_smem_desc<BK>(bbase + t0 * kTileB + kk * kOzMmaK);
-                            oz_mma(dcol, ad, bd, idesc, (kk > 0) ? 1u : accum);
+                            const uint64_t ad = desc_a0 + soff + (uint64_t)((s * kTileA + kk * kOzMmaK) >> 4);
+                            const uint64_t bd = desc_b0 + soff + (uint64_t)((t0 * kTileB + kk * kOzMmaK) >> 4);
+                            oz_mma(dcol, ad, bd, idesc, (s == 0 && kk == 0) ? acc0 : 1u);
                         }
-                        touched |= run;
                     }
                 }
                 oz_commit(&empty_bar[st]);
@@ -337,10 +353,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 #pragma unroll
                 for(int j = 0; j < 32; ++j)
                     h[j] = 0.0;
-                for(int d = p.d_hi - 1; d >= p.d_lo; --d)
+#pragma unroll 1
+                for(int d = DHI - 1; d >= DLO; --d)
                 {
                     uint32_t v[32];
-                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)((d - p.d_lo) * BN + half * 32), v);
+                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)((d - DLO) * BN + half * 32), v);
 #pragma unroll
                     for(int j = 0; j < 32; ++j)
                         h[j] = fma(h[j], 0x1p-7, (double)(int)v[j]);
@@ -355,7 +372,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         {
                             double* cp = p.C + gr + (int64_t)gc * p.ldc;
                             const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
-                            const double pq = ldexp(h[j], er + ec - 14 - 7 * p.d_lo);
+                            const double pq = ldexp(h[j], er + ec - 14 - 7 * DLO);
                             double out;
                             if(zero)
                                 out = 0.0;
@@ -433,10 +450,25 @@ __global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, in
     oz_merge_exp(exps, o, mx);
 }
 
-// Slices: dst[s][o][k] (int8, row pitch K_pad, slice stride O_pad * K_pad).  Rows o >= O and
-// columns k >= K are written as zero.  A 64 x 64 tile goes through shared memory so that
-// both the double reads and the int8 writes are coalesced whatever (so, sk) is.
+// Slices: slice s of row o, k lives in the K panel kc = k / BK as dst[((s * K_pad / BK + kc)
+// * O_pad + o) * BK + swizzled(k % BK)]: every panel is the row-major image of O_pad rows of
+// BK bytes with the 16-byte chunks of row o permuted the way the tensor cores' shared-memory
+// layout (SWIZZLE_64B for BK = 64, SWIZZLE_32B for BK = 32) expects, so a tile of whole
+// 8-row groups copies verbatim into 1 KB-aligned shared memory.  Rows o >= O and columns
+// k >= K are written as zero.  A 64 x 64 tile goes through shared memory so that both the
+// double reads and the int8 writes are coalesced whatever (so, sk) is.
 constexpr int kOzSliceTile = 64;
+
+// 16-byte chunk c (of BK / 16) of row o lands at chunk oz_swizzle_chunk<BK>(o, c): the
+// address bits [4, 4 + log2(BK / 16)) are XORed with bits [7, ...) of the row's offset
+// (row * BK), the 32B / 64B swizzle patterns of the UMMA shared-memory descriptor.
+template <int BK>
+__host__ __device__ constexpr int oz_swizzle_chunk(int o, int c)
+{
+    return BK == 64 ? (c ^ ((o >> 1) & 3)) : (c ^ ((o >> 2) & 1));
+}
+
+template <int BK>
 __global__ void __launch_bounds__(256)
     oz_slice_kernel(const double* src, int64_t so, int64_t sk, int O, int K, const int* exps, int S,
                     int8_t* dst, int O_pad, int K_pad)
@@ -485,11 +517,15 @@ __global__ void __launch_bounds__(256)
             }
         }
     }
+    const int k   = k0 + kq;              // first of this thread's 16 k (one chunk)
+    const int kc  = k / BK, c = (k % BK) / 16;
+    const int64_t nkc = K_pad / BK;
+    const int64_t off = (int64_t)o * BK + oz_swizzle_chunk<BK>(o, c) * 16;
     for(int s = 0; s < S; ++s)
     {
         uint4 w4 = make_uint4(words[s][0], words[s][1], words[s][2], words[s][3]);
-        if(k0 + kq < K_pad)
-            *reinterpret_cast<uint4*>(dst + (int64_t)s * O_pad * K_pad + (int64_t)o * K_pad + k0 + kq) = w4;
+        if(k < K_pad)
+            *reinterpret_cast<uint4*>(dst + ((int64_t)s * nkc + kc) * O_pad * BK + off) = w4;
     }
 }
 

@@ -228,7 +228,7 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     if(ws_bytes)
     {
         ws = h->borrow(ws_bytes);
-        if(!ws)
+        if(!ws && !have_invA)
         {
             // backup: recursive solve with block-solver leaves needs no workspace
             perf = rocblas_status_perf_degraded;
@@ -243,6 +243,7 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     }
     if(have_invA)
         pr.invA = invA;
+    pr.err_dev = h->err_dev;
     trsm_run<T>(pr, ws, have_invA);
     st = launch_status();
     return st != rocblas_status_success ? st : perf;
@@ -771,6 +772,9 @@ try
             h->device   = dev;
             h->sm_count = prop.multiProcessorCount;
         }
+        // the device error word of the bounded waits exists from the start, so no call made
+        // under stream capture has to allocate it
+        ensure_err(h);
     }
     cudaGetLastError();
     *handle = h;

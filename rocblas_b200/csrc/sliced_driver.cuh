@@ -1,7 +1,6 @@
 // Host side of the sliced (integer-slice, tensor-core) FP64 GEMM and of the precision form
 // of the TRSM that uses it for its trailing updates.
 #pragma once
-#include <cuda.h>
 #include <mutex>
 
 #include "ozaki_gemm.cuh"
@@ -9,27 +8,6 @@
 
 namespace rb200
 {
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda link)
-static EncodeTiledFn encode_tiled_fn()
-{
-    static EncodeTiledFn  fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void*                            p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess
-           && q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-        cudaGetLastError();
-    });
-    return fn;
-}
 
 // Element (o, k) of an operand at ptr[o * so + k * sk].
 struct SliceOperand
@@ -101,28 +79,14 @@ static void launch_exponents(SliceOperand X, int O, int K, int* exps, cudaStream
 }
 
 static void launch_slices(SliceOperand X, int O, int K, const int* exps, int S, int8_t* dst, int O_pad,
-                          int K_pad, cudaStream_t s)
+                          int K_pad, int bk, cudaStream_t s)
 {
     dim3 grid((unsigned)(K_pad / kOzSliceTile), (unsigned)(O_pad / kOzSliceTile));
-    oz_slice_kernel<<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    if(bk == 64)
+        oz_slice_kernel<64><<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    else
+        oz_slice_kernel<32><<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
     count_launch();
-}
-
-static bool make_slice_map(CUtensorMap* map, void* base, int64_t K_pad, int64_t rows, int box_rows,
-                           int bk)
-{
-    EncodeTiledFn enc = encode_tiled_fn();
-    if(!enc)
-        return false;
-    cuuint64_t dims[2]    = {(cuuint64_t)K_pad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)K_pad};
-    cuuint32_t box[2]     = {(cuuint32_t)bk, (cuuint32_t)box_rows};
-    cuuint32_t estr[2]    = {1, 1};
-    return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE,
-               bk == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
-               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
-           == CUDA_SUCCESS;
 }
 
 // One pass of the slice-pair groups [d_lo, d_hi) with output tiles 128 x bn and K steps of bk.
@@ -142,19 +106,18 @@ static int oz_stage_bytes(int ns, int bn, int bk)
 static int plan_oz_passes(int S, OzPass* out)
 {
     const int bn = tuning().oz_bn == 128 ? 128 : 64;
-    const int bk = tuning().oz_bk == 32 ? 32 : 64;
+    int       bk = tuning().oz_bk == 32 ? 32 : 64;
+    const int npass = S * bn <= 512 ? 1 : 2;
+    const int ns_max = S; // the last pass stages every slice
+    // one K depth for all passes (they share the slice panels): 64 if two stages fit
+    if(2 * oz_stage_bytes(ns_max, bn, bk) + 1024 > kOzSmemBudget)
+        bk = 32;
     auto make = [&](int lo, int hi) {
         OzPass q{lo, hi, bn, bk, std::min(S, hi), 0};
-        q.stages = (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn, q.bk);
-        if(q.stages < 2 && q.bk == 64)
-        {
-            q.bk     = 32;
-            q.stages = (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn, q.bk);
-        }
-        q.stages = std::min(8, q.stages);
+        q.stages = std::min(8, (kOzSmemBudget - 1024) / oz_stage_bytes(q.ns, q.bn, q.bk));
         return q;
     };
-    if(S * bn <= 512)
+    if(npass == 1)
     {
         out[0] = make(0, S);
         return 1;
@@ -164,20 +127,43 @@ static int plan_oz_passes(int S, OzPass* out)
     return 2;
 }
 
-template <int BN, int BK>
-static void launch_oz_pass(const CUtensorMap& mapP, const CUtensorMap& mapQ, const OzParams& p,
-                           int64_t Mp, int64_t Np, cudaStream_t s)
+template <int BN, int BK, int SC>
+static void launch_oz_kernel(const OzParams& p, int64_t Mp, int64_t Np, cudaStream_t s)
 {
     const size_t smem = (size_t)p.stages * oz_stage_bytes(p.ns, BN, BK) + 1024;
-    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN, BK>,
+    cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN, BK, SC>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / BN));
-    ozaki_gemm_kernel<BN, BK><<<grid, kOzThreads, smem, s>>>(mapP, mapQ, p);
+    ozaki_gemm_kernel<BN, BK, SC><<<grid, kOzThreads, smem, s>>>(p);
     count_launch();
 }
 
+// A single pass over all slices with BN = 64 uses the schedule unrolled for its slice count.
+template <int BN, int BK>
+static void launch_oz_pass(const OzParams& p, int64_t Mp, int64_t Np, cudaStream_t s)
+{
+    if constexpr(BN == 64)
+    {
+        if(p.d_lo == 0 && p.d_hi == p.S && p.ns == p.S)
+        {
+            switch(p.S)
+            {
+            case 1: return launch_oz_kernel<BN, BK, 1>(p, Mp, Np, s);
+            case 2: return launch_oz_kernel<BN, BK, 2>(p, Mp, Np, s);
+            case 3: return launch_oz_kernel<BN, BK, 3>(p, Mp, Np, s);
+            case 4: return launch_oz_kernel<BN, BK, 4>(p, Mp, Np, s);
+            case 5: return launch_oz_kernel<BN, BK, 5>(p, Mp, Np, s);
+            case 6: return launch_oz_kernel<BN, BK, 6>(p, Mp, Np, s);
+            case 7: return launch_oz_kernel<BN, BK, 7>(p, Mp, Np, s);
+            case 8: return launch_oz_kernel<BN, BK, 8>(p, Mp, Np, s);
+            default: break;
+            }
+        }
+    }
+    launch_oz_kernel<BN, BK, 0>(p, Mp, Np, s);
+}
+
 // Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
-// Returns false if the tensor-map encoder is unavailable.
 static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream_t s)
 {
     if(g.M <= 0 || g.N <= 0)
@@ -211,17 +197,17 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
             cudaMemsetAsync(eP, 0, 4 * Mp, s);
             cudaMemsetAsync(eQ, 0, 4 * Np, s);
         }
-        launch_slices(P, (int)g.M, (int)kc, eP, S, sP, (int)Mp, (int)Kp, s);
-        launch_slices(Q, (int)g.N, (int)kc, eQ, S, sQ, (int)Np, (int)Kp, s);
+        const int bk = passes[0].bk;
+        launch_slices(P, (int)g.M, (int)kc, eP, S, sP, (int)Mp, (int)Kp, bk, s);
+        launch_slices(Q, (int)g.N, (int)kc, eQ, S, sQ, (int)Np, (int)Kp, bk, s);
 
         for(int pi = 0; pi < npass; ++pi)
         {
             const OzPass& q = passes[pi];
-            CUtensorMap   mapP, mapQ;
-            if(!make_slice_map(&mapP, sP, Kp, (int64_t)S * Mp, kOzBM, q.bk)
-               || !make_slice_map(&mapQ, sQ, Kp, (int64_t)S * Np, q.bn, q.bk))
-                return false;
-            OzParams p{};
+            OzParams      p{};
+            p.sliceP = sP;
+            p.sliceQ = sQ;
+            p.nkc    = (int)(Kp / q.bk);
             p.M = (int)g.M;
             p.N = (int)g.N;
             p.K = (int)std::max<int64_t>(kc, 1);
@@ -248,16 +234,16 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
             if(q.bn == 128)
             {
                 if(q.bk == 64)
-                    launch_oz_pass<128, 64>(mapP, mapQ, p, Mp, Np, s);
+                    launch_oz_pass<128, 64>(p, Mp, Np, s);
                 else
-                    launch_oz_pass<128, 32>(mapP, mapQ, p, Mp, Np, s);
+                    launch_oz_pass<128, 32>(p, Mp, Np, s);
             }
             else
             {
                 if(q.bk == 64)
-                    launch_oz_pass<64, 64>(mapP, mapQ, p, Mp, Np, s);
+                    launch_oz_pass<64, 64>(p, Mp, Np, s);
                 else
-                    launch_oz_pass<64, 32>(mapP, mapQ, p, Mp, Np, s);
+                    launch_oz_pass<64, 32>(p, Mp, Np, s);
             }
         }
     }

@@ -39,12 +39,11 @@ constexpr int kChainNB      = 128;
 
 struct ChainParams
 {
-    const double* A;
-    int64_t       lda, strideA;
-    const double* invA;       // blocks of 128 x 128, ld 128
-    int64_t       strideInv;  // per system
-    double*       B;
-    int64_t       ldb, strideB;
+    BatchPtr<double> A;
+    int64_t          lda;
+    BatchPtr<double> invA;    // blocks of 128 x 128, ld 128
+    BatchPtr<double> B;
+    int64_t          ldb;
     int           k;          // triangle order
     int           ncols;      // right-hand sides (n for side L, m for side R)
     int           nb, ns;     // blocks, strips
@@ -123,9 +122,9 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
         const int     bs    = min(kChainNB, p.k - r0);
         const int     c0    = strip * W;
         const int     wv    = min(W, p.ncols - c0);
-        const double* A     = p.A + sys * p.strideA;
-        const double* inv   = p.invA + sys * p.strideInv + (int64_t)b * kChainNB * kChainNB;
-        double*       B     = p.B + sys * p.strideB;
+        const double* A     = p.A.get((int)sys);
+        const double* inv   = p.invA.get((int)sys) + (int64_t)b * kChainNB * kChainNB;
+        double*       B     = p.B.get((int)sys);
         int*          flags = p.flags + sys * (int64_t)p.nb * p.ns;
 
         // M(r, c) and C(r, col) addresses
@@ -297,7 +296,7 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
                     const int n = wn * WN + jn * 8 + 2 * t + (e & 1);
                     double    v = 0.0;
                     if(!zero && o < bs && n < wv)
-                        v = alpha * *caddr(r0 + o, c0 + n) - acc[i][jn][e];
+                        v = alpha * __ldcg(caddr(r0 + o, c0 + n)) - acc[i][jn][e];
                     Ts[o * Cfg::kPitchT + n] = v;
                 }
 
@@ -399,8 +398,8 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
     }
 }
 
-// Blocks, strips and the workspace of one chain solve: flags (systems * nb * ns ints) and an
-// 8-byte counter.
+// Blocks, strips and the workspace of one chain solve: flags (systems * nb * ns ints), then
+// (8-byte aligned) the 8-byte claim counter and a spare error word.
 struct ChainShape
 {
     int     nb, ns, w;
@@ -419,7 +418,7 @@ inline ChainShape chain_shape(int k, int ncols, int batch, int w)
 
 inline size_t chain_workspace_bytes(const ChainShape& c)
 {
-    return (size_t)c.items * sizeof(int) + 16;
+    return ((size_t)c.items * sizeof(int) + 7) / 8 * 8 + 16;
 }
 
 template <int W, bool KCP, bool KCQ>

@@ -27,6 +27,7 @@
 #include "gemm_dmma.cuh"
 #include "gemm_tile.cuh"
 #include "handle.hpp"
+#include "trsm_chain.cuh"
 #include "trtri_block.cuh"
 #include "tuning.hpp"
 
@@ -57,6 +58,7 @@ struct TrsmProblem
     BatchPtr<T> invA; // valid() when blocks are available (workspace or supplied)
     cudaStream_t stream;
     int         sm_count;
+    int*        err_dev;  // device error word of the bounded waits (or nullptr)
     int         k() const { return side_left ? m : n; }
     // op(A) lower?
     int oplower() const { return (!upper) != (trans != 0); }
@@ -300,16 +302,47 @@ static Algo choose_algo(const TrsmProblem<T>& pr)
                                                                          : Algo::recursive;
 }
 
-// Workspace bytes the call wants: invA for the recursive path unless supplied.
+// The recursive solve with few right-hand sides runs as one chain launch (trsm_chain.cuh)
+// when invA is available: FP64, more than one 128-row block, at most chain_max_cols columns.
 template <typename T>
-static size_t trsm_workspace_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
+static bool use_chain(const TrsmProblem<T>& pr)
+{
+    if(!std::is_same<T, double>::value || choose_algo(pr) != Algo::recursive)
+        return false;
+    const int64_t ncols = pr.side_left ? pr.n : pr.m;
+    return pr.k() > kInvNB && ncols <= tuning().chain_max_cols;
+}
+
+template <typename T>
+static ChainShape chain_shape_of(const TrsmProblem<T>& pr)
+{
+    const int ncols = pr.side_left ? pr.n : pr.m;
+    const int t     = tuning().chain_w;
+    const int w     = t == 32 || t == 64 ? t : (ncols <= 32 ? 32 : 64);
+    return chain_shape(pr.k(), ncols, pr.batch, w);
+}
+
+// Workspace bytes the call wants: invA for the recursive path unless supplied, then the
+// chain's flags when the chain runs.
+template <typename T>
+static size_t trsm_invA_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
 {
     if(choose_algo(pr) != Algo::recursive || have_supplied_invA)
         return 0;
     return (size_t)kInvNB * (size_t)pr.k() * sizeof(T) * (size_t)pr.batch;
 }
 
-// Run the solve.  `ws` is the workspace (nullptr => degraded path).
+template <typename T>
+static size_t trsm_workspace_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
+{
+    size_t b = trsm_invA_bytes(pr, have_supplied_invA);
+    if(use_chain(pr))
+        b = (b + 255) / 256 * 256 + chain_workspace_bytes(chain_shape_of(pr));
+    return b;
+}
+
+// Run the solve.  `ws` is the workspace of trsm_workspace_bytes (nullptr => without it: the
+// supplied invA if any, else the degraded path).
 template <typename T>
 static void trsm_run(TrsmProblem<T> pr, void* ws, bool supplied_invA)
 {
@@ -331,6 +364,45 @@ static void trsm_run(TrsmProblem<T> pr, void* ws, bool supplied_invA)
         }
         else
             pr.invA = BatchPtr<T>{};
+    }
+    if constexpr(std::is_same<T, double>::value)
+    {
+        if(ws && pr.invA.valid() && use_chain(pr))
+        {
+            const size_t     off = (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
+            const ChainShape cs  = chain_shape_of(pr);
+            int*             flags = reinterpret_cast<int*>(reinterpret_cast<char*>(ws) + off);
+            const size_t     fbytes = chain_workspace_bytes(cs);
+            cudaMemsetAsync(flags, 0, fbytes, pr.stream);
+            ChainParams c{};
+            c.A       = pr.A;
+            c.lda     = pr.lda;
+            c.invA    = pr.invA;
+            c.B       = pr.B;
+            c.ldb     = pr.ldb;
+            c.k       = k;
+            c.ncols   = pr.side_left ? pr.n : pr.m;
+            c.nb      = cs.nb;
+            c.ns      = cs.ns;
+            c.forward = pr.side_left ? pr.oplower() : !pr.oplower();
+            c.items   = cs.items;
+            c.alpha   = pr.alpha;
+            c.flags   = flags;
+            // the 8-byte claim counter and the error word follow the flags
+            const size_t tail = ((size_t)cs.items * sizeof(int) + 7) / 8 * 8;
+            c.counter = reinterpret_cast<int*>(reinterpret_cast<char*>(flags) + tail);
+            // the error word: the handle's, else a slot after the counter
+            c.error   = pr.err_dev ? pr.err_dev : c.counter + 2;
+            // KCP: M's column index (K) is contiguous in memory when M(r, c) = A(c, r)
+            const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
+            const bool kcq = pr.side_left != 0;
+            if(cs.w == 32)
+                launch_chain_w<32>(c, tM, kcq, pr.sm_count, pr.stream);
+            else
+                launch_chain_w<64>(c, tM, kcq, pr.sm_count, pr.stream);
+            count_launch();
+            return;
+        }
     }
     Recursive<T> rec{pr, k, (int)ceil_div(k, kInvNB)};
     rec.solve(0, rec.nblk, 1);

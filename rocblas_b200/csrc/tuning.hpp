@@ -25,10 +25,12 @@ struct Tuning
     int sliced_min_k         = 1024; // precision form: sliced updates only for K >= this
     int dmma_big_tile_pct    = 100000; // 128x128 DMMA tiles if tiles >= SMs * pct / 100
     int mixed_slices         = 7;    // slices of the precision form when the caller passes 0
-    int dmma_force_tile      = 0;    // 0: choose; 1..7: force one DMMA tile shape (DmmaTile)
+    int dmma_force_tile      = 0;    // 0: choose; 1..11: force one DMMA tile shape (DmmaTile)
     int dmma_big_bk          = 16;   // k depth of the 128x128 DMMA stage (16 or 32)
     int oz_bn                = 64;   // sliced GEMM output tile width (64: one pass; 128)
     int oz_bk                = 64;   // sliced GEMM K step in int8 (32 or 64)
+    int chain_max_cols       = 512;  // FP64 recursive solves with <= this many columns: chain
+    int chain_w              = 0;    // chain strip width: 0 auto (32 or 64), 32, 64
 };
 
 struct TuningEntry
@@ -45,10 +47,12 @@ static const TuningEntry kTuningEntries[] = {
     {"sliced_min_k", &Tuning::sliced_min_k, 1, 1 << 30},
     {"dmma_big_tile_pct", &Tuning::dmma_big_tile_pct, 1, 100000},
     {"mixed_slices", &Tuning::mixed_slices, 1, 8},
-    {"dmma_force_tile", &Tuning::dmma_force_tile, 0, 7},
+    {"dmma_force_tile", &Tuning::dmma_force_tile, 0, 11},
     {"dmma_big_bk", &Tuning::dmma_big_bk, 16, 32},
     {"oz_bn", &Tuning::oz_bn, 64, 128},
     {"oz_bk", &Tuning::oz_bk, 32, 64},
+    {"chain_max_cols", &Tuning::chain_max_cols, 0, 1 << 30},
+    {"chain_w", &Tuning::chain_w, 0, 64},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

@@ -10,7 +10,8 @@ torch = pytest.importorskip("torch")
 import rocblas_b200 as rb  # noqa: E402
 
 pytestmark = pytest.mark.gpu
-TILES = {1: "128x128", 2: "128x64", 3: "64x128", 4: "64x64", 5: "128x32", 6: "32x128", 7: "128x128/bk32"}
+TILES = {1: "128x128", 2: "128x64", 3: "64x128", 4: "64x64", 5: "128x32", 6: "32x128", 7: "128x128/bk32",
+         8: "128x64/warp64x32", 9: "64x128/warp32x64", 10: "64x64/warp64x32", 11: "64x64/k16"}
 
 
 def _gemm(h, ta, tb, m, n, k, alpha, A, B, beta, C):
