@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 M, N = 16384, 4096
 FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the sliced GEMM
+# kernel from one ncu capture; None until a capture of the bench's own launches exists
+SLICED_TRAFFIC_PER_LAUNCH = None
+SLICED_TRAFFIC_SOURCE = None
+
 
 def workload_name():
     return f"dtrsm L/L/N/N m={M} n={N} lda=ldb={M} alpha=1 (condition band k=0)"
@@ -98,6 +103,29 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    """The pool's measured peaks (HBM copy GB/s, bf16 dense TF/s burst and sustained)."""
+    out = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+           "source": "fallback (earlier measurement on this pool)"}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained"):
+            out[k] = float(d[k])
+        out["source"] = "MEASURED_PEAKS.json"
+    except (OSError, KeyError, ValueError):
+        pass
+    return out
+
+
+def kernel_timing(L, cls):
+    """(total ms, total work, launches) of one kernel class since timing was enabled."""
+    ms, work, n = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_int(0)
+    assert L.rocblas_b200_kernel_timing_query(cls.encode(), ctypes.byref(ms), ctypes.byref(work),
+                                              ctypes.byref(n)) == 0
+    return ms.value, work.value, n.value
 
 
 def fp64_peak_tflops(torch, dev):
@@ -390,14 +418,29 @@ def run_ours(args):
         return total, [ev_m[i].elapsed_time(ev_e[i]) for i in range(steps)], launches
 
     # ---- timed region: the precision form (headline), then the plain FP64 form ---------------
+    # Every launch of the dominant kernels is bracketed by CUDA events on its stream inside the
+    # timed region (rocblas_b200_kernel_timing_*), for the roofline of the kernel itself.
     sampler = ClockSampler(dev.index if dev.index is not None else 0)
     sampler.start()
-    total_ms, solve_ms, launches = timed(solve_mixed, args.steps, args.warmup)
+    for _ in range(max(args.warmup, 0)):
+        Bt.copy_(B0)
+        solve_mixed(Bt, At)
+    L.rocblas_b200_kernel_timing_enable(1)
+    total_ms, solve_ms, launches = timed(solve_mixed, args.steps, 0)
+    sliced_t = kernel_timing(L, "sliced")
+    mixed_chain_t = kernel_timing(L, "chain")
+    L.rocblas_b200_kernel_timing_enable(0)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = FLOPS * world / (ms_per_step * 1e-3) / 1e12
     X_mixed_band0 = Bt.clone()
-    p_total, p_solve, p_launches = timed(solve_plain, args.steps, args.warmup)
+    for _ in range(max(args.warmup, 0)):
+        Bt.copy_(B0)
+        solve_plain(Bt, At)
+    L.rocblas_b200_kernel_timing_enable(1)
+    p_total, p_solve, p_launches = timed(solve_plain, args.steps, 0)
+    chain_t = kernel_timing(L, "chain")
+    L.rocblas_b200_kernel_timing_enable(0)
     X_plain_band0 = Bt.clone()
     plain_value = FLOPS * world / (p_total / args.steps * 1e-3) / 1e12
 
@@ -476,18 +519,37 @@ def run_ours(args):
                 "refinement_iterations": 0,
             }
             del A_host, B_host
-        achieved = FLOPS / (med_mixed * 1e-3) / 1e12
-        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
-                    "kernel": f"whole rocblas_b200_dtrsm_mixed call ({S}-slice int8 tcgen05 updates, "
-                              "FP64 DMMA diagonal blocks), m*n*k FP64-equivalent flops",
-                    "peak_source": "FP64 denominator: cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured "
-                                   "in this run; MEASURED_PEAKS.json has no FP64 figure"}
+        pk = measured_peaks()
+        # dominant kernel of the headline: the integer-slice GEMM (ozaki_gemm_kernel), work =
+        # int8 tensor operations of its slice pairs (2 * pairs * M * N * K per launch), timed
+        # per launch with CUDA events on the solve's stream inside the timed region
+        s_ms, s_ops, s_n = sliced_t
+        achieved = s_ops / (s_ms * 1e-3) / 1e12 if s_ms > 0 else 0.0
+        i8_peak = 2.0 * pk["bf16_tflops_sustained"]
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": i8_peak, "unit": "TOP/s (int8)",
+                    "frac": achieved / i8_peak, "traffic": SLICED_TRAFFIC_PER_LAUNCH,
+                    "kernel": f"ozaki_gemm_kernel<64,64,{S}> (tcgen05 kind::i8, {S} slices)",
+                    "launches": s_n, "kernel_ms_per_step": s_ms / args.steps,
+                    "kernel_share_of_step": s_ms / total_ms,
+                    "peak_source": "int8 dense = 2 x bf16_tflops_sustained of " + pk["source"]
+                                   + " (B200 int8 dense rate is twice bf16); the kernel runs inside a "
+                                     "long step",
+                    "traffic_source": SLICED_TRAFFIC_SOURCE,
+                    "fp64_equivalent": {"achieved": FLOPS / (med_mixed * 1e-3) / 1e12, "peak": peak,
+                                        "unit": "TFLOP/s", "what": "whole solve, m*n*k flops, against "
+                                        "cuBLAS DGEMM 8192^3 measured in this run"}}
+        c_ms, c_fl, c_n = chain_t
+        plain_roofline = {"bound": "tensor", "kernel": "trsm_chain_kernel (mma.sync f64 DMMA)",
+                          "achieved": c_fl / (c_ms * 1e-3) / 1e12 if c_ms > 0 else 0.0, "peak": peak,
+                          "unit": "TFLOP/s", "launches": c_n,
+                          "frac": (c_fl / (c_ms * 1e-3) / 1e12) / peak if c_ms > 0 else 0.0,
+                          "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
+                                         "MEASURED_PEAKS.json has no FP64 figure"}
         extra = {
             "roofline": roofline,
             "plain_fp64": {"value": plain_value, "unit": "TFLOP/s", "ms_per_step": p_total / args.steps,
                            "solve_ms_median": med_plain, "frac_of_fp64_peak": plain_value / peak,
-                           "gpu_launches": int(p_launches)},
+                           "gpu_launches": int(p_launches), "roofline": plain_roofline},
             "precision_vs_plain": value / plain_value,
             "cpu_baseline": {"value": cpu[0], "unit": "TFLOP/s", "cores": threads, "kind": "reference",
                              "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) "
@@ -500,12 +562,7 @@ def run_ours(args):
         }
 
     if rank == 0 and not args.no_extras:
-        hbm = 6455.3
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                hbm = float(json.load(f)["hbm_gbs"])
-        except (OSError, KeyError, ValueError):
-            pass
+        hbm = measured_peaks()["hbm_gbs"]
         extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
         extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
 
@@ -531,6 +588,56 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_case(args):
+    """One kernel on one small shape, a few launches, for ncu captures (no JSON line):
+    sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
+    chain: rocblas_dtrsm L/L/N/N m x n (the chain solve)."""
+    import torch
+
+    import rocblas_b200 as rb
+    from rocblas_b200 import workloads
+
+    rb.build()
+    L = rb.lib()
+    h = rb.Handle()
+    dev = torch.device("cuda", 0)
+    m, n, k = args.m, args.n, args.k
+    minus = ctypes.c_double(-1.0)
+    one = ctypes.c_double(1.0)
+    pm = ctypes.cast(ctypes.byref(minus), ctypes.c_void_p)
+    po = ctypes.cast(ctypes.byref(one), ctypes.c_void_p)
+    g = torch.Generator(device=dev).manual_seed(5)
+    if args.case == "chain":
+        At, Bt = workloads.condition_band_lower_torch(m, n, 0, seed=5, device=dev)
+
+        def run():
+            st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
+                                 rb.diagonal_non_unit, m, n, po, ctypes.c_void_p(At.data_ptr()), m,
+                                 ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+    else:
+        A = torch.randn(k, m, dtype=torch.float64, device=dev, generator=g)
+        B = torch.randn(n, k, dtype=torch.float64, device=dev, generator=g)
+        C = torch.randn(n, m, dtype=torch.float64, device=dev, generator=g)
+        gemm_args = (h.value, rb.operation_none, rb.operation_none, m, n, k, pm,
+                     ctypes.c_void_p(A.data_ptr()), m, ctypes.c_void_p(B.data_ptr()), k, po,
+                     ctypes.c_void_p(C.data_ptr()), m)
+
+        def run():
+            if args.case == "sliced":
+                st = L.rocblas_b200_dgemm_sliced(*gemm_args, args.slices)
+            else:
+                st = L.rocblas_b200_dgemm(*gemm_args)
+            assert st == 0, st
+    for _ in range(max(args.steps, 1)):
+        run()
+    torch.cuda.synchronize()
+    code = ctypes.c_int(-1)
+    assert L.rocblas_b200_get_device_error(h.value, ctypes.byref(code)) == 0 and code.value == 0
+    print(f"case {args.case} m={m} n={n} k={k}: {args.steps} launches ok", flush=True)
+    h.close()
+
+
 def main():
     global M, N, FLOPS
     ap = argparse.ArgumentParser()
@@ -544,7 +651,13 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and serving sections (profiling runs)")
+    ap.add_argument("--case", choices=["sliced", "dmma", "chain"],
+                    help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
+    ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     M, N = args.m, args.n
     FLOPS = float(M) * M * N
     if args.impl == "reference":

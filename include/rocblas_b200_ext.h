@@ -45,7 +45,7 @@ typedef struct rocblas_b200_trsm_problem
  *   invalid_count: optional device pointer; receives the number of descriptors that broke
  *          the trsm argument rules or exceeded max_k (those entries are skipped, their B is
  *          not written).
- * Workspace: 4 * (count + 1) + 16 bytes from the handle (size query supported). */
+ * Workspace: 16 * (count + 1) + 32 bytes from the handle (size query supported). */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_vbatched(rocblas_handle                   handle,
                                                           const double*                    alpha,
                                                           const rocblas_b200_trsm_problem* problems,
@@ -58,6 +58,36 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle        
                                                           rocblas_int                      count,
                                                           rocblas_int                      max_k,
                                                           rocblas_int* invalid_count);
+
+/* Variable-size batch of any triangle order: as rocblas_b200_?trsm_vbatched, but systems with
+ * k > 512 are solved too, by the chain solve (one persistent launch over every such system,
+ * items claimed level by level), using the caller's inverted diagonal blocks:
+ *   invA: device array of `count` device pointers; entry i holds the 128 x 128 inverses of
+ *          system i's diagonal blocks in the rocblas_trsm_ex format (ld 128, stride 128 * 128,
+ *          128 * k elements), e.g. from rocblas_?trtri_strided_batched; entries of systems
+ *          with k <= 512 are not read (may be NULL);
+ *   max_k: upper bound of k over the batch, at most 32768;
+ *   max_n: upper bound of the right-hand sides (n for side left, m for side right) of the
+ *          systems with k > 512; larger systems are skipped and counted invalid.
+ * FP32 systems with k > 512 are computed in FP64 and rounded once.  Workspace from the
+ * handle (size query supported): about count * (16 + 64 + 4 * ceil(max_k / 128) *
+ * ceil(max_n / 32)) bytes.  No reference counterpart (see rocblas_b200_dtrsm_vbatched). */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_vbatched_ex(rocblas_handle                   handle,
+                                                             const double*                    alpha,
+                                                             const rocblas_b200_trsm_problem* problems,
+                                                             const double* const*             invA,
+                                                             rocblas_int                      count,
+                                                             rocblas_int                      max_k,
+                                                             rocblas_int                      max_n,
+                                                             rocblas_int* invalid_count);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched_ex(rocblas_handle                   handle,
+                                                             const float*                     alpha,
+                                                             const rocblas_b200_trsm_problem* problems,
+                                                             const float* const*              invA,
+                                                             rocblas_int                      count,
+                                                             rocblas_int                      max_k,
+                                                             rocblas_int                      max_n,
+                                                             rocblas_int* invalid_count);
 
 /* ---- the variable-size batch without any allocation ---------------------------------------
  * No counterpart in the reference.  Same contract and results as
@@ -153,6 +183,19 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices, dmma_force_tile,
  * dmma_big_bk.  Unknown keys or
  * out-of-range values return rocblas_status_invalid_value. */
+/* Per-launch timing of the main kernels with CUDA events on the launching stream, for
+ * measuring one kernel's achieved rate inside a larger call.  enable != 0 starts recording
+ * (and discards earlier records), 0 stops it.  query sums, over the recorded launches of a
+ * kernel class ("sliced": the integer-slice tensor-core GEMM, work = int8 tensor operations;
+ * "dmma": the FP64 DMMA GEMM tiles, work = FP64 flops; "chain": the chain solve, work = the
+ * trsm flop count k * k * ncols of uniform batches, 0 for variable batches), the event time
+ * in milliseconds, the work, and the launch count; it waits for the recorded events. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_kernel_timing_enable(rocblas_int enable);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_kernel_timing_query(const char* kernel_class,
+                                                               double*     total_ms,
+                                                               double*     total_work,
+                                                               rocblas_int* launches);
+
 ROCBLAS_EXPORT rocblas_status rocblas_b200_set_tuning(const char* key, rocblas_int value);
 ROCBLAS_EXPORT rocblas_status rocblas_b200_get_tuning(const char* key, rocblas_int* value);
 

@@ -140,10 +140,15 @@ SIGNATURES = {
     "rocblas_b200_dtrsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
     "rocblas_b200_strsm_vbatched": (_i, [_H, _p, _p, _i, _i, _p]),
     "rocblas_b200_dtrsm_vbatched_noalloc": (_i, [_H, _p, _p, _i, _i, _p]),
+    "rocblas_b200_dtrsm_vbatched_ex": (_i, [_H, _p, _p, _p, _i, _i, _i, _p]),
+    "rocblas_b200_strsm_vbatched_ex": (_i, [_H, _p, _p, _p, _i, _i, _i, _p]),
     "rocblas_b200_dgemm_sliced": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
     "rocblas_b200_get_device_error": (_i, [_H, ctypes.POINTER(_i)]),
+    "rocblas_b200_kernel_timing_enable": (_i, [_i]),
+    "rocblas_b200_kernel_timing_query": (_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),
     "rocblas_b200_set_tuning": (_i, [ctypes.c_char_p, _i]),
     "rocblas_b200_get_tuning": (_i, [ctypes.c_char_p, ctypes.POINTER(_i)]),
 }

@@ -15,6 +15,7 @@
 // updates and the invA leaves still fill the 148 SMs.
 #pragma once
 #include "gemm_tile.cuh"
+#include "timing.hpp"
 #include "tuning.hpp"
 
 namespace rb200
@@ -278,6 +279,7 @@ static void launch_dmma_cfg(const GemmParams<double>& p0, int batch, cudaStream_
         p.batch_base = b0;
         dim3 grid((unsigned)ceil_div(p.M, BM), (unsigned)ceil_div(p.N, BN),
                   (unsigned)std::min(65535, batch - b0));
+        TimedLaunch tl(KernelClass::dmma, s, 2.0 * p.M * p.N * p.K * grid.z);
         kern<<<grid, Cfg::kThreads, Cfg::kSmem, s>>>(p);
     }
 }

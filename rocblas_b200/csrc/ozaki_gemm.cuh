@@ -185,16 +185,36 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Persistent over output tiles: grid = min(tiles, SMs), tile t = blockIdx.x + i * gridDim.x in
+// a grouped order (kOzGroupM row tiles side by side, then the next columns) so that the tiles
+// in flight share their P and Q slice tiles in L2.  The copy ring runs across tile
+// boundaries; the MMA warp starts a tile once the epilogue has drained the previous tile's
+// accumulators (tmem_empty), and with BN = 64 the epilogue drains TMEM into registers first,
+// releases it, and only then reads and writes C, so the C traffic of one tile overlaps the
+// MMAs of the next.
+//
 // SC > 0: a single pass over all SC slices (d_lo = 0, d_hi = SC) with the slice count known
 // at compile time, so the MMA and copy schedules unroll into straight-line code; SC = 0: the
 // pass and slice count come from p at run time.
+constexpr int kOzGroupM = 8;
+
+__device__ __forceinline__ void oz_tile_coords(int t, int tiles_m, int tiles_n, int& mt, int& nt)
+{
+    const int per_group = kOzGroupM * tiles_n;
+    const int grp = t / per_group, r = t - grp * per_group;
+    const int gm  = min(kOzGroupM, tiles_m - grp * kOzGroupM); // rows in this group
+    mt = grp * kOzGroupM + r % gm;
+    nt = r / gm;
+}
+
 template <int BN, int BK, int SC>
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_gemm_kernel(const __grid_constant__ OzParams p)
 {
-    constexpr int kTileA = kOzBM * BK; // bytes per slice tile of P
-    constexpr int kTileB = BN * BK;    // bytes per slice tile of Q
-    constexpr int kMerge = kOzMaxN / BN; // Q slices per MMA
+    constexpr int  kTileA = kOzBM * BK; // bytes per slice tile of P
+    constexpr int  kTileB = BN * BK;    // bytes per slice tile of Q
+    constexpr int  kMerge = kOzMaxN / BN; // Q slices per MMA
+    constexpr bool kEarlyRelease = BN == 64; // drain TMEM to registers before touching C
     extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
     // 1 KB alignment for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -205,14 +225,16 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const int stage_bytes = S * (kTileA + kTileB);
     const int NS        = p.stages;
 
-    __shared__ uint64_t full_bar[8], empty_bar[8], acc_bar;
+    __shared__ uint64_t full_bar[8], empty_bar[8], tmem_full, tmem_empty;
     __shared__ uint32_t tmem_base_sh;
     __shared__ int      abort_flag;
     __shared__ int      issued, consumed; // K steps loaded / handed to the tensor cores
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kOzBM, n0 = blockIdx.y * BN;
-    const int nk = (p.K + BK - 1) / BK;
+    const int nk      = (p.K + BK - 1) / BK;
+    const int tiles_m = p.M_pad / kOzBM;
+    const int tiles_n = (p.N + BN - 1) / BN;
+    const int tiles   = tiles_m * tiles_n;
 
     if(threadIdx.x == 0)
     {
@@ -221,7 +243,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             mbar_init(&full_bar[i], 1);
             mbar_init(&empty_bar[i], 1);
         }
-        mbar_init(&acc_bar, 1);
+        mbar_init(&tmem_full, 1);
+        mbar_init(&tmem_empty, 4); // one arrival per epilogue warp
         abort_flag = 0;
         issued     = 0;
         consumed   = 0;
@@ -241,34 +264,41 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 
     if(warp == 0)
     {
-        // ---------------- TMA producer ----------------
+        // ---------------- copy producer ----------------
         if(lane == 0)
         {
-            for(int i = 0; i < nk; ++i)
+            const int64_t slP = (int64_t)p.nkc * p.M_pad * BK, slQ = (int64_t)p.nkc * p.N_pad * BK;
+            int it = 0; // K steps issued over all tiles
+            for(int tile = blockIdx.x; tile < tiles && !*(volatile int*)&abort_flag; tile += gridDim.x)
             {
-                const int st = i % NS;
-                const uint32_t ph = (uint32_t)((i / NS) & 1);
-                if(!mbar_wait_bounded(&empty_bar[st], ph ^ 1))
+                int mt, nt;
+                oz_tile_coords(tile, tiles_m, tiles_n, mt, nt);
+                const int m0 = mt * kOzBM, n0 = nt * BN;
+                for(int i = 0; i < nk; ++i, ++it)
                 {
-                    atomicExch(p.error, 1);
-                    atomicExch(&abort_flag, 1);
-                    break;
+                    const int st = it % NS;
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if(!mbar_wait_bounded(&empty_bar[st], ph ^ 1))
+                    {
+                        atomicExch(p.error, 1);
+                        atomicExch(&abort_flag, 1);
+                        break;
+                    }
+                    if(*(volatile int*)&abort_flag)
+                        break;
+                    unsigned char* base = smem + st * stage_bytes;
+                    mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
+                    // slice s, K panel i: rows at ((s * nkc + i) * rows_pad + row) * BK
+                    const int8_t* srcP = p.sliceP + ((int64_t)i * p.M_pad + m0) * BK;
+                    const int8_t* srcQ = p.sliceQ + ((int64_t)i * p.N_pad + n0) * BK;
+#pragma unroll
+                    for(int s = 0; s < S; ++s)
+                        bulk_load(base + s * kTileA, srcP + s * slP, kTileA, &full_bar[st]);
+#pragma unroll
+                    for(int t = 0; t < S; ++t)
+                        bulk_load(base + S * kTileA + t * kTileB, srcQ + t * slQ, kTileB, &full_bar[st]);
+                    *(volatile int*)&issued = it + 1;
                 }
-                if(*(volatile int*)&abort_flag)
-                    break;
-                unsigned char* base = smem + st * stage_bytes;
-                mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
-                // slice s, K panel i: rows at ((s * nkc + i) * rows_pad + row) * BK
-                const int8_t* srcP = p.sliceP + ((int64_t)i * p.M_pad + m0) * BK;
-                const int8_t* srcQ = p.sliceQ + ((int64_t)i * p.N_pad + n0) * BK;
-                const int64_t slP = (int64_t)p.nkc * p.M_pad * BK, slQ = (int64_t)p.nkc * p.N_pad * BK;
-#pragma unroll
-                for(int s = 0; s < S; ++s)
-                    bulk_load(base + s * kTileA, srcP + s * slP, kTileA, &full_bar[st]);
-#pragma unroll
-                for(int t = 0; t < S; ++t)
-                    bulk_load(base + S * kTileA + t * kTileB, srcQ + t * slQ, kTileB, &full_bar[st]);
-                *(volatile int*)&issued = i + 1;
             }
         }
     }
@@ -281,75 +311,116 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             // offset (start address field = byte address / 16, no carry out of its 14 bits)
             const uint64_t desc_a0 = oz_smem_desc<BK>(smem_u32(smem));
             const uint64_t desc_b0 = oz_smem_desc<BK>(smem_u32(smem) + S * kTileA);
-            int i = 0;
-            for(; i < nk; ++i)
+            int it = 0, tcount = 0;
+            bool ok = true;
+            for(int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++tcount)
             {
-                const int st = i % NS;
-                const uint32_t ph = (uint32_t)((i / NS) & 1);
-                if(!mbar_wait_bounded(&full_bar[st], ph))
+                // the epilogue has drained the previous tile's accumulators
+                if(!mbar_wait_bounded(&tmem_empty, (uint32_t)((tcount & 1) ^ 1)))
                 {
                     atomicExch(p.error, 2);
                     atomicExch(&abort_flag, 1);
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                *(volatile int*)&consumed = i + 1;
-                const uint64_t soff = (uint64_t)((st * stage_bytes) >> 4);
-                // P slice 0 comes first in every K step and covers every group of the pass, so
-                // only its first MMA of the first K step starts the accumulators
-                const uint32_t acc0 = i > 0 ? 1u : 0u;
-#pragma unroll
-                for(int s = 0; s < S; ++s)
+                for(int i = 0; i < nk; ++i, ++it)
                 {
-                    // Q slices t with d_lo <= s + t < d_hi, in runs of at most kMerge
-                    const int t_lo = max(0, DLO - s), t_hi = min(S - 1, DHI - 1 - s);
-#pragma unroll
-                    for(int t0 = t_lo; t0 <= t_hi; t0 += kMerge)
+                    const int st = it % NS;
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if(!mbar_wait_bounded(&full_bar[st], ph) || *(volatile int*)&abort_flag)
                     {
-                        const int      c     = min(kMerge, t_hi - t0 + 1);
-                        const uint32_t dcol  = tmem + (uint32_t)((s + t0 - DLO) * BN);
-                        const uint32_t idesc = oz_idesc(c * BN);
+                        atomicExch(p.error, 2);
+                        atomicExch(&abort_flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    *(volatile int*)&consumed = it + 1;
+                    const uint64_t soff = (uint64_t)((st * stage_bytes) >> 4);
+                    // P slice 0 comes first in every K step and covers every group of the
+                    // pass, so only its first MMA of a tile's first K step starts the
+                    // accumulators
+                    const uint32_t acc0 = i > 0 ? 1u : 0u;
 #pragma unroll
-                        for(int kk = 0; kk < BK / kOzMmaK; ++kk)
+                    for(int s = 0; s < S; ++s)
+                    {
+                        // Q slices t with d_lo <= s + t < d_hi, in runs of at most kMerge
+                        const int t_lo = max(0, DLO - s), t_hi = min(S - 1, DHI - 1 - s);
+#pragma unroll
+                        for(int t0 = t_lo; t0 <= t_hi; t0 += kMerge)
                         {
-                            const uint64_t ad = desc_a0 + soff + (uint64_t)((s * kTileA + kk * kOzMmaK) >> 4);
-                            const uint64_t bd = desc_b0 + soff + (uint64_t)((t0 * kTileB + kk * kOzMmaK) >> 4);
-                            oz_mma(dcol, ad, bd, idesc, (s == 0 && kk == 0) ? acc0 : 1u);
+                            const int      c     = min(kMerge, t_hi - t0 + 1);
+                            const uint32_t dcol  = tmem + (uint32_t)((s + t0 - DLO) * BN);
+                            const uint32_t idesc = oz_idesc(c * BN);
+#pragma unroll
+                            for(int kk = 0; kk < BK / kOzMmaK; ++kk)
+                            {
+                                const uint64_t ad = desc_a0 + soff + (uint64_t)((s * kTileA + kk * kOzMmaK) >> 4);
+                                const uint64_t bd = desc_b0 + soff + (uint64_t)((t0 * kTileB + kk * kOzMmaK) >> 4);
+                                oz_mma(dcol, ad, bd, idesc, (s == 0 && kk == 0) ? acc0 : 1u);
+                            }
                         }
                     }
+                    oz_commit(&empty_bar[st]);
                 }
-                oz_commit(&empty_bar[st]);
+                // the tile's accumulators are complete when its MMAs are (also on abort:
+                // drains what was issued)
+                oz_commit(&tmem_full);
             }
-            // completion of everything issued so far (also on abort: drains the issued MMAs)
-            oz_commit(&acc_bar);
         }
     }
     else
     {
         // ---------------- epilogue (warps 2..5) ----------------
-        const int quarter = warp & 3;                 // TMEM lane group this warp may access
-        const int row     = quarter * 32 + lane;
-        const int gr      = m0 + row;
-        // warp-uniform outcome: the tcgen05.ld below needs the whole warp
-        bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&acc_bar, 0));
-        if(!ok)
+        const int      quarter   = warp & 3; // TMEM lane group this warp may access
+        const int      row       = quarter * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+        const double   beta      = p.beta_ptr ? *p.beta_ptr : p.beta;
+        const bool     zero      = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
+        int            tcount    = 0;
+        for(int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++tcount)
         {
-            atomicExch(p.error, 3);
-            atomicExch(&abort_flag, 1);
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        if(__all_sync(0xffffffffu, ok && !*(volatile int*)&abort_flag))
-        {
-            const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
-            const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
+            int mt, nt;
+            oz_tile_coords(tile, tiles_m, tiles_n, mt, nt);
+            const int m0 = mt * kOzBM, n0 = nt * BN;
+            const int gr = m0 + row;
+            // warp-uniform outcome: the tcgen05.ld below needs the whole warp
+            bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&tmem_full, (uint32_t)(tcount & 1)));
+            if(!ok)
+            {
+                atomicExch(p.error, 3);
+                atomicExch(&abort_flag, 1);
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if(!__all_sync(0xffffffffu, ok && !*(volatile int*)&abort_flag))
+                break;
             int er = gr < p.M ? p.exp_rows[gr] : 0;
             if(er == kOzExpNone)
                 er = 0;
-            const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
-#pragma unroll 1
-            for(int half = 0; half < BN / 32; ++half)
-            {
-                double h[32];
+            auto store = [&](const double (&h)[32], int half) {
+                if(gr >= p.M)
+                    return;
+#pragma unroll
+                for(int j = 0; j < 32; ++j)
+                {
+                    const int gc = n0 + half * 32 + j;
+                    if(gc < p.N)
+                    {
+                        double*      cp = p.C + gr + (int64_t)gc * p.ldc;
+                        const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
+                        const double pq = ldexp(h[j], er + ec - 14 - 7 * DLO);
+                        double       out;
+                        if(zero)
+                            out = 0.0;
+                        else if(beta == 0.0)
+                            out = p.alpha * pq;
+                        else
+                            out = fma(p.alpha, pq, beta * (*cp));
+                        *cp = out;
+                    }
+                }
+            };
+            auto drain = [&](double (&h)[32], int half) {
 #pragma unroll
                 for(int j = 0; j < 32; ++j)
                     h[j] = 0.0;
@@ -362,28 +433,33 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     for(int j = 0; j < 32; ++j)
                         h[j] = fma(h[j], 0x1p-7, (double)(int)v[j]);
                 }
-                if(gr < p.M)
+            };
+            auto release = [&]() {
+                asm volatile("tcgen05.fence::before_thread_sync;");
+                __syncwarp();
+                if(lane == 0)
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tmem_empty))
+                                 : "memory");
+            };
+            if constexpr(kEarlyRelease)
+            {
+                double h0[32], h1[32];
+                drain(h0, 0);
+                drain(h1, 1);
+                release();
+                store(h0, 0);
+                store(h1, 1);
+            }
+            else
+            {
+#pragma unroll 1
+                for(int half = 0; half < BN / 32; ++half)
                 {
-#pragma unroll
-                    for(int j = 0; j < 32; ++j)
-                    {
-                        const int gc = n0 + half * 32 + j;
-                        if(gc < p.N)
-                        {
-                            double* cp = p.C + gr + (int64_t)gc * p.ldc;
-                            const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
-                            const double pq = ldexp(h[j], er + ec - 14 - 7 * DLO);
-                            double out;
-                            if(zero)
-                                out = 0.0;
-                            else if(beta == 0.0)
-                                out = p.alpha * pq;
-                            else
-                                out = fma(p.alpha, pq, beta * (*cp));
-                            *cp = out;
-                        }
-                    }
+                    double h[32];
+                    drain(h, half);
+                    store(h, half);
                 }
+                release();
             }
         }
     }

@@ -2,6 +2,7 @@
 // _batched and _strided_batched forms.  Every entry point is `extern "C"`, catches every
 // exception (as the reference's IMPL wrappers do, library/src/blas3/rocblas_trsm_imp.hpp:
 // 285-314) and validates its arguments in the reference's order before touching the GPU.
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -12,6 +13,7 @@
 #include "sliced_driver.cuh"
 #include "trsm_driver.cuh"
 #include "vbatched.cuh"
+#include "vbatched_chain.cuh"
 
 using namespace rb200;
 
@@ -447,8 +449,8 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
     int*          offsets = reinterpret_cast<int*>(state + 1);
     cudaMemsetAsync(state, 0, sizeof(VbClassState), h->stream);
     const VbProblem* probs = reinterpret_cast<const VbProblem*>(problems);
-    vb_prepass_classes_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, offsets,
-                                                                    state);
+    vb_prepass_classes_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, max_k, INT_MAX,
+                                                                    offsets, state);
     count_launch();
 
     VbParams<T> p;
@@ -470,6 +472,110 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
     if(invalid_count)
     {
         vb_copy_invalid_kernel<<<1, 1, 0, h->stream>>>(&state->invalid, invalid_count);
+        count_launch();
+    }
+    return launch_status();
+}
+
+// ---- variable-size batch of any order: strip solver for k <= 512, chain above -------------
+__global__ void vb_sum_invalid_kernel(const int* a, const int* b, rocblas_int* out)
+{
+    *out = *a + *b;
+}
+
+template <typename T>
+rocblas_status trsm_vbatched_ex_impl(rocblas_handle h, const T* alpha,
+                                     const rocblas_b200_trsm_problem* problems,
+                                     const T* const* invA, int count, int max_k, int max_n,
+                                     rocblas_int* invalid_count)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(count < 0 || max_k < 0 || max_n < 0 || max_k > kChainVbMaxNB * kChainNB)
+        return rocblas_status_invalid_size;
+    const size_t        cls_bytes = sizeof(VbClassState) + sizeof(int) * (size_t)kVbClasses * ((size_t)count + 1);
+    const bool          chain     = max_k > kChainVbMinK;
+    const ChainVbLayout cl        = chain_vb_layout<T>(count, max_k, max_n);
+    const size_t        cls_off   = chain ? cl.total : 0;
+    const size_t        ws_bytes  = cls_off + cls_bytes;
+    if(h->size_query)
+        return count ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+    if(!count)
+        return rocblas_status_success;
+    if(!alpha || !problems || (chain && !invA))
+        return rocblas_status_invalid_pointer;
+    rocblas_status st;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    char* ws = reinterpret_cast<char*>(h->borrow(ws_bytes));
+    if(!ws)
+        return rocblas_status_memory_error;
+    const VbProblem* probs = reinterpret_cast<const VbProblem*>(problems);
+    Scalar<T>        a;
+    if(h->pointer_mode == rocblas_pointer_mode_host)
+        a.val = *alpha;
+    else
+        a.ptr = alpha;
+
+    // chain part: systems with k > 512
+    ChainVbWork<T> w{};
+    if(chain)
+    {
+        w.hdr      = reinterpret_cast<ChainVbHeader<T>*>(ws + cl.hdr);
+        w.sys      = reinterpret_cast<ChainSys<T>*>(ws + cl.sys);
+        w.P        = reinterpret_cast<int*>(ws + cl.P);
+        w.G        = reinterpret_cast<int*>(ws + cl.G);
+        w.cnt      = reinterpret_cast<int*>(ws + cl.cnt);
+        w.L        = reinterpret_cast<int64_t*>(ws + cl.L);
+        w.flags    = reinterpret_cast<int*>(ws + cl.flags);
+        w.flag_cap = cl.flag_cap;
+        w.counters = reinterpret_cast<unsigned long long*>(ws + cl.counters);
+        w.invalid  = reinterpret_cast<int*>(ws + cl.invalid);
+        // counters, invalid and every flag start at zero
+        cudaMemsetAsync(ws + cl.counters, 0, cl.total - cl.counters, h->stream);
+        chain_vb_prepass_kernel<T><<<1, kVbPrepThreads, 0, h->stream>>>(probs, invA, count, max_k,
+                                                                        max_n, w);
+        count_launch();
+        for(int c = 0; c < kChainVbCombos; ++c)
+        {
+            ChainParams<T> p{};
+            p.vhdr    = w.hdr + c;
+            p.alpha   = a;
+            p.first   = 1;
+            p.counter = reinterpret_cast<int*>(w.counters + c);
+            p.error   = h->err_dev ? h->err_dev : w.invalid + 1;
+            const bool kcp = (c >> 1) != 0, kcq = (c & 1) != 0;
+            launch_chain_w<T, kChainVbW, true>(p, kcp, kcq, h->sm_count, INT64_MAX, h->stream);
+            count_launch();
+        }
+    }
+
+    // strip-solver part: systems with k <= 512
+    VbClassState* state   = reinterpret_cast<VbClassState*>(ws + cls_off);
+    int*          offsets = reinterpret_cast<int*>(state + 1);
+    cudaMemsetAsync(state, 0, sizeof(VbClassState), h->stream);
+    const int kb = std::min(max_k, kChainVbMinK);
+    vb_prepass_classes_kernel<<<1, kVbPrepThreads, 0, h->stream>>>(probs, count, kb, kChainVbMinK,
+                                                                    offsets, state);
+    count_launch();
+    VbParams<T> p;
+    p.probs = probs;
+    p.count = count;
+    p.alpha = a;
+    for(int c = kVbClasses - 1; c >= 0; --c)
+    {
+        if(c > 0 && vb_class_kmax(c - 1) >= kb)
+            continue;
+        p.offsets = offsets + (size_t)c * ((size_t)count + 1);
+        p.counter = &state->counter[c];
+        launch_vb_queue<T>(h, p, std::min(vb_class_kmax(c), std::max(kb, 1)));
+    }
+    if(invalid_count)
+    {
+        if(chain)
+            vb_sum_invalid_kernel<<<1, 1, 0, h->stream>>>(&state->invalid, w.invalid, invalid_count);
+        else
+            vb_copy_invalid_kernel<<<1, 1, 0, h->stream>>>(&state->invalid, invalid_count);
         count_launch();
     }
     return launch_status();
@@ -609,6 +715,7 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
     if(!ws || !err)
         return rocblas_status_memory_error;
     SlicedGemm g{};
+    g.sms = h->sm_count;
     g.M = m;
     g.N = n;
     g.K = k;
@@ -712,7 +819,8 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     const bool recursive = choose_algo(pr) == Algo::recursive;
     const size_t inv_bytes = recursive ? align256((size_t)kInvNB * k * sizeof(double)) : 0;
     const size_t sl_bytes  = recursive ? mixed_slice_workspace_bytes(pr, slices) : 0;
-    const size_t ws_bytes  = inv_bytes + sl_bytes;
+    const size_t ch_bytes  = recursive ? mixed_chain_workspace_bytes(pr) : 0;
+    const size_t ws_bytes  = inv_bytes + sl_bytes + (ch_bytes ? (ch_bytes + 255) / 256 * 256 : 0);
     if(h->size_query)
         return ws_bytes ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
     if((st = device_ready(h)) != rocblas_status_success)
@@ -730,6 +838,7 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     void* ws  = h->borrow(ws_bytes);
     if(!ws || !err)
         return rocblas_status_memory_error;
+    pr.err_dev = err;
     BatchPtr<double> inv;
     inv.base   = reinterpret_cast<double*>(ws);
     inv.stride = (int64_t)kInvNB * k;
@@ -739,6 +848,8 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     rec.S        = slices;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
     rec.err_dev  = err;
+    if(ch_bytes)
+        rec.chain_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes + (sl_bytes + 255) / 256 * 256;
     rec.solve_mixed(0, rec.nblk, 1);
     if(!rec.ok)
         return rocblas_status_arch_mismatch;
@@ -1131,6 +1242,85 @@ rocblas_status rocblas_b200_strsm_vbatched(rocblas_handle h, const float* alpha,
 try
 {
     return trsm_vbatched_impl<float>(h, alpha, problems, count, max_k, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dtrsm_vbatched_ex(rocblas_handle h, const double* alpha,
+                                              const rocblas_b200_trsm_problem* problems,
+                                              const double* const* invA, rocblas_int count,
+                                              rocblas_int max_k, rocblas_int max_n,
+                                              rocblas_int* invalid_count)
+try
+{
+    return trsm_vbatched_ex_impl<double>(h, alpha, problems, invA, count, max_k, max_n, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_strsm_vbatched_ex(rocblas_handle h, const float* alpha,
+                                              const rocblas_b200_trsm_problem* problems,
+                                              const float* const* invA, rocblas_int count,
+                                              rocblas_int max_k, rocblas_int max_n,
+                                              rocblas_int* invalid_count)
+try
+{
+    return trsm_vbatched_ex_impl<float>(h, alpha, problems, invA, count, max_k, max_n, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+// ---- kernel timing (rocblas_b200_ext.h) ------------------------------------------------------
+rocblas_status rocblas_b200_kernel_timing_enable(rocblas_int enable)
+try
+{
+    KernelTiming&               t = kernel_timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    for(auto& r : t.recs)
+        cudaEventSynchronize(r.e1);
+    t.recycle();
+    t.on = enable != 0;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_kernel_timing_query(const char* kernel_class, double* total_ms,
+                                                double* total_work, rocblas_int* launches)
+try
+{
+    const int cls = kernel_class_of(kernel_class);
+    if(cls < 0)
+        return rocblas_status_invalid_value;
+    if(!total_ms || !total_work || !launches)
+        return rocblas_status_invalid_pointer;
+    KernelTiming&               t = kernel_timing();
+    std::lock_guard<std::mutex> lock(t.mu);
+    double ms = 0.0, work = 0.0;
+    int    n  = 0;
+    for(auto& r : t.recs)
+    {
+        if(r.cls != cls)
+            continue;
+        float e = 0.0f;
+        if(cudaEventSynchronize(r.e1) != cudaSuccess || cudaEventElapsedTime(&e, r.e0, r.e1) != cudaSuccess)
+            return rocblas_status_internal_error;
+        ms += e;
+        work += r.work;
+        ++n;
+    }
+    *total_ms   = ms;
+    *total_work = work;
+    *launches   = n;
+    return rocblas_status_success;
 }
 catch(...)
 {

@@ -51,6 +51,7 @@ struct SlicedGemm
     double        ualpha_host;
     int           b_user;
     int           zero_guard;
+    int           sms;        // SMs of the device (persistent grid)
 };
 
 __global__ void oz_fill_kernel(int* p, int n, int v)
@@ -128,19 +129,28 @@ static int plan_oz_passes(int S, OzPass* out)
 }
 
 template <int BN, int BK, int SC>
-static void launch_oz_kernel(const OzParams& p, int64_t Mp, int64_t Np, cudaStream_t s)
+static void launch_oz_kernel(const OzParams& p, int64_t Mp, int64_t Np, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)p.stages * oz_stage_bytes(p.ns, BN, BK) + 1024;
     cudaFuncSetAttribute((const void*)ozaki_gemm_kernel<BN, BK, SC>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((unsigned)(Mp / kOzBM), (unsigned)(Np / BN));
+    // persistent: one CTA per SM (the stages fill its shared memory), at most one per tile
+    const int64_t tiles = (Mp / kOzBM) * ceil_div(p.N, BN);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, sms));
+    (void)Np;
+    // algorithmic work: int8 tensor operations of the pass's slice pairs
+    int pairs = 0;
+    for(int a = 0; a < p.ns; ++a)
+        for(int b = 0; b < p.ns; ++b)
+            pairs += (a + b >= p.d_lo && a + b < p.d_hi) ? 1 : 0;
+    TimedLaunch tl(KernelClass::sliced, s, 2.0 * pairs * (double)p.M * p.N * p.K);
     ozaki_gemm_kernel<BN, BK, SC><<<grid, kOzThreads, smem, s>>>(p);
     count_launch();
 }
 
 // A single pass over all slices with BN = 64 uses the schedule unrolled for its slice count.
 template <int BN, int BK>
-static void launch_oz_pass(const OzParams& p, int64_t Mp, int64_t Np, cudaStream_t s)
+static void launch_oz_pass(const OzParams& p, int64_t Mp, int64_t Np, int sms, cudaStream_t s)
 {
     if constexpr(BN == 64)
     {
@@ -148,19 +158,19 @@ static void launch_oz_pass(const OzParams& p, int64_t Mp, int64_t Np, cudaStream
         {
             switch(p.S)
             {
-            case 1: return launch_oz_kernel<BN, BK, 1>(p, Mp, Np, s);
-            case 2: return launch_oz_kernel<BN, BK, 2>(p, Mp, Np, s);
-            case 3: return launch_oz_kernel<BN, BK, 3>(p, Mp, Np, s);
-            case 4: return launch_oz_kernel<BN, BK, 4>(p, Mp, Np, s);
-            case 5: return launch_oz_kernel<BN, BK, 5>(p, Mp, Np, s);
-            case 6: return launch_oz_kernel<BN, BK, 6>(p, Mp, Np, s);
-            case 7: return launch_oz_kernel<BN, BK, 7>(p, Mp, Np, s);
-            case 8: return launch_oz_kernel<BN, BK, 8>(p, Mp, Np, s);
+            case 1: return launch_oz_kernel<BN, BK, 1>(p, Mp, Np, sms, s);
+            case 2: return launch_oz_kernel<BN, BK, 2>(p, Mp, Np, sms, s);
+            case 3: return launch_oz_kernel<BN, BK, 3>(p, Mp, Np, sms, s);
+            case 4: return launch_oz_kernel<BN, BK, 4>(p, Mp, Np, sms, s);
+            case 5: return launch_oz_kernel<BN, BK, 5>(p, Mp, Np, sms, s);
+            case 6: return launch_oz_kernel<BN, BK, 6>(p, Mp, Np, sms, s);
+            case 7: return launch_oz_kernel<BN, BK, 7>(p, Mp, Np, sms, s);
+            case 8: return launch_oz_kernel<BN, BK, 8>(p, Mp, Np, sms, s);
             default: break;
             }
         }
     }
-    launch_oz_kernel<BN, BK, 0>(p, Mp, Np, s);
+    launch_oz_kernel<BN, BK, 0>(p, Mp, Np, sms, s);
 }
 
 // Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
@@ -234,20 +244,26 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
             if(q.bn == 128)
             {
                 if(q.bk == 64)
-                    launch_oz_pass<128, 64>(p, Mp, Np, s);
+                    launch_oz_pass<128, 64>(p, Mp, Np, g.sms, s);
                 else
-                    launch_oz_pass<128, 32>(p, Mp, Np, s);
+                    launch_oz_pass<128, 32>(p, Mp, Np, g.sms, s);
             }
             else
             {
                 if(q.bk == 64)
-                    launch_oz_pass<64, 64>(p, Mp, Np, s);
+                    launch_oz_pass<64, 64>(p, Mp, Np, g.sms, s);
                 else
-                    launch_oz_pass<64, 32>(p, Mp, Np, s);
+                    launch_oz_pass<64, 32>(p, Mp, Np, g.sms, s);
             }
         }
     }
     return true;
+}
+
+static int mixed_chain_w()
+{
+    const int t = tuning().chain_w;
+    return t == 32 ? 32 : 64;
 }
 
 // ---- precision form of the TRSM ---------------------------------------------------------------
@@ -258,6 +274,7 @@ struct MixedRecursive : Recursive<double>
     int   S;
     void* slice_ws;
     int*  err_dev;
+    void* chain_ws = nullptr; // flags of the chain sub-solves (nullptr: recursion to the leaves)
     bool  ok = true;
 
     // Updates with a short inner dimension stay on the FP64 DMMA tiles (K < sliced_min_k):
@@ -301,6 +318,7 @@ struct MixedRecursive : Recursive<double>
         g.ualpha_dev = q.alpha.ptr;
         g.ualpha_host = q.alpha.val;
         g.zero_guard = 1;
+        g.sms = q.sm_count;
         ok = ok && run_sliced_gemm(g, slice_ws, err_dev, q.stream);
     }
 
@@ -309,6 +327,12 @@ struct MixedRecursive : Recursive<double>
         if(b1 - b0 == 1)
         {
             leaf(b0, first);
+            return;
+        }
+        // diagonal blocks of at most mixed_chain_blocks x 128 rows: one chain launch in FP64
+        if(chain_ws && b1 - b0 <= tuning().mixed_chain_blocks)
+        {
+            launch_chain_sub<double>(pr, b0, b1, first, mixed_chain_w(), chain_ws);
             return;
         }
         const int  bm = (b0 + b1) / 2;
@@ -328,6 +352,16 @@ struct MixedRecursive : Recursive<double>
         }
     }
 };
+
+// Flags of the largest chain sub-solve of the precision form (0: no chain sub-solves).
+static size_t mixed_chain_workspace_bytes(const TrsmProblem<double>& pr)
+{
+    const int nbmax = tuning().mixed_chain_blocks;
+    if(nbmax < 2)
+        return 0;
+    const int k = std::min<int64_t>((int64_t)nbmax * kInvNB, pr.k());
+    return chain_workspace_bytes(chain_shape(k, pr.side_left ? pr.n : pr.m, pr.batch, mixed_chain_w()));
+}
 
 // Largest sliced update of the recursion (the top node's off-diagonal block).
 static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S)

@@ -307,10 +307,12 @@ static Algo choose_algo(const TrsmProblem<T>& pr)
 template <typename T>
 static bool use_chain(const TrsmProblem<T>& pr)
 {
-    if(!std::is_same<T, double>::value || choose_algo(pr) != Algo::recursive)
+    if(choose_algo(pr) != Algo::recursive)
         return false;
     const int64_t ncols = pr.side_left ? pr.n : pr.m;
-    return pr.k() > kInvNB && ncols <= tuning().chain_max_cols;
+    const int64_t limit = std::is_same<T, double>::value ? tuning().chain_max_cols
+                                                         : tuning().chain_max_cols_f32;
+    return pr.k() > kInvNB && ncols <= limit;
 }
 
 template <typename T>
@@ -320,6 +322,48 @@ static ChainShape chain_shape_of(const TrsmProblem<T>& pr)
     const int t     = tuning().chain_w;
     const int w     = t == 32 || t == 64 ? t : (ncols <= 32 ? 32 : 64);
     return chain_shape(pr.k(), ncols, pr.batch, w);
+}
+
+// Chain solve of the diagonal blocks [b0, b1) of pr (all of it: 0, nblk) with invA available:
+// `first` as in Recursive::solve; `ws` holds chain_workspace_bytes of the sub-problem.
+template <typename T>
+static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first, int w, void* ws)
+{
+    const int        r0    = b0 * kInvNB;
+    const int        kk    = std::min(b1 * kInvNB, pr.k()) - r0;
+    const int        ncols = pr.side_left ? pr.n : pr.m;
+    const ChainShape cs    = chain_shape(kk, ncols, pr.batch, w);
+    int*             flags = reinterpret_cast<int*>(ws);
+    cudaMemsetAsync(flags, 0, chain_workspace_bytes(cs), pr.stream);
+    ChainParams<T> c{};
+    c.A       = pr.A.shifted(r0 + (int64_t)r0 * pr.lda);
+    c.lda     = pr.lda;
+    c.invA    = pr.invA.shifted((int64_t)b0 * kInvNB * kInvNB);
+    c.B       = pr.B.shifted(pr.side_left ? (int64_t)r0 : (int64_t)r0 * pr.ldb);
+    c.ldb     = pr.ldb;
+    c.k       = kk;
+    c.ncols   = ncols;
+    c.nb      = cs.nb;
+    c.ns      = cs.ns;
+    c.forward = pr.side_left ? pr.oplower() : !pr.oplower();
+    c.items   = cs.items;
+    c.systems = pr.batch;
+    c.alpha   = pr.alpha;
+    c.first   = first;
+    c.flags   = flags;
+    // the 8-byte claim counter and the error word follow the flags
+    const size_t tail = ((size_t)cs.items * sizeof(int) + 7) / 8 * 8;
+    c.counter = reinterpret_cast<int*>(reinterpret_cast<char*>(flags) + tail);
+    // the error word: the handle's, else a slot after the counter
+    c.error = pr.err_dev ? pr.err_dev : c.counter + 2;
+    // KCP: M's column index (K) is contiguous in memory when M(r, c) = A(c, r)
+    const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
+    const bool kcq = pr.side_left != 0;
+    if(w == 32)
+        launch_chain_w<T, 32, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+    else
+        launch_chain_w<T, 64, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+    count_launch();
 }
 
 // Workspace bytes the call wants: invA for the recursive path unless supplied, then the
@@ -365,44 +409,12 @@ static void trsm_run(TrsmProblem<T> pr, void* ws, bool supplied_invA)
         else
             pr.invA = BatchPtr<T>{};
     }
-    if constexpr(std::is_same<T, double>::value)
+    if(ws && pr.invA.valid() && use_chain(pr))
     {
-        if(ws && pr.invA.valid() && use_chain(pr))
-        {
-            const size_t     off = (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
-            const ChainShape cs  = chain_shape_of(pr);
-            int*             flags = reinterpret_cast<int*>(reinterpret_cast<char*>(ws) + off);
-            const size_t     fbytes = chain_workspace_bytes(cs);
-            cudaMemsetAsync(flags, 0, fbytes, pr.stream);
-            ChainParams c{};
-            c.A       = pr.A;
-            c.lda     = pr.lda;
-            c.invA    = pr.invA;
-            c.B       = pr.B;
-            c.ldb     = pr.ldb;
-            c.k       = k;
-            c.ncols   = pr.side_left ? pr.n : pr.m;
-            c.nb      = cs.nb;
-            c.ns      = cs.ns;
-            c.forward = pr.side_left ? pr.oplower() : !pr.oplower();
-            c.items   = cs.items;
-            c.alpha   = pr.alpha;
-            c.flags   = flags;
-            // the 8-byte claim counter and the error word follow the flags
-            const size_t tail = ((size_t)cs.items * sizeof(int) + 7) / 8 * 8;
-            c.counter = reinterpret_cast<int*>(reinterpret_cast<char*>(flags) + tail);
-            // the error word: the handle's, else a slot after the counter
-            c.error   = pr.err_dev ? pr.err_dev : c.counter + 2;
-            // KCP: M's column index (K) is contiguous in memory when M(r, c) = A(c, r)
-            const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
-            const bool kcq = pr.side_left != 0;
-            if(cs.w == 32)
-                launch_chain_w<32>(c, tM, kcq, pr.sm_count, pr.stream);
-            else
-                launch_chain_w<64>(c, tM, kcq, pr.sm_count, pr.stream);
-            count_launch();
-            return;
-        }
+        const size_t off = (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
+        launch_chain_sub<T>(pr, 0, (int)ceil_div(k, kInvNB), 1, chain_shape_of(pr).w,
+                            reinterpret_cast<char*>(ws) + off);
+        return;
     }
     Recursive<T> rec{pr, k, (int)ceil_div(k, kInvNB)};
     rec.solve(0, rec.nblk, 1);

@@ -29,8 +29,11 @@ struct Tuning
     int dmma_big_bk          = 16;   // k depth of the 128x128 DMMA stage (16 or 32)
     int oz_bn                = 64;   // sliced GEMM output tile width (64: one pass; 128)
     int oz_bk                = 64;   // sliced GEMM K step in int8 (32 or 64)
-    int chain_max_cols       = 512;  // FP64 recursive solves with <= this many columns: chain
+    int chain_max_cols       = 1 << 30; // FP64 solves (k > 128) with <= this many columns: chain
+    int chain_max_cols_f32   = 512;  // the same for FP32 (the chain computes in FP64)
     int chain_w              = 0;    // chain strip width: 0 auto (32 or 64), 32, 64
+    int mixed_chain_blocks   = 8;    // precision form: chain solves for diagonal blocks of <= this
+                                     // many 128-row blocks (< 2: recursion down to the leaves)
 };
 
 struct TuningEntry
@@ -52,7 +55,9 @@ static const TuningEntry kTuningEntries[] = {
     {"oz_bn", &Tuning::oz_bn, 64, 128},
     {"oz_bk", &Tuning::oz_bk, 32, 64},
     {"chain_max_cols", &Tuning::chain_max_cols, 0, 1 << 30},
+    {"chain_max_cols_f32", &Tuning::chain_max_cols_f32, 0, 1 << 30},
     {"chain_w", &Tuning::chain_w, 0, 64},
+    {"mixed_chain_blocks", &Tuning::mixed_chain_blocks, 0, 1 << 20},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

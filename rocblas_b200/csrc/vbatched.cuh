@@ -135,10 +135,11 @@ __global__ void __launch_bounds__(kVbPrepThreads)
 }
 
 // Per class c: offsets[c * (count + 1) + i] = work items of the class-c problems among
-// 0..i-1; offsets[c * (count + 1) + count] = the class total.
+// 0..i-1; offsets[c * (count + 1) + count] = the class total.  Problems with k > skip_above
+// belong to another path of the call: they count neither as work nor as invalid.
 __global__ void __launch_bounds__(kVbPrepThreads)
-    vb_prepass_classes_kernel(const VbProblem* probs, int count, int max_k, int* offsets,
-                              VbClassState* st)
+    vb_prepass_classes_kernel(const VbProblem* probs, int count, int max_k, int skip_above,
+                              int* offsets, VbClassState* st)
 {
     __shared__ int4 part[kVbPrepThreads];
     const int tid   = threadIdx.x;
@@ -150,6 +151,8 @@ __global__ void __launch_bounds__(kVbPrepThreads)
     for(int i = lo; i < hi; ++i)
     {
         const VbProblem p = probs[i];
+        if((p.side == kLeft ? p.m : p.n) > skip_above)
+            continue; // another path of the call solves it (or rejects it)
         if(vb_valid(p, max_k))
             sum[vb_class(p.side == kLeft ? p.m : p.n)] += vb_items(p);
         else
@@ -179,7 +182,7 @@ __global__ void __launch_bounds__(kVbPrepThreads)
         for(int c = 0; c < kVbClasses; ++c)
             offsets[c * cstride + i] = run[c];
         const VbProblem p = probs[i];
-        if(vb_valid(p, max_k))
+        if((p.side == kLeft ? p.m : p.n) <= skip_above && vb_valid(p, max_k))
             run[vb_class(p.side == kLeft ? p.m : p.n)] += vb_items(p);
     }
     if(tid == kVbPrepThreads - 1)

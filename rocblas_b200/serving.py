@@ -6,9 +6,10 @@ Requests (dtype, m, n, a resident-A key or a fresh A) arrive over time.  The ser
   budget, in arrival order; a request that cannot fit yet waits without blocking the loop;
 * keeps resident A matrices and their inverted 128 x 128 diagonal blocks (invA, the
   rocblas_trsm_ex format) on the device and reuses them for every request on that A;
-* collects small systems (k <= 512) for up to `window_us` and solves each collection with
-  one variable-size batched launch (rocblas_b200_?trsm_vbatched); large systems go to
-  rocblas_?trsm_ex (resident invA) or rocblas_?trsm (fresh A) as soon as they are admitted;
+* collects admitted requests of one dtype for up to `window_us` and solves each collection
+  with one variable-size batched call (rocblas_b200_?trsm_vbatched_ex): systems up to k = 512
+  on the strip solver's size classes, larger ones on the chain solve with the resident (or a
+  freshly built) invA, all of them in a few persistent launches;
 * runs launches on a pool of streams, each with its own rocblas handle, so work admitted
   while other work is on the GPU overlaps with it;
 * completes a request when its launch's event has fired, frees its budget and records its
@@ -34,7 +35,7 @@ from . import (
 )
 from .workloads import condition_band_lower_torch
 
-SMALL_K = 512  # systems up to this order go through the variable-size batch
+SMALL_K = 512  # systems above this order need invA (the chain solve of the variable-size batch)
 TORCH_DT = {"d": torch.float64, "s": torch.float32}
 ESIZE = {"d": 8, "s": 4}
 
@@ -166,45 +167,59 @@ class TrsmServer:
     def _alpha(self, dt):
         return ctypes.cast(ctypes.byref(self.one[dt]), ctypes.c_void_p)
 
-    def _launch_large(self, q: Request):
-        stream, h = self._next()
-        self._materialise(q, stream)
+    def _fresh_invA(self, q: Request, h):
+        """invA of a fresh A (k > SMALL_K) on the handle's stream, the trsm_ex format."""
         L = lib()
-        args = (h.value, SIDE["L"], UPLO["L"], TRANS["N"], DIAG["N"], q.m, q.n, self._alpha(q.dtype))
-        if q.a_key is not None:
-            r = self.residents[q.a_key]
-            st = L.rocblas_trsm_ex(*args, _p(r.A[q.dtype]), q.m, _p(q.B), q.m, _p(r.invA[q.dtype]),
-                                   128 * q.m, datatype_f64_r if q.dtype == "d" else datatype_f32_r)
-        else:
-            fn = L.rocblas_dtrsm if q.dtype == "d" else L.rocblas_strsm
-            st = fn(*args, _p(q.A), q.m, _p(q.B), q.m)
-        check("trsm (server)", st)
-        ev = torch.cuda.Event()
-        ev.record(stream)
-        self.inflight[self._cur].append((ev, [q], None))
+        fn = L.rocblas_dtrtri_strided_batched if q.dtype == "d" else L.rocblas_strtri_strided_batched
+        m, es = q.m, ESIZE[q.dtype]
+        inv = torch.zeros(128 * m, dtype=TORCH_DT[q.dtype], device=self.dev)
+        nfull, rem = divmod(m, 128)
+        if nfull:
+            check("trtri", fn(h.value, UPLO["L"], DIAG["N"], 128, _p(q.A), m, 128 * m + 128, _p(inv), 128,
+                              128 * 128, nfull))
+        if rem:
+            off_a = nfull * 128 * m + nfull * 128
+            check("trtri", fn(h.value, UPLO["L"], DIAG["N"], rem, ctypes.c_void_p(q.A.data_ptr() + off_a * es),
+                              m, 0, ctypes.c_void_p(inv.data_ptr() + nfull * 128 * 128 * es), 128, 0, 1))
+        return inv
 
-    def _launch_small(self, group: List[Request], dt):
+    def _launch_group(self, group: List[Request], dt):
+        """One variable-size batched call for a collection of admitted requests."""
         stream, h = self._next()
-        for q in group:
-            self._materialise(q, stream)
+        keep = []
+        with torch.cuda.stream(stream):
+            for q in group:
+                self._materialise(q, stream)
         rec = np.zeros(len(group), dtype=np.dtype([
             ("A", np.uint64), ("B", np.uint64), ("m", np.int32), ("n", np.int32), ("lda", np.int32),
             ("ldb", np.int32), ("side", np.int32), ("uplo", np.int32), ("trans", np.int32),
             ("diag", np.int32)]))
-        max_k = 1
+        invs = np.zeros(len(group), dtype=np.uint64)
+        max_k, max_n = 1, 1
         for i, q in enumerate(group):
-            A = self.residents[q.a_key].A[dt] if q.a_key is not None else q.A
+            if q.a_key is not None:
+                r = self.residents[q.a_key]
+                A, inv = r.A[dt], r.invA[dt]
+            else:
+                A = q.A
+                inv = self._fresh_invA(q, h) if q.m > SMALL_K else None
+                if inv is not None:
+                    keep.append(inv)
             rec[i] = (A.data_ptr(), q.B.data_ptr(), q.m, q.n, q.m, q.m, SIDE["L"], UPLO["L"], TRANS["N"],
                       DIAG["N"])
+            invs[i] = inv.data_ptr() if inv is not None else 0
             max_k = max(max_k, q.m)
-        host = torch.from_numpy(rec.view(np.uint8)).pin_memory()
+            max_n = max(max_n, q.n)
+        host = torch.from_numpy(np.concatenate([rec.view(np.uint8), invs.view(np.uint8)])).pin_memory()
         with torch.cuda.stream(stream):
-            desc = host.to(self.dev, non_blocking=True)
-        fn = lib().rocblas_b200_dtrsm_vbatched if dt == "d" else lib().rocblas_b200_strsm_vbatched
-        check("vbatched (server)", fn(h.value, self._alpha(dt), _p(desc), len(group), max_k, None))
+            dev = host.to(self.dev, non_blocking=True)
+        nd = rec.nbytes
+        fn = lib().rocblas_b200_dtrsm_vbatched_ex if dt == "d" else lib().rocblas_b200_strsm_vbatched_ex
+        check("vbatched_ex (server)", fn(h.value, self._alpha(dt), _p(dev), ctypes.c_void_p(dev.data_ptr() + nd),
+                                         len(group), max_k, max_n, None))
         ev = torch.cuda.Event()
         ev.record(stream)
-        self.inflight[self._cur].append((ev, list(group), (host, desc)))
+        self.inflight[self._cur].append((ev, list(group), (host, dev, keep)))
 
     # ---- the loop ----------------------------------------------------------------------
     def run(self, requests: List[Request], keep_results=False):
@@ -215,7 +230,7 @@ class TrsmServer:
             if q.bytes > self.budget - self.used:
                 raise ValueError(f"request {q.rid} needs {q.bytes} B, more than the free budget")
         pending = collections.deque()
-        small = {"d": collections.deque(), "s": collections.deque()}
+        window = {"d": collections.deque(), "s": collections.deque()}
         i = 0
         t0 = time.perf_counter()
         done = 0
@@ -232,16 +247,13 @@ class TrsmServer:
                 q = pending.popleft()
                 self.used += q.bytes
                 q.admitted = now
-                if q.m <= SMALL_K:
-                    small[q.dtype].append(q)
-                else:
-                    self._launch_large(q)
-            # small systems: launch a collection when the window closes or it is full
-            for dt, dq in small.items():
+                window[q.dtype].append(q)
+            # a collection is launched when its window closes, when it is full, or at the end
+            for dt, dq in window.items():
                 while dq and (len(dq) >= self.max_batch or now - dq[0].admitted >= self.window
                               or (i >= total and not pending)):
                     group = [dq.popleft() for _ in range(min(len(dq), self.max_batch))]
-                    self._launch_small(group, dt)
+                    self._launch_group(group, dt)
             # completions: each stream's launches finish in order, so only heads are polled
             for dq in self.inflight:
                 while dq and dq[0][0].query():

@@ -146,13 +146,15 @@ def test_device_memory_size_query(handle):
     assert L.rocblas_start_device_memory_size_query(handle.value) == rb.status_size_query_mismatch
     # small problem: no workspace
     assert _trsm(handle, m=64, n=64, lda=64, ldb=64, A=None, B=None, alpha=None) == rb.status_size_unchanged
-    # large problem: invA for 128 * k elements
+    # large problem: invA for 128 * k elements, then the chain solve's flags (one int per
+    # 128-row block and 64-column strip) and its counter
     st = _trsm(handle, m=4096, n=4096, lda=4096, ldb=4096, A=None, B=None, alpha=None)
     assert st == rb.status_size_increased
     st = _trsm(handle, m=2048, n=4096, lda=4096, ldb=4096, A=None, B=None, alpha=None)
     assert st == rb.status_size_unchanged
     assert L.rocblas_stop_device_memory_size_query(handle.value, ctypes.byref(size)) == 0
-    assert size.value == 128 * 4096 * 8
+    want = 128 * 4096 * 8 + (4096 // 128) * (4096 // 64) * 4 + 16
+    assert size.value == (want + 63) // 64 * 64  # the handle rounds sizes up to 64 bytes
     assert not L.rocblas_is_device_memory_size_query(handle.value)
 
 

@@ -26,7 +26,7 @@ def _tune(key, value):
 def chain_setting():
     L = rb.lib()
     old = {}
-    for key in ("chain_max_cols", "chain_w"):
+    for key in ("chain_max_cols", "chain_max_cols_f32", "chain_w"):
         v = ctypes.c_int(-1)
         assert L.rocblas_b200_get_tuning(key.encode(), ctypes.byref(v)) == 0
         old[key] = v.value
@@ -139,3 +139,20 @@ def test_chain_ex_supplied_invA_and_repeatability(chain_setting):
         _check("L", "U", "T", "U", m, n, 1.25, A, B, outs[0])
         assert all(np.array_equal(outs[0], o, equal_nan=True) for o in outs[1:])
         assert _err_word(h) == 0
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", [("L", "L", "N", "N"), ("L", "U", "T", "U"),
+                                                  ("R", "U", "N", "N"), ("R", "L", "T", "U")])
+def test_chain_fp32(chain_setting, side, uplo, trans, diag):
+    """FP32 systems through the chain: staged in FP32, computed in FP64, rounded once."""
+    chain_setting("chain_max_cols_f32", 1 << 20)
+    m, n = (600, 70) if side == "L" else (70, 600)
+    k = m if side == "L" else n
+    A, B = oracle.nan_triangle_problem(400, side, uplo, trans, diag, m, n, k + 1, m + 2, np.float32)
+    with rb.Handle() as h:
+        out = _solve(h, side, uplo, trans, diag, m, n, 1.5, A, B)
+        assert _err_word(h) == 0
+    X = oracle.trsm(side, uplo, trans, diag, 1.5, A, np.asfortranarray(B[:m]))
+    err = oracle.matrix_norm_1(X, out[:m])
+    assert err <= oracle.trsm_tolerance(np.float32, max(m, n)), err
+    assert np.isnan(out[m:]).all()

@@ -63,13 +63,13 @@ def test_serving_admission_respects_budget():
     biggest = max(srv._request_bytes(q) for q in reqs)
     srv.budget = base + biggest + 1024  # room for about one request at a time
     peak = [0]
-    orig = srv._launch_large
+    orig = srv._launch_group
 
-    def spy(q):
+    def spy(group, dt):
         peak[0] = max(peak[0], srv.used)
-        return orig(q)
+        return orig(group, dt)
 
-    srv._launch_large = spy
+    srv._launch_group = spy
     lat = srv.run(reqs)
     assert np.all(lat > 0)
     assert peak[0] <= srv.budget

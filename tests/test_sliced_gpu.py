@@ -141,3 +141,27 @@ def test_mixed_trsm_condition_bands(handle, kband):
     e_plain = oracle.normwise_forward_error(dm.to_host(dB), Xq)
     assert e_mixed <= max(1e-12, 10 * e_ref), (e_mixed, e_ref, e_plain)
     assert e_plain <= max(1e-12, 10 * e_ref), (e_plain, e_ref)
+
+
+@pytest.mark.parametrize("chain_blocks", [0, 4])
+def test_mixed_trsm_chain_bottom(handle, chain_blocks):
+    """The precision form with its bottom levels on the chain solve (mixed_chain_blocks > 0)
+    and with recursion down to the leaves (0): both at the FP64 oracle's level."""
+    L = rb.lib()
+    old = ctypes.c_int(-1)
+    assert L.rocblas_b200_get_tuning(b"mixed_chain_blocks", ctypes.byref(old)) == 0
+    assert L.rocblas_b200_set_tuning(b"mixed_chain_blocks", chain_blocks) == 0
+    try:
+        for side, uplo, trans, diag in [("L", "L", "N", "N"), ("R", "U", "T", "U"), ("L", "U", "N", "N")]:
+            m, n = (2100, 40) if side == "L" else (40, 2100)
+            k = m if side == "L" else n
+            A, B = oracle.nan_triangle_problem(91, side, uplo, trans, diag, m, n, k, m, np.float64)
+            out = _mixed(handle, side, uplo, trans, diag, m, n, -1.25, A, B)
+            X = oracle.trsm(side, uplo, trans, diag, -1.25, A, np.asfortranarray(B[:m]))
+            err = oracle.matrix_norm_1(X, out[:m])
+            assert err <= oracle.trsm_tolerance(np.float64, max(m, n)), (side, uplo, trans, diag, err)
+        code = ctypes.c_int(-1)
+        assert L.rocblas_b200_get_device_error(handle.value, ctypes.byref(code)) == 0
+        assert code.value == 0
+    finally:
+        L.rocblas_b200_set_tuning(b"mixed_chain_blocks", old.value)
