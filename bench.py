@@ -318,7 +318,7 @@ def bench_serving(torch, dev, n_requests, rate, seed=7):
     from rocblas_b200 import serving
 
     rng = np.random.default_rng(seed)
-    srv = serving.TrsmServer(device=dev, hbm_budget=120 << 30, n_streams=4, window_us=200.0)
+    srv = serving.TrsmServer(device=dev, hbm_budget=120 << 30, n_streams=2, window_us=200.0)
     sizes = {}
     for key in range(256):
         m = int(round(np.exp(rng.uniform(np.log(64), np.log(8192)))))

@@ -71,7 +71,7 @@ def _p(t):
 
 
 class TrsmServer:
-    def __init__(self, device="cuda", hbm_budget=120 << 30, n_streams=4, window_us=200.0,
+    def __init__(self, device="cuda", hbm_budget=120 << 30, n_streams=2, window_us=200.0,
                  max_batch=4096):
         self.dev = torch.device(device)
         self.budget = int(hbm_budget)
@@ -88,7 +88,10 @@ class TrsmServer:
         self.residents: Dict[int, Resident] = {}
         # per stream, launches complete in order: (event, [requests], keepalive)
         self.inflight = [collections.deque() for _ in self.streams]
-        self.max_inflight = 8 * n_streams  # launch slots; admission waits when they are full
+        # collections in flight at once: one per stream.  Each collection's persistent kernels
+        # fill the GPU, so a new collection is formed only when a stream frees up; requests
+        # that arrive meanwhile join the next, larger collection (continuous batching).
+        self.max_inflight = n_streams
         self.one = {"d": ctypes.c_double(1.0), "s": ctypes.c_float(1.0)}
         # request payloads are cut from a fixed pool of U(-1,1) values (a stand-in for data that
         # arrives with the request): a request's B and fresh A depend only on its seed
@@ -156,8 +159,10 @@ class TrsmServer:
 
     # ---- launches ----------------------------------------------------------------------
     def _next(self):
-        i = self.rr
-        self.rr = (self.rr + 1) % len(self.streams)
+        """A stream with nothing in flight (there is one while fewer collections than streams
+        are in flight), else the next one in turn."""
+        i = next((j for j, d in enumerate(self.inflight) if not d), self.rr)
+        self.rr = (i + 1) % len(self.streams)
         self._cur = i
         return self.streams[i], self.handles[i]
 
@@ -167,12 +172,13 @@ class TrsmServer:
     def _alpha(self, dt):
         return ctypes.cast(ctypes.byref(self.one[dt]), ctypes.c_void_p)
 
-    def _fresh_invA(self, q: Request, h):
-        """invA of a fresh A (k > SMALL_K) on the handle's stream, the trsm_ex format."""
+    def _fresh_invA(self, q: Request, h, stream):
+        """invA of a fresh A (k > SMALL_K) on the collection's stream, the trsm_ex format."""
         L = lib()
         fn = L.rocblas_dtrtri_strided_batched if q.dtype == "d" else L.rocblas_strtri_strided_batched
         m, es = q.m, ESIZE[q.dtype]
-        inv = torch.zeros(128 * m, dtype=TORCH_DT[q.dtype], device=self.dev)
+        with torch.cuda.stream(stream):
+            inv = torch.zeros(128 * m, dtype=TORCH_DT[q.dtype], device=self.dev)
         nfull, rem = divmod(m, 128)
         if nfull:
             check("trtri", fn(h.value, UPLO["L"], DIAG["N"], 128, _p(q.A), m, 128 * m + 128, _p(inv), 128,
@@ -202,7 +208,7 @@ class TrsmServer:
                 A, inv = r.A[dt], r.invA[dt]
             else:
                 A = q.A
-                inv = self._fresh_invA(q, h) if q.m > SMALL_K else None
+                inv = self._fresh_invA(q, h, stream) if q.m > SMALL_K else None
                 if inv is not None:
                     keep.append(inv)
             rec[i] = (A.data_ptr(), q.B.data_ptr(), q.m, q.n, q.m, q.m, SIDE["L"], UPLO["L"], TRANS["N"],
@@ -241,19 +247,24 @@ class TrsmServer:
             while i < total and reqs[i].arrival <= now:
                 pending.append(reqs[i])
                 i += 1
-            # admission in arrival order, within the HBM budget and the launch slots
-            while (pending and pending[0].bytes <= self.budget - self.used
-                   and self._n_inflight() < self.max_inflight):
+            # admission in arrival order, within the HBM budget
+            while pending and pending[0].bytes <= self.budget - self.used:
                 q = pending.popleft()
                 self.used += q.bytes
                 q.admitted = now
                 window[q.dtype].append(q)
-            # a collection is launched when its window closes, when it is full, or at the end
-            for dt, dq in window.items():
-                while dq and (len(dq) >= self.max_batch or now - dq[0].admitted >= self.window
-                              or (i >= total and not pending)):
-                    group = [dq.popleft() for _ in range(min(len(dq), self.max_batch))]
-                    self._launch_group(group, dt)
+            # a collection is launched when a stream is free and its window has closed (or it
+            # is full, or no more requests will come); the oldest waiting dtype goes first
+            while self._n_inflight() < self.max_inflight:
+                ready = [dt for dt, dq in window.items()
+                         if dq and (len(dq) >= self.max_batch or now - dq[0].admitted >= self.window
+                                    or (i >= total and not pending))]
+                if not ready:
+                    break
+                dt = min(ready, key=lambda d: window[d][0].admitted)
+                dq = window[dt]
+                group = [dq.popleft() for _ in range(min(len(dq), self.max_batch))]
+                self._launch_group(group, dt)
             # completions: each stream's launches finish in order, so only heads are polled
             for dq in self.inflight:
                 while dq and dq[0][0].query():
