@@ -46,6 +46,22 @@ def workload_name():
     return f"dtrsm L/L/N/N m={M} n={N} lda=ldb={M} alpha=1 (condition band k=0)"
 
 
+def max_over_ranks(dist, value, device):
+    """The largest of every rank's `value` (all ranks call it in the same order)."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(units_per_rank, world, max_ms):
+    """Whole-job rate of N independent replicas: all ranks' units over the slowest rank's time."""
+    return units_per_rank * world / (max_ms * 1e-3)
+
+
 def _env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -183,7 +199,8 @@ def run_reference(args):
     val = float(m) * m * ncols * args.steps / tot / 1e12
     del rng
     line = {
-        "metric": "dtrsm TFLOP/s", "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus,
+        "metric": "dtrsm TFLOP/s (precision form, FP64 accuracy)", "value": val, "unit": "TFLOP/s",
+        "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
@@ -314,7 +331,8 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
 def bench_serving(torch, dev, n_requests, rate, seed=7):
     """Config C4: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
     60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
-    budget.  Returns p50 / p99 latency and solves/s."""
+    budget.  The native server loop (rocblas_b200_server_run) serves the list; returns p50 /
+    p99 latency, solves/s over the server's own wall time, and its batching statistics."""
     from rocblas_b200 import serving
 
     rng = np.random.default_rng(seed)
@@ -326,13 +344,17 @@ def bench_serving(torch, dev, n_requests, rate, seed=7):
         sizes[key] = m
     reqs = serving.make_requests(n_requests, rate, seed, sizes)
     flops = float(sum(q.m * q.m * q.n for q in reqs))
-    t0 = time.perf_counter()
     lat = srv.run(reqs)
-    wall = time.perf_counter() - t0
+    st = srv.last_stats
+    wall = st["wall_s"]
     srv.close()
-    return {"requests": n_requests, "arrival_rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+    return {"requests": n_requests, "arrival_rate_per_s": rate,
+            "arrival_span_s": float(reqs[-1].arrival),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "solves_per_s": n_requests / wall,
             "tflops": flops / wall / 1e12, "wall_s": wall, "resident_matrices": 256,
+            "collections": st["collections"], "largest_collection": st["largest_collection"],
+            "peak_arena_gb": st["peak_bytes"] / 1e9, "gpu_launches": st["kernel_launches"],
             "fp64_fraction": float(np.mean([q.dtype == "d" for q in reqs])),
             "reuse_fraction": float(np.mean([q.a_key is not None for q in reqs]))}
 
@@ -410,11 +432,7 @@ def run_ours(args):
         if dist:
             dist.barrier()
         launches = L.rocblas_b200_kernel_launch_count() - l0
-        total = t0.elapsed_time(t1)
-        if dist:
-            t = torch.tensor([total], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(dist, t0.elapsed_time(t1), dev)
         return total, [ev_m[i].elapsed_time(ev_e[i]) for i in range(steps)], launches
 
     # ---- timed region: the precision form (headline), then the plain FP64 form ---------------
@@ -432,7 +450,7 @@ def run_ours(args):
     L.rocblas_b200_kernel_timing_enable(0)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
-    value = FLOPS * world / (ms_per_step * 1e-3) / 1e12
+    value = replicas_value(FLOPS, world, ms_per_step) / 1e12
     X_mixed_band0 = Bt.clone()
     for _ in range(max(args.warmup, 0)):
         Bt.copy_(B0)
@@ -442,7 +460,7 @@ def run_ours(args):
     chain_t = kernel_timing(L, "chain")
     L.rocblas_b200_kernel_timing_enable(0)
     X_plain_band0 = Bt.clone()
-    plain_value = FLOPS * world / (p_total / args.steps * 1e-3) / 1e12
+    plain_value = replicas_value(FLOPS, world, p_total / args.steps) / 1e12
 
     # ---- e2e: host buffers through the C ABI, copies inside the timed region -----------
     e2e = None

@@ -7,6 +7,8 @@
 #define ROCBLAS_B200_EXT_H
 
 #include "rocblas.h"
+#include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -88,6 +90,66 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_strsm_vbatched_ex(rocblas_handle     
                                                              rocblas_int                      max_k,
                                                              rocblas_int                      max_n,
                                                              rocblas_int* invalid_count);
+
+/* ---- continuous-batching server ------------------------------------------------------------
+ * A serving loop for streams of trsm requests (side left, lower, no transpose, non-unit: the
+ * serving workload's form) of mixed size and dtype.  The server owns one device arena of
+ * `hbm_budget` bytes (resident matrices, each admitted request's data), `n_streams` streams,
+ * and a batching window.  rocblas_b200_server_run serves a request list whose arrival times
+ * are given relative to the start of the call: requests are admitted in arrival order while
+ * their memory fits the budget, collected per dtype until a stream is free and the window has
+ * passed, and solved per collection by one variable-size batched call (resident invA reused;
+ * a request's own A is copied in and its diagonal blocks inverted).  latency_s[i] receives
+ * completion - arrival of request i on the host's steady clock.  A request's result does not
+ * depend on the other requests of its collection.  No reference counterpart. */
+typedef struct rocblas_b200_server_* rocblas_b200_server;
+
+typedef struct rocblas_b200_request
+{
+    double           arrival_s; /* seconds after the start of rocblas_b200_server_run */
+    rocblas_datatype dtype;     /* rocblas_datatype_f64_r or rocblas_datatype_f32_r */
+    rocblas_int      m;         /* order of A and rows of B */
+    rocblas_int      n;         /* right-hand sides */
+    rocblas_int      resident;  /* index from rocblas_b200_server_add_resident, or -1 */
+    const void*      B_src;     /* device: the right-hand sides, m x n, ld m */
+    const void*      A_src;     /* device: the request's own lower triangle (resident < 0) */
+    rocblas_int      lda_src;   /* its leading dimension (>= m) */
+    rocblas_int      reserved;
+    void*            X_dst;     /* device: where the solution (m x n, ld m) goes, or NULL */
+} rocblas_b200_request;
+
+typedef struct rocblas_b200_server_stats
+{
+    double  wall_s;             /* duration of the run */
+    int64_t peak_bytes;         /* largest arena use during the run */
+    int64_t collections;        /* batched solves launched */
+    int64_t largest_collection; /* requests in the largest one */
+    int64_t kernel_launches;    /* library kernels launched during the run */
+} rocblas_b200_server_stats;
+
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_create(rocblas_b200_server* server,
+                                                         size_t               hbm_budget,
+                                                         rocblas_int          n_streams,
+                                                         double               window_us,
+                                                         rocblas_int          max_batch);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_destroy(rocblas_b200_server server);
+/* Copies A (m x m lower triangle, ld lda, device) into the arena and builds its invA. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_add_resident(rocblas_b200_server server,
+                                                               rocblas_datatype    dtype,
+                                                               rocblas_int         m,
+                                                               const void*         A,
+                                                               rocblas_int         lda,
+                                                               rocblas_int*        index);
+/* Lowers (or raises, up to the arena) the admission budget; resident matrices count. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_set_budget(rocblas_b200_server server,
+                                                             size_t              hbm_budget);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_used_bytes(rocblas_b200_server server,
+                                                             size_t*             bytes);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_server_run(rocblas_b200_server          server,
+                                                      const rocblas_b200_request*  requests,
+                                                      rocblas_int                  count,
+                                                      double*                      latency_s,
+                                                      rocblas_b200_server_stats*   stats);
 
 /* ---- the variable-size batch without any allocation ---------------------------------------
  * No counterpart in the reference.  Same contract and results as

@@ -146,6 +146,13 @@ SIGNATURES = {
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
     "rocblas_b200_get_device_error": (_i, [_H, ctypes.POINTER(_i)]),
+    "rocblas_b200_server_create": (_i, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _i,
+                                        ctypes.c_double, _i]),
+    "rocblas_b200_server_destroy": (_i, [_p]),
+    "rocblas_b200_server_add_resident": (_i, [_p, _i, _i, _p, _i, ctypes.POINTER(_i)]),
+    "rocblas_b200_server_set_budget": (_i, [_p, ctypes.c_size_t]),
+    "rocblas_b200_server_used_bytes": (_i, [_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "rocblas_b200_server_run": (_i, [_p, _p, _i, _p, _p]),
     "rocblas_b200_kernel_timing_enable": (_i, [_i]),
     "rocblas_b200_kernel_timing_query": (_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i)]),

@@ -69,44 +69,62 @@ class Bench:
         assert st == 0, st
 
 
+def _pick(res):
+    return min(res, key=res.get)
+
+
 def tune(quick=False, out_dir=HERE):
     torch.cuda.init()
     b = Bench()
     report = {"device": torch.cuda.get_device_name(), "when": time.strftime("%Y-%m-%dT%H:%M:%S"),
               "entries": {}}
     big = (8192, 2048) if quick else (16384, 4096)
-
-    # ---- dmma_big_tile_pct: plain dtrsm over a few shapes ------------------------------------
-    shapes = [big, (4096, 512), (2048, 2048), (8192, 256)]
-    cands = [100, 150, 200, 300, 400]
-    res = {}
+    shapes = [big, (4096, 512), (2048, 2048), (8192, 64), (3000, 300)]
     data = {s: condition_band_lower_torch(s[0], s[1], 0, seed=5, device="cuda") for s in shapes}
-    for c in cands:
-        set_tuning("dmma_big_tile_pct", c)
+
+    def plain_sum():
         tot = 0.0
         for (m, n), (At, B0) in data.items():
             Bt = B0.clone()
             tot += b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n)))
-        res[c] = tot
-    best = min(res, key=res.get)
-    set_tuning("dmma_big_tile_pct", best)
-    report["entries"]["dmma_big_tile_pct"] = {"chosen": best, "ms_sum_over_shapes": res,
-                                              "shapes": shapes}
+        return tot
 
-    # ---- sliced_min_k: precision form at the large shape ----------------------------------
+    # ---- plain FP64: chain solve vs recursive solve (crossover in right-hand sides) ----------
+    res = {}
+    for c in [0, 512, 4096, 1 << 30]:
+        set_tuning("chain_max_cols", c)
+        res[c] = plain_sum()
+    set_tuning("chain_max_cols", _pick(res))
+    report["entries"]["chain_max_cols"] = {"chosen": _pick(res), "ms_sum_over_shapes": res,
+                                           "shapes": shapes}
+
+    # ---- chain strip width (0: 32 up to 32 columns, else 64) --------------------------------
+    res = {}
+    for c in [0, 32, 64]:
+        set_tuning("chain_w", c)
+        res[c] = plain_sum()
+    set_tuning("chain_w", _pick(res))
+    report["entries"]["chain_w"] = {"chosen": _pick(res), "ms_sum_over_shapes": res}
+
+    # ---- precision form at the large shape: sliced GEMM K depth, minimum sliced K, chain depth
     m, n = big
     At, B0 = data[big]
-    res = {}
-    for c in [512, 1024, 2048, 4096]:
-        set_tuning("sliced_min_k", c)
+
+    def mixed_ms():
         Bt = B0.clone()
-        res[c] = b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=7)))
-    best = min(res, key=res.get)
-    set_tuning("sliced_min_k", best)
-    report["entries"]["sliced_min_k"] = {"chosen": best, "ms": res, "shape": big}
+        return b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=7)))
+
+    for key, cands in (("oz_bk", [32, 64]), ("sliced_min_k", [512, 1024, 2048]),
+                       ("mixed_chain_blocks", [0, 4, 8, 16])):
+        res = {}
+        for c in cands:
+            set_tuning(key, c)
+            res[c] = mixed_ms()
+        set_tuning(key, _pick(res))
+        report["entries"][key] = {"chosen": _pick(res), "ms": res, "shape": big}
     del data
 
-    # ---- block solver vs recursive for k in (128, 512] ------------------------------------
+    # ---- block solver vs the blocked paths for k in (128, 512] ------------------------------
     res = {}
     for pct in [25, 50, 100, 200, 400]:
         set_tuning("block_min_strips_pct", pct)
@@ -116,9 +134,8 @@ def tune(quick=False, out_dir=HERE):
             Bt = B0.clone()
             tot += b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, k, n)))
         res[pct] = tot
-    best = min(res, key=res.get)
-    set_tuning("block_min_strips_pct", best)
-    report["entries"]["block_min_strips_pct"] = {"chosen": best, "ms_sum": res}
+    set_tuning("block_min_strips_pct", _pick(res))
+    report["entries"]["block_min_strips_pct"] = {"chosen": _pick(res), "ms_sum": res}
 
     # ---- slice count of the precision form: cheapest count meeting 1e-12 in every band ----
     # error measured against the plain FP64 solve of the same system (itself ~1e-15 from
@@ -145,7 +162,8 @@ def tune(quick=False, out_dir=HERE):
                                          "target": "1e-12 with a 10x margin", "shape": [mm, nn]}
 
     keys = ["block_max_k", "block_always_k", "block_min_strips_pct", "sliced_min_k",
-            "dmma_big_tile_pct", "mixed_slices"]
+            "dmma_big_tile_pct", "mixed_slices", "oz_bn", "oz_bk", "chain_max_cols",
+            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks"]
     with open(os.path.join(out_dir, "tuning.cfg"), "w") as f:
         f.write("# written by rocblas_b200/autotune.py on " + report["device"] + "\n")
         for k in keys:

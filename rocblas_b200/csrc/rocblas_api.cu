@@ -12,6 +12,7 @@
 #include "../../include/rocblas_b200_ext.h"
 #include "sliced_driver.cuh"
 #include "trsm_driver.cuh"
+#include "server.cuh"
 #include "vbatched.cuh"
 #include "vbatched_chain.cuh"
 
@@ -580,6 +581,24 @@ rocblas_status trsm_vbatched_ex_impl(rocblas_handle h, const T* alpha,
     }
     return launch_status();
 }
+
+// collection solve of the server: the variable-size batch of any order with alpha 1
+rocblas_status server_solve(_rocblas_handle* h, int dtype, const rocblas_b200_trsm_problem* probs,
+                            const void* invs, int count, int max_k, int max_n)
+{
+    if(dtype == TrsmServerCore::kF64)
+    {
+        static const double one = 1.0;
+        return trsm_vbatched_ex_impl<double>(h, &one, probs, reinterpret_cast<const double* const*>(invs),
+                                             count, max_k, max_n, nullptr);
+    }
+    static const float one = 1.0f;
+    return trsm_vbatched_ex_impl<float>(h, &one, probs, reinterpret_cast<const float* const*>(invs),
+                                        count, max_k, max_n, nullptr);
+}
+
+static_assert(sizeof(ServerRequestC) == sizeof(rocblas_b200_request), "request layout");
+static_assert(sizeof(ServerStatsC) == sizeof(rocblas_b200_server_stats), "stats layout");
 
 // ---- variable-size batch without any allocation ------------------------------------------
 // Scratch of rocblas_b200_dtrsm_vbatched_noalloc: the queue state and the prefix sums of work
@@ -1270,6 +1289,112 @@ rocblas_status rocblas_b200_strsm_vbatched_ex(rocblas_handle h, const float* alp
 try
 {
     return trsm_vbatched_ex_impl<float>(h, alpha, problems, invA, count, max_k, max_n, invalid_count);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+// ---- server (rocblas_b200_ext.h) --------------------------------------------------------------
+struct rocblas_b200_server_
+{
+    TrsmServerCore core{server_solve};
+};
+
+rocblas_status rocblas_b200_server_create(rocblas_b200_server* server, size_t hbm_budget,
+                                          rocblas_int n_streams, double window_us,
+                                          rocblas_int max_batch)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_pointer;
+    *server = nullptr;
+    int dev = 0, sms = 148;
+    if(cudaGetDevice(&dev) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return rocblas_status_internal_error;
+    }
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto*          s  = new rocblas_b200_server_();
+    rocblas_status st = s->core.create(hbm_budget, n_streams, window_us, max_batch, dev, sms);
+    if(st != rocblas_status_success)
+    {
+        delete s;
+        return st;
+    }
+    *server = s;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_server_destroy(rocblas_b200_server server)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_handle;
+    delete server;
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_server_add_resident(rocblas_b200_server server, rocblas_datatype dtype,
+                                                rocblas_int m, const void* A, rocblas_int lda,
+                                                rocblas_int* index)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_handle;
+    return server->core.add_resident((int)dtype, m, A, lda, index);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_server_set_budget(rocblas_b200_server server, size_t hbm_budget)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_handle;
+    server->core.set_budget(hbm_budget);
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_server_used_bytes(rocblas_b200_server server, size_t* bytes)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_handle;
+    if(!bytes)
+        return rocblas_status_invalid_pointer;
+    *bytes = server->core.used();
+    return rocblas_status_success;
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_server_run(rocblas_b200_server server, const rocblas_b200_request* requests,
+                                       rocblas_int count, double* latency_s,
+                                       rocblas_b200_server_stats* stats)
+try
+{
+    if(!server)
+        return rocblas_status_invalid_handle;
+    return server->core.run(reinterpret_cast<const ServerRequestC*>(requests), count, latency_s,
+                            reinterpret_cast<ServerStatsC*>(stats));
 }
 catch(...)
 {
