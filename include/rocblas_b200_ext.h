@@ -250,7 +250,9 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  * (and discards earlier records), 0 stops it.  query sums, over the recorded launches of a
  * kernel class ("sliced": the integer-slice tensor-core GEMM, work = int8 tensor operations;
  * "dmma": the FP64 DMMA GEMM tiles, work = FP64 flops; "chain": the chain solve, work = the
- * trsm flop count k * k * ncols of uniform batches, 0 for variable batches), the event time
+ * trsm flop count k * k * ncols of uniform batches, 0 for variable batches; "trtri": the
+ * diagonal-block inversions, work = 128^3 / 3 per block; "strip": the variable batch's
+ * strip-solver queues, work = 0), the event time
  * in milliseconds, the work, and the launch count; it waits for the recorded events. */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_kernel_timing_enable(rocblas_int enable);
 ROCBLAS_EXPORT rocblas_status rocblas_b200_kernel_timing_query(const char* kernel_class,

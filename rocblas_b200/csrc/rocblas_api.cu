@@ -419,6 +419,7 @@ void launch_vb_queue(rocblas_handle h, const VbParams<T>& p, int kmax)
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_persistent_kernel<T>, kBsThreads, smem);
     per_sm = std::max(per_sm, 1);
+    TimedLaunch tl(KernelClass::strip, h->stream, 0.0);
     vb_persistent_kernel<T><<<h->sm_count * per_sm, kBsThreads, smem, h->stream>>>(p);
     count_launch();
 }

@@ -145,6 +145,10 @@ class TrsmServerCore
 {
 public:
     static constexpr int kF32 = 151, kF64 = 152;
+    // staging per request: its descriptor and invA pointer, and for a fresh A the batched
+    // trtri's A pointer, invA pointer, order and leading dimension
+    static constexpr size_t kStagePerRequest
+        = sizeof(VbProblem) + sizeof(void*) + 2 * sizeof(void*) + sizeof(int64_t) + sizeof(int);
 
     explicit TrsmServerCore(ServerSolveFn solve) : solve_(solve) {}
 
@@ -173,7 +177,7 @@ public:
             if(cudaMalloc(&l.h->err_dev, 256) != cudaSuccess)
                 return rocblas_status_memory_error;
             cudaMemset(l.h->err_dev, 0, 256);
-            const size_t stage = (size_t)max_batch * (sizeof(VbProblem) + sizeof(void*));
+            const size_t stage = (size_t)max_batch * kStagePerRequest;
             if(cudaMallocHost(&l.host_stage, stage) != cudaSuccess
                || cudaMalloc(&l.dev_stage, stage) != cudaSuccess)
                 return rocblas_status_memory_error;
@@ -468,17 +472,24 @@ private:
     rocblas_status launch(Lane& l, const std::vector<int>& group, const ServerRequestC* reqs,
                           std::vector<Held>& held)
     {
-        const int  cnt = (int)group.size();
-        const int  dt  = reqs[group[0]].dtype;
-        const size_t es = dt == kF64 ? 8 : 4;
-        auto* probs = reinterpret_cast<VbProblem*>(l.host_stage);
-        auto* invs  = reinterpret_cast<const void**>(probs + cnt);
-        int   max_k = 1, max_n = 1;
+        const int    cnt = (int)group.size();
+        const int    dt  = reqs[group[0]].dtype;
+        const size_t es  = dt == kF64 ? 8 : 4;
+        // host staging: [descriptors][invA pointers][fresh A ptrs][fresh inv ptrs][lda][k]
+        char*  hs     = reinterpret_cast<char*>(l.host_stage);
+        auto*  probs  = reinterpret_cast<VbProblem*>(hs);
+        auto*  invs   = reinterpret_cast<const void**>(hs + (size_t)cnt * sizeof(VbProblem));
+        auto*  fA     = invs + cnt;
+        auto*  fInv   = reinterpret_cast<void**>(hs + (size_t)cnt * (sizeof(VbProblem) + 2 * sizeof(void*)));
+        auto*  fLda   = reinterpret_cast<int64_t*>(fInv + cnt);
+        auto*  fK     = reinterpret_cast<int*>(fLda + cnt);
+        int    nfresh = 0, fresh_nb = 0;
+        int    max_k = 1, max_n = 1;
         for(int j = 0; j < cnt; ++j)
         {
             const ServerRequestC& q = reqs[group[j]];
             Held&                 h = held[group[j]];
-            // the request's data arrives: B, and its own A with the inversion of its blocks
+            // the request's data arrives: B, and its own A
             cudaMemcpyAsync(h.B, q.B_src, h.b_bytes, cudaMemcpyDeviceToDevice, l.stream);
             const void* A;
             const void* inv = nullptr;
@@ -494,8 +505,13 @@ private:
                 A = h.A;
                 if(h.inv)
                 {
-                    build_inv(dt, q.m, h.A, h.inv, l.stream);
-                    inv = h.inv;
+                    inv          = h.inv;
+                    fA[nfresh]   = h.A;
+                    fInv[nfresh] = h.inv;
+                    fLda[nfresh] = q.m;
+                    fK[nfresh]   = q.m;
+                    fresh_nb     = std::max(fresh_nb, (int)ceil_div(q.m, kInvNB));
+                    ++nfresh;
                 }
             }
             VbProblem p;
@@ -514,10 +530,20 @@ private:
             max_k    = std::max(max_k, q.m);
             max_n    = std::max(max_n, q.n);
         }
-        const size_t bytes = (size_t)cnt * (sizeof(VbProblem) + sizeof(void*));
+        const size_t bytes = (size_t)cnt * kStagePerRequest;
         cudaMemcpyAsync(l.dev_stage, l.host_stage, bytes, cudaMemcpyHostToDevice, l.stream);
-        auto* dprobs = reinterpret_cast<const rocblas_b200_trsm_problem*>(l.dev_stage);
-        auto* dinvs  = reinterpret_cast<const char*>(l.dev_stage) + (size_t)cnt * sizeof(VbProblem);
+        const char* ds = reinterpret_cast<const char*>(l.dev_stage);
+        // the fresh A's diagonal blocks, all of them in one variable-size trtri launch
+        if(nfresh)
+        {
+            const size_t o_fA = (size_t)cnt * (sizeof(VbProblem) + sizeof(void*));
+            if(dt == kF64)
+                build_inv_batch<double>(ds, o_fA, cnt, nfresh, fresh_nb, l.stream);
+            else
+                build_inv_batch<float>(ds, o_fA, cnt, nfresh, fresh_nb, l.stream);
+        }
+        auto* dprobs = reinterpret_cast<const rocblas_b200_trsm_problem*>(ds);
+        auto* dinvs  = ds + (size_t)cnt * sizeof(VbProblem);
         const rocblas_status st = solve_(l.h, dt, dprobs, dinvs, cnt, max_k, max_n);
         if(st != rocblas_status_success)
             return st;
@@ -531,6 +557,27 @@ private:
         cudaEventRecord(l.done, l.stream);
         l.inflight = group;
         return rocblas_status_success;
+    }
+
+    // trtri of `nfresh` fresh A's whose pointer / order arrays start at device offset o_fA of
+    // the staging buffer (layout of launch()): grid (largest block count, nfresh)
+    template <typename T>
+    static void build_inv_batch(const char* ds, size_t o_fA, int cnt, int nfresh, int max_nb,
+                                cudaStream_t s)
+    {
+        TrtriParams<T> t{};
+        t.nb               = kInvNB;
+        t.k                = max_nb * kInvNB;
+        t.A.arr            = ds + o_fA;
+        t.inv.arr          = ds + o_fA + (size_t)cnt * sizeof(void*);
+        t.vlda             = reinterpret_cast<const int64_t*>(ds + o_fA + 2 * (size_t)cnt * sizeof(void*));
+        t.vk               = reinterpret_cast<const int*>(ds + o_fA + 2 * (size_t)cnt * sizeof(void*)
+                                                          + (size_t)cnt * sizeof(int64_t));
+        t.ldinv            = kInvNB;
+        t.inv_block_stride = (int64_t)kInvNB * kInvNB;
+        t.upper            = 0;
+        t.unit             = 0;
+        launch_trtri<T>(t, max_nb, nfresh, s);
     }
 
     ServerSolveFn         solve_;

@@ -17,7 +17,9 @@ enum class KernelClass : int
     sliced = 0, // ozaki_gemm_kernel (work: int8 tensor operations)
     dmma   = 1, // gemm_dmma_kernel (work: FP64 flops)
     chain  = 2, // trsm_chain_kernel (work: FP64 flops of the solve)
-    count  = 3
+    trtri  = 3, // trtri_block_kernel (work: nb^3 / 3 flops per 128-block)
+    strip  = 4, // the variable-size batch's strip-solver queues (work: 0)
+    count  = 5
 };
 
 struct KernelTiming
@@ -107,6 +109,10 @@ inline int kernel_class_of(const char* name)
         return (int)KernelClass::dmma;
     if(!std::strcmp(name, "chain"))
         return (int)KernelClass::chain;
+    if(!std::strcmp(name, "trtri"))
+        return (int)KernelClass::trtri;
+    if(!std::strcmp(name, "strip"))
+        return (int)KernelClass::strip;
     return -1;
 }
 

@@ -110,6 +110,7 @@ static void launch_trtri(const TrtriParams<T>& p0, int nblocks, int batch, cudaS
         TrtriParams<T> p = p0;
         p.batch_base     = b0;
         dim3 grid((unsigned)nblocks, (unsigned)std::min(kMaxGridYZ, batch - b0));
+        TimedLaunch tl(KernelClass::trtri, s, (double)grid.x * grid.y * kInvNB * kInvNB * kInvNB / 3.0);
         trtri_block_kernel<T><<<grid, kTrtriThreads, smem, s>>>(p);
         count_launch();
     }

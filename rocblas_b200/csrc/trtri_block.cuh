@@ -32,6 +32,10 @@ struct TrtriParams
     int64_t     inv_block_stride;
     int         upper, unit;
     int         batch_base;
+    // variable batch: order and leading dimension per entry (A and inv then come from
+    // pointer arrays); blocks beyond an entry's order exit at once
+    const int*     vk   = nullptr;
+    const int64_t* vlda = nullptr;
 };
 
 constexpr int kTrtriNB      = 128;
@@ -63,13 +67,17 @@ __global__ void __launch_bounds__(kTrtriThreads) trtri_block_kernel(TrtriParams<
     T* Ts    = Xs + kTrtriNTiles * kTrtriTile;
     T* rdiag = Ts + 3 * kTrtriTile;
 
-    const int tid   = threadIdx.x;
-    const int blk   = blockIdx.x;
-    const int batch = p.batch_base + blockIdx.y;
-    const int r0    = blk * p.nb;
-    const int bs    = min(p.nb, p.k - r0);
+    const int     tid   = threadIdx.x;
+    const int     blk   = blockIdx.x;
+    const int     batch = p.batch_base + blockIdx.y;
+    const int     k     = p.vk ? p.vk[batch] : p.k;
+    const int64_t lda   = p.vk ? p.vlda[batch] : p.lda;
+    const int     r0    = blk * p.nb;
+    if(r0 >= k)
+        return; // (variable batch) this entry has fewer blocks
+    const int bs = min(p.nb, k - r0);
 
-    const T* A   = p.A.get(batch) + r0 + (int64_t)r0 * p.lda;
+    const T* A   = p.A.get(batch) + r0 + (int64_t)r0 * lda;
     T*       out = p.inv.get(batch) + (int64_t)blk * p.inv_block_stride;
 
     // ---- stage the block in lower orientation, identity-padded to 128 ----------------
@@ -86,12 +94,12 @@ __global__ void __launch_bounds__(kTrtriThreads) trtri_block_kernel(TrtriParams<
             const int c = p.upper ? bs - 1 - j : j;
             if(i == j)
             {
-                v = p.unit ? T(1) : A[r + (int64_t)c * p.lda];
+                v = p.unit ? T(1) : A[r + (int64_t)c * lda];
                 if(v == T(0))
                     v = T(1);
             }
             else
-                v = A[r + (int64_t)c * p.lda];
+                v = A[r + (int64_t)c * lda];
         }
         else
             v = (i == j) ? T(1) : T(0);
