@@ -328,3 +328,25 @@ def test_graph_capture_host_and_device_mode(handle):
         torch.cuda.synchronize()
         _check_vs_oracle("L", "L", "N", "N", m, n, 1.0, A, B, dm.to_host(dB), np.float64)
         del g
+
+
+@pytest.mark.parametrize("dt", ["d", "s"])
+@pytest.mark.parametrize("side,uplo,trans,diag", COMBOS)
+def test_trsm_large_all_combos_residual(handle, dt, side, uplo, trans, diag):
+    """Sizes the oracle cannot check quickly (the drop-in sweep's shapes scaled down to
+    m = 2500, n = 300 and the transpose): the normwise residual of the solve in FP64 on the GPU
+    (torch as the checker), for every combination through the chain solve (FP64) and the
+    recursive solve (FP32 with more than 512 columns)."""
+    npdt, tdt = DT[dt]
+    for (m, n) in [(2500, 300), (300, 2500)]:
+        k = m if side == "L" else n
+        A, B = oracle.nan_triangle_problem(4242, side, uplo, trans, diag, m, n, k, m, npdt)
+        out, _ = _gpu_solve(handle, side, uplo, trans, diag, m, n, -0.5, A, B)
+        T = torch.from_numpy(oracle.clean_triangle(A, k, uplo, diag).astype(np.float64)).cuda()
+        opT = T if trans == "N" else T.T
+        X = torch.from_numpy(np.ascontiguousarray(out[:m]).astype(np.float64)).cuda()
+        Bd = torch.from_numpy(np.ascontiguousarray(B[:m]).astype(np.float64)).cuda()
+        R = (opT @ X if side == "L" else X @ opT) + 0.5 * Bd
+        scale = (opT.abs() @ X.abs() if side == "L" else X.abs() @ opT.abs()).sum()
+        rel = (R.abs().sum() / scale).item()
+        assert rel < (1e-13 if dt == "d" else 1e-4), (side, uplo, trans, diag, m, n, rel)
