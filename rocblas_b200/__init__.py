@@ -100,6 +100,10 @@ _H = ctypes.c_void_p
 _TRSM = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i]
 _TRSM_B = _TRSM + [_i]
 _TRSM_SB = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _i]
+# trmm: handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, C, ldc (+ batch / strides)
+_TRMM = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _i]
+_TRMM_B = _TRMM + [_i]
+_TRMM_SB = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _p, _i, _i64, _i]
 _TRTRI = [_H, _i, _i, _i, _p, _i, _p, _i]
 _TRTRI_B = _TRTRI + [_i]
 _TRTRI_SB = [_H, _i, _i, _i, _p, _i, _i64, _p, _i, _i64, _i]
@@ -119,6 +123,18 @@ SIGNATURES = {
     "rocblas_set_workspace": (_i, [_H, _p, _sz]),
     "rocblas_is_managing_device_memory": (ctypes.c_bool, [_H]),
     "rocblas_is_user_managing_device_memory": (ctypes.c_bool, [_H]),
+    "rocblas_strsv": (_i, [_H, _i, _i, _i, _i, _p, _i, _p, _i]),
+    "rocblas_dtrsv": (_i, [_H, _i, _i, _i, _i, _p, _i, _p, _i]),
+    "rocblas_strsv_batched": (_i, [_H, _i, _i, _i, _i, _p, _i, _p, _i, _i]),
+    "rocblas_dtrsv_batched": (_i, [_H, _i, _i, _i, _i, _p, _i, _p, _i, _i]),
+    "rocblas_strsv_strided_batched": (_i, [_H, _i, _i, _i, _i, _p, _i, _i64, _p, _i, _i64, _i]),
+    "rocblas_dtrsv_strided_batched": (_i, [_H, _i, _i, _i, _i, _p, _i, _i64, _p, _i, _i64, _i]),
+    "rocblas_strmm": (_i, _TRMM),
+    "rocblas_dtrmm": (_i, _TRMM),
+    "rocblas_strmm_batched": (_i, _TRMM_B),
+    "rocblas_dtrmm_batched": (_i, _TRMM_B),
+    "rocblas_strmm_strided_batched": (_i, _TRMM_SB),
+    "rocblas_dtrmm_strided_batched": (_i, _TRMM_SB),
     "rocblas_strsm": (_i, _TRSM),
     "rocblas_dtrsm": (_i, _TRSM),
     "rocblas_strsm_batched": (_i, _TRSM_B),

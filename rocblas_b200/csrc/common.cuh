@@ -69,14 +69,23 @@ enum : int
 // triangle masks used when an operand is a triangular block (stored coordinates r, c)
 enum : int
 {
-    kTriNone  = 0,
-    kTriLower = 1, // keep r >= c
-    kTriUpper = 2  // keep r <= c
+    kTriNone        = 0,
+    kTriLower       = 1, // keep r >= c
+    kTriUpper       = 2, // keep r <= c
+    kTriLowerStrict = 3, // keep r > c
+    kTriUpperStrict = 4  // keep r < c
 };
 
 __device__ __forceinline__ bool tri_keep(int tri, int64_t r, int64_t c)
 {
-    return tri == kTriNone || (tri == kTriLower ? r >= c : r <= c);
+    switch(tri)
+    {
+    case kTriLower: return r >= c;
+    case kTriUpper: return r <= c;
+    case kTriLowerStrict: return r > c;
+    case kTriUpperStrict: return r < c;
+    default: return true;
+    }
 }
 
 } // namespace rb200

@@ -269,6 +269,236 @@ BatchPtr<T> arrayed(const void* arr)
     return b;
 }
 
+// ---- trmm ----------------------------------------------------------------------------------
+// C := alpha op(A) B (side L) or alpha B op(A) (side R), A triangular; the reference's
+// out-of-place API (rocblas-functions.h:18300-18393), with C == B allowed when ldc == ldb.
+// One GEMM on the tiles of the solve with A's unused triangle masked at load time; a unit
+// diagonal is the strict triangle plus B itself (C := alpha op(A_strict) B + alpha B).  In
+// place, B is first copied to the workspace.
+
+template <typename T>
+__global__ void copy_matrix_kernel(BatchPtr<T> src, int64_t lds, BatchPtr<T> dst, int64_t ldd, int m,
+                                   int n, int batch_base)
+{
+    const T*  s = src.get(batch_base + blockIdx.z);
+    T*        d = dst.get(batch_base + blockIdx.z);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if(i < m)
+        d[i + (int64_t)j * ldd] = s[i + (int64_t)j * lds];
+}
+
+template <typename T>
+void copy_matrix(BatchPtr<T> src, int64_t lds, BatchPtr<T> dst, int64_t ldd, int m, int n, int batch,
+                 cudaStream_t s)
+{
+    for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+        for(int j0 = 0; j0 < n; j0 += kMaxGridYZ)
+        {
+            dim3 grid((unsigned)ceil_div(m, 256), (unsigned)std::min(kMaxGridYZ, n - j0),
+                      (unsigned)std::min(kMaxGridYZ, batch - b0));
+            copy_matrix_kernel<T><<<grid, 256, 0, s>>>(src.shifted((int64_t)j0 * lds), lds,
+                                                       dst.shifted((int64_t)j0 * ldd), ldd, m,
+                                                       std::min(kMaxGridYZ, n - j0), b0);
+            count_launch();
+        }
+}
+
+// rocblas_trmm_arg_check (library/src/blas3/rocblas_trmm.hpp:51-105)
+template <typename T>
+rocblas_status trmm_arg_check(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                              rocblas_operation trans, rocblas_diagonal diag, int64_t m, int64_t n,
+                              const T* alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
+                              const void* C, int64_t ldc, int64_t batch)
+{
+    if(side != rocblas_side_left && side != rocblas_side_right)
+        return rocblas_status_invalid_value;
+    if(uplo != rocblas_fill_lower && uplo != rocblas_fill_upper)
+        return rocblas_status_invalid_value;
+    if(trans != rocblas_operation_none && trans != rocblas_operation_transpose
+       && trans != rocblas_operation_conjugate_transpose)
+        return rocblas_status_invalid_value;
+    if(diag != rocblas_diagonal_non_unit && diag != rocblas_diagonal_unit)
+        return rocblas_status_invalid_value;
+    if(batch < 0 || m < 0 || n < 0 || ldc < m || ldb < m
+       || (side == rocblas_side_left ? lda < m : lda < n))
+        return rocblas_status_invalid_size;
+    if(!m || !n || !batch)
+        return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
+    if(!h->size_query)
+    {
+        if(!C || !alpha
+           || (h->pointer_mode == rocblas_pointer_mode_host && *alpha != T(0) && (!A || !B)))
+            return rocblas_status_invalid_pointer;
+    }
+    if(B == C && ldb != ldc)
+        return rocblas_status_invalid_value;
+    return rocblas_status_continue;
+}
+
+template <typename T>
+rocblas_status trmm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                         rocblas_operation trans, rocblas_diagonal diag, int m, int n,
+                         const T* alpha, const void* Aptr, BatchPtr<T> A, int lda, const void* Bptr,
+                         BatchPtr<T> B, int ldb, const void* Cptr, BatchPtr<T> C, int ldc, int batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st = trmm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr,
+                                          ldb, Cptr, ldc, batch);
+    if(st != rocblas_status_continue)
+        return st;
+    const bool   in_place = Bptr == Cptr;
+    const size_t ws_bytes = in_place ? sizeof(T) * (size_t)m * n * batch : 0;
+    if(h->size_query)
+        return ws_bytes ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    if(h->pointer_mode == rocblas_pointer_mode_host && *alpha == T(0))
+    {
+        zero_fill<T>(C, ldc, m, n, batch, h->stream);
+        return launch_status();
+    }
+    BatchPtr<T> src = B;
+    int64_t     lds = ldb;
+    if(in_place)
+    {
+        void* ws = h->borrow(ws_bytes);
+        if(!ws)
+            return rocblas_status_memory_error;
+        src.base   = reinterpret_cast<T*>(ws);
+        src.arr    = nullptr;
+        src.stride = (int64_t)m * n;
+        src.offset = 0;
+        lds        = m;
+        copy_matrix<T>(B, ldb, src, lds, m, n, batch, h->stream);
+    }
+    const bool unit = diag == rocblas_diagonal_unit;
+    if(unit && !in_place)
+        copy_matrix<T>(B, ldb, C, ldc, m, n, batch, h->stream); // C := B, the diagonal's part
+    const bool lower = uplo == rocblas_fill_lower;
+    const int  tri   = unit ? (lower ? kTriLowerStrict : kTriUpperStrict) : (lower ? kTriLower : kTriUpper);
+    GemmParams<T> g{};
+    g.M = m;
+    g.N = n;
+    if(side == rocblas_side_left)
+    {
+        g.K = m;
+        g.P = A; g.ldp = lda; g.transP = trans != rocblas_operation_none; g.triP = tri;
+        g.Q = src; g.ldq = lds; g.transQ = 0; g.triQ = kTriNone;
+    }
+    else
+    {
+        g.K = n;
+        g.P = src; g.ldp = lds; g.transP = 0; g.triP = kTriNone;
+        g.Q = A; g.ldq = lda; g.transQ = trans != rocblas_operation_none; g.triQ = tri;
+    }
+    g.C = C;
+    g.ldc = ldc;
+    g.a_imm = T(1); g.a_user = 1;              // a = alpha
+    g.b_imm = T(0); g.b_user = unit ? 1 : 0;   // b = alpha (unit: C holds B) or 0
+    g.ualpha.val = h->pointer_mode == rocblas_pointer_mode_host ? *alpha : T(1);
+    g.ualpha.ptr = h->pointer_mode == rocblas_pointer_mode_host ? nullptr : alpha;
+    g.zero_guard = 1;
+    launch_gemm<T>(g, batch, h->stream, h->sm_count);
+    return launch_status();
+}
+
+// ---- trsv ----------------------------------------------------------------------------------
+// x := op(A)^-1 x (rocblas-functions.h:9900-9908, batched :10041-10050, strided :10198-10209).
+// The vector x with increment incx > 0 is a 1 x n row matrix with leading dimension incx, and
+// op(A) x = b is x^T op(A)^T = b^T: a trsm with side right, m = 1 and the transpose flipped.
+// A negative increment (x traversed backwards) goes through a reversed contiguous copy.
+
+template <typename T>
+__global__ void trsv_reverse_kernel(BatchPtr<T> x, int64_t incx, T* tmp, int n, int to_tmp, int batch_base)
+{
+    const int b = batch_base + blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    // element i of the vector lives at x + (n - 1 - i) * |incx| when incx < 0
+    T* xp = x.get(b) + (int64_t)(n - 1 - i) * (-incx);
+    T* tp = tmp + (int64_t)b * n + i;
+    if(to_tmp)
+        *tp = *xp;
+    else
+        *xp = *tp;
+}
+
+// rocblas_trsv_arg_check (library/src/blas2/rocblas_trsv.hpp:31-80)
+template <typename T>
+rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
+                         rocblas_diagonal diag, int n, const void* Aptr, BatchPtr<T> A, int lda,
+                         const void* xptr, BatchPtr<T> x, int incx, int batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(uplo != rocblas_fill_lower && uplo != rocblas_fill_upper)
+        return rocblas_status_invalid_value;
+    if(trans != rocblas_operation_none && trans != rocblas_operation_transpose
+       && trans != rocblas_operation_conjugate_transpose)
+        return rocblas_status_invalid_value;
+    if(diag != rocblas_diagonal_unit && diag != rocblas_diagonal_non_unit)
+        return rocblas_status_invalid_value;
+    if(n < 0 || lda < n || lda < 1 || !incx || batch < 0)
+        return rocblas_status_invalid_size;
+    if(!n || !batch)
+        return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
+    if(!h->size_query && (!Aptr || !xptr))
+        return rocblas_status_invalid_pointer;
+    const rocblas_operation flip
+        = trans == rocblas_operation_none ? rocblas_operation_transpose : rocblas_operation_none;
+    static const T one = T(1);
+    // the solve's alpha is 1 whatever the pointer mode
+    const rocblas_pointer_mode mode = h->pointer_mode;
+    h->pointer_mode                 = rocblas_pointer_mode_host;
+    rocblas_status st;
+    if(incx > 0)
+    {
+        st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, xptr, x,
+                          incx, batch, nullptr, BatchPtr<T>{}, 0);
+    }
+    else if(h->size_query)
+    {
+        st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, xptr, x,
+                          1, batch, nullptr, BatchPtr<T>{}, 0);
+    }
+    else
+    {
+        st = device_ready(h);
+        T* tmp = nullptr;
+        if(st == rocblas_status_success
+           && cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(T) * (size_t)n * batch, h->stream)
+                  != cudaSuccess)
+        {
+            cudaGetLastError();
+            st = rocblas_status_memory_error;
+        }
+        if(st == rocblas_status_success)
+        {
+            for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+            {
+                dim3 grid((unsigned)ceil_div(n, 256), (unsigned)std::min(kMaxGridYZ, batch - b0));
+                trsv_reverse_kernel<T><<<grid, 256, 0, h->stream>>>(x, incx, tmp, n, 1, b0);
+                count_launch();
+            }
+            st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, tmp,
+                              strided<T>(tmp, n), 1, batch, nullptr, BatchPtr<T>{}, 0);
+            if(st == rocblas_status_success || st == rocblas_status_perf_degraded)
+                for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+                {
+                    dim3 grid((unsigned)ceil_div(n, 256), (unsigned)std::min(kMaxGridYZ, batch - b0));
+                    trsv_reverse_kernel<T><<<grid, 256, 0, h->stream>>>(x, incx, tmp, n, 0, b0);
+                    count_launch();
+                }
+            cudaFreeAsync(tmp, h->stream);
+        }
+    }
+    h->pointer_mode = mode;
+    return st;
+}
+
 // ---- trtri ---------------------------------------------------------------------------------
 // rocblas_trtri_arg_check (library/src/blas3/rocblas_trtri.hpp:30-64)
 rocblas_status trtri_arg_check(rocblas_fill uplo, rocblas_diagonal diag, int64_t n,
@@ -1295,6 +1525,106 @@ catch(...)
 {
     return exception_status();
 }
+
+// ---- trsv (rocblas-functions.h:9900-9908, 10041-10050, 10198-10209) ------------------------
+#define TRSV_ALL(T, S)                                                                              \
+    rocblas_status rocblas_##S##trsv(rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, \
+                                     rocblas_diagonal diag, rocblas_int n, const T* A,              \
+                                     rocblas_int lda, T* x, rocblas_int incx)                       \
+    try                                                                                             \
+    {                                                                                               \
+        return trsv_impl<T>(h, uplo, transA, diag, n, A, strided<T>(A, 0), lda, x,                  \
+                            strided<T>(x, 0), incx, 1);                                             \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trsv_batched(rocblas_handle h, rocblas_fill uplo,                   \
+                                             rocblas_operation transA, rocblas_diagonal diag,       \
+                                             rocblas_int n, const T* const A[], rocblas_int lda,    \
+                                             T* const x[], rocblas_int incx,                        \
+                                             rocblas_int batch_count)                               \
+    try                                                                                             \
+    {                                                                                               \
+        return trsv_impl<T>(h, uplo, transA, diag, n, A, arrayed<T>(A), lda, x, arrayed<T>(x), incx, \
+                            batch_count);                                                           \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trsv_strided_batched(                                               \
+        rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, rocblas_diagonal diag,       \
+        rocblas_int n, const T* A, rocblas_int lda, rocblas_stride stride_A, T* x,                  \
+        rocblas_int incx, rocblas_stride stride_x, rocblas_int batch_count)                         \
+    try                                                                                             \
+    {                                                                                               \
+        return trsv_impl<T>(h, uplo, transA, diag, n, A, strided<T>(A, stride_A), lda, x,           \
+                            strided<T>(x, stride_x), incx, batch_count);                            \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }
+TRSV_ALL(float, s)
+TRSV_ALL(double, d)
+
+// ---- trmm (rocblas-functions.h:18300-18393, 18630-18644, 18904-18921) -----------------------
+#define TRMM_PLAIN(NAME, T)                                                                         \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
+                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
+                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda, const T* B,      \
+                        rocblas_int ldb, T* C, rocblas_int ldc)                                     \
+    try                                                                                             \
+    {                                                                                               \
+        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, 0), lda, B,   \
+                            strided<T>(B, 0), ldb, C, strided<T>(C, 0), ldc, 1);                    \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }
+TRMM_PLAIN(rocblas_strmm, float)
+TRMM_PLAIN(rocblas_dtrmm, double)
+
+#define TRMM_BATCHED(NAME, T)                                                                       \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
+                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
+                        rocblas_int n, const T* alpha, const T* const A[], rocblas_int lda,          \
+                        const T* const B[], rocblas_int ldb, T* const C[], rocblas_int ldc,          \
+                        rocblas_int batch_count)                                                    \
+    try                                                                                             \
+    {                                                                                               \
+        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, arrayed<T>(A), lda, B,      \
+                            arrayed<T>(B), ldb, C, arrayed<T>(C), ldc, batch_count);                \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }
+TRMM_BATCHED(rocblas_strmm_batched, float)
+TRMM_BATCHED(rocblas_dtrmm_batched, double)
+
+#define TRMM_STRIDED(NAME, T)                                                                       \
+    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
+                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
+                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda,                  \
+                        rocblas_stride stride_A, const T* B, rocblas_int ldb,                       \
+                        rocblas_stride stride_B, T* C, rocblas_int ldc, rocblas_stride stride_C,    \
+                        rocblas_int batch_count)                                                    \
+    try                                                                                             \
+    {                                                                                               \
+        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, stride_A),    \
+                            lda, B, strided<T>(B, stride_B), ldb, C, strided<T>(C, stride_C), ldc,  \
+                            batch_count);                                                           \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }
+TRMM_STRIDED(rocblas_strmm_strided_batched, float)
+TRMM_STRIDED(rocblas_dtrmm_strided_batched, double)
 
 // ---- server (rocblas_b200_ext.h) --------------------------------------------------------------
 struct rocblas_b200_server_

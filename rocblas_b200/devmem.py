@@ -81,6 +81,29 @@ def trsm_strided_batched(handle, side, uplo, trans, diag, m, n, alpha, A, lda, s
     return check("rocblas_trsm_strided_batched", st, allow)
 
 
+def trmm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, C, ldc, alpha_on_device=False,
+         allow=(status_success,)):
+    """rocblas_?trmm on device tensors: C := alpha op(A) B (side L) or alpha B op(A) (side R);
+    C may be B (in place, ldc == ldb)."""
+    dbl = _is_double(C)
+    fn = lib().rocblas_dtrmm if dbl else lib().rocblas_strmm
+    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, C.device)
+    st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
+            m, n, aptr, _ptr(A), lda, _ptr(B), ldb, _ptr(C), ldc)
+    _restore(handle, alpha_on_device)
+    return check("rocblas_trmm", st, allow)
+
+
+def trmm_strided_batched(handle, side, uplo, trans, diag, m, n, alpha, A, lda, stride_a, B, ldb,
+                         stride_b, C, ldc, stride_c, batch, allow=(status_success,)):
+    dbl = _is_double(C)
+    fn = lib().rocblas_dtrmm_strided_batched if dbl else lib().rocblas_strmm_strided_batched
+    keep, aptr = _alpha(handle, alpha, dbl, False, C.device)
+    st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
+            m, n, aptr, _ptr(A), lda, stride_a, _ptr(B), ldb, stride_b, _ptr(C), ldc, stride_c, batch)
+    return check("rocblas_trmm_strided_batched", st, allow)
+
+
 def trsm_batched(handle, side, uplo, trans, diag, m, n, alpha, A_list, lda, B_list, ldb,
                  alpha_on_device=False, allow=(status_success,)):
     """A_list / B_list: lists of device tensors; their addresses are gathered into device
@@ -147,6 +170,7 @@ def build_invA(handle, uplo, diag, A, lda, k, nb=128):
     return invA
 
 
-__all__ = ["to_device", "to_host", "empty", "trsm", "trsm_ex", "trsm_strided_batched",
+__all__ = ["to_device", "to_host", "empty", "trsm", "trsm_ex", "trsm_strided_batched", "trmm",
+           "trmm_strided_batched",
            "trsm_batched", "trtri", "trtri_strided_batched", "build_invA", "status_perf_degraded",
            "pointer_mode_host", "pointer_mode_device"]
