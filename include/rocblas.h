@@ -524,6 +524,266 @@ ROCBLAS_EXPORT rocblas_status rocblas_dtrmm_strided_batched(rocblas_handle    ha
                                                             rocblas_stride    stride_C,
                                                             rocblas_int       batch_count);
 
+/* ---- ILP64 (_64) forms: the same functions with 64-bit sizes, leading dimensions,
+ * increments and batch counts (trsm: rocblas-functions.h:19441-19492, 19631-19685,
+ * 19839-19901; trsv: 9930-9970, 10074-10118, 10237-10290; trmm: 18426-18485, 18679-18741,
+ * 18962-19037).  The order of A must fit in 32 bits (A is k x k); a larger one is
+ * rocblas_status_invalid_size. --------------------------------------------------------- */
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsm_64(rocblas_handle    handle,
+                                               rocblas_side      side,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           m,
+                                               int64_t           n,
+                                               const float*      alpha,
+                                               const float*      A,
+                                               int64_t           lda,
+                                               float*            B,
+                                               int64_t           ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsm_batched_64(rocblas_handle      handle,
+                                                       rocblas_side        side,
+                                                       rocblas_fill        uplo,
+                                                       rocblas_operation   transA,
+                                                       rocblas_diagonal    diag,
+                                                       int64_t             m,
+                                                       int64_t             n,
+                                                       const float*        alpha,
+                                                       const float* const* A,
+                                                       int64_t             lda,
+                                                       float* const*       B,
+                                                       int64_t             ldb,
+                                                       int64_t             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsm_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_side      side,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           m,
+                                                               int64_t           n,
+                                                               const float*      alpha,
+                                                               const float*      A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_a,
+                                                               float*            B,
+                                                               int64_t           ldb,
+                                                               rocblas_stride    stride_b,
+                                                               int64_t           batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsv_64(rocblas_handle    handle,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           n,
+                                               const float*      A,
+                                               int64_t           lda,
+                                               float*            x,
+                                               int64_t           incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsv_batched_64(rocblas_handle      handle,
+                                                       rocblas_fill        uplo,
+                                                       rocblas_operation   transA,
+                                                       rocblas_diagonal    diag,
+                                                       int64_t             n,
+                                                       const float* const* A,
+                                                       int64_t             lda,
+                                                       float* const*       x,
+                                                       int64_t             incx,
+                                                       int64_t             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strsv_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           n,
+                                                               const float*      A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_A,
+                                                               float*            x,
+                                                               int64_t           incx,
+                                                               rocblas_stride    stride_x,
+                                                               int64_t           batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strmm_64(rocblas_handle    handle,
+                                               rocblas_side      side,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           m,
+                                               int64_t           n,
+                                               const float*      alpha,
+                                               const float*      A,
+                                               int64_t           lda,
+                                               const float*      B,
+                                               int64_t           ldb,
+                                               float*            C,
+                                               int64_t           ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strmm_batched_64(rocblas_handle      handle,
+                                                       rocblas_side        side,
+                                                       rocblas_fill        uplo,
+                                                       rocblas_operation   transA,
+                                                       rocblas_diagonal    diag,
+                                                       int64_t             m,
+                                                       int64_t             n,
+                                                       const float*        alpha,
+                                                       const float* const* A,
+                                                       int64_t             lda,
+                                                       const float* const* B,
+                                                       int64_t             ldb,
+                                                       float* const*       C,
+                                                       int64_t             ldc,
+                                                       int64_t             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_strmm_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_side      side,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           m,
+                                                               int64_t           n,
+                                                               const float*      alpha,
+                                                               const float*      A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_A,
+                                                               const float*      B,
+                                                               int64_t           ldb,
+                                                               rocblas_stride    stride_B,
+                                                               float*            C,
+                                                               int64_t           ldc,
+                                                               rocblas_stride    stride_C,
+                                                               int64_t           batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm_64(rocblas_handle    handle,
+                                               rocblas_side      side,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           m,
+                                               int64_t           n,
+                                               const double*     alpha,
+                                               const double*     A,
+                                               int64_t           lda,
+                                               double*           B,
+                                               int64_t           ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm_batched_64(rocblas_handle       handle,
+                                                       rocblas_side         side,
+                                                       rocblas_fill         uplo,
+                                                       rocblas_operation    transA,
+                                                       rocblas_diagonal     diag,
+                                                       int64_t              m,
+                                                       int64_t              n,
+                                                       const double*        alpha,
+                                                       const double* const* A,
+                                                       int64_t              lda,
+                                                       double* const*       B,
+                                                       int64_t              ldb,
+                                                       int64_t              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsm_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_side      side,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           m,
+                                                               int64_t           n,
+                                                               const double*     alpha,
+                                                               const double*     A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_a,
+                                                               double*           B,
+                                                               int64_t           ldb,
+                                                               rocblas_stride    stride_b,
+                                                               int64_t           batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsv_64(rocblas_handle    handle,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           n,
+                                               const double*     A,
+                                               int64_t           lda,
+                                               double*           x,
+                                               int64_t           incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsv_batched_64(rocblas_handle       handle,
+                                                       rocblas_fill         uplo,
+                                                       rocblas_operation    transA,
+                                                       rocblas_diagonal     diag,
+                                                       int64_t              n,
+                                                       const double* const* A,
+                                                       int64_t              lda,
+                                                       double* const*       x,
+                                                       int64_t              incx,
+                                                       int64_t              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrsv_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           n,
+                                                               const double*     A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_A,
+                                                               double*           x,
+                                                               int64_t           incx,
+                                                               rocblas_stride    stride_x,
+                                                               int64_t           batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrmm_64(rocblas_handle    handle,
+                                               rocblas_side      side,
+                                               rocblas_fill      uplo,
+                                               rocblas_operation transA,
+                                               rocblas_diagonal  diag,
+                                               int64_t           m,
+                                               int64_t           n,
+                                               const double*     alpha,
+                                               const double*     A,
+                                               int64_t           lda,
+                                               const double*     B,
+                                               int64_t           ldb,
+                                               double*           C,
+                                               int64_t           ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrmm_batched_64(rocblas_handle       handle,
+                                                       rocblas_side         side,
+                                                       rocblas_fill         uplo,
+                                                       rocblas_operation    transA,
+                                                       rocblas_diagonal     diag,
+                                                       int64_t              m,
+                                                       int64_t              n,
+                                                       const double*        alpha,
+                                                       const double* const* A,
+                                                       int64_t              lda,
+                                                       const double* const* B,
+                                                       int64_t              ldb,
+                                                       double* const*       C,
+                                                       int64_t              ldc,
+                                                       int64_t              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_dtrmm_strided_batched_64(rocblas_handle    handle,
+                                                               rocblas_side      side,
+                                                               rocblas_fill      uplo,
+                                                               rocblas_operation transA,
+                                                               rocblas_diagonal  diag,
+                                                               int64_t           m,
+                                                               int64_t           n,
+                                                               const double*     alpha,
+                                                               const double*     A,
+                                                               int64_t           lda,
+                                                               rocblas_stride    stride_A,
+                                                               const double*     B,
+                                                               int64_t           ldb,
+                                                               rocblas_stride    stride_B,
+                                                               double*           C,
+                                                               int64_t           ldc,
+                                                               rocblas_stride    stride_C,
+                                                               int64_t           batch_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,17 @@ _TRSM_SB = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _i]
 _TRMM = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _i]
 _TRMM_B = _TRMM + [_i]
 _TRMM_SB = [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _p, _i, _i64, _i]
+# the ILP64 (_64) forms: every size, leading dimension, increment and batch count 64-bit
+_L = _i64
+_TRSM_64 = [_H, _i, _i, _i, _i, _L, _L, _p, _p, _L, _p, _L]
+_TRSM_B_64 = _TRSM_64 + [_L]
+_TRSM_SB_64 = [_H, _i, _i, _i, _i, _L, _L, _p, _p, _L, _i64, _p, _L, _i64, _L]
+_TRMM_64 = [_H, _i, _i, _i, _i, _L, _L, _p, _p, _L, _p, _L, _p, _L]
+_TRMM_B_64 = _TRMM_64 + [_L]
+_TRMM_SB_64 = [_H, _i, _i, _i, _i, _L, _L, _p, _p, _L, _i64, _p, _L, _i64, _p, _L, _i64, _L]
+_TRSV_64 = [_H, _i, _i, _i, _L, _p, _L, _p, _L]
+_TRSV_B_64 = _TRSV_64 + [_L]
+_TRSV_SB_64 = [_H, _i, _i, _i, _L, _p, _L, _i64, _p, _L, _i64, _L]
 _TRTRI = [_H, _i, _i, _i, _p, _i, _p, _i]
 _TRTRI_B = _TRTRI + [_i]
 _TRTRI_SB = [_H, _i, _i, _i, _p, _i, _i64, _p, _i, _i64, _i]
@@ -145,6 +156,10 @@ SIGNATURES = {
     "rocblas_trsm_batched_ex": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i, _p, _i, _i]),
     "rocblas_trsm_strided_batched_ex": (
         _i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _i, _p, _i, _i64, _i]),
+    **{f"rocblas_{t}{name}_64": (_i, sig) for t in "sd" for name, sig in (
+        ("trsm", _TRSM_64), ("trsm_batched", _TRSM_B_64), ("trsm_strided_batched", _TRSM_SB_64),
+        ("trmm", _TRMM_64), ("trmm_batched", _TRMM_B_64), ("trmm_strided_batched", _TRMM_SB_64),
+        ("trsv", _TRSV_64), ("trsv_batched", _TRSV_B_64), ("trsv_strided_batched", _TRSV_SB_64))},
     "rocblas_strtri": (_i, _TRTRI),
     "rocblas_dtrtri": (_i, _TRTRI),
     "rocblas_strtri_batched": (_i, _TRTRI_B),

@@ -162,8 +162,8 @@ rocblas_status trsm_arg_check(rocblas_handle h, rocblas_side side, rocblas_fill 
 template <typename T>
 rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                          rocblas_operation trans, rocblas_diagonal diag, int m, int n,
-                         const T* alpha, const void* Aptr, BatchPtr<T> A, int lda,
-                         const void* Bptr, BatchPtr<T> B, int ldb, int batch,
+                         const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
+                         const void* Bptr, BatchPtr<T> B, int64_t ldb, int batch,
                          const void* invA_ptr, BatchPtr<T> invA, int64_t invA_size)
 {
     if(!h)
@@ -339,8 +339,9 @@ rocblas_status trmm_arg_check(rocblas_handle h, rocblas_side side, rocblas_fill 
 template <typename T>
 rocblas_status trmm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                          rocblas_operation trans, rocblas_diagonal diag, int m, int n,
-                         const T* alpha, const void* Aptr, BatchPtr<T> A, int lda, const void* Bptr,
-                         BatchPtr<T> B, int ldb, const void* Cptr, BatchPtr<T> C, int ldc, int batch)
+                         const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
+                         const void* Bptr, BatchPtr<T> B, int64_t ldb, const void* Cptr,
+                         BatchPtr<T> C, int64_t ldc, int batch)
 {
     if(!h)
         return rocblas_status_invalid_handle;
@@ -427,13 +428,10 @@ __global__ void trsv_reverse_kernel(BatchPtr<T> x, int64_t incx, T* tmp, int n, 
 }
 
 // rocblas_trsv_arg_check (library/src/blas2/rocblas_trsv.hpp:31-80)
-template <typename T>
-rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
-                         rocblas_diagonal diag, int n, const void* Aptr, BatchPtr<T> A, int lda,
-                         const void* xptr, BatchPtr<T> x, int incx, int batch)
+inline rocblas_status trsv_arg_check(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
+                                     rocblas_diagonal diag, int64_t n, const void* A, int64_t lda,
+                                     const void* x, int64_t incx, int64_t batch)
 {
-    if(!h)
-        return rocblas_status_invalid_handle;
     if(uplo != rocblas_fill_lower && uplo != rocblas_fill_upper)
         return rocblas_status_invalid_value;
     if(trans != rocblas_operation_none && trans != rocblas_operation_transpose
@@ -445,8 +443,21 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
         return rocblas_status_invalid_size;
     if(!n || !batch)
         return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
-    if(!h->size_query && (!Aptr || !xptr))
+    if(!h->size_query && (!A || !x))
         return rocblas_status_invalid_pointer;
+    return rocblas_status_continue;
+}
+
+template <typename T>
+rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
+                         rocblas_diagonal diag, int n, const void* Aptr, BatchPtr<T> A, int64_t lda,
+                         const void* xptr, BatchPtr<T> x, int64_t incx, int batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status ast = trsv_arg_check(h, uplo, trans, diag, n, Aptr, lda, xptr, incx, batch);
+    if(ast != rocblas_status_continue)
+        return ast;
     const rocblas_operation flip
         = trans == rocblas_operation_none ? rocblas_operation_transpose : rocblas_operation_none;
     static const T one = T(1);
@@ -497,6 +508,153 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
     }
     h->pointer_mode = mode;
     return st;
+}
+
+// ---- ILP64 bodies ---------------------------------------------------------------------------
+// The _64 entry points (rocblas_internal_trsm_launcher_64,
+// library/src/src64/blas3/rocblas_trsm_kernels_64.cpp:31-225, and the trsv / trmm twins in
+// library/src/src64/blas2/rocblas_trsv_kernels_64.cpp:28-86 and src64/blas3) take 64-bit sizes,
+// leading dimensions, increments and batch counts.  Leading dimensions are 64-bit in every
+// kernel of this library, so only sizes need splitting:
+// * the order k of A stays a 32-bit size: A is k x k, so a larger k cannot be in memory, and the
+//   reference returns invalid_size for it as this does;
+// * the dimension of B that the solve (or product) treats independently - its columns for side
+//   left, its rows for side right - is cut into chunks.  Columns of B are the GEMM tiles' grid
+//   y dimension (at most 65535 tiles of at least 32 columns), so side left takes 2^20 columns
+//   per chunk; rows are the grid x dimension, so side right takes 2^28 rows;
+// * the batch is cut into chunks of 2^30.
+// The 32-bit entry points run through the same bodies, so a 32-bit size beyond a chunk is
+// split as well.
+constexpr int64_t kIlpColChunk   = int64_t(1) << 20;
+constexpr int64_t kIlpRowChunk   = int64_t(1) << 28;
+constexpr int64_t kIlpBatchChunk = int64_t(1) << 30;
+
+template <typename T>
+BatchPtr<T> batch_advance(BatchPtr<T> p, int64_t b0)
+{
+    if(p.arr)
+        p.arr = reinterpret_cast<T* const*>(p.arr) + b0;
+    else if(p.base)
+        p.base += b0 * p.stride;
+    return p;
+}
+
+// Folds the statuses of chunked calls: an error ends the loop and is returned; otherwise
+// perf_degraded (or, in a size query, size_increased) outranks success (size_unchanged).
+struct ChunkStatus
+{
+    rocblas_status st = rocblas_status_continue;
+
+    bool add(rocblas_status s)
+    {
+        const bool ok = s == rocblas_status_success || s == rocblas_status_perf_degraded
+                        || s == rocblas_status_size_unchanged || s == rocblas_status_size_increased;
+        if(!ok || st == rocblas_status_continue)
+        {
+            st = s;
+            return ok;
+        }
+        if(s == rocblas_status_perf_degraded || s == rocblas_status_size_increased)
+            st = s;
+        return true;
+    }
+};
+
+template <typename T>
+rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                            rocblas_operation trans, rocblas_diagonal diag, int64_t m, int64_t n,
+                            const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
+                            const void* Bptr, BatchPtr<T> B, int64_t ldb, int64_t batch,
+                            const void* invA_ptr = nullptr, BatchPtr<T> invA = BatchPtr<T>{},
+                            int64_t invA_size = 0)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st
+        = trsm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr, ldb, batch);
+    if(st != rocblas_status_continue)
+        return st;
+    const bool left = side == rocblas_side_left;
+    if((left ? m : n) > INT32_MAX)
+        return rocblas_status_invalid_size;
+    const int64_t dim   = left ? n : m;
+    const int64_t chunk = left ? kIlpColChunk : kIlpRowChunk;
+    ChunkStatus   cs;
+    for(int64_t b0 = 0; b0 < batch; b0 += kIlpBatchChunk)
+    {
+        const int nb = (int)std::min(kIlpBatchChunk, batch - b0);
+        for(int64_t d0 = 0; d0 < dim; d0 += chunk)
+        {
+            const int nd = (int)std::min(chunk, dim - d0);
+            st = trsm_impl<T>(h, side, uplo, trans, diag, left ? (int)m : nd, left ? nd : (int)n,
+                              alpha, Aptr, batch_advance(A, b0), lda, Bptr,
+                              batch_advance(B, b0).shifted(left ? d0 * ldb : d0), ldb, nb, invA_ptr,
+                              batch_advance(invA, b0), invA_size);
+            if(!cs.add(st))
+                return cs.st;
+        }
+    }
+    return cs.st;
+}
+
+template <typename T>
+rocblas_status trsv_impl_64(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
+                            rocblas_diagonal diag, int64_t n, const void* Aptr, BatchPtr<T> A,
+                            int64_t lda, const void* xptr, BatchPtr<T> x, int64_t incx,
+                            int64_t batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st = trsv_arg_check(h, uplo, trans, diag, n, Aptr, lda, xptr, incx, batch);
+    if(st != rocblas_status_continue)
+        return st;
+    if(n > INT32_MAX)
+        return rocblas_status_invalid_size;
+    ChunkStatus cs;
+    for(int64_t b0 = 0; b0 < batch; b0 += kIlpBatchChunk)
+    {
+        st = trsv_impl<T>(h, uplo, trans, diag, (int)n, Aptr, batch_advance(A, b0), lda, xptr,
+                          batch_advance(x, b0), incx, (int)std::min(kIlpBatchChunk, batch - b0));
+        if(!cs.add(st))
+            return cs.st;
+    }
+    return cs.st;
+}
+
+template <typename T>
+rocblas_status trmm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                            rocblas_operation trans, rocblas_diagonal diag, int64_t m, int64_t n,
+                            const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
+                            const void* Bptr, BatchPtr<T> B, int64_t ldb, const void* Cptr,
+                            BatchPtr<T> C, int64_t ldc, int64_t batch)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_status st = trmm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr,
+                                          ldb, Cptr, ldc, batch);
+    if(st != rocblas_status_continue)
+        return st;
+    const bool left = side == rocblas_side_left;
+    if((left ? m : n) > INT32_MAX)
+        return rocblas_status_invalid_size;
+    const int64_t dim   = left ? n : m;
+    const int64_t chunk = left ? kIlpColChunk : kIlpRowChunk;
+    ChunkStatus   cs;
+    for(int64_t b0 = 0; b0 < batch; b0 += kIlpBatchChunk)
+    {
+        const int nb = (int)std::min(kIlpBatchChunk, batch - b0);
+        for(int64_t d0 = 0; d0 < dim; d0 += chunk)
+        {
+            const int nd = (int)std::min(chunk, dim - d0);
+            st = trmm_impl<T>(h, side, uplo, trans, diag, left ? (int)m : nd, left ? nd : (int)n,
+                              alpha, Aptr, batch_advance(A, b0), lda, Bptr,
+                              batch_advance(B, b0).shifted(left ? d0 * ldb : d0), ldb, Cptr,
+                              batch_advance(C, b0).shifted(left ? d0 * ldc : d0), ldc, nb);
+            if(!cs.add(st))
+                return cs.st;
+        }
+    }
+    return cs.st;
 }
 
 // ---- trtri ---------------------------------------------------------------------------------
@@ -1304,61 +1462,64 @@ bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
 }
 
 // ---- trsm ------------------------------------------------------------------------------------
-#define TRSM_PLAIN(NAME, T)                                                                       \
+#define TRSM_PLAIN(NAME, T, I)                                                                    \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
-                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda, T* B,        \
-                        rocblas_int ldb)                                                         \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
+                        const T* A, I lda, T* B, I ldb)                                          \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, 0), lda,   \
-                            B, strided<T>(B, 0), ldb, 1, nullptr, BatchPtr<T>{}, 0);             \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, 0),     \
+                               lda, B, strided<T>(B, 0), ldb, 1);                                \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_PLAIN(rocblas_strsm, float)
-TRSM_PLAIN(rocblas_dtrsm, double)
+TRSM_PLAIN(rocblas_strsm, float, rocblas_int)
+TRSM_PLAIN(rocblas_dtrsm, double, rocblas_int)
+TRSM_PLAIN(rocblas_strsm_64, float, int64_t)
+TRSM_PLAIN(rocblas_dtrsm_64, double, int64_t)
 
-#define TRSM_BATCHED(NAME, T)                                                                     \
+#define TRSM_BATCHED(NAME, T, I)                                                                  \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
-                        rocblas_int n, const T* alpha, const T* const A[], rocblas_int lda,      \
-                        T* const B[], rocblas_int ldb, rocblas_int batch_count)                  \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
+                        const T* const A[], I lda, T* const B[], I ldb, I batch_count)            \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, arrayed<T>(A), lda, B,   \
-                            arrayed<T>(B), ldb, batch_count, nullptr, BatchPtr<T>{}, 0);         \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A, arrayed<T>(A), lda,   \
+                               B, arrayed<T>(B), ldb, batch_count);                              \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_BATCHED(rocblas_strsm_batched, float)
-TRSM_BATCHED(rocblas_dtrsm_batched, double)
+TRSM_BATCHED(rocblas_strsm_batched, float, rocblas_int)
+TRSM_BATCHED(rocblas_dtrsm_batched, double, rocblas_int)
+TRSM_BATCHED(rocblas_strsm_batched_64, float, int64_t)
+TRSM_BATCHED(rocblas_dtrsm_batched_64, double, int64_t)
 
-#define TRSM_STRIDED(NAME, T)                                                                     \
+#define TRSM_STRIDED(NAME, T, I)                                                                  \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, rocblas_int m,           \
-                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda,              \
-                        rocblas_stride stride_a, T* B, rocblas_int ldb, rocblas_stride stride_b, \
-                        rocblas_int batch_count)                                                 \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
+                        const T* A, I lda, rocblas_stride stride_a, T* B, I ldb,                 \
+                        rocblas_stride stride_b, I batch_count)                                  \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, stride_a), \
-                            lda, B, strided<T>(B, stride_b), ldb, batch_count, nullptr,          \
-                            BatchPtr<T>{}, 0);                                                   \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A,                       \
+                               strided<T>(A, stride_a), lda, B, strided<T>(B, stride_b), ldb,    \
+                               batch_count);                                                     \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_STRIDED(rocblas_strsm_strided_batched, float)
-TRSM_STRIDED(rocblas_dtrsm_strided_batched, double)
+TRSM_STRIDED(rocblas_strsm_strided_batched, float, rocblas_int)
+TRSM_STRIDED(rocblas_dtrsm_strided_batched, double, rocblas_int)
+TRSM_STRIDED(rocblas_strsm_strided_batched_64, float, int64_t)
+TRSM_STRIDED(rocblas_dtrsm_strided_batched_64, double, int64_t)
 
 // rocblas_trsm_ex type switch (library/src/blas3/rocblas_trsm.cpp:28-73)
 rocblas_status rocblas_trsm_ex(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
@@ -1371,12 +1532,12 @@ try
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
-        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+        return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 strided<float>((const float*)A, 0), lda, B,
                                 strided<float>((float*)B, 0), ldb, 1, invA,
                                 strided<float>((const float*)invA, 0), invA_size);
     case rocblas_datatype_f64_r:
-        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+        return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  strided<double>((const double*)A, 0), lda, B,
                                  strided<double>((double*)B, 0), ldb, 1, invA,
                                  strided<double>((const double*)invA, 0), invA_size);
@@ -1404,11 +1565,11 @@ try
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
-        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+        return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 arrayed<float>(A), lda, B, arrayed<float>(B), ldb, batch_count,
                                 invA, arrayed<float>(invA), invA_size);
     case rocblas_datatype_f64_r:
-        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+        return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  arrayed<double>(A), lda, B, arrayed<double>(B), ldb, batch_count,
                                  invA, arrayed<double>(invA), invA_size);
     case rocblas_datatype_f32_c:
@@ -1437,12 +1598,12 @@ try
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
-        return trsm_impl<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
+        return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 strided<float>((const float*)A, stride_A), lda, B,
                                 strided<float>((float*)B, stride_B), ldb, batch_count, invA,
                                 strided<float>((const float*)invA, stride_invA), invA_size);
     case rocblas_datatype_f64_r:
-        return trsm_impl<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
+        return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  strided<double>((const double*)A, stride_A), lda, B,
                                  strided<double>((double*)B, stride_B), ldb, batch_count, invA,
                                  strided<double>((const double*)invA, stride_invA), invA_size);
@@ -1527,104 +1688,97 @@ catch(...)
 }
 
 // ---- trsv (rocblas-functions.h:9900-9908, 10041-10050, 10198-10209) ------------------------
-#define TRSV_ALL(T, S)                                                                              \
-    rocblas_status rocblas_##S##trsv(rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, \
-                                     rocblas_diagonal diag, rocblas_int n, const T* A,              \
-                                     rocblas_int lda, T* x, rocblas_int incx)                       \
+#define TRSV_ALL(T, S, I, SUF)                                                                     \
+    rocblas_status rocblas_##S##trsv##SUF(rocblas_handle h, rocblas_fill uplo,                      \
+                                          rocblas_operation transA, rocblas_diagonal diag, I n,     \
+                                          const T* A, I lda, T* x, I incx)                          \
     try                                                                                             \
     {                                                                                               \
-        return trsv_impl<T>(h, uplo, transA, diag, n, A, strided<T>(A, 0), lda, x,                  \
-                            strided<T>(x, 0), incx, 1);                                             \
+        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(A, 0), lda, x,               \
+                               strided<T>(x, 0), incx, 1);                                          \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }                                                                                               \
-    rocblas_status rocblas_##S##trsv_batched(rocblas_handle h, rocblas_fill uplo,                   \
-                                             rocblas_operation transA, rocblas_diagonal diag,       \
-                                             rocblas_int n, const T* const A[], rocblas_int lda,    \
-                                             T* const x[], rocblas_int incx,                        \
-                                             rocblas_int batch_count)                               \
+    rocblas_status rocblas_##S##trsv_batched##SUF(rocblas_handle h, rocblas_fill uplo,              \
+                                                  rocblas_operation transA, rocblas_diagonal diag,  \
+                                                  I n, const T* const A[], I lda, T* const x[],     \
+                                                  I incx, I batch_count)                            \
     try                                                                                             \
     {                                                                                               \
-        return trsv_impl<T>(h, uplo, transA, diag, n, A, arrayed<T>(A), lda, x, arrayed<T>(x), incx, \
-                            batch_count);                                                           \
+        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, arrayed<T>(A), lda, x, arrayed<T>(x),   \
+                               incx, batch_count);                                                  \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }                                                                                               \
-    rocblas_status rocblas_##S##trsv_strided_batched(                                               \
-        rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, rocblas_diagonal diag,       \
-        rocblas_int n, const T* A, rocblas_int lda, rocblas_stride stride_A, T* x,                  \
-        rocblas_int incx, rocblas_stride stride_x, rocblas_int batch_count)                         \
+    rocblas_status rocblas_##S##trsv_strided_batched##SUF(                                          \
+        rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, rocblas_diagonal diag, I n,  \
+        const T* A, I lda, rocblas_stride stride_A, T* x, I incx, rocblas_stride stride_x,          \
+        I batch_count)                                                                              \
     try                                                                                             \
     {                                                                                               \
-        return trsv_impl<T>(h, uplo, transA, diag, n, A, strided<T>(A, stride_A), lda, x,           \
-                            strided<T>(x, stride_x), incx, batch_count);                            \
+        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(A, stride_A), lda, x,        \
+                               strided<T>(x, stride_x), incx, batch_count);                         \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }
-TRSV_ALL(float, s)
-TRSV_ALL(double, d)
+TRSV_ALL(float, s, rocblas_int, )
+TRSV_ALL(double, d, rocblas_int, )
+TRSV_ALL(float, s, int64_t, _64)
+TRSV_ALL(double, d, int64_t, _64)
 
 // ---- trmm (rocblas-functions.h:18300-18393, 18630-18644, 18904-18921) -----------------------
-#define TRMM_PLAIN(NAME, T)                                                                         \
-    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
-                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
-                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda, const T* B,      \
-                        rocblas_int ldb, T* C, rocblas_int ldc)                                     \
+#define TRMM_ALL(T, S, I, SUF)                                                                      \
+    rocblas_status rocblas_##S##trmm##SUF(rocblas_handle h, rocblas_side side, rocblas_fill uplo,   \
+                                          rocblas_operation transA, rocblas_diagonal diag, I m,     \
+                                          I n, const T* alpha, const T* A, I lda, const T* B,       \
+                                          I ldb, T* C, I ldc)                                       \
     try                                                                                             \
     {                                                                                               \
-        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, 0), lda, B,   \
-                            strided<T>(B, 0), ldb, C, strided<T>(C, 0), ldc, 1);                    \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, 0), lda,  \
+                               B, strided<T>(B, 0), ldb, C, strided<T>(C, 0), ldc, 1);              \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trmm_batched##SUF(                                                  \
+        rocblas_handle h, rocblas_side side, rocblas_fill uplo, rocblas_operation transA,           \
+        rocblas_diagonal diag, I m, I n, const T* alpha, const T* const A[], I lda,                 \
+        const T* const B[], I ldb, T* const C[], I ldc, I batch_count)                              \
+    try                                                                                             \
+    {                                                                                               \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A, arrayed<T>(A), lda, B,  \
+                               arrayed<T>(B), ldb, C, arrayed<T>(C), ldc, batch_count);             \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trmm_strided_batched##SUF(                                          \
+        rocblas_handle h, rocblas_side side, rocblas_fill uplo, rocblas_operation transA,           \
+        rocblas_diagonal diag, I m, I n, const T* alpha, const T* A, I lda,                         \
+        rocblas_stride stride_A, const T* B, I ldb, rocblas_stride stride_B, T* C, I ldc,           \
+        rocblas_stride stride_C, I batch_count)                                                     \
+    try                                                                                             \
+    {                                                                                               \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A,                         \
+                               strided<T>(A, stride_A), lda, B, strided<T>(B, stride_B), ldb, C,    \
+                               strided<T>(C, stride_C), ldc, batch_count);                          \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }
-TRMM_PLAIN(rocblas_strmm, float)
-TRMM_PLAIN(rocblas_dtrmm, double)
-
-#define TRMM_BATCHED(NAME, T)                                                                       \
-    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
-                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
-                        rocblas_int n, const T* alpha, const T* const A[], rocblas_int lda,          \
-                        const T* const B[], rocblas_int ldb, T* const C[], rocblas_int ldc,          \
-                        rocblas_int batch_count)                                                    \
-    try                                                                                             \
-    {                                                                                               \
-        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, arrayed<T>(A), lda, B,      \
-                            arrayed<T>(B), ldb, C, arrayed<T>(C), ldc, batch_count);                \
-    }                                                                                               \
-    catch(...)                                                                                      \
-    {                                                                                               \
-        return exception_status();                                                                  \
-    }
-TRMM_BATCHED(rocblas_strmm_batched, float)
-TRMM_BATCHED(rocblas_dtrmm_batched, double)
-
-#define TRMM_STRIDED(NAME, T)                                                                       \
-    rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                     \
-                        rocblas_operation transA, rocblas_diagonal diag, rocblas_int m,             \
-                        rocblas_int n, const T* alpha, const T* A, rocblas_int lda,                  \
-                        rocblas_stride stride_A, const T* B, rocblas_int ldb,                       \
-                        rocblas_stride stride_B, T* C, rocblas_int ldc, rocblas_stride stride_C,    \
-                        rocblas_int batch_count)                                                    \
-    try                                                                                             \
-    {                                                                                               \
-        return trmm_impl<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, stride_A),    \
-                            lda, B, strided<T>(B, stride_B), ldb, C, strided<T>(C, stride_C), ldc,  \
-                            batch_count);                                                           \
-    }                                                                                               \
-    catch(...)                                                                                      \
-    {                                                                                               \
-        return exception_status();                                                                  \
-    }
-TRMM_STRIDED(rocblas_strmm_strided_batched, float)
-TRMM_STRIDED(rocblas_dtrmm_strided_batched, double)
+TRMM_ALL(float, s, rocblas_int, )
+TRMM_ALL(double, d, rocblas_int, )
+TRMM_ALL(float, s, int64_t, _64)
+TRMM_ALL(double, d, int64_t, _64)
 
 // ---- server (rocblas_b200_ext.h) --------------------------------------------------------------
 struct rocblas_b200_server_

@@ -169,3 +169,42 @@ def test_workspace_ownership(handle):
     assert L.rocblas_is_managing_device_memory(handle.value)
     assert not L.rocblas_is_user_managing_device_memory(handle.value)
     assert L.rocblas_set_workspace(None, None, 0) == rb.status_invalid_handle
+
+
+def test_ilp64_arguments_and_size_query(handle):
+    """The _64 forms: the 32-bit argument rules on 64-bit values, invalid_size for an order of A
+    beyond 32 bits (src64/blas3/rocblas_trsm_kernels_64.cpp:57-62,
+    src64/blas2/rocblas_trsv_kernels_64.cpp:50-51), and a size query over a B whose rows are
+    cut into chunks (2^28 rows for side right) equal to the query of one full chunk.  No call
+    here reaches the device."""
+    L = rb.lib()
+    one = ctypes.c_double(1.0)
+    p = ctypes.cast(ctypes.byref(one), ctypes.c_void_p)
+    big = (1 << 31) + 5
+    X, Y = 0x1000, 0x2000  # never dereferenced: every call returns before any device work
+    h = handle.value
+    lo, nn, nu = rb.fill_lower, rb.operation_none, rb.diagonal_non_unit
+    f = L.rocblas_dtrsm_64
+    assert f(h, rb.side_left, lo, nn, nu, big, 4, p, X, big, Y, big) == rb.status_invalid_size
+    assert f(h, rb.side_right, lo, nn, nu, 4, big, p, X, big, Y, 4) == rb.status_invalid_size
+    assert f(h, rb.side_both, lo, nn, nu, big, 4, p, X, big, Y, big) == rb.status_invalid_value
+    assert f(h, rb.side_left, lo, nn, nu, 8, big, p, X, 7, Y, 8) == rb.status_invalid_size
+    assert f(h, rb.side_left, lo, nn, nu, 8, 0, None, None, 8, None, 8) == rb.status_success
+    assert L.rocblas_dtrsm_strided_batched_64(h, rb.side_left, lo, nn, nu, 8, 8, p, X, 8, 64, Y, 8, 64,
+                                              -1) == rb.status_invalid_size
+    assert L.rocblas_dtrsv_64(h, lo, nn, nu, big, X, big, Y, 1) == rb.status_invalid_size
+    assert L.rocblas_dtrsv_64(h, lo, nn, nu, 8, X, 8, Y, 0) == rb.status_invalid_size
+    assert L.rocblas_dtrmm_64(h, rb.side_left, lo, nn, nu, big, 4, p, X, big, Y, big, Y + 64,
+                              big) == rb.status_invalid_size
+    assert L.rocblas_dtrmm_64(h, rb.side_left, lo, nn, nu, 8, 8, p, X, 8, Y, 8, Y, 9) == rb.status_invalid_value
+
+    size64, size32 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    m64 = (1 << 31) + 77  # nine chunks of rows
+    assert L.rocblas_start_device_memory_size_query(h) == 0
+    assert f(h, rb.side_right, lo, nn, nu, m64, 1024, p, None, 1024, None, m64) == rb.status_size_increased
+    assert L.rocblas_stop_device_memory_size_query(h, ctypes.byref(size64)) == 0
+    assert L.rocblas_start_device_memory_size_query(h) == 0
+    assert L.rocblas_dtrsm(h, rb.side_right, lo, nn, nu, 1 << 28, 1024, p, None, 1024, None,
+                           1 << 28) == rb.status_size_increased
+    assert L.rocblas_stop_device_memory_size_query(h, ctypes.byref(size32)) == 0
+    assert size64.value == size32.value > 0
