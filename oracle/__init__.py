@@ -44,8 +44,8 @@ CBLAS_COL_MAJOR = 102
 
 def build(force: bool = False) -> str:
     """Compile the C oracle with the committed Makefile."""
-    src = os.path.join(HERE, "trsm_oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    newest = max(os.path.getmtime(os.path.join(HERE, f)) for f in ("trsm_oracle.c", "trsm_oracle_complex.c"))
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
         subprocess.check_call(["make", "-s", "-C", HERE])
     return LIB_PATH
 
@@ -71,6 +71,15 @@ def _load():
             f.restype = None
         lib.oracle_matrix_norm_1_d.argtypes = [i64, i64, p, i64, p, i64]
         lib.oracle_matrix_norm_1_d.restype = d
+        for pre in "cz":  # trsm_oracle_complex.c: alpha as (re, im)
+            f = getattr(lib, f"oracle_{pre}trsm")
+            f.argtypes = [i, i, i, i, i64, i64, d, d, p, i64, p, i64]
+            f.restype = None
+            f = getattr(lib, f"oracle_{pre}trmm")
+            f.argtypes = [i, i, i, i, i64, i64, d, d, p, i64, p, i64, p, i64]
+            f.restype = None
+        lib.oracle_matrix_norm_1_z.argtypes = [i64, i64, p, i64, p, i64]
+        lib.oracle_matrix_norm_1_z.restype = d
         _lib = lib
     return _lib
 
@@ -87,7 +96,23 @@ def _f(x, dtype):
 def _prec(dtype, precision):
     if precision is not None:
         return precision
-    return "s" if np.dtype(dtype) == np.float32 else "d"
+    dt = np.dtype(dtype)
+    if dt == np.complex64:
+        return "c"
+    if dt == np.complex128:
+        return "z"
+    return "s" if dt == np.float32 else "d"
+
+
+_PREC_DTYPE = {"s": np.float32, "d": np.float64, "q": np.float64, "c": np.complex64, "z": np.complex128}
+
+
+def _alpha_args(pre, alpha):
+    """alpha as the C functions take it: (re, im) for the complex ones."""
+    if pre in "cz":
+        a = complex(alpha)
+        return (a.real, a.imag)
+    return (float(alpha),)
 
 
 def trsm(side, uplo, trans, diag, alpha, A, B, precision=None):
@@ -99,13 +124,13 @@ def trsm(side, uplo, trans, diag, alpha, A, B, precision=None):
     "q" (__float128 arithmetic, float64 storage).
     """
     pre = _prec(B.dtype, precision)
-    dt = np.float32 if pre == "s" else np.float64
+    dt = _PREC_DTYPE[pre]
     A = _f(A, dt)
     X = np.array(B, dtype=dt, order="F", copy=True)
     m, n = X.shape
     getattr(_load(), f"oracle_{pre}trsm")(
         _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
-        m, n, float(alpha), A.ctypes.data, A.shape[0], X.ctypes.data, X.shape[0])
+        m, n, *_alpha_args(pre, alpha), A.ctypes.data, A.shape[0], X.ctypes.data, X.shape[0])
     return X
 
 
@@ -113,14 +138,14 @@ def trmm(side, uplo, trans, diag, alpha, A, X, precision=None):
     """Return alpha op(A) X (side L) or alpha X op(A) (side R); only the triangle of A is
     read, and with diag U its diagonal is taken as 1."""
     pre = _prec(X.dtype, precision)
-    dt = np.float32 if pre == "s" else np.float64
+    dt = _PREC_DTYPE[pre]
     A = _f(A, dt)
     X = _f(X, dt)
     m, n = X.shape
     C = np.empty((m, n), dtype=dt, order="F")
     getattr(_load(), f"oracle_{pre}trmm")(
         _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
-        m, n, float(alpha), A.ctypes.data, A.shape[0], X.ctypes.data, X.shape[0],
+        m, n, *_alpha_args(pre, alpha), A.ctypes.data, A.shape[0], X.ctypes.data, X.shape[0],
         C.ctypes.data, m)
     return C
 
@@ -158,6 +183,11 @@ def invA_blocks(uplo, diag, A, k, nb=128, precision=None):
 def matrix_norm_1(gold, x):
     """The reference's forward-error norm (clients/include/norm.hpp:449-492), restated in
     C; the running sums are never reset per column, exactly as in the reference."""
+    if np.iscomplexobj(gold) or np.iscomplexobj(x):
+        g = np.asfortranarray(gold, dtype=np.complex128)
+        v = np.asfortranarray(x, dtype=np.complex128)
+        m, n = g.shape
+        return _load().oracle_matrix_norm_1_z(m, n, g.ctypes.data, g.shape[0], v.ctypes.data, v.shape[0])
     g = np.asfortranarray(gold, dtype=np.float64)
     v = np.asfortranarray(x, dtype=np.float64)
     m, n = g.shape
@@ -216,7 +246,10 @@ def _load_blas():
         lib.scipy_cblas_strsm.argtypes = [i, i, i, i, i, i, i, f, p, i, p, i]
         lib.scipy_cblas_dtrmm.argtypes = [i, i, i, i, i, i, i, d, p, i, p, i]
         lib.scipy_cblas_strmm.argtypes = [i, i, i, i, i, i, i, f, p, i, p, i]
-        for fn in ("scipy_cblas_dtrsm", "scipy_cblas_strsm", "scipy_cblas_dtrmm", "scipy_cblas_strmm"):
+        for fn in ("scipy_cblas_ztrsm", "scipy_cblas_ctrsm", "scipy_cblas_ztrmm", "scipy_cblas_ctrmm"):
+            getattr(lib, fn).argtypes = [i, i, i, i, i, i, i, p, p, i, p, i]  # alpha by pointer
+        for fn in ("scipy_cblas_dtrsm", "scipy_cblas_strsm", "scipy_cblas_dtrmm", "scipy_cblas_strmm",
+                   "scipy_cblas_ztrsm", "scipy_cblas_ctrsm", "scipy_cblas_ztrmm", "scipy_cblas_ctrmm"):
             getattr(lib, fn).restype = None
         lib.scipy_openblas_set_num_threads.argtypes = [i]
         lib.scipy_openblas_get_num_threads.restype = i
@@ -237,14 +270,27 @@ def cblas_config():
     return _load_blas().scipy_openblas_get_config().decode()
 
 
+_CBLAS_PRE = {np.dtype(np.float32): "s", np.dtype(np.float64): "d", np.dtype(np.complex64): "c",
+              np.dtype(np.complex128): "z"}
+
+
+def _cblas_alpha(dtype, alpha):
+    """A complex alpha goes to cblas by pointer (the array keeps it alive)."""
+    if np.iscomplexobj(np.empty(0, dtype=dtype)):
+        a = np.array([alpha], dtype=dtype)
+        return a, ctypes.c_void_p(a.ctypes.data)
+    return None, float(alpha)
+
+
 def cblas_trsm_inplace(side, uplo, trans, diag, alpha, A, B):
     """cblas_?trsm(CblasColMajor, ...) on Fortran-ordered arrays, B overwritten."""
     lib = _load_blas()
-    fn = lib.scipy_cblas_strsm if B.dtype == np.float32 else lib.scipy_cblas_dtrsm
+    fn = getattr(lib, f"scipy_cblas_{_CBLAS_PRE[B.dtype]}trsm")
     assert A.flags.f_contiguous and B.flags.f_contiguous and A.dtype == B.dtype
     m, n = B.shape
+    keep, a = _cblas_alpha(B.dtype, alpha)
     fn(CBLAS_COL_MAJOR, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
-       _code(DIAG, diag), m, n, float(alpha), A.ctypes.data, A.shape[0], B.ctypes.data, B.shape[0])
+       _code(DIAG, diag), m, n, a, A.ctypes.data, A.shape[0], B.ctypes.data, B.shape[0])
     return B
 
 
@@ -257,10 +303,11 @@ def cblas_trmm(side, uplo, trans, diag, alpha, A, X):
     lib = _load_blas()
     C = np.array(X, order="F", copy=True)
     A = _f(A, C.dtype)
-    fn = lib.scipy_cblas_strmm if C.dtype == np.float32 else lib.scipy_cblas_dtrmm
+    fn = getattr(lib, f"scipy_cblas_{_CBLAS_PRE[C.dtype]}trmm")
     m, n = C.shape
+    keep, a = _cblas_alpha(C.dtype, alpha)
     fn(CBLAS_COL_MAJOR, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
-       _code(DIAG, diag), m, n, float(alpha), A.ctypes.data, A.shape[0], C.ctypes.data, C.shape[0])
+       _code(DIAG, diag), m, n, a, A.ctypes.data, A.shape[0], C.ctypes.data, C.shape[0])
     return C
 
 

@@ -52,6 +52,17 @@ def nan_triangle_problem(seed, side, uplo, trans, diag, m, n, lda, ldb, dtype):
     A[:k, :k] = blk
     B = np.full((ldb, n), np.nan, dtype=np.float64, order="F")
     B[:m, :] = rng.uniform(-1.0, 1.0, size=(m, n))
+    if np.issubdtype(np.dtype(dtype), np.complexfloating):
+        # complex: the same real parts, then imaginary parts U(-1,1)/k off the diagonal,
+        # U(-0.5,0.5) on it and U(-1,1) in B (drawn after, so real streams are unchanged)
+        im = np.where(mask, rng.uniform(-1.0, 1.0, size=(k, k)) / max(k, 1), 0.0)
+        if diag in ("N", 131):
+            im[np.arange(k), np.arange(k)] = rng.uniform(-0.5, 0.5, size=k)
+        Ac = A.astype(np.complex128, order="F")
+        Ac[:k, :k] += 1j * im
+        Bc = B.astype(np.complex128, order="F")
+        Bc[:m, :] += 1j * rng.uniform(-1.0, 1.0, size=(m, n))
+        return Ac.astype(dtype, order="F"), Bc.astype(dtype, order="F")
     return A.astype(dtype, order="F"), B.astype(dtype, order="F")
 
 

@@ -10,6 +10,7 @@ those reference-side answers on fixed inputs so that they travel with the reposi
   A (unused triangle = NaN, diag-U cases with a NaN diagonal), B, alpha, and
   X = cblas_?trsm(A, B) computed by the host CBLAS (OpenBLAS as bundled with scipy, one of
   the CBLAS builds the reference links, clients/CMakeLists.txt:103-165);
+* ``cblas_<c|z>.npz`` -- the same for complex data, trans C included, complex alpha;
 * ``protocol_<dt>.npz`` -- rocblas-test's recipe: diagonally dominant integer A, integer X,
   B = op(A) X / alpha via cblas_?trmm; the known X is the answer.
 
@@ -65,7 +66,34 @@ def main():
             out[key + "_X"] = X
             out[key + "_alpha"] = np.array(alpha)
         np.savez_compressed(os.path.join(HERE, f"protocol_{name}.npz"), **out)
+    complex_fixtures()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+
+
+# complex: trans C as well (conj(A)), complex alpha
+COMBOS_C = list(itertools.product("LR", "UL", "NTC", "NU"))
+SHAPES_C = [(21, 13, 3, 2), (5, 1, 1, 0)]
+
+
+def complex_fixtures():
+    """``cblas_<c|z>.npz``: the same recipe with complex A and B (imaginary parts drawn after the
+    real ones) and X from cblas_{c,z}trsm."""
+    oracle.cblas_set_threads(1)
+    for dt, name in ((np.complex128, "z"), (np.complex64, "c")):
+        out = {}
+        for ci, (side, uplo, trans, diag) in enumerate(COMBOS_C):
+            for si, (m, n, pa, pb) in enumerate(SHAPES_C):
+                k = m if side == "L" else n
+                seed = 5000 + 1000 * ci + si
+                A, B = oracle.nan_triangle_problem(seed, side, uplo, trans, diag, m, n, k + pa, m + pb, dt)
+                alpha = 0.75 - 0.5j if (ci + si) % 2 else 1.0 + 0.0j
+                X = oracle.cblas_trsm(side, uplo, trans, diag, alpha, A, np.asfortranarray(B[:m]))
+                key = f"{side}{uplo}{trans}{diag}_{m}x{n}"
+                out[key + "_A"] = A
+                out[key + "_B"] = B
+                out[key + "_alpha"] = np.array(alpha)
+                out[key + "_X"] = X
+        np.savez_compressed(os.path.join(HERE, f"cblas_{name}.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -115,3 +115,52 @@ def test_workload_generators_shapes_and_nan_triangle():
     assert np.all(np.abs(A[40, :40]) <= d[40] * 6.0 / np.sqrt(64))
     assert float(Bt.abs().max()) <= 1.0
     del torch
+
+
+COMBOS_C = list(itertools.product("LR", "UL", "NTC", "NU"))
+
+
+@pytest.mark.parametrize("dt", ["z", "c"])
+def test_complex_oracle_matches_cblas_golden(dt):
+    """The complex restatement (trsm_oracle_complex.c) against cblas_{c,z}trsm answers
+    recorded in tests/golden (all 24 side/uplo/trans/diag combinations, trans C included)."""
+    z = np.load(os.path.join(GOLDEN, f"cblas_{dt}.npz"))
+    keys = _cases(z)
+    assert len(keys) == 24 * 2
+    eps = np.finfo(np.complex128 if dt == "z" else np.complex64).eps
+    for key in keys:
+        combo, shape = key.split("_")
+        side, uplo, trans, diag = combo
+        m, n = map(int, shape.split("x"))
+        A, B, X, alpha = z[key + "_A"], z[key + "_B"], z[key + "_X"], complex(z[key + "_alpha"])
+        got = oracle.trsm(side, uplo, trans, diag, alpha, A, np.asfortranarray(B[:m]))
+        assert got.dtype == A.dtype and not np.isnan(got).any(), key
+        err = oracle.matrix_norm_1(X, got)
+        assert err <= 64 * eps, (key, err)
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", COMBOS_C)
+def test_complex_oracle_vs_live_cblas_and_trmm(side, uplo, trans, diag):
+    m, n = 40, 27
+    k = m if side == "L" else n
+    alpha = -1.5 + 0.25j
+    A, B = oracle.nan_triangle_problem(12, side, uplo, trans, diag, m, n, k + 1, m, np.complex128)
+    X = oracle.trsm(side, uplo, trans, diag, alpha, A, B)
+    Xc = oracle.cblas_trsm(side, uplo, trans, diag, alpha, A, B)
+    assert oracle.matrix_norm_1(Xc, X) < 1e-14
+    # the forward operator: trmm against the host CBLAS, and op(A) X / alpha gives back B
+    R = oracle.trmm(side, uplo, trans, diag, 1 / alpha, A, X)
+    assert oracle.matrix_norm_1(oracle.cblas_trmm(side, uplo, trans, diag, 1 / alpha, A, X), R) < 1e-14
+    assert oracle.matrix_norm_1(B, R) <= oracle.trsm_tolerance(np.complex128, k)
+    # trans C differs from trans T exactly by conj(A)
+    if trans == "C":
+        Xt = oracle.trsm(side, uplo, "T", diag, alpha, np.conj(A), B)
+        assert oracle.matrix_norm_1(Xt, X) == 0.0
+
+
+def test_complex_matrix_norm_uses_modulus():
+    gold = np.array([[3 + 4j]], dtype=np.complex128, order="F")
+    x = np.array([[0j]], dtype=np.complex128, order="F")
+    assert oracle.matrix_norm_1(gold, x) == 1.0
+    x[0, 0] = 3 + 0j
+    assert abs(oracle.matrix_norm_1(gold, x) - 4.0 / 5.0) < 1e-15
