@@ -37,6 +37,15 @@ extern "C" {
 typedef struct _rocblas_handle* rocblas_handle; /* rocblas-types.h:64 */
 typedef int32_t rocblas_int;                    /* rocblas-types.h:80 (LP64 API) */
 typedef int64_t rocblas_stride;                 /* rocblas-types.h:84 */
+/* complex element types: the C definitions of rocblas-complex-types.h:82-91 */
+typedef struct
+{
+    float x, y;
+} rocblas_float_complex;
+typedef struct
+{
+    double x, y;
+} rocblas_double_complex;
 typedef float   rocblas_float;
 typedef double  rocblas_double;
 
@@ -783,6 +792,519 @@ ROCBLAS_EXPORT rocblas_status rocblas_dtrmm_strided_batched_64(rocblas_handle   
                                                                int64_t           ldc,
                                                                rocblas_stride    stride_C,
                                                                int64_t           batch_count);
+
+/* ---- complex (c, z): declarations starting at rocblas-functions.h:19414 (trsm), 19602
+ * (trsm_batched), 19806 (trsm_strided_batched), 9910 / 10052 / 10211 (trsv forms) and 18395 /
+ * 18646 / 18923 (trmm forms), and their ILP64 forms.  trans C solves with conj(A)^T.  rocblas_trsm_ex and its batched forms take
+ * compute_type rocblas_datatype_f32_c / f64_c. ------------------------------------------- */
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm(rocblas_handle               handle,
+                                            rocblas_side                 side,
+                                            rocblas_fill                 uplo,
+                                            rocblas_operation            transA,
+                                            rocblas_diagonal             diag,
+                                            rocblas_int                  m,
+                                            rocblas_int                  n,
+                                            const rocblas_float_complex* alpha,
+                                            const rocblas_float_complex* A,
+                                            rocblas_int                  lda,
+                                            rocblas_float_complex*       B,
+                                            rocblas_int                  ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm_batched(rocblas_handle                      handle,
+                                                    rocblas_side                        side,
+                                                    rocblas_fill                        uplo,
+                                                    rocblas_operation                   transA,
+                                                    rocblas_diagonal                    diag,
+                                                    rocblas_int                         m,
+                                                    rocblas_int                         n,
+                                                    const rocblas_float_complex*        alpha,
+                                                    const rocblas_float_complex* const* A,
+                                                    rocblas_int                         lda,
+                                                    rocblas_float_complex* const*       B,
+                                                    rocblas_int                         ldb,
+                                                    rocblas_int                         batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm_strided_batched(rocblas_handle               handle,
+                                                            rocblas_side                 side,
+                                                            rocblas_fill                 uplo,
+                                                            rocblas_operation            transA,
+                                                            rocblas_diagonal             diag,
+                                                            rocblas_int                  m,
+                                                            rocblas_int                  n,
+                                                            const rocblas_float_complex* alpha,
+                                                            const rocblas_float_complex* A,
+                                                            rocblas_int                  lda,
+                                                            rocblas_stride               stride_a,
+                                                            rocblas_float_complex*       B,
+                                                            rocblas_int                  ldb,
+                                                            rocblas_stride               stride_b,
+                                                            rocblas_int                  batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv(rocblas_handle               handle,
+                                            rocblas_fill                 uplo,
+                                            rocblas_operation            transA,
+                                            rocblas_diagonal             diag,
+                                            rocblas_int                  n,
+                                            const rocblas_float_complex* A,
+                                            rocblas_int                  lda,
+                                            rocblas_float_complex*       x,
+                                            rocblas_int                  incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv_batched(rocblas_handle                      handle,
+                                                    rocblas_fill                        uplo,
+                                                    rocblas_operation                   transA,
+                                                    rocblas_diagonal                    diag,
+                                                    rocblas_int                         n,
+                                                    const rocblas_float_complex* const* A,
+                                                    rocblas_int                         lda,
+                                                    rocblas_float_complex* const*       x,
+                                                    rocblas_int                         incx,
+                                                    rocblas_int                         batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv_strided_batched(rocblas_handle               handle,
+                                                            rocblas_fill                 uplo,
+                                                            rocblas_operation            transA,
+                                                            rocblas_diagonal             diag,
+                                                            rocblas_int                  n,
+                                                            const rocblas_float_complex* A,
+                                                            rocblas_int                  lda,
+                                                            rocblas_stride               stride_A,
+                                                            rocblas_float_complex*       x,
+                                                            rocblas_int                  incx,
+                                                            rocblas_stride               stride_x,
+                                                            rocblas_int                  batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm(rocblas_handle               handle,
+                                            rocblas_side                 side,
+                                            rocblas_fill                 uplo,
+                                            rocblas_operation            transA,
+                                            rocblas_diagonal             diag,
+                                            rocblas_int                  m,
+                                            rocblas_int                  n,
+                                            const rocblas_float_complex* alpha,
+                                            const rocblas_float_complex* A,
+                                            rocblas_int                  lda,
+                                            const rocblas_float_complex* B,
+                                            rocblas_int                  ldb,
+                                            rocblas_float_complex*       C,
+                                            rocblas_int                  ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm_batched(rocblas_handle                      handle,
+                                                    rocblas_side                        side,
+                                                    rocblas_fill                        uplo,
+                                                    rocblas_operation                   transA,
+                                                    rocblas_diagonal                    diag,
+                                                    rocblas_int                         m,
+                                                    rocblas_int                         n,
+                                                    const rocblas_float_complex*        alpha,
+                                                    const rocblas_float_complex* const* A,
+                                                    rocblas_int                         lda,
+                                                    const rocblas_float_complex* const* B,
+                                                    rocblas_int                         ldb,
+                                                    rocblas_float_complex* const*       C,
+                                                    rocblas_int                         ldc,
+                                                    rocblas_int                         batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm_strided_batched(rocblas_handle               handle,
+                                                            rocblas_side                 side,
+                                                            rocblas_fill                 uplo,
+                                                            rocblas_operation            transA,
+                                                            rocblas_diagonal             diag,
+                                                            rocblas_int                  m,
+                                                            rocblas_int                  n,
+                                                            const rocblas_float_complex* alpha,
+                                                            const rocblas_float_complex* A,
+                                                            rocblas_int                  lda,
+                                                            rocblas_stride               stride_A,
+                                                            const rocblas_float_complex* B,
+                                                            rocblas_int                  ldb,
+                                                            rocblas_stride               stride_B,
+                                                            rocblas_float_complex*       C,
+                                                            rocblas_int                  ldc,
+                                                            rocblas_stride               stride_C,
+                                                            rocblas_int                  batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm(rocblas_handle                handle,
+                                            rocblas_side                  side,
+                                            rocblas_fill                  uplo,
+                                            rocblas_operation             transA,
+                                            rocblas_diagonal              diag,
+                                            rocblas_int                   m,
+                                            rocblas_int                   n,
+                                            const rocblas_double_complex* alpha,
+                                            const rocblas_double_complex* A,
+                                            rocblas_int                   lda,
+                                            rocblas_double_complex*       B,
+                                            rocblas_int                   ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm_batched(rocblas_handle                       handle,
+                                                    rocblas_side                         side,
+                                                    rocblas_fill                         uplo,
+                                                    rocblas_operation                    transA,
+                                                    rocblas_diagonal                     diag,
+                                                    rocblas_int                          m,
+                                                    rocblas_int                          n,
+                                                    const rocblas_double_complex*        alpha,
+                                                    const rocblas_double_complex* const* A,
+                                                    rocblas_int                          lda,
+                                                    rocblas_double_complex* const*       B,
+                                                    rocblas_int                          ldb,
+                                                    rocblas_int                          batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm_strided_batched(rocblas_handle                handle,
+                                                            rocblas_side                  side,
+                                                            rocblas_fill                  uplo,
+                                                            rocblas_operation             transA,
+                                                            rocblas_diagonal              diag,
+                                                            rocblas_int                   m,
+                                                            rocblas_int                   n,
+                                                            const rocblas_double_complex* alpha,
+                                                            const rocblas_double_complex* A,
+                                                            rocblas_int                   lda,
+                                                            rocblas_stride                stride_a,
+                                                            rocblas_double_complex*       B,
+                                                            rocblas_int                   ldb,
+                                                            rocblas_stride                stride_b,
+                                                            rocblas_int                   batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv(rocblas_handle                handle,
+                                            rocblas_fill                  uplo,
+                                            rocblas_operation             transA,
+                                            rocblas_diagonal              diag,
+                                            rocblas_int                   n,
+                                            const rocblas_double_complex* A,
+                                            rocblas_int                   lda,
+                                            rocblas_double_complex*       x,
+                                            rocblas_int                   incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv_batched(rocblas_handle                       handle,
+                                                    rocblas_fill                         uplo,
+                                                    rocblas_operation                    transA,
+                                                    rocblas_diagonal                     diag,
+                                                    rocblas_int                          n,
+                                                    const rocblas_double_complex* const* A,
+                                                    rocblas_int                          lda,
+                                                    rocblas_double_complex* const*       x,
+                                                    rocblas_int                          incx,
+                                                    rocblas_int                          batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv_strided_batched(rocblas_handle                handle,
+                                                            rocblas_fill                  uplo,
+                                                            rocblas_operation             transA,
+                                                            rocblas_diagonal              diag,
+                                                            rocblas_int                   n,
+                                                            const rocblas_double_complex* A,
+                                                            rocblas_int                   lda,
+                                                            rocblas_stride                stride_A,
+                                                            rocblas_double_complex*       x,
+                                                            rocblas_int                   incx,
+                                                            rocblas_stride                stride_x,
+                                                            rocblas_int                   batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm(rocblas_handle                handle,
+                                            rocblas_side                  side,
+                                            rocblas_fill                  uplo,
+                                            rocblas_operation             transA,
+                                            rocblas_diagonal              diag,
+                                            rocblas_int                   m,
+                                            rocblas_int                   n,
+                                            const rocblas_double_complex* alpha,
+                                            const rocblas_double_complex* A,
+                                            rocblas_int                   lda,
+                                            const rocblas_double_complex* B,
+                                            rocblas_int                   ldb,
+                                            rocblas_double_complex*       C,
+                                            rocblas_int                   ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_batched(rocblas_handle                       handle,
+                                                    rocblas_side                         side,
+                                                    rocblas_fill                         uplo,
+                                                    rocblas_operation                    transA,
+                                                    rocblas_diagonal                     diag,
+                                                    rocblas_int                          m,
+                                                    rocblas_int                          n,
+                                                    const rocblas_double_complex*        alpha,
+                                                    const rocblas_double_complex* const* A,
+                                                    rocblas_int                          lda,
+                                                    const rocblas_double_complex* const* B,
+                                                    rocblas_int                          ldb,
+                                                    rocblas_double_complex* const*       C,
+                                                    rocblas_int                          ldc,
+                                                    rocblas_int                          batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_strided_batched(rocblas_handle                handle,
+                                                            rocblas_side                  side,
+                                                            rocblas_fill                  uplo,
+                                                            rocblas_operation             transA,
+                                                            rocblas_diagonal              diag,
+                                                            rocblas_int                   m,
+                                                            rocblas_int                   n,
+                                                            const rocblas_double_complex* alpha,
+                                                            const rocblas_double_complex* A,
+                                                            rocblas_int                   lda,
+                                                            rocblas_stride                stride_A,
+                                                            const rocblas_double_complex* B,
+                                                            rocblas_int                   ldb,
+                                                            rocblas_stride                stride_B,
+                                                            rocblas_double_complex*       C,
+                                                            rocblas_int                   ldc,
+                                                            rocblas_stride                stride_C,
+                                                            rocblas_int                   batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm_64(rocblas_handle               handle,
+                                               rocblas_side                 side,
+                                               rocblas_fill                 uplo,
+                                               rocblas_operation            transA,
+                                               rocblas_diagonal             diag,
+                                               int64_t                      m,
+                                               int64_t                      n,
+                                               const rocblas_float_complex* alpha,
+                                               const rocblas_float_complex* A,
+                                               int64_t                      lda,
+                                               rocblas_float_complex*       B,
+                                               int64_t                      ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm_batched_64(rocblas_handle                      handle,
+                                                       rocblas_side                        side,
+                                                       rocblas_fill                        uplo,
+                                                       rocblas_operation                   transA,
+                                                       rocblas_diagonal                    diag,
+                                                       int64_t                             m,
+                                                       int64_t                             n,
+                                                       const rocblas_float_complex*        alpha,
+                                                       const rocblas_float_complex* const* A,
+                                                       int64_t                             lda,
+                                                       rocblas_float_complex* const*       B,
+                                                       int64_t                             ldb,
+                                                       int64_t                             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsm_strided_batched_64(rocblas_handle               handle,
+                                                               rocblas_side                 side,
+                                                               rocblas_fill                 uplo,
+                                                               rocblas_operation            transA,
+                                                               rocblas_diagonal             diag,
+                                                               int64_t                      m,
+                                                               int64_t                      n,
+                                                               const rocblas_float_complex* alpha,
+                                                               const rocblas_float_complex* A,
+                                                               int64_t                      lda,
+                                                               rocblas_stride               stride_a,
+                                                               rocblas_float_complex*       B,
+                                                               int64_t                      ldb,
+                                                               rocblas_stride               stride_b,
+                                                               int64_t                      batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv_64(rocblas_handle               handle,
+                                               rocblas_fill                 uplo,
+                                               rocblas_operation            transA,
+                                               rocblas_diagonal             diag,
+                                               int64_t                      n,
+                                               const rocblas_float_complex* A,
+                                               int64_t                      lda,
+                                               rocblas_float_complex*       x,
+                                               int64_t                      incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv_batched_64(rocblas_handle                      handle,
+                                                       rocblas_fill                        uplo,
+                                                       rocblas_operation                   transA,
+                                                       rocblas_diagonal                    diag,
+                                                       int64_t                             n,
+                                                       const rocblas_float_complex* const* A,
+                                                       int64_t                             lda,
+                                                       rocblas_float_complex* const*       x,
+                                                       int64_t                             incx,
+                                                       int64_t                             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrsv_strided_batched_64(rocblas_handle               handle,
+                                                               rocblas_fill                 uplo,
+                                                               rocblas_operation            transA,
+                                                               rocblas_diagonal             diag,
+                                                               int64_t                      n,
+                                                               const rocblas_float_complex* A,
+                                                               int64_t                      lda,
+                                                               rocblas_stride               stride_A,
+                                                               rocblas_float_complex*       x,
+                                                               int64_t                      incx,
+                                                               rocblas_stride               stride_x,
+                                                               int64_t                      batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm_64(rocblas_handle               handle,
+                                               rocblas_side                 side,
+                                               rocblas_fill                 uplo,
+                                               rocblas_operation            transA,
+                                               rocblas_diagonal             diag,
+                                               int64_t                      m,
+                                               int64_t                      n,
+                                               const rocblas_float_complex* alpha,
+                                               const rocblas_float_complex* A,
+                                               int64_t                      lda,
+                                               const rocblas_float_complex* B,
+                                               int64_t                      ldb,
+                                               rocblas_float_complex*       C,
+                                               int64_t                      ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm_batched_64(rocblas_handle                      handle,
+                                                       rocblas_side                        side,
+                                                       rocblas_fill                        uplo,
+                                                       rocblas_operation                   transA,
+                                                       rocblas_diagonal                    diag,
+                                                       int64_t                             m,
+                                                       int64_t                             n,
+                                                       const rocblas_float_complex*        alpha,
+                                                       const rocblas_float_complex* const* A,
+                                                       int64_t                             lda,
+                                                       const rocblas_float_complex* const* B,
+                                                       int64_t                             ldb,
+                                                       rocblas_float_complex* const*       C,
+                                                       int64_t                             ldc,
+                                                       int64_t                             batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrmm_strided_batched_64(rocblas_handle               handle,
+                                                               rocblas_side                 side,
+                                                               rocblas_fill                 uplo,
+                                                               rocblas_operation            transA,
+                                                               rocblas_diagonal             diag,
+                                                               int64_t                      m,
+                                                               int64_t                      n,
+                                                               const rocblas_float_complex* alpha,
+                                                               const rocblas_float_complex* A,
+                                                               int64_t                      lda,
+                                                               rocblas_stride               stride_A,
+                                                               const rocblas_float_complex* B,
+                                                               int64_t                      ldb,
+                                                               rocblas_stride               stride_B,
+                                                               rocblas_float_complex*       C,
+                                                               int64_t                      ldc,
+                                                               rocblas_stride               stride_C,
+                                                               int64_t                      batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm_64(rocblas_handle                handle,
+                                               rocblas_side                  side,
+                                               rocblas_fill                  uplo,
+                                               rocblas_operation             transA,
+                                               rocblas_diagonal              diag,
+                                               int64_t                       m,
+                                               int64_t                       n,
+                                               const rocblas_double_complex* alpha,
+                                               const rocblas_double_complex* A,
+                                               int64_t                       lda,
+                                               rocblas_double_complex*       B,
+                                               int64_t                       ldb);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm_batched_64(rocblas_handle                       handle,
+                                                       rocblas_side                         side,
+                                                       rocblas_fill                         uplo,
+                                                       rocblas_operation                    transA,
+                                                       rocblas_diagonal                     diag,
+                                                       int64_t                              m,
+                                                       int64_t                              n,
+                                                       const rocblas_double_complex*        alpha,
+                                                       const rocblas_double_complex* const* A,
+                                                       int64_t                              lda,
+                                                       rocblas_double_complex* const*       B,
+                                                       int64_t                              ldb,
+                                                       int64_t                              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsm_strided_batched_64(rocblas_handle                handle,
+                                                               rocblas_side                  side,
+                                                               rocblas_fill                  uplo,
+                                                               rocblas_operation             transA,
+                                                               rocblas_diagonal              diag,
+                                                               int64_t                       m,
+                                                               int64_t                       n,
+                                                               const rocblas_double_complex* alpha,
+                                                               const rocblas_double_complex* A,
+                                                               int64_t                       lda,
+                                                               rocblas_stride                stride_a,
+                                                               rocblas_double_complex*       B,
+                                                               int64_t                       ldb,
+                                                               rocblas_stride                stride_b,
+                                                               int64_t                       batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv_64(rocblas_handle                handle,
+                                               rocblas_fill                  uplo,
+                                               rocblas_operation             transA,
+                                               rocblas_diagonal              diag,
+                                               int64_t                       n,
+                                               const rocblas_double_complex* A,
+                                               int64_t                       lda,
+                                               rocblas_double_complex*       x,
+                                               int64_t                       incx);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv_batched_64(rocblas_handle                       handle,
+                                                       rocblas_fill                         uplo,
+                                                       rocblas_operation                    transA,
+                                                       rocblas_diagonal                     diag,
+                                                       int64_t                              n,
+                                                       const rocblas_double_complex* const* A,
+                                                       int64_t                              lda,
+                                                       rocblas_double_complex* const*       x,
+                                                       int64_t                              incx,
+                                                       int64_t                              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrsv_strided_batched_64(rocblas_handle                handle,
+                                                               rocblas_fill                  uplo,
+                                                               rocblas_operation             transA,
+                                                               rocblas_diagonal              diag,
+                                                               int64_t                       n,
+                                                               const rocblas_double_complex* A,
+                                                               int64_t                       lda,
+                                                               rocblas_stride                stride_A,
+                                                               rocblas_double_complex*       x,
+                                                               int64_t                       incx,
+                                                               rocblas_stride                stride_x,
+                                                               int64_t                       batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_64(rocblas_handle                handle,
+                                               rocblas_side                  side,
+                                               rocblas_fill                  uplo,
+                                               rocblas_operation             transA,
+                                               rocblas_diagonal              diag,
+                                               int64_t                       m,
+                                               int64_t                       n,
+                                               const rocblas_double_complex* alpha,
+                                               const rocblas_double_complex* A,
+                                               int64_t                       lda,
+                                               const rocblas_double_complex* B,
+                                               int64_t                       ldb,
+                                               rocblas_double_complex*       C,
+                                               int64_t                       ldc);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_batched_64(rocblas_handle                       handle,
+                                                       rocblas_side                         side,
+                                                       rocblas_fill                         uplo,
+                                                       rocblas_operation                    transA,
+                                                       rocblas_diagonal                     diag,
+                                                       int64_t                              m,
+                                                       int64_t                              n,
+                                                       const rocblas_double_complex*        alpha,
+                                                       const rocblas_double_complex* const* A,
+                                                       int64_t                              lda,
+                                                       const rocblas_double_complex* const* B,
+                                                       int64_t                              ldb,
+                                                       rocblas_double_complex* const*       C,
+                                                       int64_t                              ldc,
+                                                       int64_t                              batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_strided_batched_64(rocblas_handle                handle,
+                                                               rocblas_side                  side,
+                                                               rocblas_fill                  uplo,
+                                                               rocblas_operation             transA,
+                                                               rocblas_diagonal              diag,
+                                                               int64_t                       m,
+                                                               int64_t                       n,
+                                                               const rocblas_double_complex* alpha,
+                                                               const rocblas_double_complex* A,
+                                                               int64_t                       lda,
+                                                               rocblas_stride                stride_A,
+                                                               const rocblas_double_complex* B,
+                                                               int64_t                       ldb,
+                                                               rocblas_stride                stride_B,
+                                                               rocblas_double_complex*       C,
+                                                               int64_t                       ldc,
+                                                               rocblas_stride                stride_C,
+                                                               int64_t                       batch_count);
 
 #ifdef __cplusplus
 }

@@ -156,7 +156,13 @@ SIGNATURES = {
     "rocblas_trsm_batched_ex": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i, _p, _i, _i]),
     "rocblas_trsm_strided_batched_ex": (
         _i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _i64, _p, _i, _i64, _i, _p, _i, _i64, _i]),
-    **{f"rocblas_{t}{name}_64": (_i, sig) for t in "sd" for name, sig in (
+    **{f"rocblas_{t}{name}": (_i, sig) for t in "cz" for name, sig in (
+        ("trsm", _TRSM), ("trsm_batched", _TRSM_B), ("trsm_strided_batched", _TRSM_SB),
+        ("trmm", _TRMM), ("trmm_batched", _TRMM_B), ("trmm_strided_batched", _TRMM_SB),
+        ("trsv", [_H, _i, _i, _i, _i, _p, _i, _p, _i]),
+        ("trsv_batched", [_H, _i, _i, _i, _i, _p, _i, _p, _i, _i]),
+        ("trsv_strided_batched", [_H, _i, _i, _i, _i, _p, _i, _i64, _p, _i, _i64, _i]))},
+    **{f"rocblas_{t}{name}_64": (_i, sig) for t in "sdcz" for name, sig in (
         ("trsm", _TRSM_64), ("trsm_batched", _TRSM_B_64), ("trsm_strided_batched", _TRSM_SB_64),
         ("trmm", _TRMM_64), ("trmm_batched", _TRMM_B_64), ("trmm_strided_batched", _TRMM_SB_64),
         ("trsv", _TRSV_64), ("trsv_batched", _TRSV_B_64), ("trsv_strided_batched", _TRSV_SB_64))},

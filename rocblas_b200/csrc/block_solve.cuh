@@ -33,6 +33,14 @@ constexpr int kBsThreads = 256;
 constexpr int kBsChunk   = 64;  // panel rows per update chunk
 constexpr int kBlockSolveMaxK = 512;
 
+// The largest order one CTA solves: the k x 32 strip of C lives in shared memory, so complex
+// double (16-byte elements) stops at 256 to stay within 227 KB.
+template <typename T>
+constexpr int block_solve_max_k()
+{
+    return sizeof(T) > 8 ? 256 : kBlockSolveMaxK;
+}
+
 // One system (or a uniform batch of systems).
 template <typename T>
 struct BlockSolveParams
@@ -42,6 +50,7 @@ struct BlockSolveParams
     int         tM;             // M(i,j) = tM ? A(j,i) : A(i,j)
     int         rev;            // M upper: rows reversed
     int         unit;
+    int         conj;           // M's entries are conjugated (complex trans C)
     BatchPtr<T> A;
     int64_t     lda;
     BatchPtr<T> B;
@@ -61,7 +70,7 @@ constexpr size_t block_solve_smem_bytes(int k)
 // The core: solve M Y = alpha C for one strip.  The caller resolves pointers / sizes.
 template <typename T>
 __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, int k,
-                                  int side_left, int tM, int rev, int unit, T alpha,
+                                  int side_left, int tM, int rev, int unit, int conj, T alpha,
                                   int s0, int ncols, unsigned char* smem_raw)
 {
     T* Cs    = reinterpret_cast<T*>(smem_raw);
@@ -82,7 +91,7 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
     auto mval = [&](int i, int j) -> T {
         const int a = rev ? k - 1 - i : i, b = rev ? k - 1 - j : j;
         const int r = tM ? b : a, c = tM ? a : b;
-        return A[r + (int64_t)c * lda];
+        return conj_if(A[r + (int64_t)c * lda], conj);
     };
 
     if(alpha == T(0))
@@ -204,7 +213,7 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
                 {
                     if(lane == t)
                         y[q] *= dl;
-                    const T v = __shfl_sync(0xffffffffu, y[q], t);
+                    const T v = shfl_idx(y[q], t);
                     if(lane > t)
                         y[q] -= lt * v;
                 }
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__(kBsThreads) block_solve_kernel(BlockSolveParam
     const T ua    = p.ualpha.get();
     const T alpha = ua == T(0) ? T(0) : (p.first ? ua : T(1));
     block_solve_strip<T>(p.A.get(batch), p.lda, p.B.get(batch), p.ldb, p.k, p.side_left, p.tM,
-                         p.rev, p.unit, alpha, s0, ncols, smem_raw);
+                         p.rev, p.unit, p.conj, alpha, s0, ncols, smem_raw);
 }
 
 } // namespace rb200

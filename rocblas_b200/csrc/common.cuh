@@ -34,6 +34,90 @@ struct BatchPtr
     __host__ __device__ bool valid() const { return base != nullptr || arr != nullptr; }
 };
 
+// ---- complex numbers --------------------------------------------------------------------------
+// rocblas_float_complex / rocblas_double_complex are {x, y} pairs of float / double
+// (library/include/internal/rocblas-complex-types.h:82-91); cplx<R> has that layout and the
+// arithmetic the kernels need.  Complex division uses Smith's scaling (R. L. Smith, "Algorithm
+// 116: Complex division", CACM 5(8), 1962) so that |d|^2 is never formed.
+template <typename R>
+struct cplx
+{
+    R x, y;
+    __host__ __device__ constexpr cplx() : x(0), y(0) {}
+    __host__ __device__ constexpr cplx(R re) : x(re), y(0) {}
+    __host__ __device__ constexpr cplx(R re, R im) : x(re), y(im) {}
+    __host__ __device__ cplx& operator+=(const cplx& b) { x += b.x; y += b.y; return *this; }
+    __host__ __device__ cplx& operator-=(const cplx& b) { x -= b.x; y -= b.y; return *this; }
+    __host__ __device__ cplx& operator*=(const cplx& b) { *this = *this * b; return *this; }
+    friend __host__ __device__ cplx operator+(cplx a, cplx b) { return {a.x + b.x, a.y + b.y}; }
+    friend __host__ __device__ cplx operator-(cplx a, cplx b) { return {a.x - b.x, a.y - b.y}; }
+    friend __host__ __device__ cplx operator-(cplx a) { return {-a.x, -a.y}; }
+    friend __host__ __device__ cplx operator*(cplx a, cplx b)
+    {
+        return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+    }
+    friend __host__ __device__ cplx operator/(cplx n, cplx d)
+    {
+        const R ax = d.x < R(0) ? -d.x : d.x, ay = d.y < R(0) ? -d.y : d.y;
+        if(ax >= ay)
+        {
+            const R r = d.y / d.x, den = d.x + d.y * r;
+            return {(n.x + n.y * r) / den, (n.y - n.x * r) / den};
+        }
+        const R r = d.x / d.y, den = d.x * r + d.y;
+        return {(n.x * r + n.y) / den, (n.y * r - n.x) / den};
+    }
+    friend __host__ __device__ bool operator==(cplx a, cplx b) { return a.x == b.x && a.y == b.y; }
+    friend __host__ __device__ bool operator!=(cplx a, cplx b) { return !(a == b); }
+};
+
+template <typename T>
+struct is_cplx
+{
+    static constexpr bool value = false;
+};
+template <typename R>
+struct is_cplx<cplx<R>>
+{
+    static constexpr bool value = true;
+};
+
+// v, or conj(v) when c (real types: v)
+template <typename T>
+__host__ __device__ __forceinline__ T conj_if(T v, int)
+{
+    return v;
+}
+template <typename R>
+__host__ __device__ __forceinline__ cplx<R> conj_if(cplx<R> v, int c)
+{
+    return c ? cplx<R>(v.x, -v.y) : v;
+}
+
+// warp broadcast of lane `src`'s value
+template <typename T>
+__device__ __forceinline__ T shfl_idx(T v, int src)
+{
+    return __shfl_sync(0xffffffffu, v, src);
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> shfl_idx(cplx<R> v, int src)
+{
+    return {__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
+// read-only load
+template <typename T>
+__device__ __forceinline__ T ldg_val(const T* p)
+{
+    return __ldg(p);
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> ldg_val(const cplx<R>* p)
+{
+    return {__ldg(&p->x), __ldg(&p->y)};
+}
+
 // A scalar that is either an immediate (host pointer mode) or read on the device from a
 // device pointer (device pointer mode).  Reading on the device means no device-to-host
 // synchronisation is needed, unlike the reference launcher
@@ -44,7 +128,7 @@ struct Scalar
 {
     T        val = T(1);
     const T* ptr = nullptr;
-    __device__ __forceinline__ T get() const { return ptr ? __ldg(ptr) : val; }
+    __device__ __forceinline__ T get() const { return ptr ? ldg_val(ptr) : val; }
 };
 
 __host__ __device__ constexpr int64_t ceil_div(int64_t a, int64_t b)

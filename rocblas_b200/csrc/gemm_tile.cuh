@@ -29,6 +29,7 @@ struct GemmParams
     BatchPtr<T> P, Q, C;
     int64_t     ldp, ldq, ldc;
     int         transP, transQ; // 0: op(X) = X, 1: op(X) = X^T
+    int         conjP, conjQ;   // complex types: op(X) conjugated as well (trans C); else unused
     int         triP, triQ;     // kTri* mask in stored coordinates (triangular invA blocks)
     T           a_imm;          // a = a_user ? ualpha : a_imm
     int         a_user;

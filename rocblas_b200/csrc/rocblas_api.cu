@@ -164,7 +164,8 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                          rocblas_operation trans, rocblas_diagonal diag, int m, int n,
                          const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
                          const void* Bptr, BatchPtr<T> B, int64_t ldb, int batch,
-                         const void* invA_ptr, BatchPtr<T> invA, int64_t invA_size)
+                         const void* invA_ptr, BatchPtr<T> invA, int64_t invA_size,
+                         int conj = -1)
 {
     if(!h)
         return rocblas_status_invalid_handle;
@@ -188,6 +189,9 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     pr.upper     = uplo == rocblas_fill_upper;
     pr.trans     = trans != rocblas_operation_none;
     pr.unit      = diag == rocblas_diagonal_unit;
+    // complex trans C reads conj(A); trsv's side-right form of trans C asks for conj(A)
+    // without the transpose through `conj`
+    pr.conj = is_cplx<T>::value && (conj >= 0 ? conj != 0 : trans == rocblas_operation_conjugate_transpose);
     pr.m = m;
     pr.n = n;
     pr.batch = batch;
@@ -201,7 +205,8 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     const int64_t k = pr.k();
     // a supplied invA smaller than 128 * k elements is ignored (rocblas_trsm_kernels.hpp:3832-3836)
     rocblas_status perf = rocblas_status_success;
-    bool           have_invA = invA_ptr != nullptr;
+    // complex solves use block-solver leaves and do not read a supplied invA
+    bool           have_invA = invA_ptr != nullptr && !is_cplx<T>::value;
     if(have_invA && invA_size / kInvNB < k)
     {
         have_invA = false;
@@ -267,6 +272,18 @@ BatchPtr<T> arrayed(const void* arr)
     BatchPtr<T> b;
     b.arr = arr;
     return b;
+}
+
+// TA: the ABI's element type; T: the library's (same layout; cplx<R> for the complex structs)
+template <typename T, typename TA>
+const T* as_impl(const TA* p)
+{
+    return reinterpret_cast<const T*>(p);
+}
+template <typename T, typename TA>
+T* as_impl(TA* p)
+{
+    return reinterpret_cast<T*>(p);
 }
 
 // ---- trmm ----------------------------------------------------------------------------------
@@ -386,6 +403,7 @@ rocblas_status trmm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     {
         g.K = m;
         g.P = A; g.ldp = lda; g.transP = trans != rocblas_operation_none; g.triP = tri;
+        g.conjP = trans == rocblas_operation_conjugate_transpose;
         g.Q = src; g.ldq = lds; g.transQ = 0; g.triQ = kTriNone;
     }
     else
@@ -393,6 +411,7 @@ rocblas_status trmm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
         g.K = n;
         g.P = src; g.ldp = lds; g.transP = 0; g.triP = kTriNone;
         g.Q = A; g.ldq = lda; g.transQ = trans != rocblas_operation_none; g.triQ = tri;
+        g.conjQ = trans == rocblas_operation_conjugate_transpose;
     }
     g.C = C;
     g.ldc = ldc;
@@ -458,8 +477,10 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
     rocblas_status ast = trsv_arg_check(h, uplo, trans, diag, n, Aptr, lda, xptr, incx, batch);
     if(ast != rocblas_status_continue)
         return ast;
+    // op(A) x = b is x^T op(A)^T = b^T: op(A)^T is A^T for N, A for T, conj(A) for C
     const rocblas_operation flip
         = trans == rocblas_operation_none ? rocblas_operation_transpose : rocblas_operation_none;
+    const int conj = trans == rocblas_operation_conjugate_transpose ? 1 : 0;
     static const T one = T(1);
     // the solve's alpha is 1 whatever the pointer mode
     const rocblas_pointer_mode mode = h->pointer_mode;
@@ -468,12 +489,12 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
     if(incx > 0)
     {
         st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, xptr, x,
-                          incx, batch, nullptr, BatchPtr<T>{}, 0);
+                          incx, batch, nullptr, BatchPtr<T>{}, 0, conj);
     }
     else if(h->size_query)
     {
         st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, xptr, x,
-                          1, batch, nullptr, BatchPtr<T>{}, 0);
+                          1, batch, nullptr, BatchPtr<T>{}, 0, conj);
     }
     else
     {
@@ -495,7 +516,7 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
                 count_launch();
             }
             st = trsm_impl<T>(h, rocblas_side_right, uplo, flip, diag, 1, n, &one, Aptr, A, lda, tmp,
-                              strided<T>(tmp, n), 1, batch, nullptr, BatchPtr<T>{}, 0);
+                              strided<T>(tmp, n), 1, batch, nullptr, BatchPtr<T>{}, 0, conj);
             if(st == rocblas_status_success || st == rocblas_status_perf_degraded)
                 for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
                 {
@@ -1462,64 +1483,64 @@ bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
 }
 
 // ---- trsm ------------------------------------------------------------------------------------
-#define TRSM_PLAIN(NAME, T, I)                                                                    \
+#define TRSM_PLAIN(NAME, TA, T, I)                                                                \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
-                        const T* A, I lda, T* B, I ldb)                                          \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n,                \
+                        const TA* alpha, const TA* A, I lda, TA* B, I ldb)                        \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A, strided<T>(A, 0),     \
-                               lda, B, strided<T>(B, 0), ldb, 1);                                \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
+                               strided<T>(as_impl<T>(A), 0), lda, B,                             \
+                               strided<T>(as_impl<T>(B), 0), ldb, 1);                            \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_PLAIN(rocblas_strsm, float, rocblas_int)
-TRSM_PLAIN(rocblas_dtrsm, double, rocblas_int)
-TRSM_PLAIN(rocblas_strsm_64, float, int64_t)
-TRSM_PLAIN(rocblas_dtrsm_64, double, int64_t)
-
-#define TRSM_BATCHED(NAME, T, I)                                                                  \
+#define TRSM_BATCHED(NAME, TA, T, I)                                                              \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
-                        const T* const A[], I lda, T* const B[], I ldb, I batch_count)            \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n,                \
+                        const TA* alpha, const TA* const A[], I lda, TA* const B[], I ldb,       \
+                        I batch_count)                                                           \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A, arrayed<T>(A), lda,   \
-                               B, arrayed<T>(B), ldb, batch_count);                              \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
+                               arrayed<T>(A), lda, B, arrayed<T>(B), ldb, batch_count);          \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_BATCHED(rocblas_strsm_batched, float, rocblas_int)
-TRSM_BATCHED(rocblas_dtrsm_batched, double, rocblas_int)
-TRSM_BATCHED(rocblas_strsm_batched_64, float, int64_t)
-TRSM_BATCHED(rocblas_dtrsm_batched_64, double, int64_t)
-
-#define TRSM_STRIDED(NAME, T, I)                                                                  \
+#define TRSM_STRIDED(NAME, TA, T, I)                                                              \
     rocblas_status NAME(rocblas_handle h, rocblas_side side, rocblas_fill uplo,                  \
-                        rocblas_operation trans, rocblas_diagonal diag, I m, I n, const T* alpha, \
-                        const T* A, I lda, rocblas_stride stride_a, T* B, I ldb,                 \
-                        rocblas_stride stride_b, I batch_count)                                  \
+                        rocblas_operation trans, rocblas_diagonal diag, I m, I n,                \
+                        const TA* alpha, const TA* A, I lda, rocblas_stride stride_a, TA* B,     \
+                        I ldb, rocblas_stride stride_b, I batch_count)                           \
     try                                                                                          \
     {                                                                                            \
-        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, alpha, A,                       \
-                               strided<T>(A, stride_a), lda, B, strided<T>(B, stride_b), ldb,    \
-                               batch_count);                                                     \
+        return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
+                               strided<T>(as_impl<T>(A), stride_a), lda, B,                      \
+                               strided<T>(as_impl<T>(B), stride_b), ldb, batch_count);           \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
         return exception_status();                                                               \
     }
 
-TRSM_STRIDED(rocblas_strsm_strided_batched, float, rocblas_int)
-TRSM_STRIDED(rocblas_dtrsm_strided_batched, double, rocblas_int)
-TRSM_STRIDED(rocblas_strsm_strided_batched_64, float, int64_t)
-TRSM_STRIDED(rocblas_dtrsm_strided_batched_64, double, int64_t)
+#define TRSM_ALL(S, TA, T)                                                 \
+    TRSM_PLAIN(rocblas_##S##trsm, TA, T, rocblas_int)                      \
+    TRSM_PLAIN(rocblas_##S##trsm_64, TA, T, int64_t)                       \
+    TRSM_BATCHED(rocblas_##S##trsm_batched, TA, T, rocblas_int)            \
+    TRSM_BATCHED(rocblas_##S##trsm_batched_64, TA, T, int64_t)             \
+    TRSM_STRIDED(rocblas_##S##trsm_strided_batched, TA, T, rocblas_int)    \
+    TRSM_STRIDED(rocblas_##S##trsm_strided_batched_64, TA, T, int64_t)
+
+TRSM_ALL(s, float, float)
+TRSM_ALL(d, double, double)
+TRSM_ALL(c, rocblas_float_complex, cplx<float>)
+TRSM_ALL(z, rocblas_double_complex, cplx<double>)
 
 // rocblas_trsm_ex type switch (library/src/blas3/rocblas_trsm.cpp:28-73)
 rocblas_status rocblas_trsm_ex(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
@@ -1542,9 +1563,19 @@ try
                                  strided<double>((double*)B, 0), ldb, 1, invA,
                                  strided<double>((const double*)invA, 0), invA_size);
     case rocblas_datatype_f32_c:
+        return trsm_impl_64<cplx<float>>(h, side, uplo, trans, diag, m, n,
+                                         (const cplx<float>*)alpha, A,
+                                         strided<cplx<float>>((const cplx<float>*)A, 0), lda, B,
+                                         strided<cplx<float>>((cplx<float>*)B, 0), ldb, 1, invA,
+                                         strided<cplx<float>>((const cplx<float>*)invA, 0),
+                                         invA_size);
     case rocblas_datatype_f64_c:
-        // complex trsm is outside this library's scope
-        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+        return trsm_impl_64<cplx<double>>(h, side, uplo, trans, diag, m, n,
+                                          (const cplx<double>*)alpha, A,
+                                          strided<cplx<double>>((const cplx<double>*)A, 0), lda, B,
+                                          strided<cplx<double>>((cplx<double>*)B, 0), ldb, 1, invA,
+                                          strided<cplx<double>>((const cplx<double>*)invA, 0),
+                                          invA_size);
     default:
         return rocblas_status_not_implemented;
     }
@@ -1573,8 +1604,15 @@ try
                                  arrayed<double>(A), lda, B, arrayed<double>(B), ldb, batch_count,
                                  invA, arrayed<double>(invA), invA_size);
     case rocblas_datatype_f32_c:
+        return trsm_impl_64<cplx<float>>(h, side, uplo, trans, diag, m, n,
+                                         (const cplx<float>*)alpha, A, arrayed<cplx<float>>(A), lda,
+                                         B, arrayed<cplx<float>>(B), ldb, batch_count, invA,
+                                         arrayed<cplx<float>>(invA), invA_size);
     case rocblas_datatype_f64_c:
-        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+        return trsm_impl_64<cplx<double>>(h, side, uplo, trans, diag, m, n,
+                                          (const cplx<double>*)alpha, A, arrayed<cplx<double>>(A),
+                                          lda, B, arrayed<cplx<double>>(B), ldb, batch_count, invA,
+                                          arrayed<cplx<double>>(invA), invA_size);
     default:
         return rocblas_status_not_implemented;
     }
@@ -1608,8 +1646,17 @@ try
                                  strided<double>((double*)B, stride_B), ldb, batch_count, invA,
                                  strided<double>((const double*)invA, stride_invA), invA_size);
     case rocblas_datatype_f32_c:
+        return trsm_impl_64<cplx<float>>(
+            h, side, uplo, trans, diag, m, n, (const cplx<float>*)alpha, A,
+            strided<cplx<float>>((const cplx<float>*)A, stride_A), lda, B,
+            strided<cplx<float>>((cplx<float>*)B, stride_B), ldb, batch_count, invA,
+            strided<cplx<float>>((const cplx<float>*)invA, stride_invA), invA_size);
     case rocblas_datatype_f64_c:
-        return h ? rocblas_status_not_implemented : rocblas_status_invalid_handle;
+        return trsm_impl_64<cplx<double>>(
+            h, side, uplo, trans, diag, m, n, (const cplx<double>*)alpha, A,
+            strided<cplx<double>>((const cplx<double>*)A, stride_A), lda, B,
+            strided<cplx<double>>((cplx<double>*)B, stride_B), ldb, batch_count, invA,
+            strided<cplx<double>>((const cplx<double>*)invA, stride_invA), invA_size);
     default:
         return rocblas_status_not_implemented;
     }
@@ -1688,14 +1735,14 @@ catch(...)
 }
 
 // ---- trsv (rocblas-functions.h:9900-9908, 10041-10050, 10198-10209) ------------------------
-#define TRSV_ALL(T, S, I, SUF)                                                                     \
+#define TRSV_ALL(TA, T, S, I, SUF)                                                                 \
     rocblas_status rocblas_##S##trsv##SUF(rocblas_handle h, rocblas_fill uplo,                      \
                                           rocblas_operation transA, rocblas_diagonal diag, I n,     \
-                                          const T* A, I lda, T* x, I incx)                          \
+                                          const TA* A, I lda, TA* x, I incx)                        \
     try                                                                                             \
     {                                                                                               \
-        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(A, 0), lda, x,               \
-                               strided<T>(x, 0), incx, 1);                                          \
+        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(as_impl<T>(A), 0), lda, x,  \
+                               strided<T>(as_impl<T>(x), 0), incx, 1);                              \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
@@ -1703,7 +1750,7 @@ catch(...)
     }                                                                                               \
     rocblas_status rocblas_##S##trsv_batched##SUF(rocblas_handle h, rocblas_fill uplo,              \
                                                   rocblas_operation transA, rocblas_diagonal diag,  \
-                                                  I n, const T* const A[], I lda, T* const x[],     \
+                                                  I n, const TA* const A[], I lda, TA* const x[],   \
                                                   I incx, I batch_count)                            \
     try                                                                                             \
     {                                                                                               \
@@ -1716,32 +1763,37 @@ catch(...)
     }                                                                                               \
     rocblas_status rocblas_##S##trsv_strided_batched##SUF(                                          \
         rocblas_handle h, rocblas_fill uplo, rocblas_operation transA, rocblas_diagonal diag, I n,  \
-        const T* A, I lda, rocblas_stride stride_A, T* x, I incx, rocblas_stride stride_x,          \
+        const TA* A, I lda, rocblas_stride stride_A, TA* x, I incx, rocblas_stride stride_x,        \
         I batch_count)                                                                              \
     try                                                                                             \
     {                                                                                               \
-        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(A, stride_A), lda, x,        \
-                               strided<T>(x, stride_x), incx, batch_count);                         \
+        return trsv_impl_64<T>(h, uplo, transA, diag, n, A, strided<T>(as_impl<T>(A), stride_A),    \
+                               lda, x, strided<T>(as_impl<T>(x), stride_x), incx, batch_count);     \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }
-TRSV_ALL(float, s, rocblas_int, )
-TRSV_ALL(double, d, rocblas_int, )
-TRSV_ALL(float, s, int64_t, _64)
-TRSV_ALL(double, d, int64_t, _64)
+TRSV_ALL(float, float, s, rocblas_int, )
+TRSV_ALL(double, double, d, rocblas_int, )
+TRSV_ALL(rocblas_float_complex, cplx<float>, c, rocblas_int, )
+TRSV_ALL(rocblas_double_complex, cplx<double>, z, rocblas_int, )
+TRSV_ALL(float, float, s, int64_t, _64)
+TRSV_ALL(double, double, d, int64_t, _64)
+TRSV_ALL(rocblas_float_complex, cplx<float>, c, int64_t, _64)
+TRSV_ALL(rocblas_double_complex, cplx<double>, z, int64_t, _64)
 
 // ---- trmm (rocblas-functions.h:18300-18393, 18630-18644, 18904-18921) -----------------------
-#define TRMM_ALL(T, S, I, SUF)                                                                      \
+#define TRMM_ALL(TA, T, S, I, SUF)                                                                  \
     rocblas_status rocblas_##S##trmm##SUF(rocblas_handle h, rocblas_side side, rocblas_fill uplo,   \
                                           rocblas_operation transA, rocblas_diagonal diag, I m,     \
-                                          I n, const T* alpha, const T* A, I lda, const T* B,       \
-                                          I ldb, T* C, I ldc)                                       \
+                                          I n, const TA* alpha, const TA* A, I lda, const TA* B,    \
+                                          I ldb, TA* C, I ldc)                                      \
     try                                                                                             \
     {                                                                                               \
-        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A, strided<T>(A, 0), lda,  \
-                               B, strided<T>(B, 0), ldb, C, strided<T>(C, 0), ldc, 1);              \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, as_impl<T>(alpha), A,             \
+                               strided<T>(as_impl<T>(A), 0), lda, B, strided<T>(as_impl<T>(B), 0),  \
+                               ldb, C, strided<T>(as_impl<T>(C), 0), ldc, 1);                       \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
@@ -1749,12 +1801,13 @@ TRSV_ALL(double, d, int64_t, _64)
     }                                                                                               \
     rocblas_status rocblas_##S##trmm_batched##SUF(                                                  \
         rocblas_handle h, rocblas_side side, rocblas_fill uplo, rocblas_operation transA,           \
-        rocblas_diagonal diag, I m, I n, const T* alpha, const T* const A[], I lda,                 \
-        const T* const B[], I ldb, T* const C[], I ldc, I batch_count)                              \
+        rocblas_diagonal diag, I m, I n, const TA* alpha, const TA* const A[], I lda,               \
+        const TA* const B[], I ldb, TA* const C[], I ldc, I batch_count)                            \
     try                                                                                             \
     {                                                                                               \
-        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A, arrayed<T>(A), lda, B,  \
-                               arrayed<T>(B), ldb, C, arrayed<T>(C), ldc, batch_count);             \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, as_impl<T>(alpha), A,             \
+                               arrayed<T>(A), lda, B, arrayed<T>(B), ldb, C, arrayed<T>(C), ldc,    \
+                               batch_count);                                                        \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
@@ -1762,23 +1815,28 @@ TRSV_ALL(double, d, int64_t, _64)
     }                                                                                               \
     rocblas_status rocblas_##S##trmm_strided_batched##SUF(                                          \
         rocblas_handle h, rocblas_side side, rocblas_fill uplo, rocblas_operation transA,           \
-        rocblas_diagonal diag, I m, I n, const T* alpha, const T* A, I lda,                         \
-        rocblas_stride stride_A, const T* B, I ldb, rocblas_stride stride_B, T* C, I ldc,           \
+        rocblas_diagonal diag, I m, I n, const TA* alpha, const TA* A, I lda,                       \
+        rocblas_stride stride_A, const TA* B, I ldb, rocblas_stride stride_B, TA* C, I ldc,         \
         rocblas_stride stride_C, I batch_count)                                                     \
     try                                                                                             \
     {                                                                                               \
-        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, alpha, A,                         \
-                               strided<T>(A, stride_A), lda, B, strided<T>(B, stride_B), ldb, C,    \
-                               strided<T>(C, stride_C), ldc, batch_count);                          \
+        return trmm_impl_64<T>(h, side, uplo, transA, diag, m, n, as_impl<T>(alpha), A,             \
+                               strided<T>(as_impl<T>(A), stride_A), lda, B,                         \
+                               strided<T>(as_impl<T>(B), stride_B), ldb, C,                         \
+                               strided<T>(as_impl<T>(C), stride_C), ldc, batch_count);              \
     }                                                                                               \
     catch(...)                                                                                      \
     {                                                                                               \
         return exception_status();                                                                  \
     }
-TRMM_ALL(float, s, rocblas_int, )
-TRMM_ALL(double, d, rocblas_int, )
-TRMM_ALL(float, s, int64_t, _64)
-TRMM_ALL(double, d, int64_t, _64)
+TRMM_ALL(float, float, s, rocblas_int, )
+TRMM_ALL(double, double, d, rocblas_int, )
+TRMM_ALL(rocblas_float_complex, cplx<float>, c, rocblas_int, )
+TRMM_ALL(rocblas_double_complex, cplx<double>, z, rocblas_int, )
+TRMM_ALL(float, float, s, int64_t, _64)
+TRMM_ALL(double, double, d, int64_t, _64)
+TRMM_ALL(rocblas_float_complex, cplx<float>, c, int64_t, _64)
+TRMM_ALL(rocblas_double_complex, cplx<double>, z, int64_t, _64)
 
 // ---- server (rocblas_b200_ext.h) --------------------------------------------------------------
 struct rocblas_b200_server_

@@ -16,6 +16,8 @@
 //     Without workspace for invA the leaves use the block solver instead and the call
 //     reports rocblas_status_perf_degraded, as the reference's backup path does
 //     (rocblas_trsm_kernels.hpp:1926-1944).
+//   * complex types: the same recursion with block-solver leaves (no invA) and the complex
+//     DMMA tiles (gemm_cdmma.cuh) for the updates; trans C conjugates A in both.
 #pragma once
 #include <algorithm>
 #include <atomic>
@@ -24,6 +26,7 @@
 #include <type_traits>
 
 #include "block_solve.cuh"
+#include "gemm_cdmma.cuh"
 #include "gemm_dmma.cuh"
 #include "gemm_tile.cuh"
 #include "handle.hpp"
@@ -48,7 +51,8 @@ inline void count_launch()
 template <typename T>
 struct TrsmProblem
 {
-    int         side_left, upper, trans, unit; // trans: op(A) != A
+    int         side_left, upper, trans, unit; // trans: op(A) is a transpose of A
+    int         conj;                          // complex: op(A)'s entries conjugated
     int         m, n, batch;
     BatchPtr<T> A;
     int64_t     lda;
@@ -87,16 +91,26 @@ static void launch_gemm(const GemmParams<T>& p0, int batch, cudaStream_t s, int 
             count_launch();
         return;
     }
-    const size_t smem = gemm_smem_bytes<T>();
-    ensure_smem_attr<T>((const void*)gemm_tile_kernel<T>, smem);
-    for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+    else if constexpr(is_cplx<T>::value)
     {
-        GemmParams<T> p = p0;
-        p.batch_base    = b0;
-        dim3 grid((unsigned)ceil_div(p.M, kGemmBM), (unsigned)ceil_div(p.N, kGemmBN),
-                  (unsigned)std::min(kMaxGridYZ, batch - b0));
-        gemm_tile_kernel<T><<<grid, kGemmThreads, smem, s>>>(p);
-        count_launch();
+        launch_gemm_cdmma(p0, batch, s, sms);
+        for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+            count_launch();
+        return;
+    }
+    else
+    {
+        const size_t smem = gemm_smem_bytes<T>();
+        ensure_smem_attr<T>((const void*)gemm_tile_kernel<T>, smem);
+        for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+        {
+            GemmParams<T> p = p0;
+            p.batch_base    = b0;
+            dim3 grid((unsigned)ceil_div(p.M, kGemmBM), (unsigned)ceil_div(p.N, kGemmBN),
+                      (unsigned)std::min(kMaxGridYZ, batch - b0));
+            gemm_tile_kernel<T><<<grid, kGemmThreads, smem, s>>>(p);
+            count_launch();
+        }
     }
 }
 
@@ -132,6 +146,7 @@ static void launch_block_solve(const TrsmProblem<T>& pr, int m, int n, BatchPtr<
     const int mlower = pr.side_left ? pr.oplower() : !pr.oplower();
     p.rev  = !mlower;
     p.unit = pr.unit;
+    p.conj = pr.conj;
     p.A = A;
     p.lda = pr.lda;
     p.B = B;
@@ -141,7 +156,7 @@ static void launch_block_solve(const TrsmProblem<T>& pr, int m, int n, BatchPtr<
     const int    ncols   = pr.side_left ? n : m;
     const int    nstrips = (int)ceil_div(ncols, kBsW);
     const size_t smem    = block_solve_smem_bytes<T>(p.k);
-    ensure_smem_attr<T>((const void*)block_solve_kernel<T>, block_solve_smem_bytes<T>(kBlockSolveMaxK));
+    ensure_smem_attr<T>((const void*)block_solve_kernel<T>, block_solve_smem_bytes<T>(block_solve_max_k<T>()));
     for(int b0 = 0; b0 < pr.batch; b0 += kMaxGridYZ)
     {
         p.batch_base = b0;
@@ -222,6 +237,7 @@ struct Recursive
         {
             g.M = c_hi - c_lo; g.N = pr.n; g.K = x_hi - x_lo;
             opA_block(c_lo, x_lo, g.P, g.transP); g.ldp = pr.lda; g.triP = kTriNone;
+            g.conjP = pr.conj;
             g.Q = pr.B.shifted(x_lo); g.ldq = pr.ldb; g.transQ = 0; g.triQ = kTriNone;
             g.C = pr.B.shifted(c_lo); g.ldc = pr.ldb;
         }
@@ -230,6 +246,7 @@ struct Recursive
             g.M = pr.m; g.N = c_hi - c_lo; g.K = x_hi - x_lo;
             g.P = pr.B.shifted((int64_t)x_lo * pr.ldb); g.ldp = pr.ldb; g.transP = 0; g.triP = kTriNone;
             opA_block(x_lo, c_lo, g.Q, g.transQ); g.ldq = pr.lda; g.triQ = kTriNone;
+            g.conjQ = pr.conj;
             g.C = pr.B.shifted((int64_t)c_lo * pr.ldb); g.ldc = pr.ldb;
         }
         g.a_imm = T(-1); g.a_user = 0;
@@ -293,7 +310,7 @@ static Algo choose_algo(const TrsmProblem<T>& pr)
 {
     const Tuning& t = tuning();
     const int     k = pr.k();
-    if(k > std::min(t.block_max_k, kBlockSolveMaxK))
+    if(k > std::min(t.block_max_k, block_solve_max_k<T>()))
         return Algo::recursive;
     if(k <= t.block_always_k)
         return Algo::block;
@@ -308,7 +325,7 @@ static Algo choose_algo(const TrsmProblem<T>& pr)
 template <typename T>
 static bool use_chain(const TrsmProblem<T>& pr)
 {
-    if(choose_algo(pr) != Algo::recursive)
+    if(is_cplx<T>::value || choose_algo(pr) != Algo::recursive)
         return false;
     const int64_t ncols = pr.side_left ? pr.n : pr.m;
     const int64_t limit = std::is_same<T, double>::value ? tuning().chain_max_cols
@@ -372,7 +389,8 @@ static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first
 template <typename T>
 static size_t trsm_invA_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
 {
-    if(choose_algo(pr) != Algo::recursive || have_supplied_invA)
+    // complex solves use block-solver leaves and need no invA
+    if(is_cplx<T>::value || choose_algo(pr) != Algo::recursive || have_supplied_invA)
         return 0;
     return (size_t)kInvNB * (size_t)pr.k() * sizeof(T) * (size_t)pr.batch;
 }
@@ -397,25 +415,32 @@ static void trsm_run(TrsmProblem<T> pr, void* ws, bool supplied_invA)
         return;
     }
     const int k = pr.k();
-    if(!supplied_invA)
+    if constexpr(is_cplx<T>::value)
     {
-        if(ws)
-        {
-            BatchPtr<T> inv;
-            inv.base   = reinterpret_cast<T*>(ws);
-            inv.stride = (int64_t)kInvNB * k;
-            build_invA<T>(pr, inv);
-            pr.invA = inv;
-        }
-        else
-            pr.invA = BatchPtr<T>{};
+        pr.invA = BatchPtr<T>{};
     }
-    if(ws && pr.invA.valid() && use_chain(pr))
+    else
     {
-        const size_t off = (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
-        launch_chain_sub<T>(pr, 0, (int)ceil_div(k, kInvNB), 1, chain_shape_of(pr).w,
-                            reinterpret_cast<char*>(ws) + off);
-        return;
+        if(!supplied_invA)
+        {
+            if(ws)
+            {
+                BatchPtr<T> inv;
+                inv.base   = reinterpret_cast<T*>(ws);
+                inv.stride = (int64_t)kInvNB * k;
+                build_invA<T>(pr, inv);
+                pr.invA = inv;
+            }
+            else
+                pr.invA = BatchPtr<T>{};
+        }
+        if(ws && pr.invA.valid() && use_chain(pr))
+        {
+            const size_t off = (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
+            launch_chain_sub<T>(pr, 0, (int)ceil_div(k, kInvNB), 1, chain_shape_of(pr).w,
+                                reinterpret_cast<char*>(ws) + off);
+            return;
+        }
     }
     Recursive<T> rec{pr, k, (int)ceil_div(k, kInvNB)};
     rec.solve(0, rec.nblk, 1);

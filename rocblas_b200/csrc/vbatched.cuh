@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kBsThreads) vb_persistent_kernel(VbParams<T> p
         const int oplow = (q.uplo == kLower) != (trans != 0);
         const int mlow  = left ? oplow : !oplow;
         block_solve_strip<T>(reinterpret_cast<const T*>(q.A), q.lda, reinterpret_cast<T*>(q.B),
-                             q.ldb, k, left, tM, !mlow, q.diag == kUnit, alpha, strip * kBsW,
+                             q.ldb, k, left, tM, !mlow, q.diag == kUnit, 0, alpha, strip * kBsW,
                              ncols, smem_raw);
         __syncthreads();
     }

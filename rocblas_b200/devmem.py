@@ -13,7 +13,8 @@ import numpy as np
 import torch
 
 from . import (
-    DIAG, SIDE, TRANS, UPLO, check, datatype_f32_r, datatype_f64_r, lib, pointer_mode_device,
+    DIAG, SIDE, TRANS, UPLO, check, datatype_f32_c, datatype_f32_r, datatype_f64_c, datatype_f64_r,
+    lib, pointer_mode_device,
     pointer_mode_host, status_perf_degraded, status_success,
 )
 
@@ -45,13 +46,22 @@ def _is_double(t):
     return t.dtype == torch.float64
 
 
+_PREFIX = {torch.float32: "s", torch.float64: "d", torch.complex64: "c", torch.complex128: "z"}
+_DATATYPE = {torch.float32: datatype_f32_r, torch.float64: datatype_f64_r,
+             torch.complex64: datatype_f32_c, torch.complex128: datatype_f64_c}
+
+
+def _fn(name, t):
+    """rocblas_<s|d|c|z><name> for the element type of device tensor t."""
+    return getattr(lib(), f"rocblas_{_PREFIX[t.dtype]}{name}")
+
+
 def trsm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, alpha_on_device=False,
          allow=(status_success,)):
     """rocblas_?trsm on device tensors; alpha is a Python float (host pointer mode) or, with
     alpha_on_device, placed in device memory and passed in device pointer mode."""
-    dbl = _is_double(B)
-    fn = lib().rocblas_dtrsm if dbl else lib().rocblas_strsm
-    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    fn = _fn("trsm", B)
+    keep, aptr = _alpha(handle, alpha, B.dtype, alpha_on_device, B.device)
     st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
             _code(DIAG, diag), m, n, aptr, _ptr(A), lda, _ptr(B), ldb)
     _restore(handle, alpha_on_device)
@@ -60,21 +70,18 @@ def trsm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, alpha_on_
 
 def trsm_ex(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, invA, invA_size,
             alpha_on_device=False, allow=(status_success,)):
-    dbl = _is_double(B)
-    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    keep, aptr = _alpha(handle, alpha, B.dtype, alpha_on_device, B.device)
     st = lib().rocblas_trsm_ex(handle.value, _code(SIDE, side), _code(UPLO, uplo),
                                _code(TRANS, trans), _code(DIAG, diag), m, n, aptr, _ptr(A), lda,
-                               _ptr(B), ldb, _ptr(invA), invA_size,
-                               datatype_f64_r if dbl else datatype_f32_r)
+                               _ptr(B), ldb, _ptr(invA), invA_size, _DATATYPE[B.dtype])
     _restore(handle, alpha_on_device)
     return check("rocblas_trsm_ex", st, allow)
 
 
 def trsm_strided_batched(handle, side, uplo, trans, diag, m, n, alpha, A, lda, stride_a, B, ldb,
                          stride_b, batch, alpha_on_device=False, allow=(status_success,)):
-    dbl = _is_double(B)
-    fn = lib().rocblas_dtrsm_strided_batched if dbl else lib().rocblas_strsm_strided_batched
-    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, B.device)
+    fn = _fn("trsm_strided_batched", B)
+    keep, aptr = _alpha(handle, alpha, B.dtype, alpha_on_device, B.device)
     st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
             _code(DIAG, diag), m, n, aptr, _ptr(A), lda, stride_a, _ptr(B), ldb, stride_b, batch)
     _restore(handle, alpha_on_device)
@@ -85,9 +92,8 @@ def trmm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, C, ldc, a
          allow=(status_success,)):
     """rocblas_?trmm on device tensors: C := alpha op(A) B (side L) or alpha B op(A) (side R);
     C may be B (in place, ldc == ldb)."""
-    dbl = _is_double(C)
-    fn = lib().rocblas_dtrmm if dbl else lib().rocblas_strmm
-    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, C.device)
+    fn = _fn("trmm", C)
+    keep, aptr = _alpha(handle, alpha, C.dtype, alpha_on_device, C.device)
     st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
             m, n, aptr, _ptr(A), lda, _ptr(B), ldb, _ptr(C), ldc)
     _restore(handle, alpha_on_device)
@@ -96,9 +102,8 @@ def trmm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, C, ldc, a
 
 def trmm_strided_batched(handle, side, uplo, trans, diag, m, n, alpha, A, lda, stride_a, B, ldb,
                          stride_b, C, ldc, stride_c, batch, allow=(status_success,)):
-    dbl = _is_double(C)
-    fn = lib().rocblas_dtrmm_strided_batched if dbl else lib().rocblas_strmm_strided_batched
-    keep, aptr = _alpha(handle, alpha, dbl, False, C.device)
+    fn = _fn("trmm_strided_batched", C)
+    keep, aptr = _alpha(handle, alpha, C.dtype, False, C.device)
     st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag),
             m, n, aptr, _ptr(A), lda, stride_a, _ptr(B), ldb, stride_b, _ptr(C), ldc, stride_c, batch)
     return check("rocblas_trmm_strided_batched", st, allow)
@@ -108,12 +113,11 @@ def trsm_batched(handle, side, uplo, trans, diag, m, n, alpha, A_list, lda, B_li
                  alpha_on_device=False, allow=(status_success,)):
     """A_list / B_list: lists of device tensors; their addresses are gathered into device
     arrays of device pointers, as the _batched API takes them."""
-    dbl = _is_double(B_list[0])
-    fn = lib().rocblas_dtrsm_batched if dbl else lib().rocblas_strsm_batched
+    fn = _fn("trsm_batched", B_list[0])
     dev = B_list[0].device
     Ap = torch.tensor([a.data_ptr() for a in A_list], dtype=torch.int64, device=dev)
     Bp = torch.tensor([b.data_ptr() for b in B_list], dtype=torch.int64, device=dev)
-    keep, aptr = _alpha(handle, alpha, dbl, alpha_on_device, dev)
+    keep, aptr = _alpha(handle, alpha, B_list[0].dtype, alpha_on_device, dev)
     st = fn(handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans),
             _code(DIAG, diag), m, n, aptr, _ptr(Ap), lda, _ptr(Bp), ldb, len(B_list))
     _restore(handle, alpha_on_device)
@@ -139,13 +143,14 @@ def trtri_strided_batched(handle, uplo, diag, n, A, lda, stride_a, invA, ldinv, 
     return check("rocblas_trtri_strided_batched", st, allow)
 
 
-def _alpha(handle, alpha, dbl, on_device, device):
+def _alpha(handle, alpha, dtype, on_device, device):
+    """alpha of the call's element type, in host memory or (on_device) in device memory."""
     if on_device:
-        t = torch.tensor([alpha], dtype=torch.float64 if dbl else torch.float32, device=device)
+        t = torch.tensor([alpha], dtype=dtype, device=device)
         lib().rocblas_set_pointer_mode(handle.value, pointer_mode_device)
         return t, ctypes.c_void_p(t.data_ptr())
-    c = ctypes.c_double(alpha) if dbl else ctypes.c_float(alpha)
-    return c, ctypes.cast(ctypes.byref(c), ctypes.c_void_p)
+    t = torch.tensor([alpha], dtype=dtype)
+    return t, ctypes.c_void_p(t.data_ptr())
 
 
 def _restore(handle, on_device):

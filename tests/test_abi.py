@@ -87,12 +87,13 @@ def test_trsm_ex_type_switch(handle):
     ap = ctypes.cast(ctypes.byref(a), ctypes.c_void_p)
     args = [rb.side_left, rb.fill_lower, rb.operation_none, rb.diagonal_non_unit, 4, 4, ap, 1, 4, 1, 4,
             None, 0]
-    assert L.rocblas_trsm_ex(handle.value, *args, rb.datatype_f64_c) == rb.status_not_implemented
     assert L.rocblas_trsm_ex(handle.value, *args, 168) == rb.status_not_implemented  # bf16
     assert L.rocblas_trsm_ex(None, *args, rb.datatype_f64_c) == rb.status_invalid_handle
     bad = list(args)
     bad[4] = -1
-    assert L.rocblas_trsm_ex(handle.value, *bad, rb.datatype_f64_r) == rb.status_invalid_size
+    # real and complex compute types run the same argument rules
+    for dt in (rb.datatype_f64_r, rb.datatype_f32_r, rb.datatype_f64_c, rb.datatype_f32_c):
+        assert L.rocblas_trsm_ex(handle.value, *bad, dt) == rb.status_invalid_size
 
 
 def test_batched_bad_args(handle):
