@@ -328,6 +328,64 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
     return out
 
 
+def bench_complex(torch, L, h, dev, fp64_peak, m=8192, n=2048, steps=5):
+    """Complex trsm (rocblas_ztrsm / rocblas_ctrsm, L/L/N/N) at m = 8192, n = 2048: A as the
+    drop-in recipe with imaginary parts (off-diagonal (U + iU)/m, diagonal 1 + U(0,1) + iU/2),
+    B ~ U + iU.  TFLOP/s uses the reference's complex flop count, 4 m^2 n
+    (clients/include/flops.hpp:727-737); the complex DMMA update kernel is timed with CUDA events
+    and set against the cuBLAS DGEMM rate measured in the same run (its work counted as 8 real
+    flops per complex multiply-add)."""
+    out = {}
+    g = torch.Generator(device=dev)
+    g.manual_seed(99)
+    for dt, tdt, rdt in (("z", torch.complex128, torch.float64), ("c", torch.complex64, torch.float32)):
+        At = torch.complex(torch.rand(m, m, generator=g, device=dev, dtype=rdt) * 2 - 1,
+                           torch.rand(m, m, generator=g, device=dev, dtype=rdt) * 2 - 1) / m
+        At.diagonal().copy_(torch.complex(1 + torch.rand(m, generator=g, device=dev, dtype=rdt),
+                                          torch.rand(m, generator=g, device=dev, dtype=rdt) - 0.5))
+        At = At.triu().contiguous()  # (col, row) storage: upper in At is A lower
+        B0 = torch.complex(torch.rand(n, m, generator=g, device=dev, dtype=rdt) * 2 - 1,
+                           torch.rand(n, m, generator=g, device=dev, dtype=rdt) * 2 - 1)
+        Bt = torch.empty_like(B0)
+        alpha = torch.tensor([1.0 + 0.0j], dtype=tdt)
+        fn = getattr(L, f"rocblas_{dt}trsm")
+
+        def solve():
+            st = fn(h.value, 141, 122, 111, 131, m, n, ctypes.c_void_p(alpha.data_ptr()),
+                    ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+
+        for _ in range(2):
+            Bt.copy_(B0)
+            solve()
+        torch.cuda.synchronize(dev)
+        L.rocblas_b200_kernel_timing_enable(1)
+        tot = 0.0
+        for _ in range(steps):
+            Bt.copy_(B0)
+            s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            solve()
+            e0.record()
+            e0.synchronize()
+            tot += s0.elapsed_time(e0)
+        g_ms, g_work, g_n = kernel_timing(L, "dmma")
+        L.rocblas_b200_kernel_timing_enable(0)
+        ms = tot / steps
+        gemm_tf = g_work / (g_ms * 1e-3) / 1e12 if g_ms > 0 else None
+        out[dt + "trsm"] = {
+            "value": 4.0 * m * m * n / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms": ms,
+            "m": m, "n": n, "flop_count": "4 m^2 n (complex)",
+            "update_kernel": {"name": "gemm_cdmma_kernel", "achieved_tflops_fp64": gemm_tf,
+                              "frac_of_measured_dgemm": gemm_tf / fp64_peak if gemm_tf else None,
+                              "share_of_solve": g_ms / tot if tot > 0 else None, "launches": g_n},
+        }
+        del At, B0, Bt
+        torch.cuda.empty_cache()
+    out["dgemm_tflops_measured"] = fp64_peak
+    return out
+
+
 def bench_serving(torch, dev, n_requests, rate, seed=7):
     """Config C4: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
     60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
@@ -582,6 +640,7 @@ def run_ours(args):
     if rank == 0 and not args.no_extras:
         hbm = measured_peaks()["hbm_gbs"]
         extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
+        extra["complex"] = bench_complex(torch, L, h, dev, peak)
         extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
 
     if rank == 0:
@@ -609,7 +668,8 @@ def run_ours(args):
 def run_case(args):
     """One kernel on one small shape, a few launches, for ncu captures (no JSON line):
     sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
-    chain: rocblas_dtrsm L/L/N/N m x n (the chain solve)."""
+    zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
+    m x n (the chain solve)."""
     import torch
 
     import rocblas_b200 as rb
@@ -632,6 +692,19 @@ def run_case(args):
             st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
                                  rb.diagonal_non_unit, m, n, po, ctypes.c_void_p(At.data_ptr()), m,
                                  ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+    elif args.case == "zgemm":
+        A = torch.randn(k, m, dtype=torch.complex128, device=dev, generator=g)
+        B = torch.randn(n, k, dtype=torch.complex128, device=dev, generator=g)
+        C = torch.randn(n, m, dtype=torch.complex128, device=dev, generator=g)
+        za = torch.tensor([-1.0 + 0.5j], dtype=torch.complex128)
+        zb = torch.tensor([1.0 + 0.0j], dtype=torch.complex128)
+
+        def run():
+            st = L.rocblas_b200_zgemm(h.value, rb.operation_none, rb.operation_none, m, n, k,
+                                      ctypes.c_void_p(za.data_ptr()), ctypes.c_void_p(A.data_ptr()), m,
+                                      ctypes.c_void_p(B.data_ptr()), k, ctypes.c_void_p(zb.data_ptr()),
+                                      ctypes.c_void_p(C.data_ptr()), m)
             assert st == 0, st
     else:
         A = torch.randn(k, m, dtype=torch.float64, device=dev, generator=g)
@@ -669,7 +742,7 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and serving sections (profiling runs)")
-    ap.add_argument("--case", choices=["sliced", "dmma", "chain"],
+    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     args = ap.parse_args()

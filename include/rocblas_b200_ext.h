@@ -217,6 +217,40 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm(rocblas_handle    handle,
                                                  double*           C,
                                                  rocblas_int       ldc);
 
+/* ---- complex GEMM on the complex DMMA tiles of the complex trsm updates --------------------------
+ * C := alpha op(A) op(B) + beta C for complex double / complex float, computed in FP64 on the
+ * DMMA tensor path (each complex multiply-add as real 2 x 2 blocks; complex float is rounded
+ * once at the end).  op C conjugates.  Same argument meaning as rocblas_{z,c}gemm
+ * (rocblas-functions.h), host pointer mode only; needs no workspace. */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_zgemm(rocblas_handle                handle,
+                                                 rocblas_operation             transA,
+                                                 rocblas_operation             transB,
+                                                 rocblas_int                   m,
+                                                 rocblas_int                   n,
+                                                 rocblas_int                   k,
+                                                 const rocblas_double_complex* alpha,
+                                                 const rocblas_double_complex* A,
+                                                 rocblas_int                   lda,
+                                                 const rocblas_double_complex* B,
+                                                 rocblas_int                   ldb,
+                                                 const rocblas_double_complex* beta,
+                                                 rocblas_double_complex*       C,
+                                                 rocblas_int                   ldc);
+ROCBLAS_EXPORT rocblas_status rocblas_b200_cgemm(rocblas_handle               handle,
+                                                 rocblas_operation            transA,
+                                                 rocblas_operation            transB,
+                                                 rocblas_int                  m,
+                                                 rocblas_int                  n,
+                                                 rocblas_int                  k,
+                                                 const rocblas_float_complex* alpha,
+                                                 const rocblas_float_complex* A,
+                                                 rocblas_int                  lda,
+                                                 const rocblas_float_complex* B,
+                                                 rocblas_int                  ldb,
+                                                 const rocblas_float_complex* beta,
+                                                 rocblas_float_complex*       C,
+                                                 rocblas_int                  ldc);
+
 /* ---- precision form of dtrsm ----------------------------------------------------------------
  * Same contract as rocblas_dtrsm.  The blocked solve keeps the diagonal blocks in FP64
  * (inverted 128 x 128 blocks applied with FP64 tensor-core MMA) and runs every trailing

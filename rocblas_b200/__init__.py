@@ -182,6 +182,8 @@ SIGNATURES = {
     "rocblas_b200_dgemm_sliced": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
+    "rocblas_b200_zgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
+    "rocblas_b200_cgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
     "rocblas_b200_get_device_error": (_i, [_H, ctypes.POINTER(_i)]),
     "rocblas_b200_server_create": (_i, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, _i,
                                         ctypes.c_double, _i]),

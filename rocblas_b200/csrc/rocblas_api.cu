@@ -1161,9 +1161,12 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
 }
 
 // C := alpha op(A) op(B) + beta C on the FP64 DMMA tiles (host pointer mode).
-rocblas_status gemm_dmma_impl(rocblas_handle h, rocblas_operation ta, rocblas_operation tb, int m,
-                              int n, int k, const double* alpha, const double* A, int lda,
-                              const double* B, int ldb, const double* beta, double* C, int ldc)
+// C := alpha op(A) op(B) + beta C on the tiles of the trsm updates (FP64: DMMA; complex: the
+// complex DMMA tiles, trans C conjugating), with rocblas_?gemm's argument meaning.
+template <typename T>
+rocblas_status gemm_tiles_impl(rocblas_handle h, rocblas_operation ta, rocblas_operation tb, int m,
+                               int n, int k, const T* alpha, const T* A, int lda, const T* B,
+                               int ldb, const T* beta, T* C, int ldc)
 {
     if(!h)
         return rocblas_status_invalid_handle;
@@ -1187,22 +1190,24 @@ rocblas_status gemm_dmma_impl(rocblas_handle h, rocblas_operation ta, rocblas_op
     rocblas_status st;
     if((st = device_ready(h)) != rocblas_status_success)
         return st;
-    GemmParams<double> g{};
+    GemmParams<T> g{};
     g.M = m;
     g.N = n;
     g.K = k;
-    g.P = strided<double>(A, 0);
+    g.P = strided<T>(A, 0);
     g.ldp = lda;
     g.transP = nA ? 0 : 1;
-    g.Q = strided<double>(B, 0);
+    g.conjP  = ta == rocblas_operation_conjugate_transpose;
+    g.Q = strided<T>(B, 0);
     g.ldq = ldb;
     g.transQ = nB ? 0 : 1;
-    g.C = strided<double>(C, 0);
+    g.conjQ  = tb == rocblas_operation_conjugate_transpose;
+    g.C = strided<T>(C, 0);
     g.ldc = ldc;
     g.a_imm = *alpha;
     g.b_imm = *beta;
     g.zero_guard = 0;
-    launch_gemm<double>(g, 1, h->stream, h->sm_count);
+    launch_gemm<T>(g, 1, h->stream, h->sm_count);
     return launch_status();
 }
 
@@ -2018,12 +2023,29 @@ rocblas_status rocblas_b200_dgemm(rocblas_handle h, rocblas_operation transA,
                                   const double* beta, double* C, rocblas_int ldc)
 try
 {
-    return gemm_dmma_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    return gemm_tiles_impl<double>(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 catch(...)
 {
     return exception_status();
 }
+
+#define GEMM_CPLX(NAME, TA, T)                                                                    \
+    rocblas_status NAME(rocblas_handle h, rocblas_operation transA, rocblas_operation transB,     \
+                        rocblas_int m, rocblas_int n, rocblas_int k, const TA* alpha, const TA* A, \
+                        rocblas_int lda, const TA* B, rocblas_int ldb, const TA* beta, TA* C,     \
+                        rocblas_int ldc)                                                          \
+    try                                                                                           \
+    {                                                                                             \
+        return gemm_tiles_impl<T>(h, transA, transB, m, n, k, as_impl<T>(alpha), as_impl<T>(A),   \
+                                  lda, as_impl<T>(B), ldb, as_impl<T>(beta), as_impl<T>(C), ldc); \
+    }                                                                                             \
+    catch(...)                                                                                    \
+    {                                                                                             \
+        return exception_status();                                                                \
+    }
+GEMM_CPLX(rocblas_b200_zgemm, rocblas_double_complex, cplx<double>)
+GEMM_CPLX(rocblas_b200_cgemm, rocblas_float_complex, cplx<float>)
 
 rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                                         rocblas_operation transA, rocblas_diagonal diag,

@@ -170,3 +170,32 @@ def test_complex_trmm(handle, dt, side, uplo, trans, diag):
         dm.trmm(handle, side, uplo, trans, diag, m, n, alpha, dA, k, dB, m, dB, m)
         torch.cuda.synchronize()
         assert oracle.matrix_norm_1(ref, dm.to_host(dB)) <= 4 * eps * k
+
+
+@pytest.mark.parametrize("dt", ["z", "c"])
+def test_complex_gemm_entry(handle, dt):
+    """rocblas_b200_{z,c}gemm: C := alpha op(A) op(B) + beta C for every op pair (C conjugates),
+    against numpy in complex128."""
+    npdt, tdt = DT[dt]
+    rng = np.random.default_rng(3)
+    m, n, k = 150, 97, 133
+    eps = np.finfo(npdt).eps
+    alpha, beta = 0.75 - 0.5j, -1.25 + 0.25j
+    opf = {"N": lambda X: X, "T": lambda X: X.T, "C": lambda X: X.conj().T}
+    for ta, tb in itertools.product("NTC", repeat=2):
+        Ash = (m, k) if ta == "N" else (k, m)
+        Bsh = (k, n) if tb == "N" else (n, k)
+        A = (rng.uniform(-1, 1, Ash) + 1j * rng.uniform(-1, 1, Ash)).astype(npdt, order="F")
+        B = (rng.uniform(-1, 1, Bsh) + 1j * rng.uniform(-1, 1, Bsh)).astype(npdt, order="F")
+        C = (rng.uniform(-1, 1, (m, n)) + 1j * rng.uniform(-1, 1, (m, n))).astype(npdt, order="F")
+        ref = alpha * opf[ta](A.astype(np.complex128)) @ opf[tb](B.astype(np.complex128)) + beta * C
+        dA, dB, dC = dm.to_device(A), dm.to_device(B), dm.to_device(C)
+        a = torch.tensor([alpha], dtype=tdt)
+        b = torch.tensor([beta], dtype=tdt)
+        st = getattr(rb.lib(), f"rocblas_b200_{dt}gemm")(
+            handle.value, rb.TRANS[ta], rb.TRANS[tb], m, n, k, _ptr(a), _ptr(dA), Ash[0], _ptr(dB), Bsh[0],
+            _ptr(b), _ptr(dC), m)
+        assert st == 0
+        torch.cuda.synchronize()
+        got = dm.to_host(dC)
+        assert np.max(np.abs(got - ref)) <= 8 * eps * k * 4, (ta, tb)
