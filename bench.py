@@ -36,10 +36,17 @@ sys.path.insert(0, ROOT)
 M, N = 16384, 4096
 FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the sliced GEMM
-# kernel from one ncu capture; None until a capture of the bench's own launches exists
-SLICED_TRAFFIC_PER_LAUNCH = None
-SLICED_TRAFFIC_SOURCE = None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch, from one ncu capture
+# of this command's own launches at the default size (profiles/launch_list_dtrsm_16384x4096.md):
+# the sliced GEMM averaged over the 7 launches of a precision-form solve, and the chain kernel
+# of the plain solve (one launch per solve)
+SLICED_TRAFFIC_PER_LAUNCH = 1.0795e9
+SLICED_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum of "
+                         "`bench.py --no-extras --steps 2 --warmup 3`: 77 launches, mean per launch "
+                         "(0.248 / 1.035 / 4.496 GB for the 4 / 2 / 1 launches of each solve)")
+CHAIN_TRAFFIC_PER_LAUNCH = 35.57e9
+CHAIN_TRAFFIC_SOURCE = ("same capture: the 8 plain-solve launches of trsm_chain_kernel (45.5 ms each); "
+                        "A (1.07 GB) is streamed once per 64-column strip group")
 
 
 def workload_name():
@@ -619,6 +626,7 @@ def run_ours(args):
                           "achieved": c_fl / (c_ms * 1e-3) / 1e12 if c_ms > 0 else 0.0, "peak": peak,
                           "unit": "TFLOP/s", "launches": c_n,
                           "frac": (c_fl / (c_ms * 1e-3) / 1e12) / peak if c_ms > 0 else 0.0,
+                          "traffic": CHAIN_TRAFFIC_PER_LAUNCH, "traffic_source": CHAIN_TRAFFIC_SOURCE,
                           "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
                                          "MEASURED_PEAKS.json has no FP64 figure"}
         extra = {
