@@ -220,11 +220,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
-    """Config C3: `count` uneven systems (m log-uniform [16, 512], n uniform [1, 64], side and
-    uplo uniform, transA N, diag N) through rocblas_b200_?trsm_vbatched, FP64 and FP32; plus
-    the uniform strided batch (4096 x m=128, n=32) through rocblas_?trsm_strided_batched.
-    Solves/s and algorithmic GB/s against the HBM roofline."""
+def vbatched_workload(torch, dev, count, seed, dt):
+    """Config C3's systems: m log-uniform [16, 512], n uniform [1, 64], side and uplo uniform,
+    transA N, diag N, A and B by the drop-in recipe, all in two device arrays; returns the
+    device descriptor array (rocblas_b200_trsm_problem records) and the arrays behind it."""
+    tdt, es = (torch.float64, 8) if dt == "d" else (torch.float32, 4)
     rng = np.random.default_rng(seed)
     ms = np.exp(rng.uniform(np.log(16), np.log(512), size=count)).astype(np.int64)
     ns = rng.integers(1, 65, size=count)
@@ -232,42 +232,52 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
     uplos = rng.choice([121, 122], size=count)
     ks = np.where(sides == 141, ms, ns)
     order = np.argsort(ks, kind="stable")  # group equal k so that A is generated per k
+    a_off = np.zeros(count, dtype=np.int64)
+    b_off = np.zeros(count, dtype=np.int64)
+    a_tot = b_tot = 0
+    for i in order:
+        a_off[i] = a_tot
+        a_tot += int(ks[i]) ** 2
+    for i in range(count):
+        b_off[i] = b_tot
+        b_tot += int(ms[i] * ns[i])
+    Aar = torch.empty(a_tot, dtype=tdt, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    # per distinct k: off-diagonal U(-1,1)/k, diagonal 1 + U(0,1) (the drop-in recipe)
+    uk, first = np.unique(ks[order], return_index=True)
+    for j, k in enumerate(uk):
+        lo = first[j]
+        hi = first[j + 1] if j + 1 < len(uk) else count
+        cnt = hi - lo
+        base = int(a_off[order[lo]])
+        blk = (torch.rand(cnt, int(k), int(k), generator=g, device=dev, dtype=torch.float64) * 2 - 1) / k
+        idx = torch.arange(int(k), device=dev)
+        blk[:, idx, idx] = 1.0 + torch.rand(cnt, int(k), generator=g, device=dev, dtype=torch.float64)
+        Aar[base: base + cnt * int(k) * int(k)] = blk.reshape(-1).to(tdt)
+    B0 = (torch.rand(b_tot, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
+    Bar = B0.clone()
+    rec = np.zeros(count, dtype=np.dtype([
+        ("A", np.uint64), ("B", np.uint64), ("m", np.int32), ("n", np.int32), ("lda", np.int32),
+        ("ldb", np.int32), ("side", np.int32), ("uplo", np.int32), ("trans", np.int32),
+        ("diag", np.int32)]))
+    rec["A"] = Aar.data_ptr() + a_off * es
+    rec["B"] = Bar.data_ptr() + b_off * es
+    rec["m"], rec["n"], rec["lda"], rec["ldb"] = ms, ns, ks, ms
+    rec["side"], rec["uplo"], rec["trans"], rec["diag"] = sides, uplos, 111, 131
+    desc = torch.from_numpy(rec.view(np.uint8).copy()).to(dev)
+    return {"desc": desc, "A": Aar, "B": Bar, "B0": B0, "m": ms, "n": ns, "k": ks, "es": es, "g": g}
+
+
+def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
+    """Config C3: `count` uneven systems (m log-uniform [16, 512], n uniform [1, 64], side and
+    uplo uniform, transA N, diag N) through rocblas_b200_?trsm_vbatched, FP64 and FP32; plus
+    the uniform strided batch (4096 x m=128, n=32) through rocblas_?trsm_strided_batched.
+    Solves/s and algorithmic GB/s against the HBM roofline."""
     out = {}
-    for dt, tdt, es in (("d", torch.float64, 8), ("s", torch.float32, 4)):
-        a_off = np.zeros(count, dtype=np.int64)
-        b_off = np.zeros(count, dtype=np.int64)
-        a_tot = b_tot = 0
-        for i in order:
-            a_off[i] = a_tot
-            a_tot += int(ks[i]) ** 2
-        for i in range(count):
-            b_off[i] = b_tot
-            b_tot += int(ms[i] * ns[i])
-        Aar = torch.empty(a_tot, dtype=tdt, device=dev)
-        g = torch.Generator(device=dev)
-        g.manual_seed(seed)
-        # per distinct k: off-diagonal U(-1,1)/k, diagonal 1 + U(0,1) (the drop-in recipe)
-        uk, first = np.unique(ks[order], return_index=True)
-        for j, k in enumerate(uk):
-            lo = first[j]
-            hi = first[j + 1] if j + 1 < len(uk) else count
-            cnt = hi - lo
-            base = int(a_off[order[lo]])
-            blk = (torch.rand(cnt, int(k), int(k), generator=g, device=dev, dtype=torch.float64) * 2 - 1) / k
-            idx = torch.arange(int(k), device=dev)
-            blk[:, idx, idx] = 1.0 + torch.rand(cnt, int(k), generator=g, device=dev, dtype=torch.float64)
-            Aar[base: base + cnt * int(k) * int(k)] = blk.reshape(-1).to(tdt)
-        B0 = (torch.rand(b_tot, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
-        Bar = B0.clone()
-        rec = np.zeros(count, dtype=np.dtype([
-            ("A", np.uint64), ("B", np.uint64), ("m", np.int32), ("n", np.int32), ("lda", np.int32),
-            ("ldb", np.int32), ("side", np.int32), ("uplo", np.int32), ("trans", np.int32),
-            ("diag", np.int32)]))
-        rec["A"] = Aar.data_ptr() + a_off * es
-        rec["B"] = Bar.data_ptr() + b_off * es
-        rec["m"], rec["n"], rec["lda"], rec["ldb"] = ms, ns, ks, ms
-        rec["side"], rec["uplo"], rec["trans"], rec["diag"] = sides, uplos, 111, 131
-        desc = torch.from_numpy(rec.view(np.uint8).copy()).to(dev)
+    for dt, tdt in (("d", torch.float64), ("s", torch.float32)):
+        w = vbatched_workload(torch, dev, count, seed, dt)
+        desc, Aar, Bar, B0, ms, ns, ks, es, g = (w[k] for k in ("desc", "A", "B", "B0", "m", "n", "k", "es", "g"))
         alpha = ctypes.c_double(1.0) if dt == "d" else ctypes.c_float(1.0)
         ap = ctypes.cast(ctypes.byref(alpha), ctypes.c_void_p)
         fn = L.rocblas_b200_dtrsm_vbatched if dt == "d" else L.rocblas_b200_strsm_vbatched
@@ -295,7 +305,7 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
         out[f"vbatched_{dt}"] = {"systems": count, "solves_per_s": count / t, "ms": t * 1e3,
                                  "tflops": flops / t / 1e12, "algorithmic_GBps": nbytes / t / 1e9,
                                  "hbm_frac": nbytes / t / 1e9 / hbm_gbs}
-        del Aar, Bar, B0, desc
+        del Aar, Bar, B0, desc, w
         # uniform strided batch: 4096 x (m=128, n=32), side L lower
         bc, m, n = 4096, 128, 32
         As = torch.rand(bc, m, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1
@@ -677,7 +687,8 @@ def run_case(args):
     """One kernel on one small shape, a few launches, for ncu captures (no JSON line):
     sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
-    m x n (the chain solve)."""
+    m x n (the chain solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
+    C3 recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N)."""
     import torch
 
     import rocblas_b200 as rb
@@ -700,6 +711,26 @@ def run_case(args):
             st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
                                  rb.diagonal_non_unit, m, n, po, ctypes.c_void_p(At.data_ptr()), m,
                                  ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+    elif args.case == "vbatched":
+        w = vbatched_workload(torch, dev, args.count, 2024, "d")
+        one_d = ctypes.c_double(1.0)
+
+        def run():
+            st = L.rocblas_b200_dtrsm_vbatched(h.value, ctypes.cast(ctypes.byref(one_d), ctypes.c_void_p),
+                                               ctypes.c_void_p(w["desc"].data_ptr()), args.count, 512, None)
+            assert st == 0, st
+    elif args.case == "strided":
+        bc = args.count
+        As = torch.rand(bc, m, m, generator=g, device=dev, dtype=torch.float64) / m
+        idx = torch.arange(m, device=dev)
+        As[:, idx, idx] = 1.0 + torch.rand(bc, m, generator=g, device=dev, dtype=torch.float64)
+        Bs = torch.rand(bc, n, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+
+        def run():
+            st = L.rocblas_dtrsm_strided_batched(h.value, 141, 122, 111, 131, m, n, po,
+                                                 ctypes.c_void_p(As.data_ptr()), m, m * m,
+                                                 ctypes.c_void_p(Bs.data_ptr()), m, m * n, bc)
             assert st == 0, st
     elif args.case == "zgemm":
         A = torch.randn(k, m, dtype=torch.complex128, device=dev, generator=g)
@@ -750,9 +781,11 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and serving sections (profiling runs)")
-    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain"],
+    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "vbatched", "strided"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
+    ap.add_argument("--count", type=int, default=4000,
+                    help="systems of a --case vbatched (C3 recipe) or strided (m x n each) run")
     args = ap.parse_args()
     if args.case:
         run_case(args)

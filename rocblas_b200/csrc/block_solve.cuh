@@ -22,7 +22,10 @@
 //      memory in 64-row chunks.
 // k is at most kBlockSolveMaxK; larger systems use the blocked recursive path.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
+#include "mma_f64.cuh"
 
 namespace rb200
 {
@@ -36,7 +39,7 @@ constexpr int kBlockSolveMaxK = 512;
 // The largest order one CTA solves: the k x 32 strip of C lives in shared memory, so complex
 // double (16-byte elements) stops at 256 to stay within 227 KB.
 template <typename T>
-constexpr int block_solve_max_k()
+__host__ __device__ constexpr int block_solve_max_k()
 {
     return sizeof(T) > 8 ? 256 : kBlockSolveMaxK;
 }
@@ -60,11 +63,61 @@ struct BlockSolveParams
     int         batch_base;
 };
 
+// Row pitches (elements) of the strip C and of the streamed panel chunk in shared memory.  FP64
+// runs the update on DMMA, whose fragment reads (lanes (g, t) reading element (g, t) of the
+// chunk and (t, g) of the solved rows) fall on distinct bank pairs of each half-warp with a
+// pitch of 36; FP32 reads the chunk as float4, which a pitch of 36 keeps 16-byte aligned.
+// Other types keep 33, which makes the column reads of the substitution conflict-free.
 template <typename T>
-constexpr size_t block_solve_smem_bytes(int k)
+__host__ __device__ constexpr int bs_cpitch()
+{
+    return std::is_same<T, double>::value ? 36 : kBsPitch;
+}
+template <typename T>
+__host__ __device__ constexpr int bs_ppitch()
+{
+    return std::is_same<T, double>::value || std::is_same<T, float>::value ? 36 : kBsPitch;
+}
+
+template <typename T>
+__host__ __device__ constexpr size_t block_solve_smem_bytes(int k)
 {
     const int kpad = (int)ceil_div(k, 32) * 32;
-    return sizeof(T) * (size_t)(kpad * kBsPitch + 32 * 33 + 32 + kBsChunk * 33);
+    return sizeof(T) * (size_t)(kpad * bs_cpitch<T>() + 32 * 33 + 32 + kBsChunk * bs_ppitch<T>());
+}
+
+// FP64 update of one chunk on the tensor path: C[0:rows, 0:32] -= P[0:64, 0:32] X[0:32, 0:32]
+// (P: the chunk of M, pitch 36; X: the solved panel rows and C: the rows below, pitch 36; rows
+// >= `rows` do not exist and are not written).  Warp w owns rows 16 (w % 4) .. + 16 and columns
+// 16 (w / 4) .. + 16: two mma.sync m16n8k8 tiles per 8-deep k step, 8 MMAs per warp.
+__device__ __forceinline__ void bs_update_dmma(const double* Ps, const double* Xs, double* Cc,
+                                               int rows, int warp, int lane)
+{
+    constexpr int P = 36;
+    const int     wr = (warp & 3) * 16, wc = (warp >> 2) * 16;
+    const int     g = lane >> 2, t = lane & 3;
+    double        acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+#pragma unroll
+    for(int ks = 0; ks < 32; ks += 8)
+    {
+        const double a[4] = {Ps[(wr + g) * P + ks + t], Ps[(wr + g + 8) * P + ks + t],
+                             Ps[(wr + g) * P + ks + t + 4], Ps[(wr + g + 8) * P + ks + t + 4]};
+#pragma unroll
+        for(int j = 0; j < 2; ++j)
+        {
+            const double b[2] = {Xs[(ks + t) * P + wc + 8 * j + g], Xs[(ks + t + 4) * P + wc + 8 * j + g]};
+            dmma_16x8x8(acc[j], a, b);
+        }
+    }
+#pragma unroll
+    for(int j = 0; j < 2; ++j)
+#pragma unroll
+        for(int e = 0; e < 4; ++e)
+        {
+            const int r = wr + g + (e >> 1) * 8, c = wc + 8 * j + 2 * t + (e & 1);
+            if(r < rows)
+                Cc[r * P + c] -= acc[j][e];
+        }
 }
 
 // The core: solve M Y = alpha C for one strip.  The caller resolves pointers / sizes.
@@ -73,9 +126,11 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
                                   int side_left, int tM, int rev, int unit, int conj, T alpha,
                                   int s0, int ncols, unsigned char* smem_raw)
 {
+    constexpr int PC = bs_cpitch<T>(), PP = bs_ppitch<T>();
+    constexpr int NW = kBsThreads / 32; // warps
     T* Cs    = reinterpret_cast<T*>(smem_raw);
     const int kpad = ((k + 31) / 32) * 32;
-    T* Ds    = Cs + kpad * kBsPitch;
+    T* Ds    = Cs + kpad * PC;
     T* rdiag = Ds + 32 * 33;
     T* Ps    = rdiag + 32;
 
@@ -94,31 +149,44 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
         return conj_if(A[r + (int64_t)c * lda], conj);
     };
 
+    // B is walked with lanes along its contiguous direction: rows of C for side L, columns of C
+    // (rows of B) for side R
     if(alpha == T(0))
     {
         // B := 0 without reading A or B (rocblas_trsm_imp.hpp:154-157 semantics)
-        for(int idx = tid; idx < k * kBsW; idx += kBsThreads)
+        if(side_left)
         {
-            int r, col;
-            if(side_left) { r = idx % k; col = idx / k; }
-            else          { col = idx % kBsW; r = idx / kBsW; }
-            if(col < W)
-                *baddr(r, col) = T(0);
+            for(int col = warp; col < W; col += NW)
+                for(int r = lane; r < k; r += 32)
+                    *baddr(r, col) = T(0);
+        }
+        else
+        {
+            for(int r = warp; r < k; r += NW)
+                if(lane < W)
+                    *baddr(r, lane) = T(0);
         }
         return;
     }
 
     // ---- load alpha * C' (rows reversed when rev), zero-pad rows k..kpad-1 ----------------
-    for(int idx = tid; idx < kpad * kBsW; idx += kBsThreads)
-    {
-        int r, col;
-        if(side_left) { r = idx % kpad; col = idx / kpad; }
-        else          { col = idx % kBsW; r = idx / kBsW; }
+    auto load_c = [&](int r, int col) {
         T v = T(0);
         if(r < k && col < W)
             v = alpha * (*baddr(r, col));
         const int i = (r < k && rev) ? k - 1 - r : r;
-        Cs[i * kBsPitch + col] = v;
+        Cs[i * PC + col] = v;
+    };
+    if(side_left)
+    {
+        for(int col = warp; col < kBsW; col += NW)
+            for(int r = lane; r < kpad; r += 32)
+                load_c(r, col);
+    }
+    else
+    {
+        for(int r = warp; r < kpad; r += NW)
+            load_c(r, lane);
     }
     __syncthreads();
 
@@ -184,7 +252,7 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
             int       r, t;
             if(!tM) { r = idx % kBsChunk; t = idx / kBsChunk; }
             else    { t = idx % 32; r = idx / 32; }
-            Ps[r * 33 + t] = pre[u];
+            Ps[r * PP + t] = pre[u];
         }
     };
 
@@ -202,7 +270,7 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
             T y[4];
 #pragma unroll
             for(int q = 0; q < 4; ++q)
-                y[q] = Cs[(p + lane) * kBsPitch + warp + 8 * q];
+                y[q] = Cs[(p + lane) * PC + warp + 8 * q];
             const T dl = rdiag[lane];
 #pragma unroll 4
             for(int t = 0; t < 32; ++t)
@@ -220,11 +288,20 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
             }
 #pragma unroll
             for(int q = 0; q < 4; ++q)
-                Cs[(p + lane) * kBsPitch + warp + 8 * q] = y[q];
+                Cs[(p + lane) * PC + warp + 8 * q] = y[q];
         }
         __syncthreads();
 
         // ---- 3. update rows p+32 .. k-1 (chunks prefetched one step ahead) ----------------
+        // FP32 keeps this thread's column of the solved panel in registers for all chunks
+        float xr[std::is_same<T, float>::value ? 32 : 1];
+        if constexpr(std::is_same<T, float>::value)
+        {
+            if(p + 32 < k)
+#pragma unroll
+                for(int t = 0; t < 32; ++t)
+                    xr[t] = Cs[(p + t) * PC + lane];
+        }
         for(int i0 = p + 32; i0 < k; i0 += kBsChunk)
         {
             store_chunk();
@@ -233,33 +310,61 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
                 fetch_chunk(p, i0 + kBsChunk);
             else
                 fetch_diag(p + 32); // p + 32 < k here
-            const int col = lane;
-#pragma unroll
-            for(int q = 0; q < kBsChunk / 8; ++q)
+            if constexpr(std::is_same<T, double>::value)
             {
-                const int r = warp + 8 * q;
-                T         acc = T(0);
+                bs_update_dmma(Ps, Cs + (size_t)p * PC, Cs + (size_t)i0 * PC, kpad - i0, warp, lane);
+            }
+            else if constexpr(std::is_same<T, float>::value)
+            {
+#pragma unroll
+                for(int q = 0; q < kBsChunk / NW; ++q)
+                {
+                    const int r   = warp + NW * q;
+                    float     acc = 0.0f;
+#pragma unroll
+                    for(int t = 0; t < 32; t += 4)
+                    {
+                        const float4 m4 = *reinterpret_cast<const float4*>(&Ps[r * PP + t]);
+                        acc += m4.x * xr[t] + m4.y * xr[t + 1] + m4.z * xr[t + 2] + m4.w * xr[t + 3];
+                    }
+                    if(i0 + r < kpad)
+                        Cs[(i0 + r) * PC + lane] -= acc;
+                }
+            }
+            else
+            {
+                const int col = lane;
+#pragma unroll
+                for(int q = 0; q < kBsChunk / NW; ++q)
+                {
+                    const int r = warp + NW * q;
+                    T         acc = T(0);
 #pragma unroll 8
-                for(int t = 0; t < 32; ++t)
-                    acc += Ps[r * 33 + t] * Cs[(p + t) * kBsPitch + col];
-                if(i0 + r < kpad)
-                    Cs[(i0 + r) * kBsPitch + col] -= acc;
+                    for(int t = 0; t < 32; ++t)
+                        acc += Ps[r * PP + t] * Cs[(p + t) * PC + col];
+                    if(i0 + r < kpad)
+                        Cs[(i0 + r) * PC + col] -= acc;
+                }
             }
             __syncthreads();
         }
     }
 
     // ---- store Y (undo the row reversal) ---------------------------------------------------
-    for(int idx = tid; idx < k * kBsW; idx += kBsThreads)
-    {
-        int r, col;
-        if(side_left) { r = idx % k; col = idx / k; }
-        else          { col = idx % kBsW; r = idx / kBsW; }
+    auto store_y = [&](int r, int col) {
         if(col < W)
-        {
-            const int i = rev ? k - 1 - r : r;
-            *baddr(r, col) = Cs[i * kBsPitch + col];
-        }
+            *baddr(r, col) = Cs[(rev ? k - 1 - r : r) * PC + col];
+    };
+    if(side_left)
+    {
+        for(int col = warp; col < W; col += NW)
+            for(int r = lane; r < k; r += 32)
+                store_y(r, col);
+    }
+    else
+    {
+        for(int r = warp; r < k; r += NW)
+            store_y(r, lane);
     }
 }
 
