@@ -139,15 +139,15 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
     const int W    = min(kBsW, ncols - s0); // valid columns of this strip
 
     // C(r, col) address in B: side L -> B[r + (s0+col) ldb]; side R -> B[(s0+col) + r ldb]
-    auto baddr = [&](int r, int col) -> T* {
-        return side_left ? B + r + (int64_t)(s0 + col) * ldb : B + (s0 + col) + (int64_t)r * ldb;
-    };
-    // M'(i, j) (reversed, lower orientation) -> A element
-    auto mval = [&](int i, int j) -> T {
-        const int a = rev ? k - 1 - i : i, b = rev ? k - 1 - j : j;
-        const int r = tM ? b : a, c = tM ? a : b;
-        return conj_if(A[r + (int64_t)c * lda], conj);
-    };
+    T* const      B0  = B + (side_left ? (int64_t)s0 * ldb : (int64_t)s0);
+    const int64_t bdr = side_left ? 1 : ldb, bdc = side_left ? ldb : 1;
+    auto baddr = [&](int r, int col) -> T* { return B0 + r * bdr + col * bdc; };
+    // M'(i, j), the reversed lower orientation of M (= A or A^T): with a = i, b = j (or k-1-i,
+    // k-1-j when rev) it is A[a + b lda] (or A[b + a lda] when tM), i.e. M0[i dI + j dJ]
+    const int64_t sgn = rev ? -1 : 1;
+    const int64_t dI = (tM ? lda : 1) * sgn, dJ = (tM ? 1 : lda) * sgn;
+    const T* const M0 = A + (rev ? (int64_t)(k - 1) * (1 + lda) : 0);
+    auto mval = [&](int i, int j) -> T { return conj_if(M0[i * dI + j * dJ], conj); };
 
     // B is walked with lanes along its contiguous direction: rows of C for side L, columns of C
     // (rows of B) for side R
@@ -265,7 +265,33 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
         if(p + 32 < k)
             fetch_chunk(p, p + 32);
 
-        // ---- 2. substitution with shuffle broadcast -----------------------------------------
+        // ---- 2. substitution of the 32 x 32 diagonal tile ------------------------------------
+        // One warp, one column per lane held in registers: y_j *= 1/M_jj, then
+        // y_i -= M_ij y_j for i > j (the reference's column order); M_ij is a shared-memory
+        // broadcast.  Complex types (64 / 128 registers for the column) broadcast solved rows by
+        // shuffle across all warps instead: warp w owns columns w, w+8, w+16, w+24, lane = row.
+        if constexpr(!is_cplx<T>::value)
+        {
+            if(warp == 0)
+            {
+                T y[32];
+#pragma unroll
+                for(int i = 0; i < 32; ++i)
+                    y[i] = Cs[(p + i) * PC + lane];
+#pragma unroll
+                for(int j = 0; j < 32; ++j)
+                {
+                    y[j] *= rdiag[j];
+#pragma unroll
+                    for(int i = j + 1; i < 32; ++i)
+                        y[i] -= Ds[i * 33 + j] * y[j];
+                }
+#pragma unroll
+                for(int i = 0; i < 32; ++i)
+                    Cs[(p + i) * PC + lane] = y[i];
+            }
+        }
+        else
         {
             T y[4];
 #pragma unroll
@@ -369,7 +395,7 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBsThreads) block_solve_kernel(BlockSolveParams<T> p)
+__global__ void __launch_bounds__(kBsThreads, 2) block_solve_kernel(BlockSolveParams<T> p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int batch = p.batch_base + blockIdx.y;

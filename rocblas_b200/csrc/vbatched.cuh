@@ -210,7 +210,7 @@ struct VbParams
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kBsThreads) vb_persistent_kernel(VbParams<T> p)
+__global__ void __launch_bounds__(kBsThreads, 2) vb_persistent_kernel(VbParams<T> p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item;
