@@ -955,8 +955,11 @@ rocblas_status trsm_vbatched_ex_impl(rocblas_handle h, const T* alpha,
             p.first   = 1;
             p.counter = reinterpret_cast<int*>(w.counters + c);
             p.error   = h->err_dev ? h->err_dev : w.invalid + 1;
-            const bool kcp = (c >> 1) != 0, kcq = (c & 1) != 0;
-            launch_chain_w<T, kChainVbW, true>(p, kcp, kcq, h->sm_count, INT64_MAX, h->stream);
+            const bool kcp = ((c >> 1) & 1) != 0, kcq = (c & 1) != 0;
+            if(chain_vb_width(c) == kChainVbWideW)
+                launch_chain_w<T, kChainVbWideW, true>(p, kcp, kcq, h->sm_count, INT64_MAX, h->stream);
+            else
+                launch_chain_w<T, kChainVbW, true>(p, kcp, kcq, h->sm_count, INT64_MAX, h->stream);
             count_launch();
         }
     }

@@ -135,6 +135,56 @@ struct ServerStatsC // layout of rocblas_b200_server_stats
     int64_t kernel_launches;
 };
 
+// One collection's arriving data in one launch (instead of a copy call per request): for each
+// request its B (m x n, contiguous from B_src) and, for a fresh A, the lower triangle of A
+// (m x m from A_src with leading dimension lda_src; the solve and the inversion read nothing
+// else) into the request's arena blocks.  Work items are blocks of kGatherCols columns, B's
+// first and then A's; item ranges per request come from the exclusive prefix array.
+constexpr int kGatherCols = 32;
+
+struct GatherReq
+{
+    const void* srcB;
+    void*       dstB;
+    const void* srcA; // nullptr: no A to copy
+    void*       dstA;
+    int64_t     lda_src;
+    int         m, n;
+    int         itemsB, pad;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) server_gather_kernel(const GatherReq* reqs, const int* prefix,
+                                                            int cnt)
+{
+    const int bid = blockIdx.x;
+    // the request of this item: the last r with prefix[r] <= bid
+    int lo = 0, hi = cnt - 1;
+    while(lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if(prefix[mid] <= bid)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const GatherReq q    = reqs[lo];
+    const int       item = bid - prefix[lo];
+    const bool      isB  = item < q.itemsB;
+    const int       c0   = (isB ? item : item - q.itemsB) * kGatherCols;
+    const int       c1   = min(isB ? q.n : q.m, c0 + kGatherCols);
+    const T*        src  = reinterpret_cast<const T*>(isB ? q.srcB : q.srcA);
+    T*              dst  = reinterpret_cast<T*>(isB ? q.dstB : q.dstA);
+    const int64_t   lds  = isB ? q.m : q.lda_src;
+    for(int c = c0; c < c1; ++c)
+    {
+        const T* s = src + (int64_t)c * lds;
+        T*       d = dst + (int64_t)c * q.m;
+        for(int r = (isB ? 0 : c) + (int)threadIdx.x; r < q.m; r += blockDim.x)
+            d[r] = s[r];
+    }
+}
+
 // The collection solve: rocblas_b200_?trsm_vbatched_ex on the lane's handle with alpha 1
 // (dtype kF64 or kF32; invs is a device array of per-system invA pointers).
 typedef rocblas_status (*ServerSolveFn)(_rocblas_handle* h, int dtype,
@@ -145,10 +195,19 @@ class TrsmServerCore
 {
 public:
     static constexpr int kF32 = 151, kF64 = 152;
-    // staging per request: its descriptor and invA pointer, and for a fresh A the batched
-    // trtri's A pointer, invA pointer, order and leading dimension
-    static constexpr size_t kStagePerRequest
-        = sizeof(VbProblem) + sizeof(void*) + 2 * sizeof(void*) + sizeof(int64_t) + sizeof(int);
+    // staging per request: its descriptor and invA pointer, for a fresh A the batched trtri's A
+    // pointer, invA pointer, order and leading dimension, then (8-byte aligned) its gather
+    // record and its item offset
+    static constexpr size_t kStagePerRequest = sizeof(VbProblem) + sizeof(void*) + 2 * sizeof(void*)
+                                               + sizeof(int64_t) + sizeof(int) + sizeof(GatherReq)
+                                               + sizeof(int);
+    static constexpr size_t kStageSlack = 64; // alignment of the gather records, prefix[cnt]
+    static size_t gather_offset(int cnt)
+    {
+        const size_t o = (size_t)cnt * (sizeof(VbProblem) + 3 * sizeof(void*) + sizeof(int64_t)
+                                        + sizeof(int));
+        return (o + 15) & ~size_t(15);
+    }
 
     explicit TrsmServerCore(ServerSolveFn solve) : solve_(solve) {}
 
@@ -177,7 +236,7 @@ public:
             if(cudaMalloc(&l.h->err_dev, 256) != cudaSuccess)
                 return rocblas_status_memory_error;
             cudaMemset(l.h->err_dev, 0, 256);
-            const size_t stage = (size_t)max_batch * kStagePerRequest;
+            const size_t stage = (size_t)max_batch * kStagePerRequest + kStageSlack;
             if(cudaMallocHost(&l.host_stage, stage) != cudaSuccess
                || cudaMalloc(&l.dev_stage, stage) != cudaSuccess)
                 return rocblas_status_memory_error;
@@ -474,7 +533,6 @@ private:
     {
         const int    cnt = (int)group.size();
         const int    dt  = reqs[group[0]].dtype;
-        const size_t es  = dt == kF64 ? 8 : 4;
         // host staging: [descriptors][invA pointers][fresh A ptrs][fresh inv ptrs][lda][k]
         char*  hs     = reinterpret_cast<char*>(l.host_stage);
         auto*  probs  = reinterpret_cast<VbProblem*>(hs);
@@ -483,14 +541,28 @@ private:
         auto*  fInv   = reinterpret_cast<void**>(hs + (size_t)cnt * (sizeof(VbProblem) + 2 * sizeof(void*)));
         auto*  fLda   = reinterpret_cast<int64_t*>(fInv + cnt);
         auto*  fK     = reinterpret_cast<int*>(fLda + cnt);
-        int    nfresh = 0, fresh_nb = 0;
+        const size_t o_g    = gather_offset(cnt);
+        auto*        gat    = reinterpret_cast<GatherReq*>(hs + o_g);
+        auto*        prefix = reinterpret_cast<int*>(gat + cnt);
+        int    nfresh = 0, fresh_nb = 0, items = 0;
         int    max_k = 1, max_n = 1;
         for(int j = 0; j < cnt; ++j)
         {
             const ServerRequestC& q = reqs[group[j]];
             Held&                 h = held[group[j]];
-            // the request's data arrives: B, and its own A
-            cudaMemcpyAsync(h.B, q.B_src, h.b_bytes, cudaMemcpyDeviceToDevice, l.stream);
+            // the request's data arrives: B, and its own A (copied by the gather launch)
+            GatherReq& g = gat[j];
+            g.srcB    = q.B_src;
+            g.dstB    = h.B;
+            g.srcA    = nullptr;
+            g.dstA    = nullptr;
+            g.lda_src = q.lda_src;
+            g.m       = q.m;
+            g.n       = q.n;
+            g.itemsB  = (int)ceil_div(q.n, kGatherCols);
+            g.pad     = 0;
+            prefix[j] = items;
+            items += g.itemsB;
             const void* A;
             const void* inv = nullptr;
             if(q.resident >= 0)
@@ -500,8 +572,9 @@ private:
             }
             else
             {
-                cudaMemcpy2DAsync(h.A, q.m * es, q.A_src, (size_t)q.lda_src * es, q.m * es, q.m,
-                                  cudaMemcpyDeviceToDevice, l.stream);
+                g.srcA = q.A_src;
+                g.dstA = h.A;
+                items += (int)ceil_div(q.m, kGatherCols);
                 A = h.A;
                 if(h.inv)
                 {
@@ -530,9 +603,20 @@ private:
             max_k    = std::max(max_k, q.m);
             max_n    = std::max(max_n, q.n);
         }
-        const size_t bytes = (size_t)cnt * kStagePerRequest;
+        prefix[cnt] = items;
+        const size_t bytes = o_g + (size_t)cnt * sizeof(GatherReq) + ((size_t)cnt + 1) * sizeof(int);
         cudaMemcpyAsync(l.dev_stage, l.host_stage, bytes, cudaMemcpyHostToDevice, l.stream);
         const char* ds = reinterpret_cast<const char*>(l.dev_stage);
+        if(items)
+        {
+            auto* dg = reinterpret_cast<const GatherReq*>(ds + o_g);
+            auto* dp = reinterpret_cast<const int*>(dg + cnt);
+            if(dt == kF64)
+                server_gather_kernel<double><<<items, 256, 0, l.stream>>>(dg, dp, cnt);
+            else
+                server_gather_kernel<float><<<items, 256, 0, l.stream>>>(dg, dp, cnt);
+            count_launch();
+        }
         // the fresh A's diagonal blocks, all of them in one variable-size trtri launch
         if(nfresh)
         {

@@ -1,12 +1,14 @@
 // Variable-size batch with systems of any order: the systems with k > 512 go through the
-// chain solve (trsm_chain.cuh) in one persistent launch per (tM, side) combination, using an
+// chain solve (trsm_chain.cuh) in one persistent launch per combination of (tM, side) and strip
+// width (32 columns for systems with at most 32 right-hand sides, else 64), using an
 // inverted-diagonal-block array (invA, the rocblas_trsm_ex format) the caller supplies per
 // system; the systems with k <= 512 take the size classes of the strip solver (vbatched.cuh).
 //
 // A single-CTA prepass builds the chain's tables on the device from the descriptors, so the
 // call needs no host synchronisation and can be captured in a CUDA graph:
 //   1. classify every k > 512 descriptor (valid, invA present, right-hand sides within the
-//      caller's bound) into its combination c = 2 tM + side_left and its block count nb;
+//      caller's bound) into its combination c = 2 tM + side_left + 4 wide (wide: more than 32
+//      right-hand sides, strips of 64) and its block count nb;
 //   2. counting-sort the systems by (c ascending, nb descending) into ChainSys records;
 //   3. per combination: vP = prefix sums of the strips ns over its sorted systems,
 //      vcnt[j] = systems with nb > j (a prefix of the sorted order, since nb descends),
@@ -20,30 +22,37 @@ namespace rb200
 {
 
 constexpr int kChainVbMaxNB   = 256; // chain systems up to k = 32768
-constexpr int kChainVbCombos  = 4;
-constexpr int kChainVbW       = 32;  // strip width of the variable batch
+constexpr int kChainVbCombos  = 8;   // (tM, side) x strip width
+constexpr int kChainVbW       = 32;  // the narrow strip width (the flag bound assumes it)
+constexpr int kChainVbWideW   = 64;  // the strip width of systems with more than 32 columns
 constexpr int kChainVbMinK    = kBlockSolveMaxK; // k above this goes to the chain
+
+__host__ __device__ constexpr int chain_vb_width(int combo)
+{
+    return combo >= 4 ? kChainVbWideW : kChainVbW;
+}
 
 template <typename T>
 struct ChainVbWork
 {
-    ChainVbHeader<T>*   hdr;      // [4]
+    ChainVbHeader<T>*   hdr;      // [kChainVbCombos]
     ChainSys<T>*        sys;      // [count]
-    int*                P;        // [count + 4]: combination c's array starts at start_c + c
+    int*                P;        // [count + kChainVbCombos]: combination c's array starts at start_c + c
     int*                G;        // [count + 1]: global prefix (scratch)
-    int*                cnt;      // [4][kChainVbMaxNB]
-    int64_t*            L;        // [4][kChainVbMaxNB + 1]
+    int*                cnt;      // [kChainVbCombos][kChainVbMaxNB]
+    int64_t*            L;        // [kChainVbCombos][kChainVbMaxNB + 1]
     int*                flags;    // [flag_cap]
     int64_t             flag_cap;
-    unsigned long long* counters; // [4]
+    unsigned long long* counters; // [kChainVbCombos]
     int*                invalid;  // [1]
 };
 
 __device__ __forceinline__ int chain_vb_combo(const VbProblem& p)
 {
-    const int left = p.side == kLeft;
-    const int tM   = (p.trans != kOpN) != (left ? 0 : 1);
-    return 2 * tM + left;
+    const int left  = p.side == kLeft;
+    const int tM    = (p.trans != kOpN) != (left ? 0 : 1);
+    const int ncols = left ? p.n : p.m;
+    return 2 * tM + left + (ncols > kChainVbW ? 4 : 0);
 }
 
 template <typename T>
@@ -128,7 +137,7 @@ __global__ void __launch_bounds__(kVbPrepThreads)
         q.k       = k;
         q.ncols   = left ? p.n : p.m;
         q.nb      = c & 1023;
-        q.ns      = (int)ceil_div(q.ncols, kChainVbW);
+        q.ns      = (int)ceil_div(q.ncols, chain_vb_width(c >> 10));
         const int oplower = (p.uplo == kLower) != (p.trans != kOpN);
         q.forward = left ? oplower : !oplower;
         q.pad     = 0;
