@@ -15,7 +15,10 @@
 // Diagonal semantics follow rocblas_custom_trtri_device (rocblas_trtri.hpp:128-141):
 // diag == unit reads no diagonal and uses 1; a zero non-unit diagonal entry is treated as 1.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
+#include "mma_f64.cuh"
 
 namespace rb200
 {
@@ -41,16 +44,43 @@ struct TrtriParams
 constexpr int kTrtriNB      = 128;
 constexpr int kTrtriSB      = 32;  // tile order
 constexpr int kTrtriNT      = 4;   // tiles per side
-constexpr int kTrtriPitch   = 33;  // tile row pitch in smem
-constexpr int kTrtriTile    = kTrtriSB * kTrtriPitch;
 constexpr int kTrtriNTiles  = kTrtriNT * (kTrtriNT + 1) / 2; // 10 lower tiles
 constexpr int kTrtriThreads = 256;
+
+// Tile row pitch in shared memory: 33 keeps the column reads of the FMA products
+// conflict-free; FP64 runs the products on DMMA, whose fragment reads (lanes (g, t) reading
+// (g, t) of the left tile and (t, g) of the right one) need a pitch of 4 mod 16.
+template <typename T>
+__host__ __device__ constexpr int trtri_pitch()
+{
+    return std::is_same<T, double>::value ? 36 : 33;
+}
+template <typename T>
+__host__ __device__ constexpr int trtri_tile()
+{
+    return kTrtriSB * trtri_pitch<T>();
+}
 
 template <typename T>
 constexpr size_t trtri_smem_bytes()
 {
     // L tiles, X tiles, 3 temporaries, reciprocal diagonal
-    return sizeof(T) * (size_t)(2 * kTrtriNTiles * kTrtriTile + 3 * kTrtriTile + kTrtriNB);
+    return sizeof(T) * (size_t)(2 * kTrtriNTiles * trtri_tile<T>() + 3 * trtri_tile<T>() + kTrtriNB);
+}
+
+// acc (the 16 x 8 block of warp (wr, wc) of a 32 x 32 tile product) += Lt Rt, FP64 DMMA.
+__device__ __forceinline__ void trtri_tile_mma(double (&acc)[4], const double* Lt, const double* Rt,
+                                               int wr, int wc, int g, int t)
+{
+    constexpr int P = 36;
+#pragma unroll
+    for(int ks = 0; ks < kTrtriSB; ks += 8)
+    {
+        const double a[4] = {Lt[(wr + g) * P + ks + t], Lt[(wr + g + 8) * P + ks + t],
+                             Lt[(wr + g) * P + ks + t + 4], Lt[(wr + g + 8) * P + ks + t + 4]};
+        const double b[2] = {Rt[(ks + t) * P + wc + g], Rt[(ks + t + 4) * P + wc + g]};
+        dmma_16x8x8(acc, a, b);
+    }
 }
 
 __device__ __forceinline__ int trtri_tile_index(int bi, int bj)
@@ -61,6 +91,7 @@ __device__ __forceinline__ int trtri_tile_index(int bi, int bj)
 template <typename T>
 __global__ void __launch_bounds__(kTrtriThreads) trtri_block_kernel(TrtriParams<T> p)
 {
+    constexpr int kTrtriPitch = trtri_pitch<T>(), kTrtriTile = trtri_tile<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* Ls    = reinterpret_cast<T*>(smem_raw);
     T* Xs    = Ls + kTrtriNTiles * kTrtriTile;
@@ -81,33 +112,54 @@ __global__ void __launch_bounds__(kTrtriThreads) trtri_block_kernel(TrtriParams<
     T*       out = p.inv.get(batch) + (int64_t)blk * p.inv_block_stride;
 
     // ---- stage the block in lower orientation, identity-padded to 128 ----------------
-    for(int idx = tid; idx < kTrtriNB * kTrtriNB; idx += kTrtriThreads)
+    // The 10 lower 32 x 32 tiles, 40 elements per thread, row index fastest so that a lower
+    // block is read down its columns; loads are issued 8 at a time before their stores.
     {
-        // i fast so that a lower block is read down its columns
-        const int i = idx % kTrtriNB, j = idx / kTrtriNB;
-        if(j > i)
-            continue;
-        T v;
-        if(i < bs && j < bs)
+        constexpr int kPer = kTrtriNTiles * kTrtriSB * kTrtriSB / kTrtriThreads; // 40
+        constexpr int kBatch = 8;
+        static_assert(kPer % kBatch == 0, "staging batches");
+        auto coords = [&](int e, int& tl, int& i, int& j) {
+            tl = e >> 10; // tile in trtri_tile_index order
+            int bi = 0;
+            while(trtri_tile_index(bi + 1, 0) <= tl)
+                ++bi;
+            const int bj = tl - trtri_tile_index(bi, 0);
+            i = bi * kTrtriSB + (e & 31);
+            j = bj * kTrtriSB + ((e >> 5) & 31);
+        };
+#pragma unroll 1
+        for(int u0 = 0; u0 < kPer; u0 += kBatch)
         {
-            const int r = p.upper ? bs - 1 - i : i;
-            const int c = p.upper ? bs - 1 - j : j;
-            if(i == j)
+            T v[kBatch];
+#pragma unroll
+            for(int u = 0; u < kBatch; ++u)
             {
-                v = p.unit ? T(1) : A[r + (int64_t)c * lda];
-                if(v == T(0))
-                    v = T(1);
+                int tl, i, j;
+                coords(tid + (u0 + u) * kTrtriThreads, tl, i, j);
+                v[u] = T(0);
+                if(j <= i && i < bs && j < bs && !(i == j && p.unit))
+                {
+                    const int r = p.upper ? bs - 1 - i : i;
+                    const int c = p.upper ? bs - 1 - j : j;
+                    v[u] = A[r + (int64_t)c * lda];
+                }
             }
-            else
-                v = A[r + (int64_t)c * lda];
+#pragma unroll
+            for(int u = 0; u < kBatch; ++u)
+            {
+                int tl, i, j;
+                coords(tid + (u0 + u) * kTrtriThreads, tl, i, j);
+                T x = v[u];
+                if(i == j)
+                {
+                    // unit diagonal, identity padding, and a zero diagonal entry read as 1
+                    if(p.unit || i >= bs || x == T(0))
+                        x = T(1);
+                    rdiag[i] = T(1) / x;
+                }
+                Ls[tl * kTrtriTile + (i % kTrtriSB) * kTrtriPitch + (j % kTrtriSB)] = x;
+            }
         }
-        else
-            v = (i == j) ? T(1) : T(0);
-        Ls[trtri_tile_index(i / kTrtriSB, j / kTrtriSB) * kTrtriTile + (i % kTrtriSB) * kTrtriPitch
-           + (j % kTrtriSB)]
-            = v;
-        if(i == j)
-            rdiag[i] = T(1) / v;
     }
     __syncthreads();
 
@@ -140,6 +192,43 @@ __global__ void __launch_bounds__(kTrtriThreads) trtri_block_kernel(TrtriParams<
     // ---- off-diagonal tiles by distance d ------------------------------------------------
     const int c  = tid & 31;   // tile column handled by this thread
     const int rb = tid >> 5;   // rows rb, rb+8, rb+16, rb+24
+    if constexpr(std::is_same<T, double>::value)
+    {
+        // FP64: both products on DMMA, warp w owns the 16 x 8 block at rows 16 (w % 2),
+        // columns 8 (w / 2) of each 32 x 32 tile
+        const int lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3;
+        const int wr = (w & 1) * 16, wc = (w >> 1) * 8;
+        for(int d = 1; d < kTrtriNT; ++d)
+        {
+            const int npairs = kTrtriNT - d;
+            for(int pr = 0; pr < npairs; ++pr)
+            {
+                const int bj = pr, bi = pr + d;
+                double    acc[4] = {0.0, 0.0, 0.0, 0.0};
+                for(int bt = bj; bt < bi; ++bt)
+                    trtri_tile_mma(acc, Ls + trtri_tile_index(bi, bt) * kTrtriTile,
+                                   Xs + trtri_tile_index(bt, bj) * kTrtriTile, wr, wc, g, t);
+#pragma unroll
+                for(int e = 0; e < 4; ++e)
+                    Ts[pr * kTrtriTile + (wr + g + (e >> 1) * 8) * kTrtriPitch + wc + 2 * t + (e & 1)]
+                        = acc[e];
+            }
+            __syncthreads();
+            for(int pr = 0; pr < npairs; ++pr)
+            {
+                const int bj = pr, bi = pr + d;
+                double    acc[4] = {0.0, 0.0, 0.0, 0.0};
+                trtri_tile_mma(acc, Xs + trtri_tile_index(bi, bi) * kTrtriTile, Ts + pr * kTrtriTile,
+                               wr, wc, g, t);
+                T* Xo = Xs + trtri_tile_index(bi, bj) * kTrtriTile;
+#pragma unroll
+                for(int e = 0; e < 4; ++e)
+                    Xo[(wr + g + (e >> 1) * 8) * kTrtriPitch + wc + 2 * t + (e & 1)] = -acc[e];
+            }
+            __syncthreads();
+        }
+    }
+    else
     for(int d = 1; d < kTrtriNT; ++d)
     {
         const int npairs = kTrtriNT - d;
