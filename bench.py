@@ -688,7 +688,8 @@ def run_case(args):
     sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
     m x n (the chain solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
-    C3 recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N)."""
+    C3 recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
+    trtri: rocblas_dtrtri_strided_batched, --count lower m x m blocks."""
     import torch
 
     import rocblas_b200 as rb
@@ -731,6 +732,17 @@ def run_case(args):
             st = L.rocblas_dtrsm_strided_batched(h.value, 141, 122, 111, 131, m, n, po,
                                                  ctypes.c_void_p(As.data_ptr()), m, m * m,
                                                  ctypes.c_void_p(Bs.data_ptr()), m, m * n, bc)
+            assert st == 0, st
+    elif args.case == "trtri":
+        bc = args.count
+        At = torch.rand(bc, m, m, generator=g, device=dev, dtype=torch.float64) / m
+        At.diagonal(dim1=1, dim2=2).add_(1.0)
+        Inv = torch.zeros_like(At)
+
+        def run():
+            st = L.rocblas_dtrtri_strided_batched(h.value, rb.fill_lower, rb.diagonal_non_unit, m,
+                                                  ctypes.c_void_p(At.data_ptr()), m, m * m,
+                                                  ctypes.c_void_p(Inv.data_ptr()), m, m * m, bc)
             assert st == 0, st
     elif args.case == "zgemm":
         A = torch.randn(k, m, dtype=torch.complex128, device=dev, generator=g)
@@ -781,7 +793,7 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and serving sections (profiling runs)")
-    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "vbatched", "strided"],
+    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "vbatched", "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,
