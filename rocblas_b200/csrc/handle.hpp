@@ -38,6 +38,9 @@ struct _rocblas_handle
     // device word where kernels with bounded waits record a timeout (lazily allocated)
     int* err_dev = nullptr;
 
+    // streams, events and device buffers of the host-buffer entry points (lazily created)
+    struct HostPathRes* host_res = nullptr;
+
     // rounding of every workspace request (handle.hpp:56-61)
     static size_t roundup(size_t s) { return (s + 63) / 64 * 64; }
 

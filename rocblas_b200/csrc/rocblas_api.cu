@@ -5,9 +5,11 @@
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <new>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/rocblas_b200_ext.h"
 #include "sliced_driver.cuh"
@@ -1293,6 +1295,284 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     return launch_status();
 }
 
+// ---- host-buffer precision form (rocblas_b200_dtrsm_mixed_host) -----------------------------
+} // namespace
+
+// Streams, events and the device buffers of the host-buffer entry points, per handle.
+struct HostPathRes
+{
+    cudaStream_t             in = nullptr, out = nullptr, tri = nullptr;
+    std::vector<cudaEvent_t> ev;
+    void*                    dbuf   = nullptr;
+    size_t                   dbytes = 0;
+
+    bool init()
+    {
+        if(in)
+            return true;
+        if(cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking) != cudaSuccess
+           || cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking) != cudaSuccess
+           || cudaStreamCreateWithFlags(&tri, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return false;
+        }
+        return true;
+    }
+    cudaEvent_t event(size_t i)
+    {
+        while(ev.size() <= i)
+        {
+            cudaEvent_t e = nullptr;
+            if(cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            {
+                cudaGetLastError();
+                return nullptr;
+            }
+            ev.push_back(e);
+        }
+        return ev[i];
+    }
+    void* buffer(size_t bytes)
+    {
+        if(bytes <= dbytes)
+            return dbuf;
+        if(dbuf)
+            cudaFree(dbuf);
+        dbuf   = nullptr;
+        dbytes = 0;
+        if(cudaMalloc(&dbuf, bytes) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return nullptr;
+        }
+        dbytes = bytes;
+        return dbuf;
+    }
+    void release()
+    {
+        if(in)
+            cudaStreamSynchronize(in);
+        if(out)
+            cudaStreamSynchronize(out);
+        if(tri)
+            cudaStreamSynchronize(tri);
+        for(auto e : ev)
+            cudaEventDestroy(e);
+        ev.clear();
+        if(dbuf)
+            cudaFree(dbuf);
+        if(in)
+            cudaStreamDestroy(in);
+        if(out)
+            cudaStreamDestroy(out);
+        if(tri)
+            cudaStreamDestroy(tri);
+        in = out = tri = nullptr;
+        dbuf      = nullptr;
+        dbytes    = 0;
+    }
+};
+
+namespace
+{
+
+// The precision form with A and B in host memory: the call copies A's triangle and B to the
+// device, solves, and copies X back into B, returning when B holds X.  For side left the
+// three overlap: A's triangle goes over in 512-column panels in the order the solve consumes
+// them (each panel's 128-blocks inverted on a third stream as soon as it lands), the solve
+// runs right-looking over diagonal blocks so that each step needs only the panels that have
+// arrived, and each block of X rows goes back as soon as it is final.  Side right copies
+// everything first and then solves.
+rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                    rocblas_operation trans, rocblas_diagonal diag, int m, int n,
+                                    const double* alpha, const double* hA, int lda, double* hB,
+                                    int ldb, int slices)
+{
+    if(!h)
+        return rocblas_status_invalid_handle;
+    if(h->size_query)
+        return rocblas_status_size_unchanged; // the device memory is the call's own
+    const rocblas_pointer_mode mode = h->pointer_mode;
+    h->pointer_mode                 = rocblas_pointer_mode_host; // alpha is a host value here
+    rocblas_status st = trsm_arg_check<double>(h, side, uplo, trans, diag, m, n, alpha, hA, lda, hB, ldb, 1);
+    h->pointer_mode = mode;
+    if(st != rocblas_status_continue)
+        return st;
+    if(slices == 0)
+        slices = tuning().mixed_slices;
+    if(slices < 1 || slices > kOzMaxS)
+        return rocblas_status_invalid_value;
+    if(*alpha == 0.0)
+    {
+        for(int j = 0; j < n; ++j)
+            std::memset(hB + (size_t)j * ldb, 0, sizeof(double) * (size_t)m);
+        return rocblas_status_success;
+    }
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    if(!h->host_res)
+        h->host_res = new HostPathRes();
+    HostPathRes& R = *h->host_res;
+    if(!R.init())
+        return rocblas_status_internal_error;
+    const bool    left = side == rocblas_side_left;
+    const int     k    = left ? m : n;
+    const size_t  a_bytes = align256((size_t)k * k * sizeof(double));
+    const size_t  b_bytes = align256((size_t)m * n * sizeof(double));
+    char*         buf     = reinterpret_cast<char*>(R.buffer(a_bytes + b_bytes));
+    if(!buf)
+        return rocblas_status_memory_error;
+    double* dA = reinterpret_cast<double*>(buf);
+    double* dB = reinterpret_cast<double*>(buf + a_bytes);
+    const size_t es = sizeof(double);
+
+    TrsmProblem<double> pr{};
+    pr.side_left = left;
+    pr.upper     = uplo == rocblas_fill_upper;
+    pr.trans     = trans != rocblas_operation_none;
+    pr.unit      = diag == rocblas_diagonal_unit;
+    pr.m = m;
+    pr.n = n;
+    pr.batch = 1;
+    pr.A = strided<double>(dA, 0);
+    pr.lda = k;
+    pr.B = strided<double>(dB, 0);
+    pr.ldb = m;
+    pr.stream   = h->stream;
+    pr.sm_count = h->sm_count;
+    pr.alpha.val = *alpha;
+    const bool recursive = choose_algo(pr) == Algo::recursive;
+
+    // B arrives first (the updates below a diagonal block write rows of every later block)
+    cudaEvent_t eB = R.event(0);
+    if(!eB)
+        return rocblas_status_internal_error;
+    cudaMemcpy2DAsync(dB, (size_t)m * es, hB, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, R.in);
+
+    if(!left || !recursive)
+    {
+        cudaMemcpy2DAsync(dA, (size_t)k * es, hA, (size_t)lda * es, (size_t)k * es, k, cudaMemcpyHostToDevice,
+                          R.in);
+        cudaEventRecord(eB, R.in);
+        cudaStreamWaitEvent(h->stream, eB, 0);
+        const rocblas_pointer_mode saved = h->pointer_mode;
+        h->pointer_mode                  = rocblas_pointer_mode_host;
+        st = trsm_mixed_impl(h, side, uplo, trans, diag, m, n, alpha, dA, k, dB, m, slices);
+        h->pointer_mode = saved;
+        if(st != rocblas_status_success)
+            return st;
+        cudaMemcpy2DAsync(hB, (size_t)ldb * es, dB, (size_t)m * es, (size_t)m * es, n, cudaMemcpyDeviceToHost,
+                          h->stream);
+        cudaStreamSynchronize(h->stream);
+        return launch_status();
+    }
+    cudaEventRecord(eB, R.in);
+
+    // workspace of the solve: invA, slices, chain flags (as rocblas_b200_dtrsm_mixed)
+    const size_t inv_bytes = align256((size_t)kInvNB * k * sizeof(double));
+    const size_t sl_bytes  = mixed_slice_workspace_bytes(pr, slices);
+    const size_t ch_bytes  = mixed_chain_workspace_bytes(pr);
+    const size_t ws_bytes  = inv_bytes + sl_bytes + (ch_bytes ? (ch_bytes + 255) / 256 * 256 : 0);
+    int*         err       = ensure_err(h);
+    void*        ws        = h->borrow(ws_bytes);
+    if(!ws || !err)
+        return rocblas_status_memory_error;
+    pr.err_dev = err;
+    BatchPtr<double> inv;
+    inv.base   = reinterpret_cast<double*>(ws);
+    inv.stride = (int64_t)kInvNB * k;
+    pr.invA    = inv;
+
+    // A in panels of PB = 4 128-blocks (512 columns: little of the unused triangle travels
+    // with the diagonal blocks), in solve order; M = op(A), so a panel of M's columns is a
+    // panel of A's columns (trans N) or rows (trans T); the rows it needs are the ones below
+    // its diagonal block (forward solve) or above it (backward)
+    const int  nblk    = (int)ceil_div(k, kInvNB);
+    const int  PB      = 4;
+    const int  npanel  = (int)ceil_div(nblk, PB);
+    const bool forward = pr.oplower();
+    for(int q = 0; q < npanel; ++q)
+    {
+        const int p  = forward ? q : npanel - 1 - q;
+        const int c0 = p * PB * kInvNB, c1 = std::min(k, (p + 1) * PB * kInvNB);
+        const int i0 = forward ? c0 : 0, i1 = forward ? k : c1;
+        if(!pr.trans)
+            cudaMemcpy2DAsync(dA + i0 + (int64_t)c0 * k, (size_t)k * es, hA + i0 + (int64_t)c0 * lda,
+                              (size_t)lda * es, (size_t)(i1 - i0) * es, c1 - c0, cudaMemcpyHostToDevice, R.in);
+        else
+            cudaMemcpy2DAsync(dA + c0 + (int64_t)i0 * k, (size_t)k * es, hA + c0 + (int64_t)i0 * lda,
+                              (size_t)lda * es, (size_t)(c1 - c0) * es, i1 - i0, cudaMemcpyHostToDevice, R.in);
+        // the panel's diagonal 128-blocks, inverted on their own stream as soon as they land (the
+        // copy stream goes on with the next panel)
+        cudaEvent_t ec = R.event(1 + npanel + p);
+        if(!ec)
+            return rocblas_status_internal_error;
+        cudaEventRecord(ec, R.in);
+        cudaStreamWaitEvent(R.tri, ec, 0);
+        TrtriParams<double> t{};
+        t.k                = c1 - c0;
+        t.nb               = kInvNB;
+        t.A                = pr.A.shifted(c0 + (int64_t)c0 * k);
+        t.lda              = k;
+        t.inv              = inv.shifted((int64_t)(c0 / kInvNB) * kInvNB * kInvNB);
+        t.ldinv            = kInvNB;
+        t.inv_block_stride = (int64_t)kInvNB * kInvNB;
+        t.upper            = pr.upper;
+        t.unit             = pr.unit;
+        launch_trtri<double>(t, (int)ceil_div(c1 - c0, kInvNB), 1, R.tri);
+        count_launch();
+        cudaEvent_t e = R.event(1 + p);
+        if(!e)
+            return rocblas_status_internal_error;
+        cudaEventRecord(e, R.tri);
+    }
+    cudaStreamWaitEvent(h->stream, eB, 0);
+
+    MixedRecursive rec{{pr, k, nblk}};
+    rec.S        = slices;
+    rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
+    rec.err_dev  = err;
+    if(ch_bytes)
+        rec.chain_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes + (sl_bytes + 255) / 256 * 256;
+    // Right-looking over diagonal blocks of the recursion's leaf size (mixed_chain_blocks x 128
+    // rows): solve a diagonal block as soon as its panels of A have landed, send its rows of X
+    // home, and update every row not yet solved with them (one sliced product of depth = the
+    // block), so that the solve follows the transfer of A instead of waiting for all of it.
+    // alpha is applied by the first diagonal solve and the first update, which between them
+    // touch every row once.
+    const int DB    = std::max(1, tuning().mixed_chain_blocks);
+    const int ndiag = (int)ceil_div(nblk, DB);
+    size_t    nout  = 0;
+    for(int q = 0; q < ndiag && rec.ok; ++q)
+    {
+        const int d = forward ? q : ndiag - 1 - q;
+        const int b0 = d * DB, b1 = std::min(nblk, b0 + DB);
+        for(int p = b0 / PB; p <= (b1 - 1) / PB; ++p)
+            cudaStreamWaitEvent(h->stream, R.event(1 + p), 0);
+        const int first = q == 0 ? 1 : 0;
+        rec.solve_mixed(b0, b1, first);
+        // rows [r0, r1) of X are final: send them home on the out stream
+        const int   r0 = rec.row_of(b0), r1 = rec.row_of(b1);
+        cudaEvent_t e  = R.event(1 + 2 * npanel + nout++);
+        if(!e)
+            return rocblas_status_internal_error;
+        cudaEventRecord(e, h->stream);
+        cudaStreamWaitEvent(R.out, e, 0);
+        cudaMemcpy2DAsync(hB + r0, (size_t)ldb * es, dB + r0, (size_t)m * es, (size_t)(r1 - r0) * es, n,
+                          cudaMemcpyDeviceToHost, R.out);
+        if(forward && r1 < k)
+            rec.update_sliced(r1, k, r0, r1, first);
+        else if(!forward && r0 > 0)
+            rec.update_sliced(0, r0, r0, r1, first);
+    }
+    cudaStreamSynchronize(R.out);
+    cudaStreamSynchronize(h->stream);
+    if(!rec.ok)
+        return rocblas_status_arch_mismatch;
+    return launch_status();
+}
+
 } // namespace
 
 // =========================================================================================
@@ -1341,6 +1621,11 @@ try
     handle->free_mem();
     if(handle->err_dev)
         cudaFree(handle->err_dev);
+    if(handle->host_res)
+    {
+        handle->host_res->release();
+        delete handle->host_res;
+    }
     delete handle;
     return rocblas_status_success;
 }
@@ -2058,6 +2343,20 @@ rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle h, rocblas_side side, roc
 try
 {
     return trsm_mixed_impl(h, side, uplo, transA, diag, m, n, alpha, A, lda, B, ldb, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dtrsm_mixed_host(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                             rocblas_operation transA, rocblas_diagonal diag,
+                                             rocblas_int m, rocblas_int n, const double* alpha,
+                                             const double* A, rocblas_int lda, double* B,
+                                             rocblas_int ldb, rocblas_int slices)
+try
+{
+    return trsm_mixed_host_impl(h, side, uplo, transA, diag, m, n, alpha, A, lda, B, ldb, slices);
 }
 catch(...)
 {

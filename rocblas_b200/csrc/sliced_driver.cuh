@@ -1,6 +1,7 @@
 // Host side of the sliced (integer-slice, tensor-core) FP64 GEMM and of the precision form
 // of the TRSM that uses it for its trailing updates.
 #pragma once
+#include <functional>
 #include <mutex>
 
 #include "ozaki_gemm.cuh"
@@ -276,6 +277,10 @@ struct MixedRecursive : Recursive<double>
     int*  err_dev;
     void* chain_ws = nullptr; // flags of the chain sub-solves (nullptr: recursion to the leaves)
     bool  ok = true;
+    // optional hooks around every diagonal-block solve of blocks [b0, b1) (a chain sub-solve or
+    // a leaf): the host-buffer path waits for A's data before it and copies the finished rows
+    // of X out after it
+    std::function<void(int, int)> before_diag, after_diag;
 
     // Updates with a short inner dimension stay on the FP64 DMMA tiles (K < sliced_min_k):
     // slicing costs about as much as a short product and short GEMMs gain nothing from it.
@@ -326,13 +331,21 @@ struct MixedRecursive : Recursive<double>
     {
         if(b1 - b0 == 1)
         {
+            if(before_diag)
+                before_diag(b0, b1);
             leaf(b0, first);
+            if(after_diag)
+                after_diag(b0, b1);
             return;
         }
         // diagonal blocks of at most mixed_chain_blocks x 128 rows: one chain launch in FP64
         if(chain_ws && b1 - b0 <= tuning().mixed_chain_blocks)
         {
+            if(before_diag)
+                before_diag(b0, b1);
             launch_chain_sub<double>(pr, b0, b1, first, mixed_chain_w(), chain_ws);
+            if(after_diag)
+                after_diag(b0, b1);
             return;
         }
         const int  bm = (b0 + b1) / 2;
