@@ -824,6 +824,18 @@ static_assert(sizeof(VbProblem) == sizeof(rocblas_b200_trsm_problem), "descripto
 template <typename T>
 void launch_vb_queue(rocblas_handle h, const VbParams<T>& p, int kmax)
 {
+    if(kmax <= kVbWarpMaxK)
+    {
+        // the smallest class: one strip per warp (vb_warp_kernel)
+        const size_t smem   = vb_warp_smem_bytes<T>();
+        int          per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_warp_kernel<T>, 32 * kVbWarpsPerCta, smem);
+        per_sm = std::max(per_sm, 1);
+        TimedLaunch tl(KernelClass::strip, h->stream, 0.0);
+        vb_warp_kernel<T><<<h->sm_count * per_sm, 32 * kVbWarpsPerCta, smem, h->stream>>>(p);
+        count_launch();
+        return;
+    }
     const size_t smem = block_solve_smem_bytes<T>(std::max(kmax, 1));
     cudaFuncSetAttribute((const void*)vb_persistent_kernel<T>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
