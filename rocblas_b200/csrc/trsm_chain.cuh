@@ -119,17 +119,28 @@ __device__ __forceinline__ void chain_cp_async(T* smem, const T* gmem, bool vali
 
 // smem layouts: P (M rows o x K) [k][o] pitch 132 (KCP = false) or [o][k] pitch BK+4 (KCP);
 // Q (K x W) [k][n] pitch W+4 (KCQ = false) or [n][k] pitch BK+4 (KCQ); elements of type T.
+// K chunks are 32 deep in 3 stages where that fits in shared memory (fewer CTA barriers per
+// MMA), else 16 deep in 4 stages; either depth divides the 128-row blocks, so a chunk never
+// spans two blocks.
 template <typename T, int W, bool KCP, bool KCQ>
 struct ChainCfg
 {
-    static constexpr int kPitchP  = KCP ? kChainBK + 4 : kChainNB + 4;
-    static constexpr int kPitchQ  = KCQ ? kChainBK + 4 : W + 4;
-    static constexpr int kStageP  = KCP ? kChainNB * kPitchP : kChainBK * kPitchP;
-    static constexpr int kStageQ  = KCQ ? W * kPitchQ : kChainBK * kPitchQ;
+    static constexpr size_t bytes(int bk, int stages)
+    {
+        const int pp = KCP ? bk + 4 : kChainNB + 4, pq = KCQ ? bk + 4 : W + 4;
+        const int sp = KCP ? kChainNB * pp : bk * pp, sq = KCQ ? W * pq : bk * pq;
+        return sizeof(T) * (size_t)stages * (sp + sq) + sizeof(double) * (size_t)kChainNB * (W + 4);
+    }
+    static constexpr bool kDeep   = bytes(32, 3) <= 227 * 1024 - 64; // room for the static words
+    static constexpr int kBK      = kDeep ? 32 : kChainBK;
+    static constexpr int kStages  = kDeep ? 3 : kChainStages;
+    static constexpr int kPitchP  = KCP ? kBK + 4 : kChainNB + 4;
+    static constexpr int kPitchQ  = KCQ ? kBK + 4 : W + 4;
+    static constexpr int kStageP  = KCP ? kChainNB * kPitchP : kBK * kPitchP;
+    static constexpr int kStageQ  = KCQ ? W * kPitchQ : kBK * kPitchQ;
     static constexpr int kStage   = kStageP + kStageQ; // elements of T
     static constexpr int kPitchT  = W + 4;             // T tile [k = row o][n], doubles
-    static constexpr size_t kSmem = sizeof(T) * (size_t)kChainStages * kStage
-                                    + sizeof(double) * (size_t)kChainNB * kPitchT;
+    static constexpr size_t kSmem = bytes(kBK, kStages);
 };
 
 // W right-hand sides per item (32 or 64); 8 warps as 4 (rows) x 2 (columns), each warp
@@ -143,7 +154,7 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
     constexpr int WN = W / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T*         smem = reinterpret_cast<T*>(smem_raw);
-    double*    Ts   = reinterpret_cast<double*>(smem_raw + sizeof(T) * (size_t)kChainStages * Cfg::kStage);
+    double*    Ts   = reinterpret_cast<double*>(smem_raw + sizeof(T) * (size_t)Cfg::kStages * Cfg::kStage);
     __shared__ int64_t s_item;
     __shared__ int     s_abort;
 
@@ -254,12 +265,12 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
         // descending, in 16-row chunks aligned to multiples of 16 (never across a block).
         const int klo  = forward ? 0 : r0 + bs;
         const int khi  = forward ? r0 : k;
-        const int ktop = (int)ceil_div(khi, kChainBK) * kChainBK;
-        const int nk   = forward ? (int)ceil_div(khi, kChainBK) : (ktop - klo) / kChainBK;
+        const int ktop = (int)ceil_div(khi, Cfg::kBK) * Cfg::kBK;
+        const int nk   = forward ? (int)ceil_div(khi, Cfg::kBK) : (ktop - klo) / Cfg::kBK;
         const bool zero = alpha == 0.0;
         int waited = forward ? 0 : nb; // blocks known finished: [0, waited) or [waited, nb)
 
-        auto chunk_row0 = [&](int c) { return forward ? c * kChainBK : ktop - (c + 1) * kChainBK; };
+        auto chunk_row0 = [&](int c) { return forward ? c * Cfg::kBK : ktop - (c + 1) * Cfg::kBK; };
         // wait until the block holding chunk c is finished (uniform across the CTA)
         auto wait_chunk = [&](int c) -> bool {
             const int  blk  = max(chunk_row0(c), klo) / kChainNB;
@@ -292,11 +303,11 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
             const int k0 = chunk_row0(c);
             // P: M(r0 + o, k0 + kk), o < 128, kk < 16
 #pragma unroll
-            for(int i = 0; i < kChainNB * kChainBK / kChainThreads; ++i)
+            for(int i = 0; i < kChainNB * Cfg::kBK / kChainThreads; ++i)
             {
                 const int e = tid + i * kChainThreads;
                 int       o, kk;
-                if(KCP) { kk = e % kChainBK; o = e / kChainBK; }
+                if(KCP) { kk = e % Cfg::kBK; o = e / Cfg::kBK; }
                 else    { o = e % kChainNB; kk = e / kChainNB; }
                 const int  kr    = k0 + kk;
                 const bool valid = o < bs && kr >= klo && kr < khi;
@@ -306,11 +317,11 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
             }
             // Q: C(k0 + kk, c0 + n), kk < 16, n < W
 #pragma unroll
-            for(int i = 0; i < W * kChainBK / kChainThreads; ++i)
+            for(int i = 0; i < W * Cfg::kBK / kChainThreads; ++i)
             {
                 const int e = tid + i * kChainThreads;
                 int       n, kk;
-                if(KCQ) { kk = e % kChainBK; n = e / kChainBK; }
+                if(KCQ) { kk = e % Cfg::kBK; n = e / Cfg::kBK; }
                 else    { n = e % W; kk = e / W; }
                 const int  kr    = k0 + kk;
                 const bool valid = n < wv && kr >= klo && kr < khi;
@@ -330,7 +341,7 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
         {
             bool ok = true;
 #pragma unroll 1
-            for(int s = 0; s < kChainStages - 1; ++s)
+            for(int s = 0; s < Cfg::kStages - 1; ++s)
             {
                 if(s < nk && ok)
                 {
@@ -343,12 +354,12 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
 #pragma unroll 1
             for(int kt = 0; kt < nk && ok; ++kt)
             {
-                cp_async_wait<kChainStages - 2>();
+                cp_async_wait<Cfg::kStages - 2>();
                 __syncthreads();
-                const T* sP = smem + (kt % kChainStages) * Cfg::kStage;
+                const T* sP = smem + (kt % Cfg::kStages) * Cfg::kStage;
                 const T* sQ = sP + Cfg::kStageP;
 #pragma unroll
-                for(int ks = 0; ks < kChainBK / 8; ++ks)
+                for(int ks = 0; ks < Cfg::kBK / 8; ++ks)
                 {
                     const int kk = ks * 8 + t;
                     double    fa[TM][4], fb[TN][2];
@@ -374,12 +385,12 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
                         for(int jn = 0; jn < TN; ++jn)
                             dmma_16x8x8(acc[i][jn], fa[i], fb[jn]);
                 }
-                const int nxt = kt + kChainStages - 1;
+                const int nxt = kt + Cfg::kStages - 1;
                 if(nxt < nk)
                 {
                     ok = wait_chunk(nxt);
                     if(ok)
-                        load_chunk(nxt % kChainStages, nxt);
+                        load_chunk(nxt % Cfg::kStages, nxt);
                 }
                 cp_async_commit();
             }
@@ -415,16 +426,16 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
 #pragma unroll
                 for(int e = 0; e < 4; ++e)
                     acc[i][jn][e] = 0.0;
-        const int nki = (int)ceil_div(bs, kChainBK);
+        const int nki = (int)ceil_div(bs, Cfg::kBK);
         auto load_inv = [&](int stage, int c) {
             T*        sP = smem + stage * Cfg::kStage;
-            const int k0 = c * kChainBK;
+            const int k0 = c * Cfg::kBK;
 #pragma unroll
-            for(int i = 0; i < kChainNB * kChainBK / kChainThreads; ++i)
+            for(int i = 0; i < kChainNB * Cfg::kBK / kChainThreads; ++i)
             {
                 const int e = tid + i * kChainThreads;
                 int       o, kk;
-                if(KCP) { kk = e % kChainBK; o = e / kChainBK; }
+                if(KCP) { kk = e % Cfg::kBK; o = e / Cfg::kBK; }
                 else    { o = e % kChainNB; kk = e / kChainNB; }
                 const int  kr    = k0 + kk;
                 const bool tri   = forward ? kr <= o : kr >= o;
@@ -437,7 +448,7 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
             }
         };
 #pragma unroll 1
-        for(int s = 0; s < kChainStages - 1; ++s)
+        for(int s = 0; s < Cfg::kStages - 1; ++s)
         {
             if(s < nki)
                 load_inv(s, s);
@@ -446,14 +457,14 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
 #pragma unroll 1
         for(int kt = 0; kt < nki; ++kt)
         {
-            cp_async_wait<kChainStages - 2>();
+            cp_async_wait<Cfg::kStages - 2>();
             __syncthreads();
-            const T* sP = smem + (kt % kChainStages) * Cfg::kStage;
+            const T* sP = smem + (kt % Cfg::kStages) * Cfg::kStage;
 #pragma unroll
-            for(int ks = 0; ks < kChainBK / 8; ++ks)
+            for(int ks = 0; ks < Cfg::kBK / 8; ++ks)
             {
                 const int kk = ks * 8 + t;
-                const int kg = kt * kChainBK + kk; // row of T
+                const int kg = kt * Cfg::kBK + kk; // row of T
                 double    fa[TM][4], fb[TN][2];
 #pragma unroll
                 for(int i = 0; i < TM; ++i)
@@ -477,9 +488,9 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
                     for(int jn = 0; jn < TN; ++jn)
                         dmma_16x8x8(acc[i][jn], fa[i], fb[jn]);
             }
-            const int nxt = kt + kChainStages - 1;
+            const int nxt = kt + Cfg::kStages - 1;
             if(nxt < nki)
-                load_inv(nxt % kChainStages, nxt);
+                load_inv(nxt % Cfg::kStages, nxt);
             cp_async_commit();
         }
         cp_async_wait<0>();
