@@ -120,9 +120,10 @@ __device__ __forceinline__ void chain_cp_async(T* smem, const T* gmem, bool vali
 // smem layouts: P (M rows o x K) [k][o] pitch 132 (KCP = false) or [o][k] pitch BK+4 (KCP);
 // Q (K x W) [k][n] pitch W+4 (KCQ = false) or [n][k] pitch BK+4 (KCQ); elements of type T.
 // K chunks are 32 deep in 3 stages where that fits in shared memory (fewer CTA barriers per
-// MMA), else 16 deep in 4 stages; either depth divides the 128-row blocks, so a chunk never
+// MMA; measured faster for one large system), else 16 deep in 4 stages (measured faster for
+// the variable-size batch, VB); either depth divides the 128-row blocks, so a chunk never
 // spans two blocks.
-template <typename T, int W, bool KCP, bool KCQ>
+template <typename T, int W, bool KCP, bool KCQ, bool VB = false>
 struct ChainCfg
 {
     static constexpr size_t bytes(int bk, int stages)
@@ -131,7 +132,7 @@ struct ChainCfg
         const int sp = KCP ? kChainNB * pp : bk * pp, sq = KCQ ? W * pq : bk * pq;
         return sizeof(T) * (size_t)stages * (sp + sq) + sizeof(double) * (size_t)kChainNB * (W + 4);
     }
-    static constexpr bool kDeep   = bytes(32, 3) <= 227 * 1024 - 64; // room for the static words
+    static constexpr bool kDeep   = !VB && bytes(32, 3) <= 227 * 1024 - 64; // room for the static words
     static constexpr int kBK      = kDeep ? 32 : kChainBK;
     static constexpr int kStages  = kDeep ? 3 : kChainStages;
     static constexpr int kPitchP  = KCP ? kBK + 4 : kChainNB + 4;
@@ -149,7 +150,7 @@ struct ChainCfg
 template <typename T, int W, bool KCP, bool KCQ, bool VB>
 __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParams<T> p)
 {
-    using Cfg = ChainCfg<T, W, KCP, KCQ>;
+    using Cfg = ChainCfg<T, W, KCP, KCQ, VB>;
     constexpr int TM = 2, TN = W / 16; // per warp: 32 rows x W/2 columns
     constexpr int WN = W / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -545,7 +546,7 @@ inline size_t chain_workspace_bytes(const ChainShape& c)
 template <typename T, int W, bool KCP, bool KCQ, bool VB>
 static void launch_chain_cfg(const ChainParams<T>& p, int sms, int64_t max_items, cudaStream_t s)
 {
-    using Cfg = ChainCfg<T, W, KCP, KCQ>;
+    using Cfg = ChainCfg<T, W, KCP, KCQ, VB>;
     auto kern = trsm_chain_kernel<T, W, KCP, KCQ, VB>;
     cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
     int per_sm = 0;
