@@ -7,11 +7,13 @@ the tcgen05 tensor cores, FP64 diagonal blocks) and, beside it, by the plain FP6
 B ~ U(-1,1).  One step = restore the right-hand side (a device copy of 512 MiB, inside the timed
 region) + one solve through the C ABI.  A (2 GiB) and B (512 MiB) are larger than the 126 MB L2,
 so no flush is needed between steps.  Errors are reported per condition band k in {0,2,4,6}
-against the float128 oracle and the host FP64 CBLAS.
+against the float128 oracle and the host FP64 CBLAS.  The end-to-end figure (`e2e`) calls
+rocblas_b200_dtrsm_mixed_host on pinned host buffers (transfers inside the timed region).
+Extras: the variable-size and strided batches (C3), the serving loop (C4), complex z/ctrsm.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: a single solve does not shard (SURVEY: replicas only), so N ranks each run their
+Multi-GPU: a single solve does not shard (replicas only), so N ranks each run their
 own independent solve; `value` is the sum over ranks of m*n*k flops / the max-over-ranks time.
 `--impl reference` times the host CBLAS trsm (OpenBLAS bundled with scipy, the library the
 reference's ref_trsm wraps) on all host cores on a bounded column sample of the same problem.
