@@ -9,7 +9,7 @@ region) + one solve through the C ABI.  A (2 GiB) and B (512 MiB) are larger tha
 so no flush is needed between steps.  Errors are reported per condition band k in {0,2,4,6}
 against the float128 oracle and the host FP64 CBLAS.  The end-to-end figure (`e2e`) calls
 rocblas_b200_dtrsm_mixed_host on pinned host buffers (transfers inside the timed region).
-Extras: the variable-size and strided batches (C3), the serving loop (C4), complex z/ctrsm.
+Extras: the variable-size and strided batches, the serving loop, complex z/ctrsm.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -223,7 +223,7 @@ def run_reference(args):
 
 
 def vbatched_workload(torch, dev, count, seed, dt):
-    """Config C3's systems: m log-uniform [16, 512], n uniform [1, 64], side and uplo uniform,
+    """The variable-size batch's systems: m log-uniform [16, 512], n uniform [1, 64], side and uplo uniform,
     transA N, diag N, A and B by the drop-in recipe, all in two device arrays; returns the
     device descriptor array (rocblas_b200_trsm_problem records) and the arrays behind it."""
     tdt, es = (torch.float64, 8) if dt == "d" else (torch.float32, 4)
@@ -272,7 +272,7 @@ def vbatched_workload(torch, dev, count, seed, dt):
 
 
 def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
-    """Config C3: `count` uneven systems (m log-uniform [16, 512], n uniform [1, 64], side and
+    """The variable-size batch: `count` uneven systems (m log-uniform [16, 512], n uniform [1, 64], side and
     uplo uniform, transA N, diag N) through rocblas_b200_?trsm_vbatched, FP64 and FP32; plus
     the uniform strided batch (4096 x m=128, n=32) through rocblas_?trsm_strided_batched.
     Solves/s and algorithmic GB/s against the HBM roofline."""
@@ -406,7 +406,7 @@ def bench_complex(torch, L, h, dev, fp64_peak, m=8192, n=2048, steps=5):
 
 
 def bench_serving(torch, dev, n_requests, rate, seed=7):
-    """Config C4: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
+    """The serving workload: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
     60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
     budget.  The native server loop (rocblas_b200_server_run) serves the list; returns p50 /
     p99 latency, solves/s over the server's own wall time, and its batching statistics."""
@@ -698,7 +698,7 @@ def run_case(args):
     sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
     m x n (the chain solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
-    C3 recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
+    variable-size batch recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
     trtri: rocblas_dtrtri_strided_batched, --count lower m x m blocks."""
     import torch
 
@@ -807,7 +807,7 @@ def main():
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,
-                    help="systems of a --case vbatched (C3 recipe) or strided (m x n each) run")
+                    help="systems of a --case vbatched (variable-size batch recipe) or strided (m x n each) run")
     args = ap.parse_args()
     if args.case:
         run_case(args)
