@@ -17,8 +17,9 @@
 //     (the variable-size batch) a CTA rarely waits at all: the items claimed before it are
 //     mostly other systems' work of the same level;
 //   * an item accumulates M_{b,i} X_i over the finished blocks i in solve order through a
-//     cp.async pipeline of 16-deep K chunks on DMMA (mma.sync m16n8k8 f64), waiting on a
-//     block's flag (ld.acquire.gpu by one thread, then a CTA barrier) before its first chunk;
+//     cp.async pipeline of 32- or 16-deep K chunks (ChainCfg) on DMMA (mma.sync m16n8k8 f64),
+//     waiting on a block's flag (ld.acquire.gpu by one thread, then a CTA barrier) before its
+//     first chunk;
 //   * then T = alpha C_b - acc goes to shared memory, X_b = inv(M_bb) T (the caller's or the
 //     fused trtri's invA block, its triangle masked) is written over C_b, and the item's
 //     flag is released (CTA barrier, then st.release.gpu by one thread);
@@ -263,7 +264,8 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
 
         // ---- 1. acc = M[rows of b, finished rows] * X[finished rows, strip] ---------------
         // K rows of the finished blocks: forward [0, r0) ascending; backward [r0 + bs, k)
-        // descending, in 16-row chunks aligned to multiples of 16 (never across a block).
+        // descending, in chunks of Cfg::kBK rows aligned to multiples of kBK (never across a
+        // block).
         const int klo  = forward ? 0 : r0 + bs;
         const int khi  = forward ? r0 : k;
         const int ktop = (int)ceil_div(khi, Cfg::kBK) * Cfg::kBK;
