@@ -209,3 +209,29 @@ def test_ilp64_arguments_and_size_query(handle):
                            1 << 28) == rb.status_size_increased
     assert L.rocblas_stop_device_memory_size_query(h, ctypes.byref(size32)) == 0
     assert size64.value == size32.value > 0
+
+
+def test_complex_argument_rules(handle):
+    """rocblas_{c,z}trsm / trsv / trmm follow the real argument rules (checked without a device:
+    every call below returns before any device work)."""
+    L = rb.lib()
+    h = handle.value
+    z = (ctypes.c_double * 2)(1.0, 0.0)
+    zp = ctypes.cast(z, ctypes.c_void_p)
+    X, Y = 0x1000, 0x2000
+    lo, nn, nu = rb.fill_lower, rb.operation_none, rb.diagonal_non_unit
+    for S in "cz":
+        trsm = getattr(L, f"rocblas_{S}trsm")
+        assert trsm(None, rb.side_left, lo, nn, nu, 8, 8, zp, X, 8, Y, 8) == rb.status_invalid_handle
+        assert trsm(h, rb.side_both, lo, nn, nu, 8, 8, zp, X, 8, Y, 8) == rb.status_invalid_value
+        assert trsm(h, rb.side_left, lo, rb.operation_conjugate_transpose + 1, nu, 8, 8, zp, X, 8, Y, 8) \
+            == rb.status_invalid_value
+        assert trsm(h, rb.side_left, lo, nn, nu, 8, 8, zp, X, 7, Y, 8) == rb.status_invalid_size
+        assert trsm(h, rb.side_left, lo, nn, nu, 0, 8, None, None, 8, None, 8) == rb.status_success
+        assert trsm(h, rb.side_left, lo, nn, nu, 8, 8, None, X, 8, Y, 8) == rb.status_invalid_pointer
+        assert getattr(L, f"rocblas_{S}trsm_64")(h, rb.side_left, lo, nn, nu, (1 << 31) + 1, 1, zp, X,
+                                                 (1 << 31) + 1, Y, (1 << 31) + 1) == rb.status_invalid_size
+        assert getattr(L, f"rocblas_{S}trsv")(h, lo, rb.operation_conjugate_transpose, nu, 8, X, 8, Y, 0) \
+            == rb.status_invalid_size
+        assert getattr(L, f"rocblas_{S}trmm")(h, rb.side_right, lo, nn, nu, 8, 8, zp, X, 8, Y, 8, Y, 9) \
+            == rb.status_invalid_value
