@@ -1306,6 +1306,71 @@ ROCBLAS_EXPORT rocblas_status rocblas_ztrmm_strided_batched_64(rocblas_handle   
                                                                rocblas_stride                stride_C,
                                                                int64_t                       batch_count);
 
+/* ---- complex trtri: rocblas-functions.h:19099-19117, 19179-19198, 19273-19296; inv(A) is the
+ * solution of A X = I by the complex solve (a zero non-unit diagonal is not read as 1). ---- */
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrtri(rocblas_handle               handle,
+                                             rocblas_fill                 uplo,
+                                             rocblas_diagonal             diag,
+                                             rocblas_int                  n,
+                                             const rocblas_float_complex* A,
+                                             rocblas_int                  lda,
+                                             rocblas_float_complex*       invA,
+                                             rocblas_int                  ldinvA);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrtri_batched(rocblas_handle                      handle,
+                                                     rocblas_fill                        uplo,
+                                                     rocblas_diagonal                    diag,
+                                                     rocblas_int                         n,
+                                                     const rocblas_float_complex* const* A,
+                                                     rocblas_int                         lda,
+                                                     rocblas_float_complex* const*       invA,
+                                                     rocblas_int                         ldinvA,
+                                                     rocblas_int                         batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ctrtri_strided_batched(rocblas_handle               handle,
+                                                             rocblas_fill                 uplo,
+                                                             rocblas_diagonal             diag,
+                                                             rocblas_int                  n,
+                                                             const rocblas_float_complex* A,
+                                                             rocblas_int                  lda,
+                                                             rocblas_stride               stride_a,
+                                                             rocblas_float_complex*       invA,
+                                                             rocblas_int                  ldinvA,
+                                                             rocblas_stride               stride_invA,
+                                                             rocblas_int                  batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrtri(rocblas_handle                handle,
+                                             rocblas_fill                  uplo,
+                                             rocblas_diagonal              diag,
+                                             rocblas_int                   n,
+                                             const rocblas_double_complex* A,
+                                             rocblas_int                   lda,
+                                             rocblas_double_complex*       invA,
+                                             rocblas_int                   ldinvA);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrtri_batched(rocblas_handle                       handle,
+                                                     rocblas_fill                         uplo,
+                                                     rocblas_diagonal                     diag,
+                                                     rocblas_int                          n,
+                                                     const rocblas_double_complex* const* A,
+                                                     rocblas_int                          lda,
+                                                     rocblas_double_complex* const*       invA,
+                                                     rocblas_int                          ldinvA,
+                                                     rocblas_int                          batch_count);
+
+ROCBLAS_EXPORT rocblas_status rocblas_ztrtri_strided_batched(rocblas_handle                handle,
+                                                             rocblas_fill                  uplo,
+                                                             rocblas_diagonal              diag,
+                                                             rocblas_int                   n,
+                                                             const rocblas_double_complex* A,
+                                                             rocblas_int                   lda,
+                                                             rocblas_stride                stride_a,
+                                                             rocblas_double_complex*       invA,
+                                                             rocblas_int                   ldinvA,
+                                                             rocblas_stride                stride_invA,
+                                                             rocblas_int                   batch_count);
+
 #ifdef __cplusplus
 }
 #endif

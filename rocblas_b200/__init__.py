@@ -166,6 +166,8 @@ SIGNATURES = {
         ("trsm", _TRSM_64), ("trsm_batched", _TRSM_B_64), ("trsm_strided_batched", _TRSM_SB_64),
         ("trmm", _TRMM_64), ("trmm_batched", _TRMM_B_64), ("trmm_strided_batched", _TRMM_SB_64),
         ("trsv", _TRSV_64), ("trsv_batched", _TRSV_B_64), ("trsv_strided_batched", _TRSV_SB_64))},
+    **{f"rocblas_{t}{name}": (_i, sig) for t in "cz" for name, sig in (
+        ("trtri", _TRTRI), ("trtri_batched", _TRTRI_B), ("trtri_strided_batched", _TRTRI_SB))},
     "rocblas_strtri": (_i, _TRTRI),
     "rocblas_dtrtri": (_i, _TRTRI),
     "rocblas_strtri_batched": (_i, _TRTRI_B),

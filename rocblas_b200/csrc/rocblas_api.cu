@@ -761,12 +761,48 @@ struct TrtriRec
 };
 
 template <typename T>
+__global__ void set_unit_diagonal_kernel(BatchPtr<T> X, int64_t ld, int n, int batch_base)
+{
+    T*        x = X.get(batch_base + blockIdx.y);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n)
+        x[i + (int64_t)i * ld] = T(1);
+}
+
+template <typename T>
 rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag, int n,
                           const void* Aptr, BatchPtr<T> A, int lda, const void* Xptr,
                           BatchPtr<T> X, int ldinv, int batch)
 {
     if(!h)
         return rocblas_status_invalid_handle;
+    if constexpr(is_cplx<T>::value)
+    {
+        // complex: inv(A) is the solution of A X = I, by the complex solve on invA itself (the
+        // opposite triangle of the solution is exactly zero, as rocblas_trtri_fill leaves it).
+        // Unlike the reference's fused kernel a zero non-unit diagonal is not read as 1.
+        rocblas_status st = trtri_arg_check(uplo, diag, n, Aptr, lda, Xptr, ldinv, batch);
+        if(h->size_query)
+            return rocblas_status_size_unchanged;
+        if(st != rocblas_status_continue)
+            return st;
+        if((st = device_ready(h)) != rocblas_status_success)
+            return st;
+        zero_fill<T>(X, ldinv, n, n, batch, h->stream);
+        for(int b0 = 0; b0 < batch; b0 += kMaxGridYZ)
+        {
+            dim3 grid((unsigned)ceil_div(n, 256), (unsigned)std::min(kMaxGridYZ, batch - b0));
+            set_unit_diagonal_kernel<T><<<grid, 256, 0, h->stream>>>(X, ldinv, n, b0);
+            count_launch();
+        }
+        static const T             one = T(1);
+        const rocblas_pointer_mode mode = h->pointer_mode;
+        h->pointer_mode                 = rocblas_pointer_mode_host;
+        st = trsm_impl_64<T>(h, rocblas_side_left, uplo, rocblas_operation_none, diag, n, n, &one, Aptr, A,
+                             lda, Xptr, X, ldinv, batch, nullptr, BatchPtr<T>{}, 0);
+        h->pointer_mode = mode;
+        return st;
+    }
     const size_t ws_bytes = trtri_workspace_bytes<T>(n, std::max(batch, 0));
     if(h->size_query)
     {
@@ -2498,5 +2534,48 @@ catch(...)
 {
     return exception_status();
 }
+
+#define TRTRI_CPLX(S, TA, T)                                                                       \
+    rocblas_status rocblas_##S##trtri(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag,   \
+                                      rocblas_int n, const TA* A, rocblas_int lda, TA* invA,        \
+                                      rocblas_int ldinvA)                                           \
+    try                                                                                             \
+    {                                                                                               \
+        return trtri_impl<T>(h, uplo, diag, n, A, strided<T>(as_impl<T>(A), 0), lda, invA,          \
+                             strided<T>(as_impl<T>(invA), 0), ldinvA, 1);                          \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trtri_batched(rocblas_handle h, rocblas_fill uplo,                  \
+                                              rocblas_diagonal diag, rocblas_int n,                 \
+                                              const TA* const A[], rocblas_int lda,                 \
+                                              TA* const invA[], rocblas_int ldinvA,                 \
+                                              rocblas_int batch_count)                              \
+    try                                                                                             \
+    {                                                                                               \
+        return trtri_impl<T>(h, uplo, diag, n, A, arrayed<T>(A), lda, invA, arrayed<T>(invA),       \
+                             ldinvA, batch_count);                                                  \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }                                                                                               \
+    rocblas_status rocblas_##S##trtri_strided_batched(                                              \
+        rocblas_handle h, rocblas_fill uplo, rocblas_diagonal diag, rocblas_int n, const TA* A,     \
+        rocblas_int lda, rocblas_stride stride_a, TA* invA, rocblas_int ldinvA,                     \
+        rocblas_stride stride_invA, rocblas_int batch_count)                                        \
+    try                                                                                             \
+    {                                                                                               \
+        return trtri_impl<T>(h, uplo, diag, n, A, strided<T>(as_impl<T>(A), stride_a), lda, invA,   \
+                             strided<T>(as_impl<T>(invA), stride_invA), ldinvA, batch_count);      \
+    }                                                                                               \
+    catch(...)                                                                                      \
+    {                                                                                               \
+        return exception_status();                                                                  \
+    }
+TRTRI_CPLX(c, rocblas_float_complex, cplx<float>)
+TRTRI_CPLX(z, rocblas_double_complex, cplx<double>)
 
 } // extern "C"

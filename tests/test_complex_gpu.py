@@ -199,3 +199,46 @@ def test_complex_gemm_entry(handle, dt):
         torch.cuda.synchronize()
         got = dm.to_host(dC)
         assert np.max(np.abs(got - ref)) <= 8 * eps * k * 4, (ta, tb)
+
+
+@pytest.mark.parametrize("dt", ["z", "c"])
+@pytest.mark.parametrize("uplo,diag", list(itertools.product("UL", "NU")))
+def test_complex_trtri(handle, dt, uplo, diag):
+    """rocblas_{c,z}trtri: inv(A) with zeros in the opposite triangle, plain and strided batch."""
+    npdt, tdt = DT[dt]
+    eps = np.finfo(npdt).eps
+
+    def triangle(A, n):
+        Tc = np.nan_to_num(np.array(A[:n, :n], dtype=np.complex128))
+        Tc = np.tril(Tc) if uplo == "L" else np.triu(Tc)
+        if diag == "U":
+            np.fill_diagonal(Tc, 1.0)
+        return Tc
+
+    for n in (70, 300):
+        A, _ = oracle.nan_triangle_problem(90 + n, "L", uplo, "N", diag, n, 1, n + 1, n, npdt)
+        T = triangle(A, n)
+        dA = dm.to_device(A)
+        inv = dm.to_device(np.full((n + 2, n), np.nan, dtype=npdt, order="F"))
+        st = getattr(rb.lib(), f"rocblas_{dt}trtri")(handle.value, rb.UPLO[uplo], rb.DIAG[diag], n,
+                                                     _ptr(dA), A.shape[0], _ptr(inv), n + 2)
+        assert st == 0
+        torch.cuda.synchronize()
+        X = dm.to_host(inv)
+        assert np.isnan(X[n:]).all()
+        Xn = X[:n].astype(np.complex128)
+        opp = np.triu(Xn, 1) if uplo == "L" else np.tril(Xn, -1)
+        assert np.all(opp == 0)
+        assert np.max(np.abs(Xn @ T - np.eye(n))) <= 64 * eps * n
+    # strided batch of two
+    n, batch = 200, 2
+    probs = [oracle.nan_triangle_problem(95 + b, "L", uplo, "N", diag, n, 1, n, n, npdt)[0] for b in range(batch)]
+    dA = torch.cat([dm.to_device(A).reshape(-1) for A in probs])
+    inv = torch.zeros(batch * n * n, dtype=tdt, device="cuda")
+    st = getattr(rb.lib(), f"rocblas_{dt}trtri_strided_batched")(handle.value, rb.UPLO[uplo], rb.DIAG[diag], n,
+                                                                 _ptr(dA), n, n * n, _ptr(inv), n, n * n, batch)
+    assert st == 0
+    torch.cuda.synchronize()
+    for b, A in enumerate(probs):
+        Xb = inv[b * n * n:(b + 1) * n * n].view(n, n).cpu().numpy().T.astype(np.complex128)
+        assert np.max(np.abs(Xb @ triangle(A, n) - np.eye(n))) <= 64 * eps * n
