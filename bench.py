@@ -550,7 +550,7 @@ def run_ours(args):
         one_h = ctypes.c_double(1.0)
 
         def e2e_step():
-            # the host-buffer entry point: A's triangle in panels, the solve and the rows of X
+            # the host-buffer entry point: A's block rows and B's rows, the solve and the rows of X
             # coming back overlap inside the call
             st = L.rocblas_b200_dtrsm_mixed_host(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
                                                  rb.diagonal_non_unit, M, N, ctypes.byref(one_h),
@@ -569,15 +569,17 @@ def run_ours(args):
         s1.record(stream)
         torch.cuda.synchronize(dev)
         e2e_ms = s0.elapsed_time(s1) / ksteps
-        # bytes the call moves: B, and A's lower triangle in panels of 512 columns (each panel:
-        # its columns, rows from its diagonal block down)
-        pw = 512
-        a_h2d = sum((M - c0) * (min(M, c0 + pw) - c0) for c0 in range(0, M, pw)) * 8
+        # bytes the call moves: B, and A's lower triangle in block rows of host_step_blocks x 128
+        # rows (each block row: its rows, the columns from 0 to the end of its diagonal block)
+        step_blocks = ctypes.c_int()
+        assert L.rocblas_b200_get_tuning(b"host_step_blocks", ctypes.byref(step_blocks)) == 0
+        pw = 128 * step_blocks.value
+        a_h2d = sum((min(M, r0 + pw) - r0) * min(M, r0 + pw) for r0 in range(0, M, pw)) * 8
         e2e = {"value": FLOPS / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(a_h2d + B0.numel() * 8),
                "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms,
                "form": f"precision form, {S} slices, rocblas_b200_dtrsm_mixed_host on pinned host "
-                       "buffers (transfers of A's triangle and of X overlap the solve)"}
+                       "buffers (transfers of A's block rows, of B and of X overlap the left-looking solve)"}
         del A_host, B_host
 
     # ---- errors per condition band against the float128 / FP64 host oracles, CPU baseline -------

@@ -274,11 +274,12 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
 /* ---- precision form with A and B in host memory -----------------------------------------------
  * rocblas_b200_dtrsm_mixed for host buffers (pinned memory lets the copies overlap the solve):
  * A (lda x k) and B (ldb x n) are host pointers, alpha a host value whatever the handle's
- * pointer mode, and the call returns when B holds X.  For side left the transfer of A's
- * triangle (in 512-column panels, in the order the solve consumes them), the solve and the
- * transfer of finished rows of X back to B overlap on the handle's stream and two internal
- * streams; side right copies first and then solves.  Of A only the referenced triangle (with
- * the diagonal 512 x 512 blocks) is transferred.  The device copies of A
+ * pointer mode, and the call returns when B holds X.  For side left the solve runs
+ * left-looking over steps of rows (tuning key host_step_blocks, in 128-row blocks), and the
+ * transfer of each step's rows of B and block row of op(A), the solve and the transfer of
+ * finished rows of X back to B overlap on the handle's stream and three internal streams;
+ * side right copies first and then solves.  Of A only the referenced triangle (with the
+ * diagonal blocks of one step) is transferred.  The device copies of A
  * and B are kept by the handle between calls (freed by rocblas_destroy_handle). */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed_host(rocblas_handle    handle,
                                                             rocblas_side      side,

@@ -1427,11 +1427,10 @@ namespace
 
 // The precision form with A and B in host memory: the call copies A's triangle and B to the
 // device, solves, and copies X back into B, returning when B holds X.  For side left the
-// three overlap: A's triangle goes over in 512-column panels in the order the solve consumes
-// them (each panel's 128-blocks inverted on a third stream as soon as it lands), the solve
-// runs right-looking over diagonal blocks so that each step needs only the panels that have
-// arrived, and each block of X rows goes back as soon as it is final.  Side right copies
-// everything first and then solves.
+// three overlap: the solve runs left-looking over steps of rows, and each step's rows of B and
+// block row of op(A) go over in solve order on a copy stream (its 128-blocks inverted on a
+// third stream as soon as they land), so a step waits only for its own data; each step's rows
+// of X go back as soon as they are final.  Side right copies everything first and then solves.
 rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                                     rocblas_operation trans, rocblas_diagonal diag, int m, int n,
                                     const double* alpha, const double* hA, int lda, double* hB,
@@ -1492,14 +1491,12 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
     pr.alpha.val = *alpha;
     const bool recursive = choose_algo(pr) == Algo::recursive;
 
-    // B arrives first (the updates below a diagonal block write rows of every later block)
-    cudaEvent_t eB = R.event(0);
-    if(!eB)
-        return rocblas_status_internal_error;
-    cudaMemcpy2DAsync(dB, (size_t)m * es, hB, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, R.in);
-
     if(!left || !recursive)
     {
+        cudaEvent_t eB = R.event(0);
+        if(!eB)
+            return rocblas_status_internal_error;
+        cudaMemcpy2DAsync(dB, (size_t)m * es, hB, (size_t)ldb * es, (size_t)m * es, n, cudaMemcpyHostToDevice, R.in);
         cudaMemcpy2DAsync(dA, (size_t)k * es, hA, (size_t)lda * es, (size_t)k * es, k, cudaMemcpyHostToDevice,
                           R.in);
         cudaEventRecord(eB, R.in);
@@ -1515,13 +1512,21 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
         cudaStreamSynchronize(h->stream);
         return launch_status();
     }
-    cudaEventRecord(eB, R.in);
 
-    // workspace of the solve: invA, slices, chain flags (as rocblas_b200_dtrsm_mixed)
+    // Left-looking over steps of DB = host_step_blocks 128-blocks of rows, in solve order.
+    // Every step needs only its own data: its rows of B and its block row of M = op(A) (the
+    // diagonal block and the solved side), so the solve starts as soon as the first block row
+    // has landed and then follows the transfer. B_q := alpha B_q - M_q X_solved is the one
+    // update of those rows (one sliced product of depth = the rows solved so far), so alpha
+    // goes to it (to the diagonal solve in the first step, which has no update).
+    const int    nblk      = (int)ceil_div(k, kInvNB);
+    const int    DB        = std::max(1, tuning().host_step_blocks);
+    const int    nstep     = (int)ceil_div(nblk, DB);
+    const bool   forward   = pr.oplower();
     const size_t inv_bytes = align256((size_t)kInvNB * k * sizeof(double));
-    const size_t sl_bytes  = mixed_slice_workspace_bytes(pr, slices);
+    const size_t sl_bytes  = sliced_gemm_workspace_bytes(std::min(k, DB * kInvNB), n, k, slices);
     const size_t ch_bytes  = mixed_chain_workspace_bytes(pr);
-    const size_t ws_bytes  = inv_bytes + sl_bytes + (ch_bytes ? (ch_bytes + 255) / 256 * 256 : 0);
+    const size_t ws_bytes  = inv_bytes + (sl_bytes + 255) / 256 * 256 + (ch_bytes + 255) / 256 * 256;
     int*         err       = ensure_err(h);
     void*        ws        = h->borrow(ws_bytes);
     if(!ws || !err)
@@ -1532,87 +1537,62 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
     inv.stride = (int64_t)kInvNB * k;
     pr.invA    = inv;
 
-    // A in panels of PB = 4 128-blocks (512 columns: little of the unused triangle travels
-    // with the diagonal blocks), in solve order; M = op(A), so a panel of M's columns is a
-    // panel of A's columns (trans N) or rows (trans T); the rows it needs are the ones below
-    // its diagonal block (forward solve) or above it (backward)
-    const int  nblk    = (int)ceil_div(k, kInvNB);
-    const int  PB      = 4;
-    const int  npanel  = (int)ceil_div(nblk, PB);
-    const bool forward = pr.oplower();
-    for(int q = 0; q < npanel; ++q)
-    {
-        const int p  = forward ? q : npanel - 1 - q;
-        const int c0 = p * PB * kInvNB, c1 = std::min(k, (p + 1) * PB * kInvNB);
-        const int i0 = forward ? c0 : 0, i1 = forward ? k : c1;
-        if(!pr.trans)
-            cudaMemcpy2DAsync(dA + i0 + (int64_t)c0 * k, (size_t)k * es, hA + i0 + (int64_t)c0 * lda,
-                              (size_t)lda * es, (size_t)(i1 - i0) * es, c1 - c0, cudaMemcpyHostToDevice, R.in);
-        else
-            cudaMemcpy2DAsync(dA + c0 + (int64_t)i0 * k, (size_t)k * es, hA + c0 + (int64_t)i0 * lda,
-                              (size_t)lda * es, (size_t)(c1 - c0) * es, i1 - i0, cudaMemcpyHostToDevice, R.in);
-        // the panel's diagonal 128-blocks, inverted on their own stream as soon as they land (the
-        // copy stream goes on with the next panel)
-        cudaEvent_t ec = R.event(1 + npanel + p);
-        if(!ec)
-            return rocblas_status_internal_error;
-        cudaEventRecord(ec, R.in);
-        cudaStreamWaitEvent(R.tri, ec, 0);
-        TrtriParams<double> t{};
-        t.k                = c1 - c0;
-        t.nb               = kInvNB;
-        t.A                = pr.A.shifted(c0 + (int64_t)c0 * k);
-        t.lda              = k;
-        t.inv              = inv.shifted((int64_t)(c0 / kInvNB) * kInvNB * kInvNB);
-        t.ldinv            = kInvNB;
-        t.inv_block_stride = (int64_t)kInvNB * kInvNB;
-        t.upper            = pr.upper;
-        t.unit             = pr.unit;
-        launch_trtri<double>(t, (int)ceil_div(c1 - c0, kInvNB), 1, R.tri);
-        count_launch();
-        cudaEvent_t e = R.event(1 + p);
-        if(!e)
-            return rocblas_status_internal_error;
-        cudaEventRecord(e, R.tri);
-    }
-    cudaStreamWaitEvent(h->stream, eB, 0);
-
     MixedRecursive rec{{pr, k, nblk}};
     rec.S        = slices;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
     rec.err_dev  = err;
     if(ch_bytes)
         rec.chain_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes + (sl_bytes + 255) / 256 * 256;
-    // Right-looking over diagonal blocks of the recursion's leaf size (mixed_chain_blocks x 128
-    // rows): solve a diagonal block as soon as its panels of A have landed, send its rows of X
-    // home, and update every row not yet solved with them (one sliced product of depth = the
-    // block), so that the solve follows the transfer of A instead of waiting for all of it.
-    // alpha is applied by the first diagonal solve and the first update, which between them
-    // touch every row once.
-    const int DB    = std::max(1, tuning().mixed_chain_blocks);
-    const int ndiag = (int)ceil_div(nblk, DB);
-    size_t    nout  = 0;
-    for(int q = 0; q < ndiag && rec.ok; ++q)
+    for(int q = 0; q < nstep && rec.ok; ++q)
     {
-        const int d = forward ? q : ndiag - 1 - q;
+        const int d  = forward ? q : nstep - 1 - q;
         const int b0 = d * DB, b1 = std::min(nblk, b0 + DB);
-        for(int p = b0 / PB; p <= (b1 - 1) / PB; ++p)
-            cudaStreamWaitEvent(h->stream, R.event(1 + p), 0);
-        const int first = q == 0 ? 1 : 0;
+        const int r0 = rec.row_of(b0), r1 = rec.row_of(b1);
+        // the block row of M: columns [0, r1) (forward) or [r0, k) (backward); rows of A for
+        // trans N, columns of A for trans T
+        const int c0 = forward ? 0 : r0, c1 = forward ? r1 : k;
+        cudaEvent_t ea = R.event(3 * (size_t)q), et = R.event(3 * (size_t)q + 1), ex = R.event(3 * (size_t)q + 2);
+        if(!ea || !et || !ex)
+            return rocblas_status_internal_error;
+        cudaMemcpy2DAsync(dB + r0, (size_t)m * es, hB + r0, (size_t)ldb * es, (size_t)(r1 - r0) * es, n,
+                          cudaMemcpyHostToDevice, R.in);
+        if(!pr.trans)
+            cudaMemcpy2DAsync(dA + r0 + (int64_t)c0 * k, (size_t)k * es, hA + r0 + (int64_t)c0 * lda,
+                              (size_t)lda * es, (size_t)(r1 - r0) * es, c1 - c0, cudaMemcpyHostToDevice, R.in);
+        else
+            cudaMemcpy2DAsync(dA + c0 + (int64_t)r0 * k, (size_t)k * es, hA + c0 + (int64_t)r0 * lda,
+                              (size_t)lda * es, (size_t)(c1 - c0) * es, r1 - r0, cudaMemcpyHostToDevice, R.in);
+        cudaEventRecord(ea, R.in);
+
+        // the step's diagonal 128-blocks, inverted on their own stream while the update runs
+        cudaStreamWaitEvent(R.tri, ea, 0);
+        TrtriParams<double> t{};
+        t.k                = r1 - r0;
+        t.nb               = kInvNB;
+        t.A                = pr.A.shifted(r0 + (int64_t)r0 * k);
+        t.lda              = k;
+        t.inv              = inv.shifted((int64_t)b0 * kInvNB * kInvNB);
+        t.ldinv            = kInvNB;
+        t.inv_block_stride = (int64_t)kInvNB * kInvNB;
+        t.upper            = pr.upper;
+        t.unit             = pr.unit;
+        launch_trtri<double>(t, b1 - b0, 1, R.tri);
+        count_launch();
+        cudaEventRecord(et, R.tri);
+
+        cudaStreamWaitEvent(h->stream, ea, 0);
+        int first = 1;
+        if(forward && r0 > 0)
+            rec.update_sliced(r0, r1, 0, r0, 1), first = 0;
+        else if(!forward && r1 < k)
+            rec.update_sliced(r0, r1, r1, k, 1), first = 0;
+        cudaStreamWaitEvent(h->stream, et, 0);
         rec.solve_mixed(b0, b1, first);
         // rows [r0, r1) of X are final: send them home on the out stream
-        const int   r0 = rec.row_of(b0), r1 = rec.row_of(b1);
-        cudaEvent_t e  = R.event(1 + 2 * npanel + nout++);
-        if(!e)
-            return rocblas_status_internal_error;
-        cudaEventRecord(e, h->stream);
-        cudaStreamWaitEvent(R.out, e, 0);
+        cudaEventRecord(ex, h->stream);
+        cudaStreamWaitEvent(R.out, ex, 0);
         cudaMemcpy2DAsync(hB + r0, (size_t)ldb * es, dB + r0, (size_t)m * es, (size_t)(r1 - r0) * es, n,
                           cudaMemcpyDeviceToHost, R.out);
-        if(forward && r1 < k)
-            rec.update_sliced(r1, k, r0, r1, first);
-        else if(!forward && r0 > 0)
-            rec.update_sliced(0, r0, r0, r1, first);
     }
     cudaStreamSynchronize(R.out);
     cudaStreamSynchronize(h->stream);

@@ -34,6 +34,8 @@ struct Tuning
     int chain_w              = 0;    // chain strip width: 0 auto (32 or 64), 32, 64
     int mixed_chain_blocks   = 8;    // precision form: chain solves for diagonal blocks of <= this
                                      // many 128-row blocks (< 2: recursion down to the leaves)
+    int host_step_blocks     = 4;    // precision form on host buffers: rows per pipelined step,
+                                     // in 128-row blocks
 };
 
 struct TuningEntry
@@ -58,6 +60,7 @@ static const TuningEntry kTuningEntries[] = {
     {"chain_max_cols_f32", &Tuning::chain_max_cols_f32, 0, 1 << 30},
     {"chain_w", &Tuning::chain_w, 0, 64},
     {"mixed_chain_blocks", &Tuning::mixed_chain_blocks, 0, 1 << 20},
+    {"host_step_blocks", &Tuning::host_step_blocks, 1, 1 << 20},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

@@ -1,10 +1,11 @@
 """rocblas_b200_dtrsm_mixed_host: the precision form with A and B in host memory.
 
-The pipelined path (side left, recursive sizes) runs right-looking over diagonal blocks as A's
-panels arrive, so it groups the sliced updates differently from the device entry point
-rocblas_b200_dtrsm_mixed; it must meet the same error bound against the oracle and stay within
-the precision form's accuracy of the device result, for every side-left uplo/trans/diag
-combination (forward and backward solve orders, A's panels as columns or rows).  Side right
+The pipelined path (side left, recursive sizes) runs left-looking over steps of rows as their
+block rows of op(A) and rows of B arrive, so it groups the sliced updates differently from the
+device entry point rocblas_b200_dtrsm_mixed; it must meet the same error bound against the
+oracle and stay within the precision form's accuracy of the device result, for every side-left
+uplo/trans/diag combination (forward and backward solve orders, block rows copied as rows or
+columns of A) and for step sizes below, at and above the chain solve's limit.  Side right
 and small orders take the copy-then-solve path and match the device entry point bitwise.  The
 unused triangle of A is NaN in host memory and must not reach X.
 """
@@ -73,6 +74,27 @@ def test_host_path_matches_device_side_left(handle, uplo, trans, diag):
     assert err <= oracle.trsm_tolerance(np.float64, m)
     assert err <= 1e-12
     assert oracle.normwise_forward_error(got[:m], ref[:m]) <= 1e-12
+
+
+@pytest.mark.parametrize("step", [1, 3, 16])
+def test_host_path_step_sizes(handle, step):
+    """One step per 128-row block (FP64 updates only below 1024 solved rows), a ragged step
+    size, and steps of 16 blocks (each diagonal solve a recursion with its own sliced update)."""
+    L = rb.lib()
+    old = ctypes.c_int()
+    assert L.rocblas_b200_get_tuning(b"host_step_blocks", ctypes.byref(old)) == 0
+    assert L.rocblas_b200_set_tuning(b"host_step_blocks", step) == 0
+    try:
+        m, n = 4700, 70
+        for uplo, trans in (("L", "N"), ("L", "T")):
+            A, B = oracle.nan_triangle_problem(73, "L", uplo, trans, "N", m, n, m, m + 5, np.float64)
+            got = _run_host(handle, "L", uplo, trans, "N", m, n, 2.0, A, B)
+            assert np.isnan(got[m:]).all()
+            X = oracle.trsm("L", uplo, trans, "N", 2.0, A, np.asfortranarray(B[:m]))
+            assert oracle.matrix_norm_1(X, np.asfortranarray(got[:m])) <= 1e-12
+    finally:
+        L.rocblas_b200_set_tuning(b"host_step_blocks", old.value)
+    assert L.rocblas_b200_set_tuning(b"host_step_blocks", 0) == rb.status_invalid_value
 
 
 @pytest.mark.parametrize("side,m,n", [("R", 90, 1300), ("L", 300, 40)])
