@@ -654,7 +654,9 @@ def run_ours(args):
         extra = {
             "roofline": roofline,
             "plain_fp64": {"value": plain_value, "unit": "TFLOP/s", "ms_per_step": p_total / args.steps,
-                           "solve_ms_median": med_plain, "frac_of_fp64_peak": plain_value / peak,
+                           "solve_ms_median": med_plain,
+                           "solve_ms_p99": float(np.percentile(p_solve, 99)),
+                           "frac_of_fp64_peak": plain_value / peak,
                            "gpu_launches": int(p_launches), "roofline": plain_roofline},
             "precision_vs_plain": value / plain_value,
             "cpu_baseline": {"value": cpu[0], "unit": "TFLOP/s", "cores": threads, "kind": "reference",
@@ -665,6 +667,8 @@ def run_ours(args):
             "error_sample": "normwise ||X - X*||_F / ||X*||_F on right-hand sides 0..7; X* = float128 "
                             "oracle; bands: diagonal 10^(-k i/m)",
             "solve_ms_median": med_mixed,
+            "solve_ms_p99": float(np.percentile(solve_ms, 99)),
+            "solve_ms_samples": len(solve_ms),
         }
 
     if rank == 0 and not args.no_extras:
