@@ -163,7 +163,7 @@ def tune(quick=False, out_dir=HERE):
 
     keys = ["block_max_k", "block_always_k", "block_min_strips_pct", "sliced_min_k",
             "dmma_big_tile_pct", "mixed_slices", "oz_bn", "oz_bk", "chain_max_cols",
-            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks"]
+            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks", "host_step_blocks"]
     with open(os.path.join(out_dir, "tuning.cfg"), "w") as f:
         f.write("# written by rocblas_b200/autotune.py on " + report["device"] + "\n")
         for k in keys:

@@ -76,10 +76,14 @@ def test_host_path_matches_device_side_left(handle, uplo, trans, diag):
     assert oracle.normwise_forward_error(got[:m], ref[:m]) <= 1e-12
 
 
-@pytest.mark.parametrize("step", [1, 3, 16])
+@pytest.mark.parametrize("step", [1, 3, "above_chain"])
 def test_host_path_step_sizes(handle, step):
-    """One step per 128-row block (FP64 updates only below 1024 solved rows), a ragged step
-    size, and steps of 16 blocks (each diagonal solve a recursion with its own sliced update)."""
+    """One step per 128-row block, a ragged step size, and steps of more blocks than the chain
+    solve takes (each step's diagonal solve then recurses with a sliced update of its own)."""
+    if step == "above_chain":
+        mcb = ctypes.c_int()
+        assert rb.lib().rocblas_b200_get_tuning(b"mixed_chain_blocks", ctypes.byref(mcb)) == 0
+        step = max(mcb.value, 1) + 4
     L = rb.lib()
     old = ctypes.c_int()
     assert L.rocblas_b200_get_tuning(b"host_step_blocks", ctypes.byref(old)) == 0
