@@ -703,7 +703,8 @@ def run_case(args):
     """One kernel on one small shape, a few launches, for ncu captures (no JSON line):
     sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
-    m x n (the chain solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
+    m x n (the chain solve); strsm: rocblas_strsm L/L/N/N m x n (FP32: the recursive solve with
+    FFMA tile updates above 512 columns); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
     variable-size batch recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
     trtri: rocblas_dtrtri_strided_batched, --count lower m x m blocks."""
     import torch
@@ -728,6 +729,15 @@ def run_case(args):
             st = L.rocblas_dtrsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
                                  rb.diagonal_non_unit, m, n, po, ctypes.c_void_p(At.data_ptr()), m,
                                  ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+    elif args.case == "strsm":
+        At, Bt = workloads.condition_band_lower_torch(m, n, 0, seed=5, device=dev, dtype=torch.float32)
+        one_f = ctypes.c_float(1.0)
+
+        def run():
+            st = L.rocblas_strsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
+                                 rb.diagonal_non_unit, m, n, ctypes.cast(ctypes.byref(one_f), ctypes.c_void_p),
+                                 ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(Bt.data_ptr()), m)
             assert st == 0, st
     elif args.case == "vbatched":
         w = vbatched_workload(torch, dev, args.count, 2024, "d")
@@ -809,7 +819,7 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and serving sections (profiling runs)")
-    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "vbatched", "strided", "trtri"],
+    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "strsm", "vbatched", "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,
