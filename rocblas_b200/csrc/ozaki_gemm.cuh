@@ -545,7 +545,7 @@ __host__ __device__ constexpr int oz_swizzle_chunk(int o, int c)
 }
 
 template <int BK>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     oz_slice_kernel(const double* src, int64_t so, int64_t sk, int O, int K, const int* exps, int S,
                     int8_t* dst, int O_pad, int K_pad)
 {
@@ -553,13 +553,26 @@ __global__ void __launch_bounds__(256)
     const int o0 = blockIdx.y * kOzSliceTile, k0 = blockIdx.x * kOzSliceTile;
     const int tid = threadIdx.x;
     const bool o_fast = so == 1;
-    for(int idx = tid; idx < kOzSliceTile * kOzSliceTile; idx += 256)
+    // all 16 loads of a thread are issued before the first shared-memory store, so that a CTA
+    // has its whole 32 KB tile in flight at once
+    constexpr int kLoads = kOzSliceTile * kOzSliceTile / 256;
+    double        ld[kLoads];
+#pragma unroll
+    for(int it = 0; it < kLoads; ++it)
     {
-        int oo, kk;
-        if(o_fast) { oo = idx % kOzSliceTile; kk = idx / kOzSliceTile; }
-        else       { kk = idx % kOzSliceTile; oo = idx / kOzSliceTile; }
+        const int idx = tid + it * 256;
+        const int oo  = o_fast ? idx % kOzSliceTile : idx / kOzSliceTile;
+        const int kk  = o_fast ? idx / kOzSliceTile : idx % kOzSliceTile;
         const int o = o0 + oo, k = k0 + kk;
-        tile[oo][kk] = (o < O && k < K) ? src[(int64_t)o * so + (int64_t)k * sk] : 0.0;
+        ld[it] = (o < O && k < K) ? src[(int64_t)o * so + (int64_t)k * sk] : 0.0;
+    }
+#pragma unroll
+    for(int it = 0; it < kLoads; ++it)
+    {
+        const int idx = tid + it * 256;
+        const int oo  = o_fast ? idx % kOzSliceTile : idx / kOzSliceTile;
+        const int kk  = o_fast ? idx / kOzSliceTile : idx % kOzSliceTile;
+        tile[oo][kk]  = ld[it];
     }
     __syncthreads();
     // each thread: one row oo, 16 consecutive k (4 words of 4 int8) -> 256 threads = 64 x 64
