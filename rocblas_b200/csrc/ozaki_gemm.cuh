@@ -502,8 +502,10 @@ __global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, in
     const int k0 = blockIdx.y * kOzExpChunk;
     if(w >= O)
         return;
-    double mx = 0.0;
-    for(int k = k0 + lane; k < min(K, k0 + kOzExpChunk); k += 32)
+    double    mx   = 0.0;
+    const int kend = min(K, k0 + kOzExpChunk);
+#pragma unroll 8
+    for(int k = k0 + lane; k < kend; k += 32)
         mx = fmax(mx, fabs(src[(int64_t)w * so + (int64_t)k * sk]));
 #pragma unroll
     for(int off = 16; off; off >>= 1)
@@ -520,8 +522,12 @@ __global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, in
     const int k0 = blockIdx.y * kOzExpChunk;
     if(o >= O)
         return;
-    double mx = 0.0;
-    for(int k = k0; k < min(K, k0 + kOzExpChunk); ++k)
+    // unrolled so that 16 loads are in flight per thread (the maximum does not depend on the
+    // order it is taken in, so the exponents are the same)
+    double    mx   = 0.0;
+    const int kend = min(K, k0 + kOzExpChunk);
+#pragma unroll 16
+    for(int k = k0; k < kend; ++k)
         mx = fmax(mx, fabs(src[o + (int64_t)k * sk]));
     oz_merge_exp(exps, o, mx);
 }
