@@ -58,6 +58,7 @@ status_size_query_mismatch = 8
 status_size_increased = 9
 status_size_unchanged = 10
 status_invalid_value = 11
+status_check_numerics_fail = 13
 
 SIDE = {"L": side_left, "R": side_right}
 UPLO = {"U": fill_upper, "L": fill_lower}

@@ -11,6 +11,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
 #include <cuda_runtime.h>
 
 #include "../../include/rocblas.h"
@@ -40,6 +41,13 @@ struct _rocblas_handle
 
     // streams, events and device buffers of the host-buffer entry points (lazily created)
     struct HostPathRes* host_res = nullptr;
+
+    // ROCBLAS_LAYER and ROCBLAS_CHECK_NUMERICS as read at creation, and the log streams
+    int   layer_mode     = 0;
+    int   check_numerics = 0;
+    FILE* log_trace_os   = nullptr;
+    FILE* log_bench_os   = nullptr;
+    FILE* log_profile_os = nullptr;
 
     // rounding of every workspace request (handle.hpp:56-61)
     static size_t roundup(size_t s) { return (s + 63) / 64 * 64; }

@@ -6,12 +6,16 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <new>
+#include <string>
 #include <type_traits>
 #include <vector>
 
 #include "../../include/rocblas_b200_ext.h"
+#include "check_numerics.cuh"
+#include "layer_log.hpp"
 #include "sliced_driver.cuh"
 #include "trsm_driver.cuh"
 #include "server.cuh"
@@ -584,15 +588,128 @@ struct ChunkStatus
 };
 
 template <typename T>
+constexpr char prec_letter()
+{
+    return std::is_same<T, float>::value ? 's' : std::is_same<T, double>::value ? 'd'
+         : std::is_same<T, cplx<float>>::value ? 'c' : 'z';
+}
+
+// alpha's value for the log lines (read from the device in device pointer mode; NaN if null)
+template <typename T>
+void log_alpha(rocblas_handle h, const T* alpha, double* re, double* im)
+{
+    *re = *im = std::numeric_limits<double>::quiet_NaN();
+    if(!alpha)
+        return;
+    T v;
+    if(h->pointer_mode == rocblas_pointer_mode_device)
+    {
+        if(cudaMemcpyAsync(&v, alpha, sizeof(T), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess
+           || cudaStreamSynchronize(h->stream) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return;
+        }
+    }
+    else
+        v = *alpha;
+    if constexpr(is_cplx<T>::value)
+    {
+        *re = (double)v.x;
+        *im = (double)v.y;
+    }
+    else
+    {
+        *re = (double)v;
+        *im = 0.0;
+    }
+}
+
+int* ensure_err(rocblas_handle h);
+
+// Check-numerics of A's referenced triangle (inputs only) and of B; the name is the entry
+// point's, as in the log lines.
+template <typename T>
+rocblas_status trsm_check_numerics(rocblas_handle h, const TrsmLogInfo& li, rocblas_side side,
+                                   rocblas_fill uplo, int64_t m, int64_t n, BatchPtr<T> A,
+                                   int64_t lda, BatchPtr<T> B, int64_t ldb, int64_t batch,
+                                   bool is_input)
+{
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if(cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return rocblas_status_internal_error;
+    }
+    if(cap != cudaStreamCaptureStatusNone)
+        return rocblas_status_success;
+    int* err = ensure_err(h);
+    if(!err)
+        return rocblas_status_memory_error;
+    // the flags word sits beside the bounded-wait error word, in the same 256-byte allocation
+    unsigned* flags_dev = reinterpret_cast<unsigned*>(err) + 32;
+    const char* kinds[3] = {"", "batched_", "strided_batched_"};
+    std::string name = std::string("rocblas_") + kinds[li.kind] + prec_letter<T>() + "trsm";
+    if(li.ilp64)
+        name += "_64";
+    const int64_t k = side == rocblas_side_left ? m : n;
+    unsigned      fa = 0, fb = 0;
+    for(int64_t b0 = 0; b0 < batch; b0 += kIlpBatchChunk)
+    {
+        const int64_t nb = std::min(kIlpBatchChunk, batch - b0);
+        unsigned      f  = 0;
+        if(is_input)
+        {
+            if(!check_numerics_scan<T>(batch_advance(A, b0), lda, k, k, uplo == rocblas_fill_upper ? 2 : 1,
+                                       nb, flags_dev, h->stream, &f))
+                return launch_status();
+            fa |= f;
+        }
+        if(!check_numerics_scan<T>(batch_advance(B, b0), ldb, m, n, 0, nb, flags_dev, h->stream, &f))
+            return launch_status();
+        fb |= f;
+    }
+    if(is_input)
+    {
+        const rocblas_status st = check_numerics_report(name.c_str(), h->check_numerics, true, fa);
+        if(st != rocblas_status_success)
+            return st;
+    }
+    return check_numerics_report(name.c_str(), h->check_numerics, is_input, fb);
+}
+
+// li: the calling entry point (log lines and check-numerics); nullptr for the library's own
+// uses of the solve, which neither log nor check.
+template <typename T>
 rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                             rocblas_operation trans, rocblas_diagonal diag, int64_t m, int64_t n,
                             const T* alpha, const void* Aptr, BatchPtr<T> A, int64_t lda,
                             const void* Bptr, BatchPtr<T> B, int64_t ldb, int64_t batch,
                             const void* invA_ptr = nullptr, BatchPtr<T> invA = BatchPtr<T>{},
-                            int64_t invA_size = 0)
+                            int64_t invA_size = 0, const TrsmLogInfo* li = nullptr)
 {
     if(!h)
         return rocblas_status_invalid_handle;
+    // layer logging comes before the argument check (rocblas_trsm_imp.hpp:74-143)
+    if(li && h->layer_mode && !h->size_query)
+    {
+        TrsmLogCall c{};
+        c.info = *li;
+        c.prec = prec_letter<T>();
+        c.side = side;
+        c.uplo = uplo;
+        c.trans = trans;
+        c.diag = diag;
+        c.m = m;
+        c.n = n;
+        log_alpha<T>(h, alpha, &c.alpha_re, &c.alpha_im);
+        c.A = Aptr;
+        c.B = Bptr;
+        c.lda = lda;
+        c.ldb = ldb;
+        c.batch = batch;
+        write_trsm_log(h->layer_mode, h->log_trace_os, h->log_bench_os, h->log_profile_os, c);
+    }
     rocblas_status st
         = trsm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr, ldb, batch);
     if(st != rocblas_status_continue)
@@ -600,6 +717,17 @@ rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill up
     const bool left = side == rocblas_side_left;
     if((left ? m : n) > INT32_MAX)
         return rocblas_status_invalid_size;
+    // check-numerics of the inputs, after the host alpha == 0 quick return (which checks nothing)
+    const bool check = li && h->check_numerics && !h->size_query
+                       && !(h->pointer_mode == rocblas_pointer_mode_host && *alpha == T(0));
+    if(check)
+    {
+        if((st = device_ready(h)) != rocblas_status_success)
+            return st;
+        if((st = trsm_check_numerics<T>(h, *li, side, uplo, m, n, A, lda, B, ldb, batch, true))
+           != rocblas_status_success)
+            return st;
+    }
     const int64_t dim   = left ? n : m;
     const int64_t chunk = left ? kIlpColChunk : kIlpRowChunk;
     ChunkStatus   cs;
@@ -616,6 +744,13 @@ rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill up
             if(!cs.add(st))
                 return cs.st;
         }
+    }
+    if(check && (cs.st == rocblas_status_success || cs.st == rocblas_status_perf_degraded))
+    {
+        // the result (rocblas_trsm_imp.hpp:248-270)
+        st = trsm_check_numerics<T>(h, *li, side, uplo, m, n, A, lda, B, ldb, batch, false);
+        if(st != rocblas_status_success)
+            return st;
     }
     return cs.st;
 }
@@ -1633,6 +1768,19 @@ try
         ensure_err(h);
     }
     cudaGetLastError();
+    // the layer-logging and check-numerics modes of the handle (handle.cpp:856-877, 921-931)
+    if(const char* v = std::getenv("ROCBLAS_LAYER"))
+    {
+        h->layer_mode = (int)std::strtol(v, nullptr, 0);
+        if(h->layer_mode & kLayerTrace)
+            h->log_trace_os = layer_log_stream("ROCBLAS_LOG_TRACE_PATH");
+        if(h->layer_mode & kLayerBench)
+            h->log_bench_os = layer_log_stream("ROCBLAS_LOG_BENCH_PATH");
+        if(h->layer_mode & kLayerProfile)
+            h->log_profile_os = layer_log_stream("ROCBLAS_LOG_PROFILE_PATH");
+    }
+    if(const char* v = std::getenv("ROCBLAS_CHECK_NUMERICS"))
+        h->check_numerics = (int)std::strtol(v, nullptr, 0);
     *handle = h;
     return rocblas_status_success;
 }
@@ -1810,9 +1958,11 @@ bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
                         const TA* alpha, const TA* A, I lda, TA* B, I ldb)                        \
     try                                                                                          \
     {                                                                                            \
+        const TrsmLogInfo li{0, sizeof(I) == 8, 0, 0};                                           \
         return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
                                strided<T>(as_impl<T>(A), 0), lda, B,                             \
-                               strided<T>(as_impl<T>(B), 0), ldb, 1);                            \
+                               strided<T>(as_impl<T>(B), 0), ldb, 1, nullptr, BatchPtr<T>{}, 0,  \
+                               &li);                                                             \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
@@ -1826,8 +1976,10 @@ bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
                         I batch_count)                                                           \
     try                                                                                          \
     {                                                                                            \
+        const TrsmLogInfo li{1, sizeof(I) == 8, 0, 0};                                           \
         return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
-                               arrayed<T>(A), lda, B, arrayed<T>(B), ldb, batch_count);          \
+                               arrayed<T>(A), lda, B, arrayed<T>(B), ldb, batch_count, nullptr,  \
+                               BatchPtr<T>{}, 0, &li);                                           \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
@@ -1841,9 +1993,11 @@ bool rocblas_is_user_managing_device_memory(rocblas_handle handle)
                         I ldb, rocblas_stride stride_b, I batch_count)                           \
     try                                                                                          \
     {                                                                                            \
+        const TrsmLogInfo li{2, sizeof(I) == 8, stride_a, stride_b};                             \
         return trsm_impl_64<T>(h, side, uplo, trans, diag, m, n, as_impl<T>(alpha), A,           \
                                strided<T>(as_impl<T>(A), stride_a), lda, B,                      \
-                               strided<T>(as_impl<T>(B), stride_b), ldb, batch_count);           \
+                               strided<T>(as_impl<T>(B), stride_b), ldb, batch_count, nullptr,   \
+                               BatchPtr<T>{}, 0, &li);                                           \
     }                                                                                            \
     catch(...)                                                                                   \
     {                                                                                            \
@@ -1871,32 +2025,33 @@ rocblas_status rocblas_trsm_ex(rocblas_handle h, rocblas_side side, rocblas_fill
                                rocblas_datatype compute_type)
 try
 {
+    const TrsmLogInfo li{0, false, 0, 0};
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
         return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 strided<float>((const float*)A, 0), lda, B,
                                 strided<float>((float*)B, 0), ldb, 1, invA,
-                                strided<float>((const float*)invA, 0), invA_size);
+                                strided<float>((const float*)invA, 0), invA_size, &li);
     case rocblas_datatype_f64_r:
         return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  strided<double>((const double*)A, 0), lda, B,
                                  strided<double>((double*)B, 0), ldb, 1, invA,
-                                 strided<double>((const double*)invA, 0), invA_size);
+                                 strided<double>((const double*)invA, 0), invA_size, &li);
     case rocblas_datatype_f32_c:
         return trsm_impl_64<cplx<float>>(h, side, uplo, trans, diag, m, n,
                                          (const cplx<float>*)alpha, A,
                                          strided<cplx<float>>((const cplx<float>*)A, 0), lda, B,
                                          strided<cplx<float>>((cplx<float>*)B, 0), ldb, 1, invA,
                                          strided<cplx<float>>((const cplx<float>*)invA, 0),
-                                         invA_size);
+                                         invA_size, &li);
     case rocblas_datatype_f64_c:
         return trsm_impl_64<cplx<double>>(h, side, uplo, trans, diag, m, n,
                                           (const cplx<double>*)alpha, A,
                                           strided<cplx<double>>((const cplx<double>*)A, 0), lda, B,
                                           strided<cplx<double>>((cplx<double>*)B, 0), ldb, 1, invA,
                                           strided<cplx<double>>((const cplx<double>*)invA, 0),
-                                          invA_size);
+                                          invA_size, &li);
     default:
         return rocblas_status_not_implemented;
     }
@@ -1914,26 +2069,27 @@ rocblas_status rocblas_trsm_batched_ex(rocblas_handle h, rocblas_side side, rocb
                                        rocblas_int invA_size, rocblas_datatype compute_type)
 try
 {
+    const TrsmLogInfo li{1, false, 0, 0};
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
         return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 arrayed<float>(A), lda, B, arrayed<float>(B), ldb, batch_count,
-                                invA, arrayed<float>(invA), invA_size);
+                                invA, arrayed<float>(invA), invA_size, &li);
     case rocblas_datatype_f64_r:
         return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  arrayed<double>(A), lda, B, arrayed<double>(B), ldb, batch_count,
-                                 invA, arrayed<double>(invA), invA_size);
+                                 invA, arrayed<double>(invA), invA_size, &li);
     case rocblas_datatype_f32_c:
         return trsm_impl_64<cplx<float>>(h, side, uplo, trans, diag, m, n,
                                          (const cplx<float>*)alpha, A, arrayed<cplx<float>>(A), lda,
                                          B, arrayed<cplx<float>>(B), ldb, batch_count, invA,
-                                         arrayed<cplx<float>>(invA), invA_size);
+                                         arrayed<cplx<float>>(invA), invA_size, &li);
     case rocblas_datatype_f64_c:
         return trsm_impl_64<cplx<double>>(h, side, uplo, trans, diag, m, n,
                                           (const cplx<double>*)alpha, A, arrayed<cplx<double>>(A),
                                           lda, B, arrayed<cplx<double>>(B), ldb, batch_count, invA,
-                                          arrayed<cplx<double>>(invA), invA_size);
+                                          arrayed<cplx<double>>(invA), invA_size, &li);
     default:
         return rocblas_status_not_implemented;
     }
@@ -1954,30 +2110,31 @@ rocblas_status rocblas_trsm_strided_batched_ex(rocblas_handle h, rocblas_side si
                                                rocblas_datatype compute_type)
 try
 {
+    const TrsmLogInfo li{2, false, stride_A, stride_B};
     switch(compute_type)
     {
     case rocblas_datatype_f32_r:
         return trsm_impl_64<float>(h, side, uplo, trans, diag, m, n, (const float*)alpha, A,
                                 strided<float>((const float*)A, stride_A), lda, B,
                                 strided<float>((float*)B, stride_B), ldb, batch_count, invA,
-                                strided<float>((const float*)invA, stride_invA), invA_size);
+                                strided<float>((const float*)invA, stride_invA), invA_size, &li);
     case rocblas_datatype_f64_r:
         return trsm_impl_64<double>(h, side, uplo, trans, diag, m, n, (const double*)alpha, A,
                                  strided<double>((const double*)A, stride_A), lda, B,
                                  strided<double>((double*)B, stride_B), ldb, batch_count, invA,
-                                 strided<double>((const double*)invA, stride_invA), invA_size);
+                                 strided<double>((const double*)invA, stride_invA), invA_size, &li);
     case rocblas_datatype_f32_c:
         return trsm_impl_64<cplx<float>>(
             h, side, uplo, trans, diag, m, n, (const cplx<float>*)alpha, A,
             strided<cplx<float>>((const cplx<float>*)A, stride_A), lda, B,
             strided<cplx<float>>((cplx<float>*)B, stride_B), ldb, batch_count, invA,
-            strided<cplx<float>>((const cplx<float>*)invA, stride_invA), invA_size);
+            strided<cplx<float>>((const cplx<float>*)invA, stride_invA), invA_size, &li);
     case rocblas_datatype_f64_c:
         return trsm_impl_64<cplx<double>>(
             h, side, uplo, trans, diag, m, n, (const cplx<double>*)alpha, A,
             strided<cplx<double>>((const cplx<double>*)A, stride_A), lda, B,
             strided<cplx<double>>((cplx<double>*)B, stride_B), ldb, batch_count, invA,
-            strided<cplx<double>>((const cplx<double>*)invA, stride_invA), invA_size);
+            strided<cplx<double>>((const cplx<double>*)invA, stride_invA), invA_size, &li);
     default:
         return rocblas_status_not_implemented;
     }
