@@ -67,23 +67,24 @@ __device__ __forceinline__ unsigned num_flags(cplx<R> v)
     return num_flags_part(v.x) | num_flags_part(v.y) | (v.x == R(0) && v.y == R(0) ? kNumZero : 0u);
 }
 
-// rows x cols of every batch entry (blockIdx.z + batch_base); tri: 0 every element, 1 the lower
-// triangle (row >= col), 2 the upper one (row <= col). Column loop over gridDim.y.
+// rows x cols of every batch entry (blockIdx.z + batch_base), the launch covering the rows from
+// row0; tri: 0 every element, 1 the lower triangle (row >= col), 2 the upper one (row <= col).
+// Column loop over gridDim.y.
 template <typename T>
 __global__ void __launch_bounds__(256)
-    check_numerics_kernel(BatchPtr<T> A, int64_t lda, int rows, int cols, int tri, int batch_base,
-                          unsigned* flags)
+    check_numerics_kernel(BatchPtr<T> A, int64_t lda, int64_t row0, int64_t rows, int64_t cols,
+                          int tri, int batch_base, unsigned* flags)
 {
-    const int row   = blockIdx.x * 256 + threadIdx.x;
-    unsigned  local = 0;
+    const int64_t row   = row0 + (int64_t)blockIdx.x * 256 + threadIdx.x;
+    unsigned      local = 0;
     if(row < rows)
     {
         const T* a = A.get(batch_base + (int)blockIdx.z);
-        for(int col = blockIdx.y; col < cols; col += gridDim.y)
+        for(int64_t col = blockIdx.y; col < cols; col += gridDim.y)
         {
             if((tri == 1 && row < col) || (tri == 2 && row > col))
                 continue;
-            local |= num_flags(a[row + (int64_t)col * lda]);
+            local |= num_flags(a[row + col * lda]);
         }
     }
     local = __reduce_or_sync(0xffffffffu, local);
@@ -115,13 +116,19 @@ bool check_numerics_scan(BatchPtr<T> A, int64_t lda, int64_t rows, int64_t cols,
         return true;
     if(cudaMemsetAsync(flags_dev, 0, sizeof(unsigned), s) != cudaSuccess)
         return false;
-    const unsigned gx = (unsigned)((rows + 255) / 256);
-    const unsigned gy = (unsigned)std::min<int64_t>(cols, 1024);
-    for(int64_t b0 = 0; b0 < batch; b0 += 65535)
+    // rows in launches of at most 2^30 (grid x stays far below its limit); batch entries in
+    // launches of at most 65535 (grid z)
+    constexpr int64_t kRowChunk = int64_t(1) << 30;
+    const unsigned    gy        = (unsigned)std::min<int64_t>(cols, 1024);
+    for(int64_t r0 = 0; r0 < rows; r0 += kRowChunk)
     {
-        const unsigned gz = (unsigned)std::min<int64_t>(65535, batch - b0);
-        check_numerics_kernel<T><<<dim3(gx, gy, gz), 256, 0, s>>>(A, lda, (int)rows, (int)cols, tri,
-                                                                   (int)b0, flags_dev);
+        const unsigned gx = (unsigned)((std::min(kRowChunk, rows - r0) + 255) / 256);
+        for(int64_t b0 = 0; b0 < batch; b0 += 65535)
+        {
+            const unsigned gz = (unsigned)std::min<int64_t>(65535, batch - b0);
+            check_numerics_kernel<T><<<dim3(gx, gy, gz), 256, 0, s>>>(A, lda, r0, rows, cols, tri,
+                                                                       (int)b0, flags_dev);
+        }
     }
     if(cudaMemcpyAsync(flags, flags_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return false;
