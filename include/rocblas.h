@@ -125,6 +125,31 @@ typedef enum rocblas_pointer_mode_ /* rocblas-types.h:228-234 */
     rocblas_pointer_mode_device = 1
 } rocblas_pointer_mode;
 
+typedef enum rocblas_atomics_mode_ /* rocblas-types.h:239-245 */
+{
+    rocblas_atomics_not_allowed = 0,
+    rocblas_atomics_allowed     = 1
+} rocblas_atomics_mode;
+
+/* the bits of ROCBLAS_LAYER and ROCBLAS_CHECK_NUMERICS (rocblas-types.h:261-271, 321-338),
+ * read from the environment when a handle is created */
+typedef enum rocblas_layer_mode_
+{
+    rocblas_layer_mode_none        = 0x0,
+    rocblas_layer_mode_log_trace   = 0x1,
+    rocblas_layer_mode_log_bench   = 0x2,
+    rocblas_layer_mode_log_profile = 0x4
+} rocblas_layer_mode;
+
+typedef enum rocblas_check_numerics_mode_
+{
+    rocblas_check_numerics_mode_no_check     = 0x0,
+    rocblas_check_numerics_mode_info         = 0x1,
+    rocblas_check_numerics_mode_warn         = 0x2,
+    rocblas_check_numerics_mode_fail         = 0x4,
+    rocblas_check_numerics_mode_only_nan_inf = 0x8
+} rocblas_check_numerics_mode;
+
 /* ---- handle / stream / pointer mode: library/include/internal/rocblas-auxiliary.h:40-61 --- */
 ROCBLAS_EXPORT rocblas_status rocblas_create_handle(rocblas_handle* handle);
 ROCBLAS_EXPORT rocblas_status rocblas_destroy_handle(rocblas_handle handle);
@@ -134,6 +159,12 @@ ROCBLAS_EXPORT rocblas_status rocblas_set_pointer_mode(rocblas_handle       hand
                                                        rocblas_pointer_mode pointer_mode);
 ROCBLAS_EXPORT rocblas_status rocblas_get_pointer_mode(rocblas_handle        handle,
                                                        rocblas_pointer_mode* pointer_mode);
+/* rocblas-auxiliary.h:77-83: the TRSM path uses no atomics either way; the mode is kept and
+ * logged */
+ROCBLAS_EXPORT rocblas_status rocblas_set_atomics_mode(rocblas_handle       handle,
+                                                       rocblas_atomics_mode atomics_mode);
+ROCBLAS_EXPORT rocblas_status rocblas_get_atomics_mode(rocblas_handle        handle,
+                                                       rocblas_atomics_mode* atomics_mode);
 /* rocblas-auxiliary.h:97 */
 ROCBLAS_EXPORT rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr);
 

@@ -59,6 +59,7 @@ status_size_increased = 9
 status_size_unchanged = 10
 status_invalid_value = 11
 status_check_numerics_fail = 13
+atomics_not_allowed, atomics_allowed = 0, 1
 
 SIDE = {"L": side_left, "R": side_right}
 UPLO = {"U": fill_upper, "L": fill_lower}
@@ -126,6 +127,8 @@ SIGNATURES = {
     "rocblas_get_stream": (_i, [_H, ctypes.POINTER(_p)]),
     "rocblas_set_pointer_mode": (_i, [_H, _i]),
     "rocblas_get_pointer_mode": (_i, [_H, ctypes.POINTER(_i)]),
+    "rocblas_set_atomics_mode": (_i, [_H, _i]),
+    "rocblas_get_atomics_mode": (_i, [_H, ctypes.POINTER(_i)]),
     "rocblas_pointer_to_mode": (_i, [_p]),
     "rocblas_start_device_memory_size_query": (_i, [_H]),
     "rocblas_stop_device_memory_size_query": (_i, [_H, ctypes.POINTER(_sz)]),

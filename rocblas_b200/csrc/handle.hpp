@@ -45,6 +45,7 @@ struct _rocblas_handle
     // ROCBLAS_LAYER and ROCBLAS_CHECK_NUMERICS as read at creation, and the log streams
     int   layer_mode     = 0;
     int   check_numerics = 0;
+    int   atomics_mode   = 1; // rocblas_atomics_allowed, the reference's default
     FILE* log_trace_os   = nullptr;
     FILE* log_bench_os   = nullptr;
     FILE* log_profile_os = nullptr;

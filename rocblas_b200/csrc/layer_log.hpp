@@ -99,6 +99,12 @@ inline LayerProfile& layer_profile()
     return p;
 }
 
+// rocblas_atomics_mode as the logs print it (utility.hpp:380-383)
+inline const char* atomics_mode_string(int mode)
+{
+    return mode != 0 ? "atomics_allowed" : "atomics_not_allowed";
+}
+
 // letters of the enums (rocblas utility.hpp:264-306)
 inline char side_letter(int v) { return v == 141 ? 'L' : v == 142 ? 'R' : v == 143 ? 'B' : ' '; }
 inline char fill_letter(int v) { return v == 121 ? 'U' : v == 122 ? 'L' : v == 123 ? 'F' : ' '; }
@@ -124,6 +130,7 @@ struct TrsmLogCall
     double      alpha_re, alpha_im;
     const void *A, *B;
     int64_t     lda, ldb, batch;
+    bool        atomics; // the handle's atomics mode
 };
 
 inline void write_trsm_log(int layer_mode, FILE* trace_os, FILE* bench_os, FILE* profile_os,
@@ -154,7 +161,7 @@ inline void write_trsm_log(int layer_mode, FILE* trace_os, FILE* bench_os, FILE*
             os << ',' << c.info.stride_b;
         if(c.info.kind != 0)
             os << ',' << c.batch;
-        os << ",atomics_allowed";
+        os << ',' << atomics_mode_string(c.atomics);
         layer_log_line(trace_os, os.str());
     }
     if(layer_mode & kLayerBench)
@@ -176,12 +183,15 @@ inline void write_trsm_log(int layer_mode, FILE* trace_os, FILE* bench_os, FILE*
             os << " --stride_b " << c.info.stride_b;
         if(c.info.kind != 0)
             os << " --batch_count " << c.batch;
+        if(!c.atomics)
+            os << " --atomics_not_allowed";
         layer_log_line(bench_os, os.str());
     }
     if(layer_mode & kLayerProfile)
     {
         std::ostringstream os;
-        os << "rocblas_function: \"" << name << "\", atomics_mode: atomics_allowed, side: " << sl
+        os << "rocblas_function: \"" << name << "\", atomics_mode: " << atomics_mode_string(c.atomics)
+           << ", side: " << sl
            << ", uplo: " << ul << ", transA: " << tl << ", diag: " << dl << ", m: " << c.m
            << ", n: " << c.n << ", lda: " << c.lda;
         if(c.info.kind == 2)

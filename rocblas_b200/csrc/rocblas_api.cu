@@ -708,6 +708,7 @@ rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill up
         c.lda = lda;
         c.ldb = ldb;
         c.batch = batch;
+        c.atomics = h->atomics_mode != 0;
         write_trsm_log(h->layer_mode, h->log_trace_os, h->log_bench_os, h->log_profile_os, c);
     }
     rocblas_status st
@@ -1845,6 +1846,32 @@ rocblas_status rocblas_get_pointer_mode(rocblas_handle handle, rocblas_pointer_m
     if(!mode)
         return rocblas_status_invalid_pointer;
     *mode = handle->pointer_mode;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_atomics_mode(rocblas_handle handle, rocblas_atomics_mode mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(handle->layer_mode & kLayerTrace)
+        layer_log_line(handle->log_trace_os, std::string("rocblas_set_atomics_mode,")
+                                                 + atomics_mode_string(mode) + ","
+                                                 + atomics_mode_string(handle->atomics_mode));
+    handle->atomics_mode = mode;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_get_atomics_mode(rocblas_handle handle, rocblas_atomics_mode* mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!mode)
+        return rocblas_status_invalid_pointer;
+    *mode = (rocblas_atomics_mode)handle->atomics_mode;
+    if(handle->layer_mode & kLayerTrace)
+        layer_log_line(handle->log_trace_os, std::string("rocblas_get_atomics_mode,")
+                                                 + atomics_mode_string(*mode) + ","
+                                                 + atomics_mode_string(handle->atomics_mode));
     return rocblas_status_success;
 }
 

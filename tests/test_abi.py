@@ -122,6 +122,19 @@ def test_trtri_bad_args(handle):
     assert L.rocblas_dtrtri(handle.value, rb.fill_lower, rb.diagonal_unit, 4, None, 4, 1, 4) == rb.status_invalid_pointer
 
 
+def test_atomics_mode(handle):
+    """rocblas_set/get_atomics_mode (rocblas_auxiliary.cpp:87-117): allowed by default."""
+    L = rb.lib()
+    mode = ctypes.c_int(-1)
+    assert L.rocblas_get_atomics_mode(handle.value, ctypes.byref(mode)) == 0
+    assert mode.value == rb.atomics_allowed
+    assert L.rocblas_set_atomics_mode(handle.value, rb.atomics_not_allowed) == 0
+    assert L.rocblas_get_atomics_mode(handle.value, ctypes.byref(mode)) == 0
+    assert mode.value == rb.atomics_not_allowed
+    assert L.rocblas_set_atomics_mode(None, rb.atomics_allowed) == rb.status_invalid_handle
+    assert L.rocblas_get_atomics_mode(handle.value, None) == rb.status_invalid_pointer
+
+
 def test_handle_state(handle):
     L = rb.lib()
     mode = ctypes.c_int(-1)

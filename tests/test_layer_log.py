@@ -41,6 +41,8 @@ CHILD = textwrap.dedent(r"""
         == rb.status_invalid_size
     assert L.rocblas_trsm_ex(h, 141, 122, 111, 131, -1, 8, pa, A, 8, B, 8, None, 0,
                              rb.datatype_f64_r) == rb.status_invalid_size
+    assert L.rocblas_set_atomics_mode(h, rb.atomics_not_allowed) == 0
+    assert L.rocblas_dtrsm(h, 141, 122, 111, 131, -1, 8, pa, A, 8, B, 8) == rb.status_invalid_size
     assert L.rocblas_destroy_handle(h) == 0
 """)
 
@@ -78,7 +80,11 @@ def test_trace_and_bench_lines(tmp_path):
     assert trace[4] == "rocblas_ztrsm_64,L,L,C,N,-1,4,(1.5,-2),0x1000,4,0x2000,4,atomics_allowed"
     # rocblas_trsm_ex logs under the typed name, as the reference's shared implementation does
     assert trace[5] == trace[0]
-    assert len(trace) == 6
+    # the atomics mode: the set call's trace line (new mode, then the handle's old one), then
+    # the mode on the next call's line
+    assert trace[6] == "rocblas_set_atomics_mode,atomics_not_allowed,atomics_allowed"
+    assert trace[7] == trace[0].replace("atomics_allowed", "atomics_not_allowed")
+    assert len(trace) == 8
     bench = out["bench"]
     assert bench[0] == ("./rocblas-bench -f trsm -r f64_r --side L --uplo L --transposeA N --diag N "
                         "-m -1 -n 8 --alpha 0.5 --lda 8 --ldb 8")
@@ -89,6 +95,8 @@ def test_trace_and_bench_lines(tmp_path):
                         "--diag N -m -1 -n 4 --alpha 2 --lda 4 --ldb 4 --batch_count 5")
     assert bench[4] == ("./rocblas-bench --api 1 -f trsm -r f64_c --side L --uplo L --transposeA C "
                         "--diag N -m -1 -n 4 --alpha 1.5 --alphai -2 --lda 4 --ldb 4")
+    assert bench[6] == bench[0] + " --atomics_not_allowed"
+    assert len(bench) == 7
 
 
 def test_profile_counts_at_exit(tmp_path):
@@ -100,7 +108,10 @@ def test_profile_counts_at_exit(tmp_path):
                        'uplo: L, transA: N, diag: N, m: -1, n: 8, lda: 8, ldb: 8, call_count: 3 }')
     assert prof[1].startswith('- { rocblas_function: "rocblas_strided_batched_dtrsm"')
     assert prof[1].endswith("stride_A: 16, ldb: 4, stride_B: 64, batch_count: 3, call_count: 1 }")
-    assert len(prof) == 4
+    # the call with atomics not allowed is a distinct argument set
+    assert prof[4] == prof[0].replace("atomics_allowed", "atomics_not_allowed").replace("call_count: 3",
+                                                                                      "call_count: 1")
+    assert len(prof) == 5
 
 
 def test_no_layer_no_files(tmp_path):
