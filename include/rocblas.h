@@ -168,6 +168,47 @@ ROCBLAS_EXPORT rocblas_status rocblas_get_atomics_mode(rocblas_handle        han
 /* rocblas-auxiliary.h:97 */
 ROCBLAS_EXPORT rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr);
 
+/* ---- host <-> device copies: rocblas-auxiliary.h (set/get vector and matrix, the _async forms
+ * on a stream, the _64 forms with int64_t sizes); library/src/rocblas_auxiliary.cpp:305-790.
+ * n == 0 (rows == 0 or cols == 0) returns success; negative sizes, increments <= 0,
+ * elem_size <= 0, lda or ldb < rows or <= 0 return invalid_size; null pointers invalid_pointer. */
+ROCBLAS_EXPORT rocblas_status rocblas_set_vector(rocblas_int n, rocblas_int elem_size, const void* x_h, rocblas_int incx,
+                                              void* y_d, rocblas_int incy);
+ROCBLAS_EXPORT rocblas_status rocblas_set_vector_async(rocblas_int n, rocblas_int elem_size, const void* x_h,
+                                              rocblas_int incx, void* y_d, rocblas_int incy, cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_set_matrix(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_h,
+                                              rocblas_int lda, void* b_d, rocblas_int ldb);
+ROCBLAS_EXPORT rocblas_status rocblas_set_matrix_async(rocblas_int rows, rocblas_int cols, rocblas_int elem_size,
+                                              const void* a_h, rocblas_int lda, void* b_d, rocblas_int ldb,
+                                              cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_get_vector(rocblas_int n, rocblas_int elem_size, const void* x_d, rocblas_int incx,
+                                              void* y_h, rocblas_int incy);
+ROCBLAS_EXPORT rocblas_status rocblas_get_vector_async(rocblas_int n, rocblas_int elem_size, const void* x_d,
+                                              rocblas_int incx, void* y_h, rocblas_int incy, cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_get_matrix(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_d,
+                                              rocblas_int lda, void* b_h, rocblas_int ldb);
+ROCBLAS_EXPORT rocblas_status rocblas_get_matrix_async(rocblas_int rows, rocblas_int cols, rocblas_int elem_size,
+                                              const void* a_d, rocblas_int lda, void* b_h, rocblas_int ldb,
+                                              cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_set_vector_64(int64_t n, int64_t elem_size, const void* x_h, int64_t incx,
+                                              void* y_d, int64_t incy);
+ROCBLAS_EXPORT rocblas_status rocblas_set_vector_async_64(int64_t n, int64_t elem_size, const void* x_h,
+                                              int64_t incx, void* y_d, int64_t incy, cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_set_matrix_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_h,
+                                              int64_t lda, void* b_d, int64_t ldb);
+ROCBLAS_EXPORT rocblas_status rocblas_set_matrix_async_64(int64_t rows, int64_t cols, int64_t elem_size,
+                                              const void* a_h, int64_t lda, void* b_d, int64_t ldb,
+                                              cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_get_vector_64(int64_t n, int64_t elem_size, const void* x_d, int64_t incx,
+                                              void* y_h, int64_t incy);
+ROCBLAS_EXPORT rocblas_status rocblas_get_vector_async_64(int64_t n, int64_t elem_size, const void* x_d,
+                                              int64_t incx, void* y_h, int64_t incy, cudaStream_t stream);
+ROCBLAS_EXPORT rocblas_status rocblas_get_matrix_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_d,
+                                              int64_t lda, void* b_h, int64_t ldb);
+ROCBLAS_EXPORT rocblas_status rocblas_get_matrix_async_64(int64_t rows, int64_t cols, int64_t elem_size,
+                                              const void* a_d, int64_t lda, void* b_h, int64_t ldb,
+                                              cudaStream_t stream);
+
 /* ---- device memory: library/include/internal/rocblas-functions.h:25027-25122 ---------- */
 ROCBLAS_EXPORT rocblas_status rocblas_start_device_memory_size_query(rocblas_handle handle);
 ROCBLAS_EXPORT rocblas_status rocblas_stop_device_memory_size_query(rocblas_handle handle,

@@ -130,6 +130,22 @@ SIGNATURES = {
     "rocblas_set_atomics_mode": (_i, [_H, _i]),
     "rocblas_get_atomics_mode": (_i, [_H, ctypes.POINTER(_i)]),
     "rocblas_pointer_to_mode": (_i, [_p]),
+    "rocblas_set_vector": (_i, [_i, _i, _p, _i, _p, _i]),
+    "rocblas_set_vector_async": (_i, [_i, _i, _p, _i, _p, _i, _p]),
+    "rocblas_set_matrix": (_i, [_i, _i, _i, _p, _i, _p, _i]),
+    "rocblas_set_matrix_async": (_i, [_i, _i, _i, _p, _i, _p, _i, _p]),
+    "rocblas_get_vector": (_i, [_i, _i, _p, _i, _p, _i]),
+    "rocblas_get_vector_async": (_i, [_i, _i, _p, _i, _p, _i, _p]),
+    "rocblas_get_matrix": (_i, [_i, _i, _i, _p, _i, _p, _i]),
+    "rocblas_get_matrix_async": (_i, [_i, _i, _i, _p, _i, _p, _i, _p]),
+    "rocblas_set_vector_64": (_i, [_i64, _i64, _p, _i64, _p, _i64]),
+    "rocblas_set_vector_async_64": (_i, [_i64, _i64, _p, _i64, _p, _i64, _p]),
+    "rocblas_set_matrix_64": (_i, [_i64, _i64, _i64, _p, _i64, _p, _i64]),
+    "rocblas_set_matrix_async_64": (_i, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p]),
+    "rocblas_get_vector_64": (_i, [_i64, _i64, _p, _i64, _p, _i64]),
+    "rocblas_get_vector_async_64": (_i, [_i64, _i64, _p, _i64, _p, _i64, _p]),
+    "rocblas_get_matrix_64": (_i, [_i64, _i64, _i64, _p, _i64, _p, _i64]),
+    "rocblas_get_matrix_async_64": (_i, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p]),
     "rocblas_start_device_memory_size_query": (_i, [_H]),
     "rocblas_stop_device_memory_size_query": (_i, [_H, ctypes.POINTER(_sz)]),
     "rocblas_is_device_memory_size_query": (ctypes.c_bool, [_H]),

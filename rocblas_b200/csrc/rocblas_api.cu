@@ -625,6 +625,59 @@ void log_alpha(rocblas_handle h, const T* alpha, double* re, double* im)
     }
 }
 
+// Host <-> device copies of the auxiliary API (rocblas_auxiliary.cpp:305-790): the argument
+// rules of the reference, one contiguous copy when both sides are dense, else one 2D copy (a
+// vector with increments is a 2D copy of elem_size-byte rows). Copy errors are printed and the
+// call still returns success, as the reference's PRINT_IF_HIP_ERROR does.
+rocblas_status aux_copy_vector(int64_t n, int64_t es, const void* src, int64_t incs, void* dst,
+                               int64_t incd, cudaMemcpyKind kind, cudaStream_t s, bool async)
+{
+    if(n == 0)
+        return rocblas_status_success;
+    if(n < 0 || incs <= 0 || incd <= 0 || es <= 0)
+        return rocblas_status_invalid_size;
+    if(!src || !dst)
+        return rocblas_status_invalid_pointer;
+    const size_t e = (size_t)es;
+    cudaError_t  err;
+    if(incs == 1 && incd == 1)
+        err = async ? cudaMemcpyAsync(dst, src, e * n, kind, s) : cudaMemcpy(dst, src, e * n, kind);
+    else
+        err = async ? cudaMemcpy2DAsync(dst, e * incd, src, e * incs, e, n, kind, s)
+                    : cudaMemcpy2D(dst, e * incd, src, e * incs, e, n, kind);
+    if(err != cudaSuccess)
+    {
+        fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err));
+        cudaGetLastError();
+    }
+    return rocblas_status_success;
+}
+
+rocblas_status aux_copy_matrix(int64_t rows, int64_t cols, int64_t es, const void* src, int64_t lds,
+                               void* dst, int64_t ldd, cudaMemcpyKind kind, cudaStream_t s, bool async)
+{
+    if(rows == 0 || cols == 0)
+        return rocblas_status_success;
+    if(rows < 0 || cols < 0 || lds <= 0 || ldd <= 0 || rows > lds || rows > ldd || es <= 0)
+        return rocblas_status_invalid_size;
+    if(!src || !dst)
+        return rocblas_status_invalid_pointer;
+    const size_t e = (size_t)es;
+    cudaError_t  err;
+    if(lds == rows && ldd == rows)
+        err = async ? cudaMemcpyAsync(dst, src, e * rows * cols, kind, s)
+                    : cudaMemcpy(dst, src, e * rows * cols, kind);
+    else
+        err = async ? cudaMemcpy2DAsync(dst, e * ldd, src, e * lds, e * rows, cols, kind, s)
+                    : cudaMemcpy2D(dst, e * ldd, src, e * lds, e * rows, cols, kind);
+    if(err != cudaSuccess)
+    {
+        fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err));
+        cudaGetLastError();
+    }
+    return rocblas_status_success;
+}
+
 int* ensure_err(rocblas_handle h);
 
 // Check-numerics of A's referenced triangle (inputs only) and of B; the name is the entry
@@ -1873,6 +1926,182 @@ rocblas_status rocblas_get_atomics_mode(rocblas_handle handle, rocblas_atomics_m
                                                  + atomics_mode_string(*mode) + ","
                                                  + atomics_mode_string(handle->atomics_mode));
     return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_vector(rocblas_int n, rocblas_int elem_size, const void* x_h, rocblas_int incx, void* y_d,
+                                  rocblas_int incy)
+try
+{
+    return aux_copy_vector(n, elem_size, x_h, incx, y_d, incy, cudaMemcpyHostToDevice, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_vector(rocblas_int n, rocblas_int elem_size, const void* x_d, rocblas_int incx, void* y_h,
+                                  rocblas_int incy)
+try
+{
+    return aux_copy_vector(n, elem_size, x_d, incx, y_h, incy, cudaMemcpyDeviceToHost, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_vector_async(rocblas_int n, rocblas_int elem_size, const void* x_h, rocblas_int incx,
+                                        void* y_d, rocblas_int incy, cudaStream_t stream)
+try
+{
+    return aux_copy_vector(n, elem_size, x_h, incx, y_d, incy, cudaMemcpyHostToDevice, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_vector_async(rocblas_int n, rocblas_int elem_size, const void* x_d, rocblas_int incx,
+                                        void* y_h, rocblas_int incy, cudaStream_t stream)
+try
+{
+    return aux_copy_vector(n, elem_size, x_d, incx, y_h, incy, cudaMemcpyDeviceToHost, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_matrix(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_h, rocblas_int lda,
+                                  void* b_d, rocblas_int ldb)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_h, lda, b_d, ldb, cudaMemcpyHostToDevice, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_matrix(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_d, rocblas_int lda,
+                                  void* b_h, rocblas_int ldb)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_d, lda, b_h, ldb, cudaMemcpyDeviceToHost, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_matrix_async(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_h,
+                                        rocblas_int lda, void* b_d, rocblas_int ldb, cudaStream_t stream)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_h, lda, b_d, ldb, cudaMemcpyHostToDevice, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_matrix_async(rocblas_int rows, rocblas_int cols, rocblas_int elem_size, const void* a_d,
+                                        rocblas_int lda, void* b_h, rocblas_int ldb, cudaStream_t stream)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_d, lda, b_h, ldb, cudaMemcpyDeviceToHost, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_vector_64(int64_t n, int64_t elem_size, const void* x_h, int64_t incx, void* y_d,
+                                  int64_t incy)
+try
+{
+    return aux_copy_vector(n, elem_size, x_h, incx, y_d, incy, cudaMemcpyHostToDevice, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_vector_64(int64_t n, int64_t elem_size, const void* x_d, int64_t incx, void* y_h,
+                                  int64_t incy)
+try
+{
+    return aux_copy_vector(n, elem_size, x_d, incx, y_h, incy, cudaMemcpyDeviceToHost, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_vector_async_64(int64_t n, int64_t elem_size, const void* x_h, int64_t incx,
+                                        void* y_d, int64_t incy, cudaStream_t stream)
+try
+{
+    return aux_copy_vector(n, elem_size, x_h, incx, y_d, incy, cudaMemcpyHostToDevice, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_vector_async_64(int64_t n, int64_t elem_size, const void* x_d, int64_t incx,
+                                        void* y_h, int64_t incy, cudaStream_t stream)
+try
+{
+    return aux_copy_vector(n, elem_size, x_d, incx, y_h, incy, cudaMemcpyDeviceToHost, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_matrix_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_h, int64_t lda,
+                                  void* b_d, int64_t ldb)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_h, lda, b_d, ldb, cudaMemcpyHostToDevice, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_matrix_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_d, int64_t lda,
+                                  void* b_h, int64_t ldb)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_d, lda, b_h, ldb, cudaMemcpyDeviceToHost, nullptr, false);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_set_matrix_async_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_h,
+                                        int64_t lda, void* b_d, int64_t ldb, cudaStream_t stream)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_h, lda, b_d, ldb, cudaMemcpyHostToDevice, stream, true);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_get_matrix_async_64(int64_t rows, int64_t cols, int64_t elem_size, const void* a_d,
+                                        int64_t lda, void* b_h, int64_t ldb, cudaStream_t stream)
+try
+{
+    return aux_copy_matrix(rows, cols, elem_size, a_d, lda, b_h, ldb, cudaMemcpyDeviceToHost, stream, true);
+}
+catch(...)
+{
+    return exception_status();
 }
 
 rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr)

@@ -122,6 +122,34 @@ def test_trtri_bad_args(handle):
     assert L.rocblas_dtrtri(handle.value, rb.fill_lower, rb.diagonal_unit, 4, None, 4, 1, 4) == rb.status_invalid_pointer
 
 
+def test_copy_helpers_argument_rules(rocblas_lib):
+    """rocblas_{set,get}_{vector,matrix}[_async][_64] argument rules (rocblas_auxiliary.cpp:
+    305-790): quick return first, then sizes, then pointers; nothing here touches a device."""
+    L = rb.lib()
+    p = ctypes.c_void_p(0x1000)
+    for suf in ("", "_64"):
+        for d in ("set", "get"):
+            vec = getattr(L, f"rocblas_{d}_vector{suf}")
+            veca = getattr(L, f"rocblas_{d}_vector_async{suf}")
+            mat = getattr(L, f"rocblas_{d}_matrix{suf}")
+            mata = getattr(L, f"rocblas_{d}_matrix_async{suf}")
+            assert vec(0, 8, None, 1, None, 1) == rb.status_success
+            assert veca(0, 8, None, 1, None, 1, None) == rb.status_success
+            assert vec(-1, 8, p, 1, p, 1) == rb.status_invalid_size
+            assert vec(4, 0, p, 1, p, 1) == rb.status_invalid_size
+            assert vec(4, 8, p, 0, p, 1) == rb.status_invalid_size
+            assert veca(4, 8, p, 1, p, -1, None) == rb.status_invalid_size
+            assert vec(4, 8, None, 1, p, 1) == rb.status_invalid_pointer
+            assert veca(4, 8, p, 1, None, 1, None) == rb.status_invalid_pointer
+            assert mat(0, 5, 8, None, 1, None, 1) == rb.status_success
+            assert mat(5, 0, 8, None, 1, None, 1) == rb.status_success
+            assert mat(-1, 5, 8, p, 5, p, 5) == rb.status_invalid_size
+            assert mat(6, 5, 8, p, 5, p, 6) == rb.status_invalid_size  # rows > lda
+            assert mat(6, 5, 8, p, 6, p, 5) == rb.status_invalid_size  # rows > ldb
+            assert mata(6, 5, 0, p, 6, p, 6, None) == rb.status_invalid_size
+            assert mata(6, 5, 8, p, 6, None, 6, None) == rb.status_invalid_pointer
+
+
 def test_atomics_mode(handle):
     """rocblas_set/get_atomics_mode (rocblas_auxiliary.cpp:87-117): allowed by default."""
     L = rb.lib()
