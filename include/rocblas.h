@@ -125,6 +125,19 @@ typedef enum rocblas_pointer_mode_ /* rocblas-types.h:228-234 */
     rocblas_pointer_mode_device = 1
 } rocblas_pointer_mode;
 
+typedef enum rocblas_performance_metric_ /* rocblas-types.h:249-258 */
+{
+    rocblas_default_performance_metric           = 0,
+    rocblas_device_efficiency_performance_metric = 1,
+    rocblas_cu_efficiency_performance_metric     = 2
+} rocblas_performance_metric;
+
+typedef enum rocblas_math_mode_ /* rocblas-types.h:340-347 */
+{
+    rocblas_default_math     = 0x0,
+    rocblas_xf32_xdl_math_op = 0x1
+} rocblas_math_mode;
+
 typedef enum rocblas_atomics_mode_ /* rocblas-types.h:239-245 */
 {
     rocblas_atomics_not_allowed = 0,
@@ -165,6 +178,17 @@ ROCBLAS_EXPORT rocblas_status rocblas_set_atomics_mode(rocblas_handle       hand
                                                        rocblas_atomics_mode atomics_mode);
 ROCBLAS_EXPORT rocblas_status rocblas_get_atomics_mode(rocblas_handle        handle,
                                                        rocblas_atomics_mode* atomics_mode);
+/* rocblas-auxiliary.h: math mode (xf32 is a GEMM-backend mode that this TRSM path does not
+ * have: setting it is ignored, as the reference does where its backend lacks it), the GEMM
+ * solution-selection metric and the fitness query (kept; no GEMM solution library here, so
+ * the fitness stays at the lowest double) */
+ROCBLAS_EXPORT rocblas_status rocblas_set_math_mode(rocblas_handle handle, rocblas_math_mode math_mode);
+ROCBLAS_EXPORT rocblas_status rocblas_get_math_mode(rocblas_handle handle, rocblas_math_mode* math_mode);
+ROCBLAS_EXPORT rocblas_status rocblas_set_performance_metric(rocblas_handle             handle,
+                                                             rocblas_performance_metric metric);
+ROCBLAS_EXPORT rocblas_status rocblas_get_performance_metric(rocblas_handle              handle,
+                                                             rocblas_performance_metric* metric);
+ROCBLAS_EXPORT rocblas_status rocblas_set_solution_fitness_query(rocblas_handle handle, double* fitness);
 /* rocblas-auxiliary.h:97 */
 ROCBLAS_EXPORT rocblas_pointer_mode rocblas_pointer_to_mode(void* ptr);
 

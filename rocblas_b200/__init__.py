@@ -128,6 +128,11 @@ SIGNATURES = {
     "rocblas_set_pointer_mode": (_i, [_H, _i]),
     "rocblas_get_pointer_mode": (_i, [_H, ctypes.POINTER(_i)]),
     "rocblas_set_atomics_mode": (_i, [_H, _i]),
+    "rocblas_set_math_mode": (_i, [_H, _i]),
+    "rocblas_get_math_mode": (_i, [_H, ctypes.POINTER(_i)]),
+    "rocblas_set_performance_metric": (_i, [_H, _i]),
+    "rocblas_get_performance_metric": (_i, [_H, ctypes.POINTER(_i)]),
+    "rocblas_set_solution_fitness_query": (_i, [_H, ctypes.POINTER(ctypes.c_double)]),
     "rocblas_get_atomics_mode": (_i, [_H, ctypes.POINTER(_i)]),
     "rocblas_pointer_to_mode": (_i, [_p]),
     "rocblas_set_vector": (_i, [_i, _i, _p, _i, _p, _i]),

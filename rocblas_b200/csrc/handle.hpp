@@ -46,6 +46,9 @@ struct _rocblas_handle
     int   layer_mode     = 0;
     int   check_numerics = 0;
     int   atomics_mode   = 1; // rocblas_atomics_allowed, the reference's default
+    int     math_mode          = 0; // rocblas_default_math
+    int     performance_metric = 0; // rocblas_default_performance_metric
+    double* fitness_query      = nullptr;
     FILE* log_trace_os   = nullptr;
     FILE* log_bench_os   = nullptr;
     FILE* log_profile_os = nullptr;

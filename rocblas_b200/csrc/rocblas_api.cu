@@ -1902,6 +1902,63 @@ rocblas_status rocblas_get_pointer_mode(rocblas_handle handle, rocblas_pointer_m
     return rocblas_status_success;
 }
 
+rocblas_status rocblas_set_math_mode(rocblas_handle handle, rocblas_math_mode mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    // only the default math mode exists here (rocblas_auxiliary.cpp:145-178: an unsupported mode
+    // is logged and ignored, and the call succeeds)
+    const bool supported = mode == rocblas_default_math;
+    if(handle->layer_mode & kLayerTrace)
+        layer_log_line(handle->log_trace_os, "rocblas_set_math_mode," + std::to_string((int)mode)
+                                                 + (supported ? "," : ",is not supported,")
+                                                 + atomics_mode_string(handle->atomics_mode));
+    if(supported)
+        handle->math_mode = mode;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_get_math_mode(rocblas_handle handle, rocblas_math_mode* mode)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!mode)
+        return rocblas_status_invalid_pointer;
+    *mode = (rocblas_math_mode)handle->math_mode;
+    if(handle->layer_mode & kLayerTrace)
+        layer_log_line(handle->log_trace_os, "rocblas_get_math_mode," + std::to_string((int)*mode) + ","
+                                                 + atomics_mode_string(handle->atomics_mode));
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_performance_metric(rocblas_handle handle, rocblas_performance_metric metric)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->performance_metric = metric;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_get_performance_metric(rocblas_handle handle, rocblas_performance_metric* metric)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    if(!metric)
+        return rocblas_status_invalid_pointer;
+    *metric = (rocblas_performance_metric)handle->performance_metric;
+    return rocblas_status_success;
+}
+
+rocblas_status rocblas_set_solution_fitness_query(rocblas_handle handle, double* fitness)
+{
+    if(!handle)
+        return rocblas_status_invalid_handle;
+    handle->fitness_query = fitness;
+    if(fitness)
+        *fitness = std::numeric_limits<double>::lowest();
+    return rocblas_status_success;
+}
+
 rocblas_status rocblas_set_atomics_mode(rocblas_handle handle, rocblas_atomics_mode mode)
 {
     if(!handle)

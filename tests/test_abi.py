@@ -3,6 +3,7 @@ include/rocblas.h declares, and applies the reference's argument checks and
 device-memory protocol without touching a GPU (clients/include/blas3/testing_trsm.hpp:
 33-186 is the bad-argument spec)."""
 import ctypes
+import sys
 import re
 import subprocess
 
@@ -120,6 +121,26 @@ def test_trtri_bad_args(handle):
     assert L.rocblas_dtrtri(handle.value, rb.fill_lower, rb.diagonal_unit, 4, 1, 4, 1, 3) == rb.status_invalid_size
     assert L.rocblas_dtrtri(handle.value, rb.fill_lower, rb.diagonal_unit, 0, None, 4, None, 4) == rb.status_success
     assert L.rocblas_dtrtri(handle.value, rb.fill_lower, rb.diagonal_unit, 4, None, 4, 1, 4) == rb.status_invalid_pointer
+
+
+def test_math_mode_metric_and_fitness(handle):
+    """rocblas_auxiliary.cpp:126-178 and handle.cpp: the math mode (xf32 not supported here:
+    ignored, success), the performance metric, and the fitness query set to the lowest double."""
+    L = rb.lib()
+    v = ctypes.c_int(-1)
+    assert L.rocblas_get_math_mode(handle.value, ctypes.byref(v)) == 0 and v.value == 0
+    assert L.rocblas_set_math_mode(handle.value, 1) == 0
+    assert L.rocblas_get_math_mode(handle.value, ctypes.byref(v)) == 0 and v.value == 0
+    assert L.rocblas_set_math_mode(None, 0) == rb.status_invalid_handle
+    assert L.rocblas_get_math_mode(handle.value, None) == rb.status_invalid_pointer
+    assert L.rocblas_get_performance_metric(handle.value, ctypes.byref(v)) == 0 and v.value == 0
+    assert L.rocblas_set_performance_metric(handle.value, 2) == 0
+    assert L.rocblas_get_performance_metric(handle.value, ctypes.byref(v)) == 0 and v.value == 2
+    assert L.rocblas_get_performance_metric(handle.value, None) == rb.status_invalid_pointer
+    f = ctypes.c_double(1.0)
+    assert L.rocblas_set_solution_fitness_query(handle.value, ctypes.byref(f)) == 0
+    assert f.value == -sys.float_info.max
+    assert L.rocblas_set_solution_fitness_query(handle.value, None) == 0
 
 
 def test_copy_helpers_argument_rules(rocblas_lib):
