@@ -3,9 +3,9 @@ include/rocblas.h declares, and applies the reference's argument checks and
 device-memory protocol without touching a GPU (clients/include/blas3/testing_trsm.hpp:
 33-186 is the bad-argument spec)."""
 import ctypes
-import sys
 import re
 import subprocess
+import sys
 
 import pytest
 
