@@ -293,9 +293,3 @@ class Handle:
             self.close()
         except Exception:
             pass
-
-
-def scalar_ptr(value, dtype):
-    """A host scalar as a ctypes pointer (host pointer mode alpha)."""
-    c = ctypes.c_float(value) if dtype in ("s", "float32") else ctypes.c_double(value)
-    return c, ctypes.cast(ctypes.byref(c), ctypes.c_void_p)
