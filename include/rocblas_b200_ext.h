@@ -153,16 +153,18 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_server_run(rocblas_b200_server       
 
 /* ---- the variable-size batch without any allocation ---------------------------------------
  * No counterpart in the reference.  Same contract and results as
- * rocblas_b200_dtrsm_vbatched, for callers that must not allocate device memory: code that
- * records the call into a CUDA graph by stream capture (cudaMalloc is not allowed while a
- * capture is active), applications that hand all device memory to their own pool and forbid
- * libraries to allocate, and loops that cannot afford the device-wide synchronisation of a
- * cudaFree when the handle's workspace would grow.  Its scratch (queue state and prefix sums)
+ * rocblas_b200_dtrsm_vbatched, for callers that cannot let a library allocate device memory:
+ * applications whose own pool has reserved the GPU's memory up front and which forbid
+ * libraries to allocate beside it (the allocation would fail or break the pool's budget), and
+ * solver loops on a latency budget that cannot take the device-wide synchronisation a cudaFree
+ * implies when the handle's workspace would grow.  Its scratch (queue state and prefix sums)
  * is a fixed device array inside the library, sized for at most 65536 systems (256 KiB +
  * 16 B, held on every GPU that loads the library until exit); count > 65536 returns
  * rocblas_status_invalid_size.  It calls no cudaMalloc or cudaFree and takes nothing from the
- * handle's workspace.  The first call on a device looks up the array's device address (once
- * per device) and should be made before any stream capture.  All calls share the one array:
+ * handle's workspace.  The first call on a device (and the first after that device's context
+ * was torn down and made again) sets up: it looks up the array's device address in the
+ * current context.  Make that first call before any stream capture.  All calls share the one
+ * array and find it as the previous call left it (the call clears what must start at zero):
  * calls that overlap on the GPU (for example on two streams, or two handles at once) race and
  * must be ordered by the caller. */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_vbatched_noalloc(rocblas_handle                   handle,

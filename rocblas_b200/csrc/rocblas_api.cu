@@ -2,6 +2,8 @@
 // _batched and _strided_batched forms.  Every entry point is `extern "C"`, catches every
 // exception (as the reference's IMPL wrappers do, library/src/blas3/rocblas_trsm_imp.hpp:
 // 285-314) and validates its arguments in the reference's order before touching the GPU.
+#include <cuda.h> // CUcontext and CUresult for the driver entry points (no libcuda link)
+
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -70,6 +72,26 @@ rocblas_status _rocblas_handle::free_mem()
 namespace
 {
 // Device capability of the handle's device: 0 ok, otherwise a rocblas_status to return.
+// Restores the device that was current when the scope began, if a call switched it: the
+// handle's device is made current for the call only, as the reference's
+// _rocblas_saved_device_id does (library/src/include/handle.hpp:134-170).
+class DeviceScope
+{
+    int saved_ = -1;
+
+public:
+    DeviceScope() { cudaGetDevice(&saved_); }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        if(saved_ >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != saved_)
+            cudaSetDevice(saved_);
+    }
+    DeviceScope(const DeviceScope&)            = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
+// Makes the handle's device current; the enclosing entry point holds a DeviceScope.
 rocblas_status device_ready(rocblas_handle h)
 {
     if(h->device < 0)
@@ -173,6 +195,7 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                          const void* invA_ptr, BatchPtr<T> invA, int64_t invA_size,
                          int conj = -1)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     rocblas_status st
@@ -366,6 +389,7 @@ rocblas_status trmm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                          const void* Bptr, BatchPtr<T> B, int64_t ldb, const void* Cptr,
                          BatchPtr<T> C, int64_t ldc, int batch)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     rocblas_status st = trmm_arg_check<T>(h, side, uplo, trans, diag, m, n, alpha, Aptr, lda, Bptr,
@@ -478,6 +502,7 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
                          rocblas_diagonal diag, int n, const void* Aptr, BatchPtr<T> A, int64_t lda,
                          const void* xptr, BatchPtr<T> x, int64_t incx, int batch)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     rocblas_status ast = trsv_arg_check(h, uplo, trans, diag, n, Aptr, lda, xptr, incx, batch);
@@ -741,6 +766,7 @@ rocblas_status trsm_impl_64(rocblas_handle h, rocblas_side side, rocblas_fill up
                             const void* invA_ptr = nullptr, BatchPtr<T> invA = BatchPtr<T>{},
                             int64_t invA_size = 0, const TrsmLogInfo* li = nullptr)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     // layer logging comes before the argument check (rocblas_trsm_imp.hpp:74-143)
@@ -963,6 +989,7 @@ rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal 
                           const void* Aptr, BatchPtr<T> A, int lda, const void* Xptr,
                           BatchPtr<T> X, int ldinv, int batch)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     if constexpr(is_cplx<T>::value)
@@ -1077,6 +1104,7 @@ rocblas_status trsm_vbatched_impl(rocblas_handle h, const T* alpha,
                                   const rocblas_b200_trsm_problem* problems, int count,
                                   int max_k, rocblas_int* invalid_count)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     if(count < 0 || max_k < 0 || max_k > kBlockSolveMaxK)
@@ -1139,6 +1167,7 @@ rocblas_status trsm_vbatched_ex_impl(rocblas_handle h, const T* alpha,
                                      const T* const* invA, int count, int max_k, int max_n,
                                      rocblas_int* invalid_count)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     if(count < 0 || max_k < 0 || max_n < 0 || max_k > kChainVbMaxNB * kChainNB)
@@ -1263,24 +1292,61 @@ static __device__ __align__(256) unsigned char
 
 constexpr int kVbNoAllocMaxDevices = 64;
 std::mutex    g_vb_noalloc_mutex;
-void*         g_vb_noalloc_addr[kVbNoAllocMaxDevices] = {};
+// per device: the address found at set-up and the unique id of the context it belongs to (a
+// symbol's address is only valid in the context that loaded the module; after a device reset
+// or primary-context teardown the next context gets a new id and the lookup is made again)
+void*              g_vb_noalloc_addr[kVbNoAllocMaxDevices] = {};
+unsigned long long g_vb_noalloc_ctx[kVbNoAllocMaxDevices]  = {};
 
-// Device address of the scratch array on `device` (which must be current); looked up once per
-// device.  nullptr if the lookup fails.
+// Unique id of the current context (cuCtxGetId, reached through the runtime's driver entry
+// points so the library does not link libcuda).  0 if there is none or it cannot be read.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId      = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId      get_id      = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+               cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+               cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    CUcontext          ctx = nullptr;
+    unsigned long long id  = 0;
+    if(!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+       get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of the scratch array on `device`, which must be current (the runtime has made
+// its primary context current by then).  Set-up looks it up once per device and context;
+// without a readable context id it is looked up on every call.  nullptr if the lookup fails.
 void* vb_noalloc_scratch(int device)
 {
     if(device < 0 || device >= kVbNoAllocMaxDevices)
         return nullptr;
     std::lock_guard<std::mutex> lock(g_vb_noalloc_mutex);
-    if(!g_vb_noalloc_addr[device])
+    const unsigned long long ctx = current_context_id();
+    if(!g_vb_noalloc_addr[device] || ctx == 0 || ctx != g_vb_noalloc_ctx[device])
     {
         void* ptr = nullptr;
         if(cudaGetSymbolAddress(&ptr, g_vb_noalloc_scratch) != cudaSuccess)
         {
             cudaGetLastError();
+            g_vb_noalloc_addr[device] = nullptr;
             return nullptr;
         }
         g_vb_noalloc_addr[device] = ptr;
+        g_vb_noalloc_ctx[device]  = ctx;
     }
     return g_vb_noalloc_addr[device];
 }
@@ -1289,6 +1355,7 @@ rocblas_status trsm_vbatched_noalloc_impl(rocblas_handle h, const double* alpha,
                                           const rocblas_b200_trsm_problem* problems, int count,
                                           int max_k, rocblas_int* invalid_count)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     if(count < 0 || max_k < 0 || max_k > kBlockSolveMaxK)
@@ -1358,6 +1425,7 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
                                 const double* B, int ldb, const double* beta, double* C, int ldc,
                                 int slices)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     auto okop = [](rocblas_operation t) {
@@ -1410,6 +1478,7 @@ rocblas_status gemm_tiles_impl(rocblas_handle h, rocblas_operation ta, rocblas_o
                                int n, int k, const T* alpha, const T* A, int lda, const T* B,
                                int ldb, const T* beta, T* C, int ldc)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     auto okop = [](rocblas_operation t) {
@@ -1458,6 +1527,7 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
                                const double* alpha, const double* A, int lda, double* B, int ldb,
                                int slices)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     rocblas_status st
@@ -1625,6 +1695,7 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
                                     const double* alpha, const double* hA, int lda, double* hB,
                                     int ldb, int slices)
 {
+    DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
         return rocblas_status_invalid_handle;
     if(h->size_query)
