@@ -44,7 +44,8 @@ CBLAS_COL_MAJOR = 102
 
 def build(force: bool = False) -> str:
     """Compile the C oracle with the committed Makefile."""
-    newest = max(os.path.getmtime(os.path.join(HERE, f)) for f in ("trsm_oracle.c", "trsm_oracle_complex.c"))
+    newest = max(os.path.getmtime(os.path.join(HERE, f))
+                 for f in ("trsm_oracle.c", "trsm_oracle_complex.c", "trsm_oracle_dd.c", "Makefile"))
     if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
         subprocess.check_call(["make", "-s", "-C", HERE])
     return LIB_PATH
@@ -80,6 +81,8 @@ def _load():
             f.restype = None
         lib.oracle_matrix_norm_1_z.argtypes = [i64, i64, p, i64, p, i64]
         lib.oracle_matrix_norm_1_z.restype = d
+        lib.oracle_dd_residual.argtypes = [i64, i64, i, i, p, i64, p, p, i64, d, p, i64, p, i64]
+        lib.oracle_dd_residual.restype = None
         _lib = lib
     return _lib
 
@@ -219,6 +222,67 @@ def normwise_backward_error(side, uplo, trans, diag, alpha, A, X, B, precision="
         np.fill_diagonal(tri, 1.0)
     den = np.linalg.norm(tri) * np.linalg.norm(X) + abs(alpha) * np.linalg.norm(B)
     return float(np.linalg.norm(R) / den)
+
+
+def dd_residual(lower, unit, T, Xh, Xl, alpha, B):
+    """r = alpha B - T (Xh + Xl) for a k x k triangle T (only its triangle is read), every
+    entry accumulated in double-double and rounded once (trsm_oracle_dd.c)."""
+    T = _f(T, np.float64)
+    Xh = _f(Xh, np.float64)
+    Xl = _f(Xl, np.float64) if Xl is not None else None
+    B = _f(B, np.float64)
+    k, nrhs = Xh.shape
+    R = np.empty((k, nrhs), dtype=np.float64, order="F")
+    _load().oracle_dd_residual(k, nrhs, int(bool(lower)), int(bool(unit)), T.ctypes.data, T.shape[0],
+                               Xh.ctypes.data, Xl.ctypes.data if Xl is not None else None, Xh.shape[0],
+                               float(alpha), B.ctypes.data, B.shape[0], R.ctypes.data, k)
+    return R
+
+
+def refined_solution(side, uplo, trans, diag, alpha, A, B, steps=2):
+    """The extended-precision solution X* of op(A) X = alpha B (side L) or X op(A) = alpha B
+    (side R) as an unevaluated sum Xh + Xl: the host CBLAS solve, then `steps` rounds of
+    Wilkinson's iterative refinement with double-double residuals (dd_residual) and CBLAS
+    corrections.  Each round multiplies the error by about cond(A, x) eps, so two rounds reach
+    far below the FP64 rounding level for the condition numbers of the benchmark bands
+    (<= 1e7); agreement with the __float128 substitution is checked in tests/test_oracle.py.
+    FP64 only; A's other triangle is never read.  B holds exactly the m rows of the problem."""
+    A = _f(A, np.float64)
+    B = _f(B, np.float64)
+    m, n = B.shape
+    left = _code(SIDE, side) == SIDE["L"]
+    notrans = _code(TRANS, trans) == TRANS["N"]
+    lower = _code(UPLO, uplo) == UPLO["L"]
+    unit = _code(DIAG, diag) == DIAG["U"]
+    k = m if left else n
+    # as a side-left, non-transposed system S Y = alpha C
+    if left == notrans:
+        S = A
+    else:
+        S = np.asfortranarray(A[:k, :k].T)
+        lower = not lower
+    C = B if left else np.asfortranarray(B.T)
+    up = "L" if lower else "U"
+    dg = "U" if unit else "N"
+    Xh = cblas_trsm("L", up, "N", dg, alpha, S, C)
+    Xl = np.zeros_like(Xh)
+    for _ in range(steps):
+        r = dd_residual(lower, unit, S, Xh, Xl, alpha, C)
+        d = cblas_trsm("L", up, "N", dg, 1.0, S, r)
+        t = Xl + d
+        s = Xh + t
+        Xl = t - (s - Xh)  # Fast2Sum: |t| << |Xh| wherever Xh is not 0
+        Xh = s
+    if not left:
+        Xh, Xl = np.asfortranarray(Xh.T), np.asfortranarray(Xl.T)
+    return Xh, Xl
+
+
+def forward_error_dd(X, Xh, Xl):
+    """||X - (Xh + Xl)||_F / ||Xh + Xl||_F, with the difference formed as (X - Xh) - Xl."""
+    X = np.asarray(X, dtype=np.float64)
+    d = (X - Xh) - Xl
+    return float(np.linalg.norm(d) / np.linalg.norm(Xh))
 
 
 # ---------------------------------------------------------------------------------------

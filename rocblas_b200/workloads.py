@@ -36,6 +36,62 @@ def condition_band_lower_torch(m, n, kband, seed, device="cuda", dtype=None):
     return At.to(dtype).contiguous(), Bt.to(dtype).contiguous()
 
 
+def graded_sigma(m, kband):
+    """Singular values graded geometrically from 1 to 10^-kband: kappa_2 = 10^kband."""
+    return 10.0 ** (-kband * np.arange(m) / max(m - 1, 1))
+
+
+def graded_condition_lower_torch(m, n, kband, seed, device="cuda"):
+    """Lower-triangular A (m x m, lda = m) with singular values exactly 10^(-kband i/(m-1)),
+    i = 0..m-1, so kappa_2(A) = 10^kband, and conditioning that no diagonal scaling removes
+    (the construction of LAPACK's dlatms for a triangular factor): A = R^T with R the
+    triangular factor of the QR factorisation of U diag(sigma) V^T, U and V Haar-random
+    orthogonal (Q factors of Gaussian matrices).  The upper triangle is NaN; B ~ U(-1, 1)
+    (m x n).  kband = 0 gives an orthogonal triangle, i.e. a diagonal of +-1.
+
+    Returns (ncols, ld) views of column-major storage, as condition_band_lower_torch does.
+    The factorisations run in FP64 on the device (torch.linalg.qr)."""
+    return next(graded_condition_bands_torch(m, n, [kband], seed, device))[1:]
+
+
+def graded_condition_bands_torch(m, n, kbands, seed, device="cuda"):
+    """graded_condition_lower_torch for several bands with one pair U, V (two of the
+    factorisations shared): yields (kband, At, Bt) in the order of kbands."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    U, _ = torch.linalg.qr(torch.randn(m, m, generator=g, device=device, dtype=torch.float64))
+    V, _ = torch.linalg.qr(torch.randn(m, m, generator=g, device=device, dtype=torch.float64))
+    for kband in kbands:
+        sig = torch.from_numpy(graded_sigma(m, kband)).to(device)
+        M = (U * sig.view(1, m)) @ V.T
+        R = torch.linalg.qr(M, mode="r")[1]
+        del M
+        # R upper triangular in row-major == At (row-major A^T) with A = R^T lower triangular:
+        # At[j, i] = A(i, j) = R(j, i), so At is R itself
+        nan_mask = torch.ones(m, m, dtype=torch.bool, device=device).tril_(-1)
+        R.masked_fill_(nan_mask, float("nan"))
+        del nan_mask
+        Bt = torch.rand(n, m, generator=g, device=device, dtype=torch.float64) * 2.0 - 1.0
+        yield kband, R.contiguous(), Bt.contiguous()
+
+
+def graded_condition_problem(seed, m, n, kband, dtype=np.float64):
+    """Host (numpy) version of graded_condition_lower_torch's construction (different RNG
+    stream), for sizes the CPU oracle handles: column-major A (m x m, NaN upper triangle)
+    and B (m x n)."""
+    rng = np.random.default_rng(seed)
+    U, _ = np.linalg.qr(rng.standard_normal((m, m)))
+    V, _ = np.linalg.qr(rng.standard_normal((m, m)))
+    M = (U * graded_sigma(m, kband)[None, :]) @ V.T
+    R = np.linalg.qr(M, mode="r")
+    A = np.array(R.T, order="F")
+    A[np.triu_indices(m, 1)] = np.nan
+    B = rng.uniform(-1.0, 1.0, size=(m, n))
+    return np.asfortranarray(A.astype(dtype)), np.asfortranarray(B.astype(dtype))
+
+
 def nan_triangle_problem(seed, side, uplo, trans, diag, m, n, lda, ldb, dtype):
     """The drop-in workload recipe: strictly-triangular entries of A ~ U(-1,1)/k, diagonal
     1 + U(0,1), the unused triangle NaN (so stray reads show up as NaN results); with

@@ -164,3 +164,36 @@ def test_complex_matrix_norm_uses_modulus():
     assert oracle.matrix_norm_1(gold, x) == 1.0
     x[0, 0] = 3 + 0j
     assert abs(oracle.matrix_norm_1(gold, x) - 4.0 / 5.0) < 1e-15
+
+
+@pytest.mark.parametrize("side,uplo,trans,diag", COMBOS)
+def test_dd_refined_solution_matches_float128(side, uplo, trans, diag):
+    """The extended-precision X* of the benchmarks (host CBLAS + two double-double refinement
+    steps) agrees with the __float128 substitution to the rounding of the latter's double
+    output, on square, tall, wide and degenerate shapes, padded leading dimensions included."""
+    for m, n in [(301, 21), (7, 3), (1, 1), (4, 9), (600, 5)]:
+        k = m if side == "L" else n
+        A, B = oracle.nan_triangle_problem(3, side, uplo, trans, diag, m, n, k + 7, m + 5, np.float64)
+        B = np.asfortranarray(B[:m])
+        Xq = oracle.trsm(side, uplo, trans, diag, 0.7, A, B, precision="q")
+        Xh, Xl = oracle.refined_solution(side, uplo, trans, diag, 0.7, A, B)
+        assert oracle.forward_error_dd(Xq, Xh, Xl) < 1e-16, (m, n)
+
+
+@pytest.mark.parametrize("kband", [0, 2, 4])
+def test_graded_generator_condition_and_dd_oracle(kband):
+    """Singular values graded to 10^-k give kappa_2 = 10^k exactly; scaling the rows to a unit
+    diagonal does not remove it; the dd X* matches the __float128 one on that matrix too."""
+    from rocblas_b200 import workloads
+
+    m = 256
+    A, B = workloads.graded_condition_problem(1, m, 6, kband)
+    assert np.isnan(A[np.triu_indices(m, 1)]).all()
+    T = np.tril(np.nan_to_num(A))
+    s = np.linalg.svd(T, compute_uv=False)
+    assert s[0] / s[-1] == pytest.approx(10.0 ** kband, rel=1e-6)
+    s2 = np.linalg.svd(T / np.diag(T)[:, None], compute_uv=False)
+    assert s2[0] / s2[-1] >= 0.5 * 10.0 ** kband
+    Xq = oracle.trsm("L", "L", "N", "N", 1.0, A, B, precision="q")
+    Xh, Xl = oracle.refined_solution("L", "L", "N", "N", 1.0, A, B)
+    assert oracle.forward_error_dd(Xq, Xh, Xl) < 1e-16
