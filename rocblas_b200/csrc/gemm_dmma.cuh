@@ -87,6 +87,25 @@ __device__ __forceinline__ void dmma_load_stage(double* s, const double* ptr, in
     }
 }
 
+// Narrows the K-block range [kt0, kt1) of a tile whose rows (P) or columns (Q) start at o0
+// and span O to the blocks inside the operand's triangle mask.  The mask is in stored
+// coordinates, as dmma_load_stage applies it: for P, stored (r, c) = transP ? (k, o) : (o, k);
+// for Q, transQ ? (o, k) : (k, o).  A lower mask keeps r >= c, an upper one r <= c; the strict
+// masks keep a subset of the same range.
+__device__ __forceinline__ void dmma_tri_k_range(int tri, bool trans, bool is_p, int o0, int O, int BK,
+                                                 int& kt0, int& kt1)
+{
+    if(tri == kTriNone)
+        return;
+    const bool lower    = tri == kTriLower || tri == kTriLowerStrict;
+    const bool o_is_row = is_p ? !trans : trans; // o is the stored row index
+    const bool k_le_o   = o_is_row ? lower : !lower; // the kept region has k <= o (else k >= o)
+    if(k_le_o)
+        kt1 = min(kt1, (o0 + O + BK - 1) / BK);
+    else
+        kt0 = max(kt0, o0 / BK);
+}
+
 template <int BM, int BN, int WM, int WN, int STAGES, bool KCP, bool KCQ, int BK, int MK>
 __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads,
                                   DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>::kThreads <= 256 ? 2 : 1)
@@ -125,8 +144,14 @@ __global__ void __launch_bounds__(DmmaCfg<BM, BN, WM, WN, STAGES, KCP, KCQ, BK>:
     {
         const double* P  = p.P.get(batch);
         const double* Q  = p.Q.get(batch);
-        const int     nk = (p.K + BK - 1) / BK;
+        // K blocks that can meet a masked triangle of this tile: the rest are all zeros, so
+        // a triangular operand costs half of a dense one
+        int kt0 = 0, kt1 = (p.K + BK - 1) / BK;
+        dmma_tri_k_range(p.triP, p.transP != 0, true, m0, BM, BK, kt0, kt1);
+        dmma_tri_k_range(p.triQ, p.transQ != 0, false, n0, BN, BK, kt0, kt1);
+        const int nk = kt1 > kt0 ? kt1 - kt0 : 0;
         auto load = [&](int stage, int kt) {
+            kt += kt0;
             double* sA = smem + stage * Cfg::kStage;
             double* sB = sA + Cfg::kStageA;
             dmma_load_stage<BM, NT, KCP, BK>(sA, P, p.ldp, p.triP, m0, kt * BK, p.M, p.K, tid);
