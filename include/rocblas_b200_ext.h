@@ -273,6 +273,63 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
                                                        rocblas_int       ldb,
                                                        rocblas_int       slices);
 
+/* ---- precision form with iterative refinement -------------------------------------------------
+ * rocblas_b200_dtrsm_mixed followed by FP64 iterative refinement until the result agrees with
+ * the plain FP64 form to `tolerance`.  The reference has no counterpart.  The loop is
+ * mixed-precision iterative refinement (Wilkinson; Buttari et al. 2007 for the form LAPACK's
+ * dsgesv uses) with the low-precision solve replaced by the sliced tensor-core solve:
+ *   X := precision-form solve of op(A) X = alpha B (or X op(A) = alpha B);
+ *   test: `check_columns` evenly spaced right-hand sides (columns of B for side left, rows for
+ *         side right) are also solved by the plain FP64 form, on a second stream while the
+ *         precision-form solve runs; the test passes when, for each of them,
+ *         ||x - x_fp64||_inf <= tolerance * ||x_fp64||_inf;
+ *   while the test fails and fewer than max_iterations corrections were made:
+ *         R := alpha B - op(A) X in FP64 over all right-hand sides (DMMA tiles);
+ *         D := precision-form solve of op(A) D = R (the invA blocks of the first solve are
+ *         reused);  X := X + D;  test again.
+ * If the test still fails and `fallback` is set, B is solved again from its original values by
+ * the plain FP64 form (rocblas_dtrsm).  A test on a sample is a statistical check: right-hand
+ * sides outside it are not compared.  Everything runs on the GPU; the call reads each test's
+ * maxima back to the host and so returns after the solve has completed.  alpha is a host
+ * pointer (device pointer mode returns rocblas_status_not_implemented).  Workspace: the
+ * precision form's plus two m x n copies (the original B and the residual) and the tested
+ * right-hand sides (size query supported).  options may be NULL (all defaults); info may be
+ * NULL. */
+typedef struct rocblas_b200_refine_options
+{
+    rocblas_int slices;         /* 0: the tuning table's mixed_slices */
+    rocblas_int max_iterations; /* correction solves at most (negative: 10) */
+    rocblas_int check_columns;  /* right-hand sides tested (0: 32; >= their count: all) */
+    rocblas_int fallback;       /* 1: plain FP64 solve when the test never passes */
+    double      tolerance;      /* normwise relative difference allowed (0: 1e-12) */
+} rocblas_b200_refine_options;
+
+typedef struct rocblas_b200_refine_info
+{
+    rocblas_int iterations;           /* correction solves performed */
+    rocblas_int converged;            /* 1 if the last test passed */
+    rocblas_int fell_back;            /* 1 if the plain FP64 form produced the result */
+    rocblas_int checked_columns;      /* right-hand sides in each test */
+    double      error_estimate_first; /* max ||x - x_fp64|| / ||x_fp64|| after the first solve */
+    double      error_estimate;       /* the same after the last correction */
+    double      tolerance;            /* the bound used */
+} rocblas_b200_refine_info;
+
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_refined(rocblas_handle                     handle,
+                                                         rocblas_side                       side,
+                                                         rocblas_fill                       uplo,
+                                                         rocblas_operation                  transA,
+                                                         rocblas_diagonal                   diag,
+                                                         rocblas_int                        m,
+                                                         rocblas_int                        n,
+                                                         const double*                      alpha,
+                                                         const double*                      A,
+                                                         rocblas_int                        lda,
+                                                         double*                            B,
+                                                         rocblas_int                        ldb,
+                                                         const rocblas_b200_refine_options* options,
+                                                         rocblas_b200_refine_info*          info);
+
 /* ---- precision form with A and B in host memory -----------------------------------------------
  * rocblas_b200_dtrsm_mixed for host buffers (pinned memory lets the copies overlap the solve):
  * A (lda x k) and B (ldb x n) are host pointers, alpha a host value whatever the handle's

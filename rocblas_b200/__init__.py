@@ -209,6 +209,7 @@ SIGNATURES = {
     "rocblas_b200_dgemm_sliced": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed_host": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
+    "rocblas_b200_dtrsm_refined": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p]),
     "rocblas_b200_dgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
     "rocblas_b200_zgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
     "rocblas_b200_cgemm": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i]),
@@ -226,6 +227,22 @@ SIGNATURES = {
     "rocblas_b200_set_tuning": (_i, [ctypes.c_char_p, _i]),
     "rocblas_b200_get_tuning": (_i, [ctypes.c_char_p, ctypes.POINTER(_i)]),
 }
+
+class RefineOptions(ctypes.Structure):
+    """rocblas_b200_refine_options (include/rocblas_b200_ext.h)."""
+    _fields_ = [("slices", _i), ("max_iterations", _i), ("check_columns", _i), ("fallback", _i),
+                ("tolerance", ctypes.c_double)]
+
+
+class RefineInfo(ctypes.Structure):
+    """rocblas_b200_refine_info (include/rocblas_b200_ext.h)."""
+    _fields_ = [("iterations", _i), ("converged", _i), ("fell_back", _i), ("checked_columns", _i),
+                ("error_estimate_first", ctypes.c_double), ("error_estimate", ctypes.c_double),
+                ("tolerance", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
 
 _lib = None
 

@@ -18,6 +18,7 @@
 #include "../../include/rocblas_b200_ext.h"
 #include "check_numerics.cuh"
 #include "layer_log.hpp"
+#include "refine.cuh"
 #include "sliced_driver.cuh"
 #include "trsm_driver.cuh"
 #include "server.cuh"
@@ -1522,6 +1523,55 @@ rocblas_status gemm_tiles_impl(rocblas_handle h, rocblas_operation ta, rocblas_o
     return launch_status();
 }
 
+// Workspace of one precision-form solve: invA blocks, the largest sliced update's slice
+// panels, the chain sub-solves' flags (all zero when the problem is small enough for the plain
+// path, which needs none).
+struct MixedPlan
+{
+    bool   recursive = false;
+    size_t inv_bytes = 0, sl_bytes = 0, ch_bytes = 0, total = 0;
+};
+
+MixedPlan mixed_plan(const TrsmProblem<double>& pr, int slices)
+{
+    MixedPlan p;
+    p.recursive = choose_algo(pr) == Algo::recursive;
+    if(!p.recursive)
+        return p;
+    p.inv_bytes = align256((size_t)kInvNB * pr.k() * sizeof(double));
+    p.sl_bytes  = mixed_slice_workspace_bytes(pr, slices);
+    p.ch_bytes  = mixed_chain_workspace_bytes(pr);
+    p.total     = p.inv_bytes + align256(p.sl_bytes) + align256(p.ch_bytes);
+    return p;
+}
+
+// The precision-form solve of pr (alpha, A, B as set there) on the workspace laid out by
+// mixed_plan.  invA is built into the workspace when build_inv, else the blocks already there
+// (from an earlier solve with the same A) are used.  false if the GPU lacks the tensor path.
+bool mixed_run(TrsmProblem<double> pr, int slices, const MixedPlan& plan, void* ws, int* err, bool build_inv)
+{
+    if(!plan.recursive)
+    {
+        trsm_run<double>(pr, nullptr, false);
+        return true;
+    }
+    pr.err_dev = err;
+    BatchPtr<double> inv;
+    inv.base   = reinterpret_cast<double*>(ws);
+    inv.stride = (int64_t)kInvNB * pr.k();
+    if(build_inv)
+        build_invA<double>(pr, inv);
+    pr.invA = inv;
+    MixedRecursive rec{{pr, (int)pr.k(), (int)ceil_div(pr.k(), kInvNB)}};
+    rec.S        = slices;
+    rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + plan.inv_bytes;
+    rec.err_dev  = err;
+    if(plan.ch_bytes)
+        rec.chain_ws = reinterpret_cast<unsigned char*>(ws) + plan.inv_bytes + align256(plan.sl_bytes);
+    rec.solve_mixed(0, rec.nblk, 1);
+    return rec.ok;
+}
+
 rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
                                rocblas_operation trans, rocblas_diagonal diag, int m, int n,
                                const double* alpha, const double* A, int lda, double* B, int ldb,
@@ -1561,43 +1611,20 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     pr.ldb = ldb;
     pr.stream   = h->stream;
     pr.sm_count = h->sm_count;
-    const int64_t k = pr.k();
-    const bool recursive = choose_algo(pr) == Algo::recursive;
-    const size_t inv_bytes = recursive ? align256((size_t)kInvNB * k * sizeof(double)) : 0;
-    const size_t sl_bytes  = recursive ? mixed_slice_workspace_bytes(pr, slices) : 0;
-    const size_t ch_bytes  = recursive ? mixed_chain_workspace_bytes(pr) : 0;
-    const size_t ws_bytes  = inv_bytes + sl_bytes + (ch_bytes ? (ch_bytes + 255) / 256 * 256 : 0);
+    const MixedPlan plan = mixed_plan(pr, slices);
     if(h->size_query)
-        return ws_bytes ? h->set_optimal_size(ws_bytes) : rocblas_status_size_unchanged;
+        return plan.total ? h->set_optimal_size(plan.total) : rocblas_status_size_unchanged;
     if((st = device_ready(h)) != rocblas_status_success)
         return st;
     if(h->pointer_mode == rocblas_pointer_mode_host)
         pr.alpha.val = *alpha;
     else
         pr.alpha.ptr = alpha;
-    if(!recursive)
-    {
-        trsm_run<double>(pr, nullptr, false);
-        return launch_status();
-    }
-    int*  err = ensure_err(h);
-    void* ws  = h->borrow(ws_bytes);
-    if(!ws || !err)
+    int*  err = plan.recursive ? ensure_err(h) : nullptr;
+    void* ws  = plan.total ? h->borrow(plan.total) : nullptr;
+    if(plan.recursive && (!ws || !err))
         return rocblas_status_memory_error;
-    pr.err_dev = err;
-    BatchPtr<double> inv;
-    inv.base   = reinterpret_cast<double*>(ws);
-    inv.stride = (int64_t)kInvNB * k;
-    build_invA<double>(pr, inv);
-    pr.invA = inv;
-    MixedRecursive rec{{pr, (int)k, (int)ceil_div(k, kInvNB)}};
-    rec.S        = slices;
-    rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
-    rec.err_dev  = err;
-    if(ch_bytes)
-        rec.chain_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes + (sl_bytes + 255) / 256 * 256;
-    rec.solve_mixed(0, rec.nblk, 1);
-    if(!rec.ok)
+    if(!mixed_run(pr, slices, plan, ws, err, true))
         return rocblas_status_arch_mismatch;
     return launch_status();
 }
@@ -1683,6 +1710,243 @@ struct HostPathRes
 
 namespace
 {
+
+// ---- precision form with iterative refinement (rocblas_b200_dtrsm_refined) -------------------
+// Mixed-precision iterative refinement (Wilkinson's; Buttari, Dongarra et al. 2007 for the
+// form of LAPACK's dsgesv) around the sliced solve: the test compares the result on a sample
+// of right-hand sides with the plain FP64 form's solution of the same right-hand sides, solved
+// on a second stream while the sliced solve runs; corrections use FP64 residuals on the DMMA
+// tiles and the sliced solve with the first solve's invA.
+
+// C := C - op(A) X (side left, C rows x cols, K = m) or C - X op(A) (side right, K = n) in FP64
+// on the DMMA tiles; A's triangle is masked at load time (the strict triangle for a unit
+// diagonal, whose part the caller has already put into C), and K blocks outside it are skipped.
+void refine_product(const TrsmProblem<double>& pr, const double* X, int64_t ldx, double* C, int64_t ldc,
+                    int rows, int cols)
+{
+    GemmParams<double> g{};
+    const int tri = pr.unit ? (pr.upper ? kTriUpperStrict : kTriLowerStrict) : (pr.upper ? kTriUpper : kTriLower);
+    g.M = rows;
+    g.N = cols;
+    if(pr.side_left)
+    {
+        g.K = pr.m;
+        g.P = pr.A; g.ldp = pr.lda; g.transP = pr.trans; g.triP = tri;
+        g.Q = strided<double>(X, 0); g.ldq = ldx; g.transQ = 0; g.triQ = kTriNone;
+    }
+    else
+    {
+        g.K = pr.n;
+        g.P = strided<double>(X, 0); g.ldp = ldx; g.transP = 0; g.triP = kTriNone;
+        g.Q = pr.A; g.ldq = pr.lda; g.transQ = pr.trans; g.triQ = tri;
+    }
+    g.C = strided<double>(C, 0);
+    g.ldc = ldc;
+    g.a_imm = -1.0; g.a_user = 0;
+    g.b_imm = 1.0;  g.b_user = 0;
+    g.ualpha.val = 1.0;
+    g.zero_guard = 0;
+    launch_gemm<double>(g, 1, pr.stream, pr.sm_count);
+}
+
+// O := alpha B0(src) - (unit ? X(src) : 0) and, when Xs is given, Xs := X(src), for the rows x
+// cols output O (ld ldo); X is pr's B.  sampled: src picks the tested right-hand sides.
+void refine_prep(const TrsmProblem<double>& pr, const double* B0, int64_t ldb0, int rows, int cols, int sampled,
+                 int64_t nrhs, double alpha, int unit, double* O, int64_t ldo, double* Xs)
+{
+    const dim3 grid((unsigned)ceil_div(rows, 256), (unsigned)std::min(cols, 65535));
+    refine_prep_kernel<<<grid, 256, 0, pr.stream>>>(pr.B.base, pr.ldb, B0, ldb0, rows, cols, sampled,
+                                                    pr.side_left, nrhs, alpha, unit, O, ldo, Xs, ldo);
+    count_launch();
+}
+
+rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                 rocblas_operation trans, rocblas_diagonal diag, int m, int n,
+                                 const double* alpha, const double* A, int lda, double* B, int ldb,
+                                 const rocblas_b200_refine_options* opt, rocblas_b200_refine_info* info)
+{
+    DeviceScope device_scope; // the caller's current device is restored on return
+    if(!h)
+        return rocblas_status_invalid_handle;
+    rocblas_b200_refine_info out{};
+    rocblas_status st
+        = trsm_arg_check<double>(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, 1);
+    if(st != rocblas_status_continue)
+    {
+        if(st == rocblas_status_success && info)
+        {
+            out.converged = 1;
+            *info         = out;
+        }
+        return st;
+    }
+    if(h->pointer_mode != rocblas_pointer_mode_host)
+        return rocblas_status_not_implemented;
+    const int S = opt && opt->slices ? opt->slices : tuning().mixed_slices;
+    if(S < 1 || S > kOzMaxS || (opt && (opt->check_columns < 0 || opt->tolerance < 0.0)))
+        return rocblas_status_invalid_value;
+    const bool   left     = side == rocblas_side_left;
+    const int    nrhs     = left ? n : m;
+    const int    max_it   = opt ? (opt->max_iterations < 0 ? 10 : opt->max_iterations) : 10;
+    const int    c        = std::min(nrhs, opt && opt->check_columns > 0 ? opt->check_columns : 32);
+    const bool   fallback = opt ? opt->fallback != 0 : true;
+    const double tol      = opt && opt->tolerance > 0.0 ? opt->tolerance : 1e-12;
+    out.checked_columns   = c;
+    out.tolerance         = tol;
+    if(*alpha == 0.0)
+    {
+        if(h->size_query)
+            return rocblas_status_size_unchanged;
+        if((st = device_ready(h)) != rocblas_status_success)
+            return st;
+        zero_fill<double>(strided<double>(B, 0), ldb, m, n, 1, h->stream);
+        out.converged = 1;
+        if(info)
+            *info = out;
+        return launch_status();
+    }
+    TrsmProblem<double> pr{};
+    pr.side_left = left;
+    pr.upper     = uplo == rocblas_fill_upper;
+    pr.trans     = trans != rocblas_operation_none;
+    pr.unit      = diag == rocblas_diagonal_unit;
+    pr.m = m;
+    pr.n = n;
+    pr.batch = 1;
+    pr.A = strided<double>(A, 0);
+    pr.lda = lda;
+    pr.B = strided<double>(B, 0);
+    pr.ldb = ldb;
+    pr.stream    = h->stream;
+    pr.sm_count  = h->sm_count;
+    pr.alpha.val = *alpha;
+    // the tested right-hand sides, solved by the plain FP64 form: side left m x c, side right
+    // c x n (the same rows of B), ld = their row count
+    TrsmProblem<double> ps = pr;
+    const int           srows = left ? m : c, scols = left ? c : n;
+    ps.m   = srows;
+    ps.n   = scols;
+    ps.ldb = srows;
+    // workspace: the precision form's | B0 (m x n) | R (m x n) | the tested right-hand sides |
+    // their chain flags | the test's maxima
+    const MixedPlan plan  = mixed_plan(pr, S);
+    const size_t    mn    = (size_t)m * n * sizeof(double);
+    const size_t    smp   = (size_t)srows * scols * sizeof(double);
+    const size_t    fl    = use_chain(ps) ? chain_workspace_bytes(chain_shape_of(ps)) : 0;
+    const size_t    o_b0  = align256(plan.total), o_r = o_b0 + align256(mn);
+    const size_t    o_xs  = o_r + (max_it > 0 ? align256(mn) : 0), o_fl = o_xs + align256(smp);
+    const size_t    o_mx  = o_fl + align256(fl);
+    const size_t    total = o_mx + align256(sizeof(double) * 2 * (size_t)c);
+    if(h->size_query)
+        return h->set_optimal_size(total);
+    if((st = device_ready(h)) != rocblas_status_success)
+        return st;
+    if(!h->host_res)
+        h->host_res = new HostPathRes();
+    HostPathRes& res = *h->host_res;
+    cudaEvent_t  ev_ready = nullptr, ev_ref = nullptr;
+    if(!res.init() || !(ev_ready = res.event(0)) || !(ev_ref = res.event(1)))
+        return rocblas_status_internal_error;
+    int*           err = ensure_err(h);
+    unsigned char* ws  = reinterpret_cast<unsigned char*>(h->borrow(total));
+    if(!ws || !err)
+        return rocblas_status_memory_error;
+    pr.err_dev = ps.err_dev = err;
+    double*      B0 = reinterpret_cast<double*>(ws + o_b0);
+    double*      R  = reinterpret_cast<double*>(ws + o_r);
+    double*      Xs = reinterpret_cast<double*>(ws + o_xs);
+    double*      mx = reinterpret_cast<double*>(ws + o_mx);
+    cudaStream_t s  = h->stream;
+
+    // B0 := B; the tested right-hand sides gathered; invA built once for every solve below
+    cudaMemcpy2DAsync(B0, (size_t)m * sizeof(double), B, (size_t)ldb * sizeof(double),
+                      (size_t)m * sizeof(double), n, cudaMemcpyDeviceToDevice, s);
+    refine_prep(pr, B0, m, srows, scols, 1, nrhs, 1.0, 0, Xs, srows, nullptr);
+    if(plan.recursive)
+    {
+        BatchPtr<double> inv;
+        inv.base   = reinterpret_cast<double*>(ws);
+        inv.stride = (int64_t)kInvNB * pr.k();
+        build_invA<double>(pr, inv);
+        ps.invA = inv;
+    }
+    // the reference solve of the tested right-hand sides on the side stream, overlapping the
+    // precision-form solve (it is latency-bound and takes the SMs the solve leaves idle)
+    cudaEventRecord(ev_ready, s);
+    cudaStreamWaitEvent(res.tri, ev_ready, 0);
+    ps.B      = strided<double>(Xs, 0);
+    ps.stream = res.tri;
+    trsm_run<double>(ps, fl ? ws + o_fl : nullptr, plan.recursive);
+    cudaEventRecord(ev_ref, res.tri);
+
+    if(!mixed_run(pr, S, plan, ws, err, false))
+        return rocblas_status_arch_mismatch;
+    cudaStreamWaitEvent(s, ev_ref, 0);
+
+    // the test: max over the tested right-hand sides v of ||x_v - xref_v||_inf / ||xref_v||_inf
+    std::vector<double> hmx(2 * (size_t)c);
+    auto test = [&](double* err_est) -> rocblas_status {
+        refine_compare_kernel<<<(unsigned)c, 256, 0, s>>>(B, ldb, Xs, srows, scols, left, nrhs, mx);
+        count_launch();
+        if(cudaMemcpyAsync(hmx.data(), mx, hmx.size() * sizeof(double), cudaMemcpyDeviceToHost, s)
+               != cudaSuccess
+           || cudaStreamSynchronize(s) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return rocblas_status_internal_error;
+        }
+        double e = 0.0;
+        for(int v = 0; v < c; ++v)
+        {
+            const double d = hmx[2 * (size_t)v], x = hmx[2 * (size_t)v + 1];
+            const double ev = d == 0.0 ? 0.0 : d / x; // x == 0 with d != 0: inf
+            if(!(ev <= e))                            // NaN propagates
+                e = ev;
+        }
+        *err_est = e;
+        return rocblas_status_success;
+    };
+
+    double e = 0.0;
+    if((st = test(&e)) != rocblas_status_success)
+        return st;
+    out.error_estimate_first = e;
+    TrsmProblem<double> prc = pr; // the correction solve: op(A) D = R
+    prc.B         = strided<double>(R, 0);
+    prc.ldb       = m;
+    prc.alpha.val = 1.0;
+    while(!(e <= tol) && out.iterations < max_it)
+    {
+        // R := alpha B0 - op(A) X in FP64, D := the precision-form solve of op(A) D = R, X += D
+        refine_prep(pr, B0, m, m, n, 0, nrhs, *alpha, pr.unit, R, m, nullptr);
+        refine_product(pr, B, ldb, R, m, m, n);
+        if(!mixed_run(prc, S, plan, ws, err, false))
+            return rocblas_status_arch_mismatch;
+        const dim3 grid((unsigned)ceil_div(m, 256), (unsigned)std::min(n, 65535));
+        refine_update_kernel<<<grid, 256, 0, s>>>(B, ldb, R, m, m, n);
+        count_launch();
+        ++out.iterations;
+        if((st = test(&e)) != rocblas_status_success)
+            return st;
+    }
+    out.error_estimate = e;
+    out.converged      = e <= tol;
+    if(!out.converged && fallback)
+    {
+        // the plain FP64 form from the original right-hand sides
+        cudaMemcpy2DAsync(B, (size_t)ldb * sizeof(double), B0, (size_t)m * sizeof(double),
+                          (size_t)m * sizeof(double), n, cudaMemcpyDeviceToDevice, s);
+        st = trsm_impl<double>(h, side, uplo, trans, diag, m, n, alpha, A, strided<double>(A, 0), lda, B,
+                               strided<double>(B, 0), ldb, 1, nullptr, BatchPtr<double>{}, 0);
+        if(st != rocblas_status_success && st != rocblas_status_perf_degraded)
+            return st;
+        out.fell_back = 1;
+    }
+    if(info)
+        *info = out;
+    return launch_status();
+}
+
 
 // The precision form with A and B in host memory: the call copies A's triangle and B to the
 // device, solves, and copies X back into B, returning when B holds X.  For side left the
@@ -2912,6 +3176,21 @@ rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle h, rocblas_side side, roc
 try
 {
     return trsm_mixed_impl(h, side, uplo, transA, diag, m, n, alpha, A, lda, B, ldb, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dtrsm_refined(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
+                                          rocblas_operation transA, rocblas_diagonal diag,
+                                          rocblas_int m, rocblas_int n, const double* alpha,
+                                          const double* A, rocblas_int lda, double* B, rocblas_int ldb,
+                                          const rocblas_b200_refine_options* options,
+                                          rocblas_b200_refine_info*          info)
+try
+{
+    return trsm_refined_impl(h, side, uplo, transA, diag, m, n, alpha, A, lda, B, ldb, options, info);
 }
 catch(...)
 {

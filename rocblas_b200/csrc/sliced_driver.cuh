@@ -184,9 +184,13 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
     OzPass        passes[2];
     const int     npass = plan_oz_passes(S, passes);
     const int64_t K = std::max<int64_t>(g.K, 0);
-    for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kOzKMax)
+    // K ranges with their own exponents, accumulated in FP64 through C (beta = 1 after the
+    // first): at most kOzKMax keeps the int32 sums exact, shorter ones keep more bits of
+    // entries far below their row's (column's) maximum
+    const int64_t kchunk = std::max<int64_t>(64, std::min<int64_t>(kOzKMax, tuning().sliced_k_chunk / 64 * 64));
+    for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kchunk)
     {
-        const int64_t kc = std::min<int64_t>(kOzKMax, K - k0);
+        const int64_t kc = std::min<int64_t>(kchunk, K - k0);
         const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kOzSliceTile);
         unsigned char* w = reinterpret_cast<unsigned char*>(ws);
         int8_t* sP = reinterpret_cast<int8_t*>(w);

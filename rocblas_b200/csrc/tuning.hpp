@@ -36,6 +36,9 @@ struct Tuning
                                      // many 128-row blocks (< 2: recursion down to the leaves)
     int host_step_blocks     = 4;    // precision form on host buffers: rows per pipelined step,
                                      // in 128-row blocks
+    int sliced_k_chunk       = 16384; // sliced GEMM: K range per set of row / column exponents
+                                      // (multiple of 64, at most 16384); shorter ranges keep
+                                      // more bits of entries far below their row's maximum
 };
 
 struct TuningEntry
@@ -61,6 +64,7 @@ static const TuningEntry kTuningEntries[] = {
     {"chain_w", &Tuning::chain_w, 0, 64},
     {"mixed_chain_blocks", &Tuning::mixed_chain_blocks, 0, 1 << 20},
     {"host_step_blocks", &Tuning::host_step_blocks, 1, 1 << 20},
+    {"sliced_k_chunk", &Tuning::sliced_k_chunk, 64, 16384},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

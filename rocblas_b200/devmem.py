@@ -68,6 +68,24 @@ def trsm(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, alpha_on_
     return check("rocblas_trsm", st, allow)
 
 
+def trsm_refined(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, slices=0,
+                 max_iterations=-1, check_columns=0, fallback=1, tolerance=0.0,
+                 allow=(status_success,)):
+    """rocblas_b200_dtrsm_refined on FP64 device tensors (host alpha); returns the
+    rocblas_b200_refine_info fields as a dict."""
+    from . import RefineInfo, RefineOptions
+
+    a = ctypes.c_double(alpha)
+    opts = RefineOptions(slices, max_iterations, check_columns, fallback, tolerance)
+    info = RefineInfo()
+    st = lib().rocblas_b200_dtrsm_refined(
+        handle.value, _code(SIDE, side), _code(UPLO, uplo), _code(TRANS, trans), _code(DIAG, diag), m, n,
+        ctypes.cast(ctypes.byref(a), ctypes.c_void_p), _ptr(A), lda, _ptr(B), ldb,
+        ctypes.cast(ctypes.byref(opts), ctypes.c_void_p), ctypes.cast(ctypes.byref(info), ctypes.c_void_p))
+    check("rocblas_b200_dtrsm_refined", st, allow)
+    return info.as_dict()
+
+
 def trsm_ex(handle, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, invA, invA_size,
             alpha_on_device=False, allow=(status_success,)):
     keep, aptr = _alpha(handle, alpha, B.dtype, alpha_on_device, B.device)
