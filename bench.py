@@ -1,22 +1,26 @@
 """TRSM benchmark: one JSON line on rank 0.
 
 Headline workload: dtrsm side=L, uplo=L, transA=N, diag=N, m=16384, n=4096, alpha=1, lda=ldb=m,
-solved by the precision form (rocblas_b200_dtrsm_mixed: trailing updates from int8 slices on
-the tcgen05 tensor cores, FP64 diagonal blocks) and, beside it, by the plain FP64 form
-(rocblas_dtrsm).  A is the condition-band recipe (band k=0) with a NaN upper triangle;
-B ~ U(-1,1).  One step = restore the right-hand side (a device copy of 512 MiB, inside the timed
-region) + one solve through the C ABI.  A (2 GiB) and B (512 MiB) are larger than the 126 MB L2,
-so no flush is needed between steps.  Errors are reported per condition band k in {0,2,4,6}
-against the float128 oracle and the host FP64 CBLAS.  The end-to-end figure (`e2e`) calls
+solved by the refined precision form (rocblas_b200_dtrsm_refined: trailing updates from int8
+slices on the tcgen05 tensor cores, FP64 diagonal blocks, then the test against the plain FP64
+solve of sampled right-hand sides and, when it fails, FP64-residual corrections) and, beside it,
+by the plain FP64 form (rocblas_dtrsm).  A is the condition-band recipe at k=0 (off-diagonal
+N(0,1)/sqrt(m), diagonal 1 + U(0, 0.1)) with a NaN upper triangle; B ~ U(-1,1).  One step =
+restore the right-hand side (a device copy of 512 MiB, inside the timed region) + one solve
+through the C ABI.  A (2 GiB) and B (512 MiB) are larger than the 126 MB L2, so no flush is
+needed between steps.  Errors are reported for that matrix and for matrices with singular values
+graded from 1 to 10^-k, k in {0,2,4,6}, against the oracle's extended-precision X* and the host
+FP64 CBLAS, with the refinement's iteration counts.  The end-to-end figure (`e2e`) calls
 rocblas_b200_dtrsm_mixed_host on pinned host buffers (transfers inside the timed region).
-Extras: the variable-size and strided batches, the serving loop, complex z/ctrsm.
+Extras: the drop-in sweep (16 combinations, FP32 and FP64, 8192-sized), the variable-size and
+strided batches, the serving loop, complex z/ctrsm.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU: a single solve does not shard (replicas only), so N ranks each run their
 own independent solve; `value` is the sum over ranks of m*n*k flops / the max-over-ranks time.
 `--impl reference` times the host CBLAS trsm (OpenBLAS bundled with scipy, the library the
-reference's ref_trsm wraps) on all host cores on a bounded column sample of the same problem.
+reference's ref_trsm wraps) on all host cores on the whole problem, every step.
 """
 from __future__ import annotations
 
@@ -49,6 +53,9 @@ SLICED_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.s
 CHAIN_TRAFFIC_PER_LAUNCH = 35.57e9
 CHAIN_TRAFFIC_SOURCE = ("same capture: the 8 plain-solve launches of trsm_chain_kernel (45.5 ms each); "
                         "A (1.07 GB) is streamed once per 64-column strip group")
+
+
+METRIC = "dtrsm TFLOP/s (refined precision form, FP64 accuracy)"
 
 
 def workload_name():
@@ -145,6 +152,15 @@ def measured_peaks():
     return out
 
 
+def headline_slices(L, S):
+    """The slice count a call with `S` uses (0: the tuning table's mixed_slices)."""
+    if S:
+        return S
+    v = ctypes.c_int(0)
+    assert L.rocblas_b200_get_tuning(b"mixed_slices", ctypes.byref(v)) == 0
+    return v.value
+
+
 def kernel_timing(L, cls):
     """(total ms, total work, launches) of one kernel class since timing was enabled."""
     ms, work, n = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_int(0)
@@ -186,37 +202,36 @@ def cpu_cblas_sample(A_host, B_host, ncols, threads):
 
 
 def run_reference(args):
+    """The reference arm: host CBLAS cblas_dtrsm (OpenBLAS, the library rocblas-test's
+    ref_trsm wraps) on all host cores, on the whole headline problem (all N right-hand sides)
+    per step; the reference's own GPU path is HIP and does not run here."""
     rank, world, _ = _env_rank()
     if rank != 0:
         return
     import oracle
 
     threads = os.cpu_count() or 1
-    rng = np.random.default_rng(0)
     m = M
     # host copy of the same recipe (numpy stream): lower triangle, zeros above for the CBLAS
-    ncols = min(N, 512)
-    A, B = oracle.condition_band_problem(0, m, ncols, 0)
+    A, B = oracle.condition_band_problem(0, m, N, 0)
     A = np.asfortranarray(np.tril(np.nan_to_num(A, nan=0.0)))
     for _ in range(args.warmup):
-        cpu_cblas_sample(A, B, ncols, threads)
+        cpu_cblas_sample(A, B, N, threads)
     times = []
     for _ in range(args.steps):
-        _, dt, _ = cpu_cblas_sample(A, B, ncols, threads)
+        _, dt, _ = cpu_cblas_sample(A, B, N, threads)
         times.append(dt)
     tot = sum(times)
-    val = float(m) * m * ncols * args.steps / tot / 1e12
-    del rng
+    val = float(m) * m * N * args.steps / tot / 1e12
     line = {
-        "metric": "dtrsm TFLOP/s (precision form, FP64 accuracy)", "value": val, "unit": "TFLOP/s",
-        "n_gpus": args.gpus,
+        "metric": METRIC, "value": val, "unit": "TFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
         "config": {"workload": workload_name(), "m": M, "n": N},
         "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
                          "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) on "
-                                   f"{ncols} of the {N} right-hand sides per step, full m={M}"},
+                                   f"the whole problem per step (all {N} right-hand sides, m={M})"},
         "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -347,6 +362,112 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
     return out
 
 
+SWEEP_SHAPES = ((8192, 8192), (8192, 512), (512, 8192))
+
+
+def sweep_matrix(torch, dev, k, uplo, diag, tdt, g):
+    """The drop-in recipe on the device: strictly-triangular entries U(-1,1)/k, diagonal
+    1 + U(0,1), the other triangle NaN, and for diag U a NaN diagonal (it must not be read);
+    returned as the (ncols, ld) view of column-major storage."""
+    At = (torch.rand(k, k, generator=g, device=dev, dtype=torch.float64) * 2 - 1) / k
+    At.diagonal().copy_(1.0 + torch.rand(k, generator=g, device=dev, dtype=torch.float64))
+    # At[j, i] = A(i, j): A lower <=> At upper, so A's upper triangle is At's strict lower one
+    mask = torch.ones(k, k, dtype=torch.bool, device=dev)
+    mask = mask.tril_(-1) if uplo == "L" else mask.triu_(1)
+    At.masked_fill_(mask, float("nan"))
+    if diag == "U":
+        At.diagonal().fill_(float("nan"))
+    return At.to(tdt).contiguous()
+
+
+def _timed_median(torch, fn, reset, reps):
+    """Median of `reps` event-timed calls of fn after one untimed call; reset() before each
+    call, outside the timing."""
+    times = []
+    for r in range(reps + 1):
+        reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        if r:
+            times.append(e0.elapsed_time(e1))
+    return statistics.median(times) * 1e-3
+
+
+def bench_sweep(torch, rb, L, h, dev, reps=3):
+    """The drop-in sweep: rocblas_{d,s}trsm for all 16 side/uplo/trans/diag combinations at
+    m = n = 8192 and the rectangular 8192 x 512 and 512 x 8192, alpha = 1, lda = k, ldb = m,
+    plus rocblas_trsm_ex with a caller-supplied invA (NB = 128, built by
+    rocblas_?trtri_strided_batched the way testing_trsm_ex.hpp:329-336 builds it) at 8192^2.
+    Each entry: TFLOP/s (m n k flops) of the median of `reps` event-timed solves after one
+    warm-up, B restored from a copy before each solve (outside the timing)."""
+    import itertools
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(8192)
+    out = {}
+    for dt, tdt in (("d", torch.float64), ("s", torch.float32)):
+        alpha = ctypes.c_double(1.0) if dt == "d" else ctypes.c_float(1.0)
+        ap = ctypes.cast(ctypes.byref(alpha), ctypes.c_void_p)
+        fn = getattr(L, f"rocblas_{dt}trsm")
+        res = {}
+        mats = {}
+        for m, n in SWEEP_SHAPES:
+            B0 = (torch.rand(n, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
+            Bt = torch.empty_like(B0)
+            shape = {}
+            for side, uplo, trans, diag in itertools.product("LR", "UL", "NT", "NU"):
+                k = m if side == "L" else n
+                key = (k, uplo, diag)
+                if key not in mats:
+                    mats = {kk: v for kk, v in mats.items() if kk[0] == k}  # keep memory bounded
+                    mats[key] = sweep_matrix(torch, dev, k, uplo, diag, tdt, g)
+                At = mats[key]
+
+                def solve():
+                    st = fn(h.value, rb.SIDE[side], rb.UPLO[uplo], rb.TRANS[trans], rb.DIAG[diag], m, n, ap,
+                            ctypes.c_void_p(At.data_ptr()), k, ctypes.c_void_p(Bt.data_ptr()), m)
+                    assert st == 0, (side, uplo, trans, diag, m, n, st)
+
+                t = _timed_median(torch, solve, lambda: Bt.copy_(B0), reps)
+                shape[side + uplo + trans + diag] = float(m) * n * k / t / 1e12
+            vals = sorted(shape.values())
+            res[f"{m}x{n}"] = {"tflops": shape, "min": vals[0], "median": statistics.median(vals),
+                               "max": vals[-1]}
+            del B0, Bt
+        mats.clear()
+        # _ex with the caller's invA at 8192^2, L/L/N/N and R/U/T/N
+        m = n = 8192
+        ex = {}
+        for side, uplo, trans, diag in (("L", "L", "N", "N"), ("R", "U", "T", "N")):
+            At = sweep_matrix(torch, dev, m, uplo, diag, tdt, g)
+            inv = torch.zeros(128 * m, dtype=tdt, device=dev)
+            tri = getattr(L, f"rocblas_{dt}trtri_strided_batched")
+            st = tri(h.value, rb.UPLO[uplo], rb.DIAG[diag], 128, ctypes.c_void_p(At.data_ptr()), m, 128 * m + 128,
+                     ctypes.c_void_p(inv.data_ptr()), 128, 128 * 128, m // 128)
+            assert st == 0, st
+            B0 = (torch.rand(n, m, generator=g, device=dev, dtype=torch.float64) * 2 - 1).to(tdt)
+            Bt = torch.empty_like(B0)
+
+            def solve_ex():
+                st = L.rocblas_trsm_ex(h.value, rb.SIDE[side], rb.UPLO[uplo], rb.TRANS[trans], rb.DIAG[diag], m,
+                                       n, ap, ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(Bt.data_ptr()), m,
+                                       ctypes.c_void_p(inv.data_ptr()), 128 * m,
+                                       rb.datatype_f64_r if dt == "d" else rb.datatype_f32_r)
+                assert st == 0, st
+
+            t = _timed_median(torch, solve_ex, lambda: Bt.copy_(B0), reps)
+            ex[side + uplo + trans + diag] = float(m) * n * m / t / 1e12
+            del At, inv, B0, Bt
+        res["ex_invA_8192x8192"] = ex
+        out[dt + "trsm"] = res
+        torch.cuda.empty_cache()
+    out["unit"] = "TFLOP/s"
+    return out
+
+
 def bench_complex(torch, L, h, dev, fp64_peak, m=8192, n=2048, steps=5):
     """Complex trsm (rocblas_ztrsm / rocblas_ctrsm, L/L/N/N) at m = 8192, n = 2048: A as the
     drop-in recipe with imaginary parts (off-diagonal (U + iU)/m, diagonal 1 + U(0,1) + iU/2),
@@ -436,6 +557,50 @@ def bench_serving(torch, dev, n_requests, rate, seed=7):
             "reuse_fraction": float(np.mean([q.a_key is not None for q in reqs]))}
 
 
+ERROR_COLUMNS = 64  # right-hand sides per band checked against the extended-precision X*
+
+
+def band_errors(torch, dev, Ab, Bb, solve_plain, solve_refined, threads):
+    """One condition band at the headline size: the plain FP64 form and the refined precision
+    form solved on the GPU (one event-timed call each), and their normwise forward errors on
+    ERROR_COLUMNS right-hand sides spread over B, against the oracle's extended-precision X*
+    (host CBLAS solve + two double-double refinement steps) and against the host FP64 CBLAS
+    solution itself."""
+    import oracle
+
+    def once(fn):
+        X = Bb.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn(X, Ab)
+        e1.record()
+        e1.synchronize()
+        return X, e0.elapsed_time(e1), r
+
+    Xp, p_ms, _ = once(solve_plain)
+    Xr, r_ms, info = once(solve_refined)
+    cols = np.linspace(0, Bb.shape[0] - 1, ERROR_COLUMNS).round().astype(np.int64)
+    A_host = np.asfortranarray(np.nan_to_num(Ab.cpu().numpy().T, nan=0.0))
+    B_s = np.asfortranarray(Bb[cols].cpu().numpy().T)
+    oracle.cblas_set_threads(threads)
+    Xh, Xl = oracle.refined_solution("L", "L", "N", "N", 1.0, A_host, B_s)
+    Xc = oracle.cblas_trsm("L", "L", "N", "N", 1.0, A_host, B_s)
+    Xr_s = Xr[cols].cpu().numpy().T
+    Xp_s = Xp[cols].cpu().numpy().T
+    del A_host
+    return {
+        "refined_vs_xstar": oracle.forward_error_dd(Xr_s, Xh, Xl),
+        "plain_fp64_vs_xstar": oracle.forward_error_dd(Xp_s, Xh, Xl),
+        "fp64_cblas_vs_xstar": oracle.forward_error_dd(Xc, Xh, Xl),
+        "refined_vs_fp64_cblas": oracle.normwise_forward_error(Xr_s, Xc),
+        "refinement_iterations": info["iterations"],
+        "converged": info["converged"], "fell_back": info["fell_back"],
+        "error_estimate_first_solve": info["error_estimate_first"],
+        "error_estimate_final": info["error_estimate"], "test_tolerance": info["tolerance"],
+        "refined_ms": r_ms, "plain_ms": p_ms,
+    }
+
+
 def run_ours(args):
     import torch
 
@@ -472,16 +637,25 @@ def run_ours(args):
         if st != 0:
             raise rb.RocblasError("rocblas_dtrsm", st)
 
-    def solve_mixed(Bbuf, Abuf):
-        st = L.rocblas_b200_dtrsm_mixed(h.value, *args_common, ctypes.c_void_p(Abuf.data_ptr()), M,
-                                        ctypes.c_void_p(Bbuf.data_ptr()), M, S)
+    opts = rb.RefineOptions(S, -1, args.check_columns, 1, 0.0)
+    opts_p = ctypes.cast(ctypes.byref(opts), ctypes.c_void_p)
+    last_info = rb.RefineInfo()
+    info_p = ctypes.cast(ctypes.byref(last_info), ctypes.c_void_p)
+
+    def solve_refined(Bbuf, Abuf):
+        # the headline: precision-form solve, the test against the plain FP64 solve of sampled
+        # right-hand sides and, if it fails, FP64-residual corrections (the call returns once
+        # the test has been read)
+        st = L.rocblas_b200_dtrsm_refined(h.value, *args_common, ctypes.c_void_p(Abuf.data_ptr()), M,
+                                          ctypes.c_void_p(Bbuf.data_ptr()), M, opts_p, info_p)
         if st != 0:
-            raise rb.RocblasError("rocblas_b200_dtrsm_mixed", st)
+            raise rb.RocblasError("rocblas_b200_dtrsm_refined", st)
+        return last_info.as_dict()
 
     # workspace by the size-query protocol, reserved before timing (no allocation inside)
     assert L.rocblas_start_device_memory_size_query(h.value) == 0
     L.rocblas_dtrsm(h.value, *args_common, None, M, None, M)
-    L.rocblas_b200_dtrsm_mixed(h.value, *args_common, None, M, None, M, S)
+    L.rocblas_b200_dtrsm_refined(h.value, *args_common, None, M, None, M, opts_p, None)
     ws = ctypes.c_size_t(0)
     assert L.rocblas_stop_device_memory_size_query(h.value, ctypes.byref(ws)) == 0
     assert L.rocblas_set_device_memory_size(h.value, ws.value) == 0
@@ -512,23 +686,23 @@ def run_ours(args):
         total = max_over_ranks(dist, t0.elapsed_time(t1), dev)
         return total, [ev_m[i].elapsed_time(ev_e[i]) for i in range(steps)], launches
 
-    # ---- timed region: the precision form (headline), then the plain FP64 form ---------------
+    # ---- timed region: the refined precision form (headline), then the plain FP64 form -------
     # Every launch of the dominant kernels is bracketed by CUDA events on its stream inside the
     # timed region (rocblas_b200_kernel_timing_*), for the roofline of the kernel itself.
     sampler = ClockSampler(dev.index if dev.index is not None else 0)
     sampler.start()
     for _ in range(max(args.warmup, 0)):
         Bt.copy_(B0)
-        solve_mixed(Bt, At)
+        solve_refined(Bt, At)
     L.rocblas_b200_kernel_timing_enable(1)
-    total_ms, solve_ms, launches = timed(solve_mixed, args.steps, 0)
+    total_ms, solve_ms, launches = timed(solve_refined, args.steps, 0)
+    headline_info = last_info.as_dict()
     sliced_t = kernel_timing(L, "sliced")
     mixed_chain_t = kernel_timing(L, "chain")
     L.rocblas_b200_kernel_timing_enable(0)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = replicas_value(FLOPS, world, ms_per_step) / 1e12
-    X_mixed_band0 = Bt.clone()
     for _ in range(max(args.warmup, 0)):
         Bt.copy_(B0)
         solve_plain(Bt, At)
@@ -536,7 +710,6 @@ def run_ours(args):
     p_total, p_solve, p_launches = timed(solve_plain, args.steps, 0)
     chain_t = kernel_timing(L, "chain")
     L.rocblas_b200_kernel_timing_enable(0)
-    X_plain_band0 = Bt.clone()
     plain_value = replicas_value(FLOPS, world, p_total / args.steps) / 1e12
 
     # ---- e2e: host buffers through the C ABI, copies inside the timed region -----------
@@ -578,71 +751,54 @@ def run_ours(args):
         e2e = {"value": FLOPS / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(a_h2d + B0.numel() * 8),
                "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms,
-               "form": f"precision form, {S} slices, rocblas_b200_dtrsm_mixed_host on pinned host "
+               "form": f"precision form, {headline_slices(L, S)} slices, rocblas_b200_dtrsm_mixed_host on pinned host "
                        "buffers (transfers of A's block rows, of B and of X overlap the left-looking solve)"}
         del A_host, B_host
 
-    # ---- errors per condition band against the float128 / FP64 host oracles, CPU baseline -------
+    # ---- errors per condition band against the extended-precision oracle, CPU baseline --------
     extra = {}
+    peak = None
     if rank == 0:
         import oracle
 
         peak = fp64_peak_tflops(torch, dev)
-        med_mixed = statistics.median(solve_ms)
+        med_ref = statistics.median(solve_ms)
         med_plain = statistics.median(p_solve)
         threads = os.cpu_count() or 1
-        cols = list(range(8))
-        bands = {}
-        cpu = None
-        for kb in (0, 2, 4, 6):
-            if kb == 0:
-                Ab, Bb, Xm, Xp = At, B0, X_mixed_band0, X_plain_band0
-            else:
-                Ab, Bb = workloads.condition_band_lower_torch(M, N, kb, seed=99 + kb, device=dev)
-                Xm, Xp = Bb.clone(), Bb.clone()
-                solve_mixed(Xm, Ab)
-                solve_plain(Xp, Ab)
-                torch.cuda.synchronize(dev)
-            A_host = np.asfortranarray(np.nan_to_num(Ab.cpu().numpy().T, nan=0.0))
-            B_host = np.asfortranarray(Bb.cpu().numpy().T)
-            Xq = oracle.trsm("L", "L", "N", "N", 1.0, A_host, np.asfortranarray(B_host[:, cols]),
-                             precision="q")
-            Xm_h = Xm.cpu().numpy().T
-            Xp_h = Xp.cpu().numpy().T
-            if kb == 0:
-                ncols = min(N, 512)
-                cpu_tflops, cpu_s, Xc = cpu_cblas_sample(A_host, B_host, ncols, threads)
-                cpu = (cpu_tflops, cpu_s, ncols)
-                Xc8 = Xc[:, cols]
-            else:
-                _, _, Xc8 = cpu_cblas_sample(A_host, B_host, len(cols), threads)
-            bands[f"k{kb}"] = {
-                "precision_form_vs_float128": oracle.normwise_forward_error(Xm_h[:, cols], Xq),
-                "plain_fp64_vs_float128": oracle.normwise_forward_error(Xp_h[:, cols], Xq),
-                "fp64_cblas_vs_float128": oracle.normwise_forward_error(Xc8, Xq),
-                "precision_form_vs_fp64_cblas": oracle.normwise_forward_error(Xm_h[:, cols], Xc8),
-                "refinement_iterations": 0,
-            }
-            del A_host, B_host
+        bands = {"c2_recipe_k0": band_errors(torch, dev, At, B0, solve_plain, solve_refined, threads)}
+        if not args.no_bands:
+            for kb, Ab, Bb in workloads.graded_condition_bands_torch(M, N, (0, 2, 4, 6), seed=99, device=dev):
+                bands[f"graded_k{kb}"] = band_errors(torch, dev, Ab, Bb, solve_plain, solve_refined, threads)
+                del Ab, Bb
+            torch.cuda.empty_cache()
+        # host CBLAS on the whole headline problem (all N right-hand sides), all host cores
+        A_host = np.asfortranarray(np.nan_to_num(At.cpu().numpy().T, nan=0.0))
+        B_host = np.asfortranarray(B0.cpu().numpy().T)
+        cpu_tflops, cpu_s, _ = cpu_cblas_sample(A_host, B_host, N, threads)
+        del A_host, B_host
         pk = measured_peaks()
         # dominant kernel of the headline: the integer-slice GEMM (ozaki_gemm_kernel), work =
         # int8 tensor operations of its slice pairs (2 * pairs * M * N * K per launch), timed
-        # per launch with CUDA events on the solve's stream inside the timed region
+        # per launch with CUDA events on the solve's stream inside the timed region.  The peak is
+        # the burst figure: the kernel is timed in short launches and the clocks stay at their
+        # maximum (the `clocks` record), not under the power cap the sustained figure saw.
         s_ms, s_ops, s_n = sliced_t
         achieved = s_ops / (s_ms * 1e-3) / 1e12 if s_ms > 0 else 0.0
-        i8_peak = 2.0 * pk["bf16_tflops_sustained"]
+        i8_peak = 2.0 * pk["bf16_tflops"]
+        S_used = headline_slices(L, S)
         roofline = {"bound": "tensor", "achieved": achieved, "peak": i8_peak, "unit": "TOP/s (int8)",
                     "frac": achieved / i8_peak, "traffic": SLICED_TRAFFIC_PER_LAUNCH,
-                    "kernel": f"ozaki_gemm_kernel<64,64,{S}> (tcgen05 kind::i8, {S} slices)",
+                    "kernel": f"ozaki_gemm_kernel<64,64,{S_used}> (tcgen05 kind::i8, {S_used} slices)",
                     "launches": s_n, "kernel_ms_per_step": s_ms / args.steps,
                     "kernel_share_of_step": s_ms / total_ms,
-                    "peak_source": "int8 dense = 2 x bf16_tflops_sustained of " + pk["source"]
-                                   + " (B200 int8 dense rate is twice bf16); the kernel runs inside a "
-                                     "long step",
+                    "peak_source": "int8 dense = 2 x bf16_tflops (burst) of " + pk["source"]
+                                   + " (B200's dense int8 rate is twice bf16)",
+                    "frac_of_sustained": achieved / (2.0 * pk["bf16_tflops_sustained"]),
+                    "sm_mhz_median": clocks.get("sm_mhz"),
                     "traffic_source": SLICED_TRAFFIC_SOURCE,
-                    "fp64_equivalent": {"achieved": FLOPS / (med_mixed * 1e-3) / 1e12, "peak": peak,
-                                        "unit": "TFLOP/s", "what": "whole solve, m*n*k flops, against "
-                                        "cuBLAS DGEMM 8192^3 measured in this run"}}
+                    "fp64_equivalent": {"achieved": FLOPS / (med_ref * 1e-3) / 1e12, "peak": peak,
+                                        "unit": "TFLOP/s", "what": "whole refined solve, m*n*k flops, "
+                                        "against cuBLAS DGEMM 8192^3 measured in this run"}}
         c_ms, c_fl, c_n = chain_t
         plain_roofline = {"bound": "tensor", "kernel": "trsm_chain_kernel (mma.sync f64 DMMA)",
                           "achieved": c_fl / (c_ms * 1e-3) / 1e12 if c_ms > 0 else 0.0, "peak": peak,
@@ -651,47 +807,70 @@ def run_ours(args):
                           "traffic": CHAIN_TRAFFIC_PER_LAUNCH, "traffic_source": CHAIN_TRAFFIC_SOURCE,
                           "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul fp64) measured in this run; "
                                          "MEASURED_PEAKS.json has no FP64 figure"}
+        worst = max(b["refined_vs_xstar"] for b in bands.values())
         extra = {
+            # the two targets and the accuracy evidence first, where a truncated record keeps them
+            "plain_fp64_tflops": plain_value,
+            "refined_vs_plain": value / plain_value,
+            "plain_frac_of_measured_dgemm": plain_value / peak,
+            "max_refined_error_vs_xstar": worst,
+            "refinement_iterations": {k: b["refinement_iterations"] for k, b in bands.items()},
+            "headline_refine_info": headline_info,
             "roofline": roofline,
             "plain_fp64": {"value": plain_value, "unit": "TFLOP/s", "ms_per_step": p_total / args.steps,
                            "solve_ms_median": med_plain,
                            "solve_ms_p99": float(np.percentile(p_solve, 99)),
                            "frac_of_fp64_peak": plain_value / peak,
                            "gpu_launches": int(p_launches), "roofline": plain_roofline},
-            "precision_vs_plain": value / plain_value,
-            "cpu_baseline": {"value": cpu[0], "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+            "cpu_baseline": {"value": cpu_tflops, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
                              "sample": f"host cblas_dtrsm (OpenBLAS {oracle.cblas_config().split()[1]}) "
-                                       f"on {cpu[2]} of the {N} right-hand sides, full m={M}, "
-                                       f"{cpu[1]:.2f} s"},
+                                       f"on the whole problem (all {N} right-hand sides, m={M}), one solve, "
+                                       f"{cpu_s:.2f} s"},
             "error_bands": bands,
-            "error_sample": "normwise ||X - X*||_F / ||X*||_F on right-hand sides 0..7; X* = float128 "
-                            "oracle; bands: diagonal 10^(-k i/m)",
-            "solve_ms_median": med_mixed,
+            "error_sample": f"normwise ||X - X*||_F / ||X*||_F on {ERROR_COLUMNS} right-hand sides spread "
+                            "over B (linspace); X* = host CBLAS solve + 2 double-double refinement steps "
+                            "(oracle.refined_solution); bands: c2_recipe_k0 = the headline matrix, "
+                            "graded_kK = singular values graded 1..10^-K (kappa_2 = 10^K, dlatms-style)",
+            "solve_ms_median": med_ref,
             "solve_ms_p99": float(np.percentile(solve_ms, 99)),
             "solve_ms_samples": len(solve_ms),
         }
 
     if rank == 0 and not args.no_extras:
         hbm = measured_peaks()["hbm_gbs"]
+        extra["sweep"] = bench_sweep(torch, rb, L, h, dev)
         extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
         extra["complex"] = bench_complex(torch, L, h, dev, peak)
         extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
 
     if rank == 0:
         line = {
-            "metric": "dtrsm TFLOP/s (precision form, FP64 accuracy)", "value": value,
+            "metric": METRIC, "value": value,
             "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": workload_name(), "m": M, "n": N,
-                       "form": f"precision form: int8-slice tensor-core updates ({S} slices), FP64 diagonal blocks",
+                       "form": f"refined precision form: int8-slice tensor-core updates "
+                               f"({headline_slices(L, S)} slices), FP64 diagonal blocks; test: agreement to "
+                               f"1e-12 with the plain FP64 form on {args.check_columns or 32} right-hand sides "
+                               "(solved on a second stream), FP64-residual corrections if it fails",
                        "l2": "inputs larger than L2 (A 2 GiB, B 512 MiB); no flush",
                        "step": "device copy of B (512 MiB) + one solve",
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
         }
-        line.update(extra)
+        early = ("plain_fp64_tflops", "refined_vs_plain", "plain_frac_of_measured_dgemm",
+                 "max_refined_error_vs_xstar", "refinement_iterations")
+        head = {k: line[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup",
+                                     "ms_per_step", "higher_is_better", "scaling", "vs_baseline",
+                                     "dtype", "data")}
+        head.update({k: extra[k] for k in early if k in extra})
+        head.update({k: v for k, v in line.items() if k not in head})
+        head.update({k: v for k, v in extra.items() if k not in head})
+        # the targets again as the last key, so that either end of a cut record shows them
+        head["targets"] = {k: extra.get(k) for k in early}
+        line = head
         print(json.dumps(line), flush=True)
     h.close()
     if dist:
@@ -793,7 +972,7 @@ def run_case(args):
 
         def run():
             if args.case == "sliced":
-                st = L.rocblas_b200_dgemm_sliced(*gemm_args, args.slices)
+                st = L.rocblas_b200_dgemm_sliced(*gemm_args, headline_slices(L, args.slices))
             else:
                 st = L.rocblas_b200_dgemm(*gemm_args)
             assert st == 0, st
@@ -815,10 +994,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--m", type=int, default=M, help="problem size (profiling runs use smaller)")
     ap.add_argument("--n", type=int, default=N)
-    ap.add_argument("--slices", type=int, default=7, help="slices of the precision form")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="slices of the precision form (0: the tuning table's mixed_slices)")
     ap.add_argument("--serving-requests", type=int, default=200000)
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched and serving sections (profiling runs)")
+                    help="skip the sweep, batched, complex and serving sections (profiling runs)")
+    ap.add_argument("--no-bands", action="store_true",
+                    help="skip the graded condition bands (errors of the headline matrix only)")
+    ap.add_argument("--check-columns", type=int, default=0,
+                    help="right-hand sides the refined form's test uses (0: its default, 32)")
     ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "strsm", "vbatched", "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")

@@ -1,8 +1,8 @@
 """Autotuner for the thresholds in the library's tuning table (csrc/tuning.hpp).
 
 It times the candidate values of each entry on the GPU through the C ABI, keeps the fastest
-(or, for the slice count of the precision form, the cheapest count that meets the accuracy
-target in every condition band), and writes
+(or, for the slice count and exponent chunk of the precision form, the fastest pair that meets
+the accuracy target in every condition band), and writes
 
   rocblas_b200/tuning.cfg   "key value" lines, read by the library at first use
   rocblas_b200/tuning.json  the measurements behind every choice
@@ -20,7 +20,7 @@ import time
 import torch
 
 from . import HERE, Handle, lib
-from .workloads import condition_band_lower_torch
+from .workloads import condition_band_lower_torch, graded_condition_bands_torch
 
 
 
@@ -106,20 +106,56 @@ def tune(quick=False, out_dir=HERE):
     set_tuning("chain_w", _pick(res))
     report["entries"]["chain_w"] = {"chosen": _pick(res), "ms_sum_over_shapes": res}
 
-    # ---- precision form at the large shape: sliced GEMM K depth, minimum sliced K, chain depth
+    # ---- precision form: slice count and exponent chunk ---------------------------------
+    # The fastest (slices, sliced_k_chunk) at the large shape whose worst error over the
+    # condition bands stays 10x under the 1e-12 target.  Errors are measured at the large
+    # shape's height (they grow with m) on 64 right-hand sides, against the plain FP64 solve
+    # of the same system, on matrices with singular values graded from 1 to 10^-k (kappa_2 =
+    # 10^k, not removable by diagonal scaling) and on the condition-band recipe itself.
     m, n = big
     At, B0 = data[big]
+    nb = 64
+    bands = [condition_band_lower_torch(m, nb, 0, seed=40, device="cuda")]
+    bands += [(A_, B_) for _, A_, B_ in graded_condition_bands_torch(m, nb, (2, 4, 6), seed=41, device="cuda")]
+    plain = []
+    for A_, B_ in bands:
+        Xp = B_.clone()
+        b.dtrsm(A_, Xp, m, nb)
+        plain.append(Xp)
+    torch.cuda.synchronize()
 
-    def mixed_ms():
+    def mixed_ms(S):
         Bt = B0.clone()
-        return b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=7)))
+        return b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=S)))
 
-    for key, cands in (("oz_bk", [32, 64]), ("sliced_min_k", [512, 1024, 2048]),
-                       ("mixed_chain_blocks", [0, 4, 8, 16])):
+    cands = {}
+    for S in (7, 8):
+        for chunk in (16384, 4096, 2048):
+            set_tuning("sliced_k_chunk", chunk)
+            worst = 0.0
+            for (A_, B_), Xp in zip(bands, plain):
+                Xm = B_.clone()
+                b.dtrsm(A_, Xm, m, nb, mixed_slices=S)
+                torch.cuda.synchronize()
+                worst = max(worst, float(torch.linalg.norm(Xm - Xp) / torch.linalg.norm(Xp)))
+            cands[f"{S},{chunk}"] = {"worst_band_error": worst, "ms": mixed_ms(S)}
+    ok = {k: v for k, v in cands.items() if v["worst_band_error"] <= 1e-13}
+    pick = min(ok, key=lambda k: ok[k]["ms"]) if ok else "8,2048"
+    S_best, chunk_best = (int(x) for x in pick.split(","))
+    set_tuning("mixed_slices", S_best)
+    set_tuning("sliced_k_chunk", chunk_best)
+    report["entries"]["mixed_slices"] = {"chosen": S_best, "sliced_k_chunk": chunk_best, "candidates": cands,
+                                         "target": "worst band error <= 1e-13 (1e-12 with a 10x margin)",
+                                         "shape": [m, n], "error_shape": [m, nb]}
+    del bands, plain
+
+    # ---- precision form at the large shape: sliced GEMM K depth, minimum sliced K, chain depth
+    for key, cands_k in (("oz_bk", [32, 64]), ("sliced_min_k", [512, 1024, 2048]),
+                         ("mixed_chain_blocks", [0, 4, 8, 16])):
         res = {}
-        for c in cands:
+        for c in cands_k:
             set_tuning(key, c)
-            res[c] = mixed_ms()
+            res[c] = mixed_ms(S_best)
         set_tuning(key, _pick(res))
         report["entries"][key] = {"chosen": _pick(res), "ms": res, "shape": big}
     del data
@@ -137,33 +173,9 @@ def tune(quick=False, out_dir=HERE):
     set_tuning("block_min_strips_pct", _pick(res))
     report["entries"]["block_min_strips_pct"] = {"chosen": _pick(res), "ms_sum": res}
 
-    # ---- slice count of the precision form: cheapest count meeting 1e-12 in every band ----
-    # error measured against the plain FP64 solve of the same system (itself ~1e-15 from
-    # the exact solution on these bands)
-    mm, nn = (2048, 64) if quick else (4096, 64)
-    chosen = 8
-    errs = {}
-    for S in (5, 6, 7, 8):
-        worst = 0.0
-        for kb in (0, 2, 4, 6):
-            At, B0 = condition_band_lower_torch(mm, nn, kb, seed=40 + kb, device="cuda")
-            Xm, Xp = B0.clone(), B0.clone()
-            b.dtrsm(At, Xm, mm, nn, mixed_slices=S)
-            b.dtrsm(At, Xp, mm, nn)
-            torch.cuda.synchronize()
-            worst = max(worst, float(torch.linalg.norm(Xm - Xp) / torch.linalg.norm(Xp)))
-        errs[S] = worst
-    for S in (5, 6, 7, 8):
-        if errs[S] <= 1e-13:  # a 10x margin under the 1e-12 target at the tuning size
-            chosen = S
-            break
-    set_tuning("mixed_slices", chosen)
-    report["entries"]["mixed_slices"] = {"chosen": chosen, "worst_band_error": errs,
-                                         "target": "1e-12 with a 10x margin", "shape": [mm, nn]}
-
     keys = ["block_max_k", "block_always_k", "block_min_strips_pct", "sliced_min_k",
             "dmma_big_tile_pct", "mixed_slices", "oz_bn", "oz_bk", "chain_max_cols",
-            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks", "host_step_blocks"]
+            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks", "host_step_blocks", "sliced_k_chunk"]
     with open(os.path.join(out_dir, "tuning.cfg"), "w") as f:
         f.write("# written by rocblas_b200/autotune.py on " + report["device"] + "\n")
         for k in keys:
