@@ -280,8 +280,9 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  * dsgesv uses) with the low-precision solve replaced by the sliced tensor-core solve:
  *   X := precision-form solve of op(A) X = alpha B (or X op(A) = alpha B);
  *   test: `check_columns` evenly spaced right-hand sides (columns of B for side left, rows for
- *         side right) are also solved by the plain FP64 form, on a second stream while the
- *         precision-form solve runs; the test passes when, for each of them,
+ *         side right) are also solved by the plain FP64 form, on a second stream and a few SMs
+ *         of their own (tuning key refine_check_sms) while the precision-form solve runs on
+ *         the others; the test passes when, for each of them,
  *         ||x - x_fp64||_inf <= tolerance * ||x_fp64||_inf;
  *   while the test fails and fewer than max_iterations corrections were made:
  *         R := alpha B - op(A) X in FP64 over all right-hand sides (DMMA tiles);
@@ -299,7 +300,7 @@ typedef struct rocblas_b200_refine_options
 {
     rocblas_int slices;         /* 0: the tuning table's mixed_slices */
     rocblas_int max_iterations; /* correction solves at most (negative: 10) */
-    rocblas_int check_columns;  /* right-hand sides tested (0: 32; >= their count: all) */
+    rocblas_int check_columns;  /* right-hand sides tested (0: 8; >= their count: all) */
     rocblas_int fallback;       /* 1: plain FP64 solve when the test never passes */
     double      tolerance;      /* normwise relative difference allowed (0: 1e-12) */
 } rocblas_b200_refine_options;

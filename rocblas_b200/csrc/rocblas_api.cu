@@ -1788,7 +1788,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     const bool   left     = side == rocblas_side_left;
     const int    nrhs     = left ? n : m;
     const int    max_it   = opt ? (opt->max_iterations < 0 ? 10 : opt->max_iterations) : 10;
-    const int    c        = std::min(nrhs, opt && opt->check_columns > 0 ? opt->check_columns : 32);
+    const int    c        = std::min(nrhs, opt && opt->check_columns > 0 ? opt->check_columns : 8);
     const bool   fallback = opt ? opt->fallback != 0 : true;
     const double tol      = opt && opt->tolerance > 0.0 ? opt->tolerance : 1e-12;
     out.checked_columns   = c;
@@ -1821,18 +1821,23 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     pr.sm_count  = h->sm_count;
     pr.alpha.val = *alpha;
     // the tested right-hand sides, solved by the plain FP64 form: side left m x c, side right
-    // c x n (the same rows of B), ld = their row count
+    // c x n (the same rows of B), ld = their row count.  That solve is a chain of dependent
+    // steps whose CTAs hold their SMs while they wait, so it gets a few SMs of its own
+    // (refine_check_sms, chain strips of 32) and the sliced solve's persistent kernels size
+    // their grids for the others.
     TrsmProblem<double> ps = pr;
     const int           srows = left ? m : c, scols = left ? c : n;
     ps.m   = srows;
     ps.n   = scols;
     ps.ldb = srows;
+    const bool ps_chain = use_chain(ps);
+    ps.sm_count         = std::max(1, std::min(tuning().refine_check_sms, h->sm_count / 4));
     // workspace: the precision form's | B0 (m x n) | R (m x n) | the tested right-hand sides |
     // their chain flags | the test's maxima
     const MixedPlan plan  = mixed_plan(pr, S);
     const size_t    mn    = (size_t)m * n * sizeof(double);
     const size_t    smp   = (size_t)srows * scols * sizeof(double);
-    const size_t    fl    = use_chain(ps) ? chain_workspace_bytes(chain_shape_of(ps)) : 0;
+    const size_t    fl    = ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, 32)) : 0;
     const size_t    o_b0  = align256(plan.total), o_r = o_b0 + align256(mn);
     const size_t    o_xs  = o_r + (max_it > 0 ? align256(mn) : 0), o_fl = o_xs + align256(smp);
     const size_t    o_mx  = o_fl + align256(fl);
@@ -1844,8 +1849,9 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     if(!h->host_res)
         h->host_res = new HostPathRes();
     HostPathRes& res = *h->host_res;
-    cudaEvent_t  ev_ready = nullptr, ev_ref = nullptr;
-    if(!res.init() || !(ev_ready = res.event(0)) || !(ev_ref = res.event(1)))
+    cudaEvent_t  ev_ready = nullptr, ev_ref = nullptr, ev_copied = nullptr, ev_inv = nullptr;
+    if(!res.init() || !(ev_ready = res.event(0)) || !(ev_ref = res.event(1)) || !(ev_copied = res.event(2))
+       || !(ev_inv = res.event(3)))
         return rocblas_status_internal_error;
     int*           err = ensure_err(h);
     unsigned char* ws  = reinterpret_cast<unsigned char*>(h->borrow(total));
@@ -1858,10 +1864,16 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     double*      mx = reinterpret_cast<double*>(ws + o_mx);
     cudaStream_t s  = h->stream;
 
-    // B0 := B; the tested right-hand sides gathered; invA built once for every solve below
+    // On the side stream, once the caller's earlier work on B is done: B0 := B and the tested
+    // right-hand sides gathered, while the main stream builds invA (once, for every solve below).
+    TrsmProblem<double> pside = pr;
+    pside.stream              = res.tri;
+    cudaEventRecord(ev_ready, s);
+    cudaStreamWaitEvent(res.tri, ev_ready, 0);
     cudaMemcpy2DAsync(B0, (size_t)m * sizeof(double), B, (size_t)ldb * sizeof(double),
-                      (size_t)m * sizeof(double), n, cudaMemcpyDeviceToDevice, s);
-    refine_prep(pr, B0, m, srows, scols, 1, nrhs, 1.0, 0, Xs, srows, nullptr);
+                      (size_t)m * sizeof(double), n, cudaMemcpyDeviceToDevice, res.tri);
+    refine_prep(pside, B0, m, srows, scols, 1, nrhs, 1.0, 0, Xs, srows, nullptr);
+    cudaEventRecord(ev_copied, res.tri);
     if(plan.recursive)
     {
         BatchPtr<double> inv;
@@ -1870,16 +1882,22 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
         build_invA<double>(pr, inv);
         ps.invA = inv;
     }
-    // the reference solve of the tested right-hand sides on the side stream, overlapping the
-    // precision-form solve (it is latency-bound and takes the SMs the solve leaves idle)
-    cudaEventRecord(ev_ready, s);
-    cudaStreamWaitEvent(res.tri, ev_ready, 0);
+    // the solve overwrites B: it waits for the copies; the reference solve of the tested
+    // right-hand sides waits for invA and then runs beside the precision-form solve
+    cudaStreamWaitEvent(s, ev_copied, 0);
+    cudaEventRecord(ev_inv, s);
+    cudaStreamWaitEvent(res.tri, ev_inv, 0);
     ps.B      = strided<double>(Xs, 0);
     ps.stream = res.tri;
-    trsm_run<double>(ps, fl ? ws + o_fl : nullptr, plan.recursive);
+    if(ps_chain && plan.recursive)
+        launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, 32, ws + o_fl);
+    else
+        trsm_run<double>(ps, nullptr, false);
     cudaEventRecord(ev_ref, res.tri);
 
-    if(!mixed_run(pr, S, plan, ws, err, false))
+    TrsmProblem<double> pr1 = pr; // the first solve shares the GPU with the reference solve
+    pr1.sm_count            = std::max(1, h->sm_count - ps.sm_count);
+    if(!mixed_run(pr1, S, plan, ws, err, false))
         return rocblas_status_arch_mismatch;
     cudaStreamWaitEvent(s, ev_ref, 0);
 

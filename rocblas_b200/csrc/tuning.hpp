@@ -39,6 +39,8 @@ struct Tuning
     int sliced_k_chunk       = 16384; // sliced GEMM: K range per set of row / column exponents
                                       // (multiple of 64, at most 16384); shorter ranges keep
                                       // more bits of entries far below their row's maximum
+    int refine_check_sms     = 4;    // refined form: SMs of the FP64 solve of the tested
+                                     // right-hand sides, which runs beside the sliced solve
 };
 
 struct TuningEntry
@@ -65,6 +67,7 @@ static const TuningEntry kTuningEntries[] = {
     {"mixed_chain_blocks", &Tuning::mixed_chain_blocks, 0, 1 << 20},
     {"host_step_blocks", &Tuning::host_step_blocks, 1, 1 << 20},
     {"sliced_k_chunk", &Tuning::sliced_k_chunk, 64, 16384},
+    {"refine_check_sms", &Tuning::refine_check_sms, 1, 1024},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

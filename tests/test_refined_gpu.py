@@ -88,7 +88,7 @@ def test_refined_all_combos(handle, side, uplo, trans, diag):
     assert oracle.matrix_norm_1(X, out[:m]) <= oracle.trsm_tolerance(np.float64, max(m, n))
     assert np.isnan(out[m:]).all()
     assert info["converged"] == 1 and info["fell_back"] == 0, info
-    assert info["checked_columns"] == min(32, n if side == "L" else m)
+    assert info["checked_columns"] == min(8, n if side == "L" else m)
     assert info["tolerance"] == 1e-12
     assert info["error_estimate"] <= info["tolerance"]
 
