@@ -43,7 +43,7 @@ M, N = 16384, 4096
 FLOPS = float(M) * M * N  # m*n*k, k = m (clients/include/flops.hpp:722-725)
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch, from one ncu capture
-# of this command's own launches at the default size (profiles/launch_list_dtrsm_16384x4096.md):
+# of this command's own launches at the default size:
 # the sliced GEMM averaged over the 7 launches of a precision-form solve, and the chain kernel
 # of the plain solve (one launch per solve)
 SLICED_TRAFFIC_PER_LAUNCH = 1.0795e9

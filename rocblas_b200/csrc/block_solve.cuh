@@ -15,9 +15,11 @@
 // shared memory, and walks the diagonal in 32-row panels:
 //   1. stage the 32 x 32 diagonal tile of M (reciprocal diagonal precomputed, as the
 //      reference does at :3204-3219);
-//   2. forward substitution with warp shuffles: warp w owns columns w, w+8, w+16, w+24,
-//      lane l owns row l; each solved row value is broadcast with __shfl_sync (the
-//      reference broadcasts through LDS with two __syncthreads per row, :3225-3248);
+//   2. forward substitution of the diagonal tile: for real types one warp solves it, one
+//      column per lane held in registers, with the tile's entries broadcast from shared
+//      memory; complex types, whose column would need too many registers, spread the columns
+//      over the warps and broadcast each solved row value with __shfl_sync (the reference
+//      broadcasts through LDS with two __syncthreads per row, :3225-3248);
 //   3. rank-32 update of the remaining rows from panels of M streamed through shared
 //      memory in 64-row chunks.
 // k is at most kBlockSolveMaxK; larger systems use the blocked recursive path.
@@ -210,7 +212,13 @@ __device__ void block_solve_strip(const T* A, int64_t lda, T* B, int64_t ldb, in
                 if(j < i)
                     v = mval(p + i, p + j);
                 else if(i == j)
-                    v = unit ? T(1) : mval(p + i, p + i);
+                {
+                    // unit 1: a unit diagonal, not read; unit 2: read, and a zero entry
+                    // counts as 1 (the trtri rule for singular matrices)
+                    v = unit == 1 ? T(1) : mval(p + i, p + i);
+                    if(unit == 2 && v == T(0))
+                        v = T(1);
+                }
             }
             else if(i == j)
                 v = T(1); // padding rows solve 0 = 0

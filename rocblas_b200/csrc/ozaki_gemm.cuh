@@ -2,8 +2,8 @@
 //
 //     C := beta * C + alpha * P * Q            (P: M x K, Q: K x N, C: M x N, FP64)
 //
-// Used by the precision form of the TRSM (the trailing updates of the blocked solve and the
-// refinement residual).  The reference computes these updates with FP64 GEMMs
+// Used by the precision form of the TRSM for the trailing updates of the blocked solve (the
+// refinement's FP64 residuals run on the DMMA tiles, gemm_dmma.cuh).  The reference computes these updates with FP64 GEMMs
 // (rocblas_internal_gemm -> Tensile, library/src/blas3/Tensile/gemm_templates.cpp:41-181).
 //
 // Method (a multi-limb split in the style of Ozaki's error-free matrix product):

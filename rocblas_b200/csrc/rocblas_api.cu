@@ -73,6 +73,10 @@ rocblas_status _rocblas_handle::free_mem()
 namespace
 {
 // Device capability of the handle's device: 0 ok, otherwise a rocblas_status to return.
+// Set by the complex trtri while it solves A X = I: complex solves then read a zero non-unit
+// diagonal entry of A as 1 (the trtri rule), and no other call sees it.
+thread_local bool t_zero_diag_is_one = false;
+
 // Restores the device that was current when the scope began, if a call switched it: the
 // handle's device is made current for the call only, as the reference's
 // _rocblas_saved_device_id does (library/src/include/handle.hpp:134-170).
@@ -218,7 +222,7 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     pr.side_left = side == rocblas_side_left;
     pr.upper     = uplo == rocblas_fill_upper;
     pr.trans     = trans != rocblas_operation_none;
-    pr.unit      = diag == rocblas_diagonal_unit;
+    pr.unit      = diag == rocblas_diagonal_unit ? 1 : (is_cplx<T>::value && t_zero_diag_is_one ? 2 : 0);
     // complex trans C reads conj(A); trsv's side-right form of trans C asks for conj(A)
     // without the transpose through `conj`
     pr.conj = is_cplx<T>::value && (conj >= 0 ? conj != 0 : trans == rocblas_operation_conjugate_transpose);
@@ -997,7 +1001,9 @@ rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal 
     {
         // complex: inv(A) is the solution of A X = I, by the complex solve on invA itself (the
         // opposite triangle of the solution is exactly zero, as rocblas_trtri_fill leaves it).
-        // Unlike the reference's fused kernel a zero non-unit diagonal is not read as 1.
+        // A zero non-unit diagonal entry is read as 1, as the reference's trtri does
+        // (library/src/blas3/rocblas_trtri.hpp:128-141): the solve's diagonal tiles apply that
+        // rule while t_zero_diag_is_one is set.
         rocblas_status st = trtri_arg_check(uplo, diag, n, Aptr, lda, Xptr, ldinv, batch);
         if(h->size_query)
             return rocblas_status_size_unchanged;
@@ -1015,8 +1021,10 @@ rocblas_status trtri_impl(rocblas_handle h, rocblas_fill uplo, rocblas_diagonal 
         static const T             one = T(1);
         const rocblas_pointer_mode mode = h->pointer_mode;
         h->pointer_mode                 = rocblas_pointer_mode_host;
+        t_zero_diag_is_one = true;
         st = trsm_impl_64<T>(h, rocblas_side_left, uplo, rocblas_operation_none, diag, n, n, &one, Aptr, A,
                              lda, Xptr, X, ldinv, batch, nullptr, BatchPtr<T>{}, 0);
+        t_zero_diag_is_one = false;
         h->pointer_mode = mode;
         return st;
     }
@@ -1224,6 +1232,7 @@ rocblas_status trsm_vbatched_ex_impl(rocblas_handle h, const T* alpha,
             p.first   = 1;
             p.counter = reinterpret_cast<int*>(w.counters + c);
             p.error   = h->err_dev ? h->err_dev : w.invalid + 1;
+            p.wait_cycles = 1ll << tuning().wait_cycles_log2;
             const bool kcp = ((c >> 1) & 1) != 0, kcq = (c & 1) != 0;
             if(chain_vb_width(c) == kChainVbWideW)
                 launch_chain_w<T, kChainVbWideW, true>(p, kcp, kcq, h->sm_count, INT64_MAX, h->stream);

@@ -93,6 +93,7 @@ struct ChainParams
     int*           flags;   // one per item id, zero at launch
     int*           counter; // 8-byte claim counter, zero at launch
     int*           error;   // set to 4 if a wait timed out
+    long long      wait_cycles = 1ll << 31; // a flag wait gives up after this many clock cycles
 };
 
 __device__ __forceinline__ int chain_ld_acquire(const int* p)
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kChainThreads, 1) trsm_chain_kernel(ChainParam
                 const long long t0 = clock64();
                 while(chain_ld_acquire(f) == 0)
                 {
-                    if(clock64() - t0 > (1ll << 31))
+                    if(clock64() - t0 > p.wait_cycles)
                     {
                         atomicExch(p.error, 4);
                         s_abort = 1;

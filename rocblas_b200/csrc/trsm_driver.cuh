@@ -342,6 +342,11 @@ static ChainShape chain_shape_of(const TrsmProblem<T>& pr)
     return chain_shape(pr.k(), ncols, pr.batch, w);
 }
 
+__global__ void chain_set_counter_kernel(int* counter, int v)
+{
+    counter[0] = v; // low word of the 8-byte claim counter; the launch's memset zeroed both
+}
+
 // Chain solve of the diagonal blocks [b0, b1) of pr (all of it: 0, nblk) with invA available:
 // `first` as in Recursive::solve; `ws` holds chain_workspace_bytes of the sub-problem.
 template <typename T>
@@ -373,7 +378,15 @@ static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first
     const size_t tail = ((size_t)cs.items * sizeof(int) + 7) / 8 * 8;
     c.counter = reinterpret_cast<int*>(reinterpret_cast<char*>(flags) + tail);
     // the error word: the handle's, else a slot after the counter
-    c.error = pr.err_dev ? pr.err_dev : c.counter + 2;
+    c.error       = pr.err_dev ? pr.err_dev : c.counter + 2;
+    c.wait_cycles = 1ll << tuning().wait_cycles_log2;
+    if(tuning().chain_first_item > 0)
+    {
+        // failure injection (tests): the items before it are never claimed, so their flags
+        // stay 0 and every wait on them runs out
+        chain_set_counter_kernel<<<1, 1, 0, pr.stream>>>(c.counter, tuning().chain_first_item);
+        count_launch();
+    }
     // KCP: M's column index (K) is contiguous in memory when M(r, c) = A(c, r)
     const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
     const bool kcq = pr.side_left != 0;

@@ -41,6 +41,11 @@ struct Tuning
                                       // more bits of entries far below their row's maximum
     int refine_check_sms     = 4;    // refined form: SMs of the FP64 solve of the tested
                                      // right-hand sides, which runs beside the sliced solve
+    int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
+                                     // cycles (2^31: about a second), records error 4, returns
+    int chain_first_item     = 0;    // failure injection for tests: uniform chain launches start
+                                     // claiming items here, so the flags of the items before it
+                                     // are never set and the waits on them run out (0: off)
 };
 
 struct TuningEntry
@@ -68,6 +73,8 @@ static const TuningEntry kTuningEntries[] = {
     {"host_step_blocks", &Tuning::host_step_blocks, 1, 1 << 20},
     {"sliced_k_chunk", &Tuning::sliced_k_chunk, 64, 16384},
     {"refine_check_sms", &Tuning::refine_check_sms, 1, 1024},
+    {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
+    {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)

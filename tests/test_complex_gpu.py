@@ -242,3 +242,31 @@ def test_complex_trtri(handle, dt, uplo, diag):
     for b, A in enumerate(probs):
         Xb = inv[b * n * n:(b + 1) * n * n].view(n, n).cpu().numpy().T.astype(np.complex128)
         assert np.max(np.abs(Xb @ triangle(A, n) - np.eye(n))) <= 64 * eps * n
+
+
+@pytest.mark.parametrize("dt", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+def test_complex_trtri_zero_diagonal_reads_as_one(handle, dt, uplo):
+    """rocblas_trtri.hpp:128-141: a zero entry on a non-unit diagonal is read as 1 ("the matrix
+    is singular"); the complex trtri returns the inverse of the triangle with those entries
+    replaced by 1, and the real kernel's rule is the same."""
+    npdt, tdt = DT[dt]
+    eps = np.finfo(npdt).eps
+    n = 300
+    A, _ = oracle.nan_triangle_problem(77, "L", uplo, "N", "N", n, 1, n, n, npdt)
+    for i in (0, 5, 131, n - 1):
+        A[i, i] = 0
+    T = np.nan_to_num(np.array(A[:n, :n], dtype=np.complex128))
+    T = np.tril(T) if uplo == "L" else np.triu(T)
+    d = np.diag(T).copy()
+    d[d == 0] = 1
+    np.fill_diagonal(T, d)
+    dA = dm.to_device(A)
+    inv = dm.to_device(np.zeros((n, n), dtype=npdt, order="F"))
+    st = getattr(rb.lib(), f"rocblas_{dt}trtri")(handle.value, rb.UPLO[uplo], rb.DIAG["N"], n, _ptr(dA), n,
+                                                 _ptr(inv), n)
+    assert st == 0
+    torch.cuda.synchronize()
+    X = dm.to_host(inv).astype(np.complex128)
+    assert np.isfinite(X).all()
+    assert np.max(np.abs(X @ T - np.eye(n))) <= 64 * eps * n
