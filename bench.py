@@ -317,9 +317,31 @@ def bench_batched(torch, rb, L, h, dev, hbm_gbs, count=20000, seed=2024):
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
         t = statistics.median(times) * 1e-3
+        # the same call captured once into a CUDA graph and replayed (prepass and class
+        # launches in one graph launch)
+        cap = torch.cuda.Stream(dev)
+        h.set_stream(ctypes.c_void_p(cap.cuda_stream))
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize(dev)
+        with torch.cuda.graph(graph, stream=cap):
+            run()
+        h.set_stream(ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        gtimes = []
+        for r in range(11):
+            Bar.copy_(B0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            graph.replay()
+            e1.record()
+            e1.synchronize()
+            if r:
+                gtimes.append(e0.elapsed_time(e1))
+        del graph
+        tg = statistics.median(gtimes) * 1e-3
         flops = float(np.sum(ms * ns * ks))
         nbytes = float(np.sum(es * (ks * (ks + 1) / 2 + 2 * ms * ns)))
         out[f"vbatched_{dt}"] = {"systems": count, "solves_per_s": count / t, "ms": t * 1e3,
+                                 "graph_replay_ms": tg * 1e3, "graph_solves_per_s": count / tg,
                                  "tflops": flops / t / 1e12, "algorithmic_GBps": nbytes / t / 1e9,
                                  "hbm_frac": nbytes / t / 1e9 / hbm_gbs}
         del Aar, Bar, B0, desc, w
