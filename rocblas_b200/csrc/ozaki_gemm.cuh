@@ -514,18 +514,21 @@ __global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, in
         oz_merge_exp(exps, w, mx);
 }
 
-// one thread per row o and K chunk, for operands whose rows are adjacent in memory
-// (so == 1): consecutive threads read consecutive addresses
+// one thread per row o and K chunk of kOzExpRowsChunk, for operands whose rows are adjacent
+// in memory (so == 1): consecutive threads read consecutive addresses.  The chunk is short so
+// that the grid has enough threads to keep HBM busy (rows are few, K is long).
+constexpr int kOzExpRowsChunk = 64;
+
 __global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, int K, int* exps)
 {
     const int o  = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k0 = blockIdx.y * kOzExpChunk;
+    const int k0 = blockIdx.y * kOzExpRowsChunk;
     if(o >= O)
         return;
     // unrolled so that 16 loads are in flight per thread (the maximum does not depend on the
     // order it is taken in, so the exponents are the same)
     double    mx   = 0.0;
-    const int kend = min(K, k0 + kOzExpChunk);
+    const int kend = min(K, k0 + kOzExpRowsChunk);
 #pragma unroll 16
     for(int k = k0; k < kend; ++k)
         mx = fmax(mx, fabs(src[o + (int64_t)k * sk]));
@@ -595,19 +598,29 @@ __global__ void __launch_bounds__(256, 4)
 #pragma unroll
         for(int w = 0; w < 4; ++w)
             words[s][w] = 0;
+    // Slice s of x is the s-th base-128 digit of x 2^-e (|x 2^-e| < 1) with x's sign, i.e. what
+    // S rounds of v *= 128, q = trunc(v), v -= q produce.  Those digits are the 7-bit fields of
+    // the integer W = trunc(|x| 2^(7S - e)) < 2^(7S) <= 2^56, so one exact power-of-two scaling
+    // and one conversion replace the S rounds of FP64 arithmetic.
+    const int  se     = 7 * S - e;
+    const bool direct = se <= 1023; // 2^se is a normal double (se >= 7 - 1025 always)
+    const double scale = direct ? __longlong_as_double((long long)(1023 + se) << 52) : 0.0;
 #pragma unroll
     for(int j = 0; j < 16; ++j)
     {
-        double v = ldexp(tile[oo][kq + j], -e); // |v| < 1, exact
+        const double x = tile[oo][kq + j];
+        // exact (a scaling by a power of two); bits pushed below 2^-1074 are below 1 and would
+        // be truncated anyway.  Only rows whose largest entry is tiny take the ldexp path.
+        const double             w   = direct ? x * scale : ldexp(x, se);
+        const unsigned long long W   = __double2ull_rz(fabs(w));
+        const bool               neg = signbit(x);
 #pragma unroll
         for(int s = 0; s < kOzMaxS; ++s)
         {
             if(s < S)
             {
-                v *= 128.0;
-                const double q = trunc(v);
-                v -= q; // exact
-                const uint32_t b = (uint32_t)(uint8_t)(int8_t)(int)q;
+                const uint32_t d = (uint32_t)(W >> (7 * (S - 1 - s))) & 127u;
+                const uint32_t b = (neg ? 0u - d : d) & 0xFFu;
                 words[s][j >> 2] |= b << (8 * (j & 3));
             }
         }

@@ -69,7 +69,8 @@ static void launch_exponents(SliceOperand X, int O, int K, int* exps, cudaStream
     const unsigned kchunks = (unsigned)std::max<int64_t>(1, ceil_div(K, kOzExpChunk));
     if(X.so == 1)
     {
-        dim3 grid((unsigned)ceil_div(O, 128), kchunks);
+        const unsigned rchunks = (unsigned)std::max<int64_t>(1, ceil_div(K, kOzExpRowsChunk));
+        dim3 grid((unsigned)ceil_div(O, 128), rchunks);
         oz_exponent_rows_kernel<<<grid, 128, 0, s>>>(X.ptr, X.sk, O, K, exps);
     }
     else
