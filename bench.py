@@ -902,7 +902,8 @@ def run_ours(args):
 
 def run_case(args):
     """One kernel on one small shape, a few launches, for ncu captures (no JSON line):
-    sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; dmma: rocblas_b200_dgemm m x n x k;
+    sliced: rocblas_b200_dgemm_sliced m x n x k, S slices; crt: rocblas_b200_dgemm_crt m x n x k
+    with --moduli moduli; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
     m x n (the chain solve); strsm: rocblas_strsm L/L/N/N m x n (FP32: the recursive solve with
     FFMA tile updates above 512 columns); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
@@ -995,6 +996,8 @@ def run_case(args):
         def run():
             if args.case == "sliced":
                 st = L.rocblas_b200_dgemm_sliced(*gemm_args, headline_slices(L, args.slices))
+            elif args.case == "crt":
+                st = L.rocblas_b200_dgemm_crt(*gemm_args, args.moduli)
             else:
                 st = L.rocblas_b200_dgemm(*gemm_args)
             assert st == 0, st
@@ -1025,7 +1028,9 @@ def main():
                     help="skip the graded condition bands (errors of the headline matrix only)")
     ap.add_argument("--check-columns", type=int, default=0,
                     help="right-hand sides the refined form's test uses (0: its default, 8)")
-    ap.add_argument("--case", choices=["sliced", "dmma", "zgemm", "chain", "strsm", "vbatched", "strided", "trtri"],
+    ap.add_argument("--moduli", type=int, default=16, help="moduli of a --case crt GEMM")
+    ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "vbatched", "strided",
+                                       "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,

@@ -199,6 +199,33 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle    handle
                                                         rocblas_int       ldc,
                                                         rocblas_int       slices);
 
+/* ---- FP64 GEMM from residues modulo small moduli on the tensor cores ----------------------
+ * C := alpha op(A) op(B) + beta C in FP64 (column-major).  Every row of op(A) and column of
+ * op(B) is scaled by a power of two and truncated to a b-bit integer (b = 55 for 16 moduli and
+ * k <= 4096 per exponent range); the exact integer product is computed modulo `moduli`
+ * pairwise coprime moduli <= 256 as int8 x int8 -> int32 tensor-core products and rebuilt by
+ * the Chinese remainder theorem, then scaled back and rounded once to FP64.  moduli is 14, 15
+ * or 16 (0: 16); fewer moduli keep fewer bits (b drops by about 4 per modulus).  Inputs must be
+ * finite.  alpha and beta are host pointers (host pointer mode only; device mode returns
+ * rocblas_status_not_implemented).  The reference has no counterpart; it is the second engine
+ * of the precision form of the trsm (tuning key mixed_moduli).  Workspace from the handle
+ * (size query supported). */
+ROCBLAS_EXPORT rocblas_status rocblas_b200_dgemm_crt(rocblas_handle    handle,
+                                                     rocblas_operation transA,
+                                                     rocblas_operation transB,
+                                                     rocblas_int       m,
+                                                     rocblas_int       n,
+                                                     rocblas_int       k,
+                                                     const double*     alpha,
+                                                     const double*     A,
+                                                     rocblas_int       lda,
+                                                     const double*     B,
+                                                     rocblas_int       ldb,
+                                                     const double*     beta,
+                                                     double*           C,
+                                                     rocblas_int       ldc,
+                                                     rocblas_int       moduli);
+
 /* ---- FP64 GEMM on the DMMA tiles of the trsm updates -----------------------------------------
  * C := alpha op(A) op(B) + beta C (column-major FP64), the engine of rocblas_dtrsm's trailing
  * updates (mma.sync m16n8k8 .f64 tiles fed by cp.async), exposed as a GEMM.  Same argument

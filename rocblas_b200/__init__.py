@@ -207,6 +207,7 @@ SIGNATURES = {
     "rocblas_b200_dtrsm_vbatched_ex": (_i, [_H, _p, _p, _p, _i, _i, _i, _p]),
     "rocblas_b200_strsm_vbatched_ex": (_i, [_H, _p, _p, _p, _i, _i, _i, _p]),
     "rocblas_b200_dgemm_sliced": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
+    "rocblas_b200_dgemm_crt": (_i, [_H, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dtrsm_mixed_host": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _i]),
     "rocblas_b200_dtrsm_refined": (_i, [_H, _i, _i, _i, _i, _i, _i, _p, _p, _i, _p, _i, _p, _p]),

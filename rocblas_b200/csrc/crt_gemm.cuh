@@ -1,0 +1,685 @@
+// FP64-accurate GEMM update on the Blackwell tensor cores from residues modulo small primes
+// (a Chinese-remainder form of the integer emulation of an FP64 product).
+//
+//     C := beta * C + alpha * P * Q            (P: M x K, Q: K x N, C: M x N, FP64)
+//
+// Method:
+//   * every row r of P is scaled by 2^(b - e_r) (e_r = 1 + exponent of its largest entry) and
+//     truncated to the integer P'(r,k) = trunc(P(r,k) 2^(b - e_r)), |P'| < 2^b; every column c
+//     of Q the same way with exponents f_c, Q'(k,c);
+//   * the exact integer product X = P' Q' (|X| < K 2^2b) is computed modulo NM pairwise
+//     coprime moduli p_i <= 256 (crt_modulus): residues P'_i = P' mod p_i, Q'_i = Q' mod p_i in
+//     the symmetric range fit int8, and C_i = P'_i Q'_i is one tcgen05.mma kind::i8 GEMM whose
+//     int32 accumulation is exact (|C_i| <= K 128^2 <= 2^28 for K <= 16384);
+//   * X is rebuilt from its residues y_i = (C_i (P/p_i)^-1) mod p_i (P = prod p_i) as
+//     X = sum_i y_i (P/p_i) - q P with q = rint(sum_i y_i / p_i): the sum is taken modulo 2^128
+//     in four 32-bit limbs, which is exact because |X| < P / 8 by the choice of b
+//     (2b + log2 K <= log2 P - 3), and q from a 24-bit fixed-point sum whose error (< 2^-13) is
+//     far inside the 3/8 margin that bound leaves;
+//   * P Q ~= 2^(e_r + f_c - 2b) X, rounded once to FP64 in the epilogue.
+// With 16 moduli (P ~ 2^125.4) and K <= 4096, b = 55: every entry keeps 55 bits relative to its
+// row's (column's) largest entry and the product of the truncated operands is exact, at 16 int8
+// GEMMs where the 7-bit slice form (ozaki_gemm.cuh) needs 36 slice-pair products for 56 bits.
+//
+// Kernel layout (persistent, one CTA per SM, 320 threads; output tiles 128 x 256; the tiles of
+// a CTA are t = blockIdx.x + j * gridDim.x in a grouped order, so the CTAs in flight work on
+// neighbouring tiles and, being in step, on the same modulus, and share its residue panels in L2):
+//   warp 0    copy producer: per work item (tile, modulus) and 64-deep K step, one bulk copy of
+//             the 128 x 64 P residue tile and one of the 256 x 64 Q tile into a ring stage; the
+//             residue kernel writes the panels in the tensor cores' SWIZZLE_64B order;
+//   warp 1    TMEM owner and MMA issuer: one 128 x 256 int32 accumulator per item, two
+//             accumulators (all 512 TMEM columns) so that an item's MMAs overlap the drain of the
+//             previous one;
+//   warps 2-5 residue epilogue: tcgen05.ld of the accumulator (lanes = rows), y_i as one byte
+//             per entry into the CTA's scratch slot in global memory (L2), two slots so that a
+//             tile's residues are written while the previous tile is rebuilt;
+//   warps 6-9 reconstruction: once all NM residues of a tile are in its slot, each thread takes
+//             one row, rebuilds X for 16 columns at a time and writes beta C + alpha 2^s X.
+// Every mbarrier wait is bounded; on timeout the kernel records the error, drains its in-flight
+// copies and MMAs (again bounded), frees TMEM and returns.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <type_traits>
+
+#include "ozaki_gemm.cuh"
+
+namespace rb200
+{
+
+constexpr int kCrtMaxModuli = 16;
+constexpr int kCrtBN        = 256;  // output tile width: N of one MMA
+constexpr int kCrtBK        = 64;   // int8 K of one ring stage (SWIZZLE_64B rows)
+constexpr int kCrtThreads   = 320;  // 10 warps
+constexpr int kCrtKMax      = 16384; // |C_i| <= K 128^2 <= 2^28 keeps the residue step in int32
+constexpr int kCrtMaxBits   = 60;   // W < 2^60: three 20-bit fields in the residue kernel
+constexpr int kCrtNPad      = kCrtBN;
+constexpr int kCrtSmemBudget = 226 * 1024;
+constexpr int kCrtChunks    = kCrtBN / 16; // 16-column chunks of a tile's scratch
+constexpr int64_t kCrtSlotBytes = (int64_t)kCrtMaxModuli * kOzBM * kCrtBN; // one tile's residues
+
+// Moduli, largest first: 2^8, 3*5*17, 11*23, 251, 13*19, 241, 239, 233, 229, 227, 223, 7*31, 211,
+// 199, 197, 193 are pairwise coprime, so any prefix is a valid set; a symmetric residue of each
+// fits int8 ([-128, 127] for 256, [-(p-1)/2, (p-1)/2] for the odd ones).
+__host__ __device__ constexpr uint32_t crt_modulus(int i)
+{
+    return i == 0    ? 256u
+           : i == 1  ? 255u
+           : i == 2  ? 253u
+           : i == 3  ? 251u
+           : i == 4  ? 247u
+           : i == 5  ? 241u
+           : i == 6  ? 239u
+           : i == 7  ? 233u
+           : i == 8  ? 229u
+           : i == 9  ? 227u
+           : i == 10 ? 223u
+           : i == 11 ? 217u
+           : i == 12 ? 211u
+           : i == 13 ? 199u
+           : i == 14 ? 197u
+                     : 193u;
+}
+
+// 128-bit unsigned integers for the compile-time CRT constants.
+struct CrtU128
+{
+    unsigned long long lo, hi;
+};
+
+__host__ __device__ constexpr uint32_t crt_limb(CrtU128 a, int j)
+{
+    return (uint32_t)(j == 0 ? a.lo : j == 1 ? a.lo >> 32 : j == 2 ? a.hi : a.hi >> 32);
+}
+
+// a * m mod 2^128
+__host__ __device__ constexpr CrtU128 crt_mul(CrtU128 a, uint32_t m)
+{
+    const unsigned long long l0 = (a.lo & 0xffffffffull) * m;
+    const unsigned long long l1 = (a.lo >> 32) * m + (l0 >> 32);
+    const unsigned long long h0 = (a.hi & 0xffffffffull) * m + (l1 >> 32);
+    const unsigned long long h1 = (a.hi >> 32) * m + (h0 >> 32);
+    return {(l0 & 0xffffffffull) | (l1 << 32), (h0 & 0xffffffffull) | (h1 << 32)};
+}
+
+// floor(a / d) and a mod d for 0 < d < 2^32 (long division by 32-bit limbs)
+__host__ __device__ constexpr CrtU128 crt_div(CrtU128 a, uint32_t d)
+{
+    unsigned long long q[4] = {0, 0, 0, 0};
+    unsigned long long r    = 0;
+    for(int j = 3; j >= 0; --j)
+    {
+        const unsigned long long cur = (r << 32) | crt_limb(a, j);
+        q[j] = cur / d;
+        r    = cur % d;
+    }
+    return {q[0] | (q[1] << 32), q[2] | (q[3] << 32)};
+}
+
+__host__ __device__ constexpr uint32_t crt_rem(CrtU128 a, uint32_t d)
+{
+    unsigned long long r = 0;
+    for(int j = 3; j >= 0; --j)
+        r = ((r << 32) | crt_limb(a, j)) % d;
+    return (uint32_t)r;
+}
+
+// inverse of a modulo p (a, p coprime), by the extended Euclidean algorithm
+__host__ __device__ constexpr uint32_t crt_inverse(uint32_t a, uint32_t p)
+{
+    long long r0 = p, r1 = a % p, t0 = 0, t1 = 1;
+    while(r1 != 0)
+    {
+        const long long q = r0 / r1;
+        const long long r2 = r0 - q * r1, t2 = t0 - q * t1;
+        r0 = r1;
+        r1 = r2;
+        t0 = t1;
+        t1 = t2;
+    }
+    return (uint32_t)(((t0 % (long long)p) + (long long)p) % (long long)p);
+}
+
+// P = product of the first nm moduli
+__host__ __device__ constexpr CrtU128 crt_product(int nm)
+{
+    CrtU128 p{1, 0};
+    for(int i = 0; i < nm; ++i)
+        p = crt_mul(p, crt_modulus(i));
+    return p;
+}
+
+// M_i = P / p_i, w_i = M_i^-1 mod p_i, R_i = round(2^24 / p_i)
+__host__ __device__ constexpr CrtU128 crt_cofactor(int nm, int i)
+{
+    return crt_div(crt_product(nm), crt_modulus(i));
+}
+
+__host__ __device__ constexpr uint32_t crt_weight(int nm, int i)
+{
+    return crt_inverse(crt_rem(crt_cofactor(nm, i), crt_modulus(i)), crt_modulus(i));
+}
+
+__host__ __device__ constexpr uint32_t crt_recip24(int i)
+{
+    return ((1u << 24) + crt_modulus(i) / 2) / crt_modulus(i);
+}
+
+// the largest symmetric residue kept as is (larger ones have p subtracted)
+__host__ __device__ constexpr uint32_t crt_half(int i)
+{
+    return crt_modulus(i) == 256u ? 127u : (crt_modulus(i) - 1) / 2;
+}
+
+__host__ __device__ constexpr bool crt_tables_ok(int nm)
+{
+    for(int i = 0; i < nm; ++i)
+    {
+        const uint32_t p = crt_modulus(i);
+        for(int j = 0; j < i; ++j)
+        {
+            uint32_t a = p, b = crt_modulus(j);
+            while(b)
+            {
+                const uint32_t t = a % b;
+                a = b;
+                b = t;
+            }
+            if(a != 1)
+                return false; // not coprime
+        }
+        if(crt_rem(crt_mul(crt_cofactor(nm, i), crt_weight(nm, i)), p) != 1)
+            return false; // w_i is not the inverse of M_i
+        for(int j = 0; j < nm; ++j)
+            if(j != i && crt_rem(crt_cofactor(nm, i), crt_modulus(j)) != 0)
+                return false; // M_i must vanish modulo the other moduli
+    }
+    return (crt_product(nm).hi >> 63) == 0; // P < 2^127: X_sym and its limbs stay signed-safe
+}
+static_assert(crt_tables_ok(8) && crt_tables_ok(12) && crt_tables_ok(14) && crt_tables_ok(15)
+                  && crt_tables_ok(16),
+              "CRT constants");
+
+// log2 P of the first nm moduli (host side, for the choice of b)
+inline double crt_log2_product(int nm)
+{
+    double s = 0.0;
+    for(int i = 0; i < nm; ++i)
+        s += __builtin_log2((double)crt_modulus(i));
+    return s;
+}
+
+// Bits b kept per entry for a pass of depth K: K 2^2b <= P / 8.
+inline int crt_bits(int nm, int64_t K)
+{
+    int lk = 0;
+    while((int64_t(1) << lk) < std::max<int64_t>(K, 1))
+        ++lk;
+    const int b = (int)((crt_log2_product(nm) - 3.0 - lk) / 2.0);
+    return std::min(b, kCrtMaxBits);
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [I0, I1).
+template <int I0, int I1, class F>
+__host__ __device__ __forceinline__ void crt_static_for(F&& f)
+{
+    if constexpr(I0 < I1)
+    {
+        f(std::integral_constant<int, I0>{});
+        crt_static_for<I0 + 1, I1>(f);
+    }
+}
+
+// ---- residues --------------------------------------------------------------------------------
+// Operand element (o, k) at src[o * so + k * sk]; exps[o] from launch_exponents (1 + exponent of
+// the row's largest |x|; kOzExpNone for an all-zero row, whose residues are 0).  The residue
+// modulo p_i of row o, column k lives in the K panel kc = k / 64 as
+// dst[((i * K_pad / 64 + kc) * O_pad + o) * 64 + swizzled(k % 64)], the layout of the slice
+// panels (ozaki_gemm.cuh): every panel is the row-major image of O_pad rows of 64 bytes with the
+// 16-byte chunks of a row permuted for SWIZZLE_64B.  Rows o >= O and columns k >= K are zero.
+//
+// Per entry: W = trunc(|x| 2^(bits - e)) < 2^bits (one exact power-of-two scaling and a 64-bit
+// conversion), split into three 20-bit fields W = a 2^40 + m 2^20 + c, so that
+// W mod p = (a (2^40 mod p) + m (2^20 mod p) + c) mod p is one 32-bit remainder by a constant.
+template <int NM>
+__global__ void __launch_bounds__(256, 2)
+    crt_residue_kernel(const double* src, int64_t so, int64_t sk, int O, int K, const int* exps,
+                       int bits, int8_t* dst, int O_pad, int K_pad)
+{
+    __shared__ double tile[kOzSliceTile][kOzSliceTile + 1];
+    const int  o0 = blockIdx.y * kOzSliceTile, k0 = blockIdx.x * kOzSliceTile;
+    const int  tid    = threadIdx.x;
+    const bool o_fast = so == 1;
+    constexpr int kLoads = kOzSliceTile * kOzSliceTile / 256;
+    double        ld[kLoads];
+#pragma unroll
+    for(int it = 0; it < kLoads; ++it)
+    {
+        const int idx = tid + it * 256;
+        const int oo  = o_fast ? idx % kOzSliceTile : idx / kOzSliceTile;
+        const int kk  = o_fast ? idx / kOzSliceTile : idx % kOzSliceTile;
+        const int o = o0 + oo, k = k0 + kk;
+        ld[it] = (o < O && k < K) ? src[(int64_t)o * so + (int64_t)k * sk] : 0.0;
+    }
+#pragma unroll
+    for(int it = 0; it < kLoads; ++it)
+    {
+        const int idx = tid + it * 256;
+        const int oo  = o_fast ? idx % kOzSliceTile : idx / kOzSliceTile;
+        const int kk  = o_fast ? idx / kOzSliceTile : idx % kOzSliceTile;
+        tile[oo][kk]  = ld[it];
+    }
+    __syncthreads();
+    // each thread: one row oo, 16 consecutive k (one 16-byte chunk per modulus)
+    const int oo = tid >> 2, kq = (tid & 3) * 16;
+    const int o  = o0 + oo;
+    const int k  = k0 + kq;
+    if(o >= O_pad || k >= K_pad)
+        return;
+    int e = (o < O) ? exps[o] : 0;
+    if(e == kOzExpNone)
+        e = 0; // all-zero row
+    const int    se     = bits - e;
+    const bool   direct = se <= 1023; // 2^se is a normal double (se >= bits - 1025 > -1022)
+    const double scale  = direct ? __longlong_as_double((long long)(1023 + se) << 52) : 0.0;
+    uint32_t     fa[16], fm[16], fc[16];
+    uint32_t     negmask = 0;
+#pragma unroll
+    for(int j = 0; j < 16; ++j)
+    {
+        const double x = tile[oo][kq + j];
+        // exact scaling; |w| < 2^bits <= 2^60
+        const double             w = direct ? x * scale : ldexp(x, se);
+        const unsigned long long W = __double2ull_rz(fabs(w));
+        fa[j] = (uint32_t)(W >> 40);
+        fm[j] = (uint32_t)(W >> 20) & 0xFFFFFu;
+        fc[j] = (uint32_t)W & 0xFFFFFu;
+        negmask |= (signbit(x) ? 1u : 0u) << j;
+    }
+    const int     kc  = k / kCrtBK, c = (k % kCrtBK) / 16;
+    const int64_t nkc = K_pad / kCrtBK;
+    int8_t* out = dst + (int64_t)kc * O_pad * kCrtBK + (int64_t)o * kCrtBK + oz_swizzle_chunk<kCrtBK>(o, c) * 16;
+    crt_static_for<0, NM>([&](auto I) {
+        constexpr int      i    = decltype(I)::value;
+        constexpr uint32_t p    = crt_modulus(i);
+        constexpr uint32_t k40  = (uint32_t)((1ull << 40) % p);
+        constexpr uint32_t k20  = (uint32_t)((1ull << 20) % p);
+        constexpr uint32_t half = crt_half(i);
+        uint32_t           words[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for(int j = 0; j < 16; ++j)
+        {
+            const uint32_t t = fa[j] * k40 + fm[j] * k20 + fc[j]; // < 2^29
+            const uint32_t r = t % p;
+            int            s = r > half ? (int)r - (int)p : (int)r;
+            if((negmask >> j) & 1u)
+                s = -s; // -(-128) = 128 for p = 256: the same byte, the same residue
+            words[j >> 2] |= ((uint32_t)s & 0xFFu) << (8 * (j & 3));
+        }
+        *reinterpret_cast<uint4*>(out + (int64_t)i * nkc * O_pad * kCrtBK)
+            = make_uint4(words[0], words[1], words[2], words[3]);
+    });
+}
+
+// ---- GEMM over the residues ------------------------------------------------------------------
+struct CrtParams
+{
+    int           M, N, K;       // logical sizes (K <= kCrtKMax)
+    int           M_pad, N_pad;  // residue-panel rows (multiples of 128 and 256)
+    int           nkc;           // 64-deep K panels per modulus
+    const int8_t* resP;          // [NM][nkc][M_pad][64], swizzled rows
+    const int8_t* resQ;          // [NM][nkc][N_pad][64]
+    const int*    exp_rows;      // e_r, M entries
+    const int*    exp_cols;      // f_c, N entries
+    int           shift;         // 2b: P Q ~= 2^(e_r + f_c - shift) X
+    double*       C;             // output (column-major, ldc)
+    int64_t       ldc;
+    double        alpha, beta;   // C := beta C + alpha P Q ; beta == 0 => C not read
+    const double* beta_ptr;      // if set, beta := *beta_ptr (device pointer mode alpha of a trsm)
+    const double* ualpha_ptr;    // if set and *ualpha_ptr == 0: C := 0 (a trsm with alpha == 0)
+    int           ualpha_zero;   // host-side form of the same condition
+    uint8_t*      scratch;       // two slots of kCrtSlotBytes per CTA
+    int           stages;
+    int*          error;         // set to a nonzero code if a wait timed out
+};
+
+// Bounded wait that also gives up once another role has aborted.
+__device__ __forceinline__ bool crt_wait(uint64_t* bar, uint32_t parity, const int* abort_flag)
+{
+    const long long t0 = clock64();
+    while(!mbar_try_wait(bar, parity))
+    {
+        if(*(volatile const int*)abort_flag)
+            return false;
+        if(clock64() - t0 > (1ll << 31))
+            return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void crt_fail(int* error, int* abort_flag, int code)
+{
+    if(!*(volatile int*)abort_flag)
+        atomicCAS(error, 0, code);
+    atomicExch(abort_flag, 1);
+}
+
+// y_i = (C_i w_i) mod p_i for the int32 accumulator value v (|v| <= 2^28)
+template <int NM, int I>
+__device__ __forceinline__ uint32_t crt_residue_of(uint32_t v)
+{
+    constexpr uint32_t p = crt_modulus(I);
+    constexpr uint32_t w = crt_weight(NM, I);
+    if constexpr(p == 256u)
+        return ((v & 255u) * w) & 255u;
+    else
+    {
+        constexpr uint32_t off = p * ((1u << 28) / p + 1); // >= 2^28, a multiple of p
+        const uint32_t     r   = (v + off) % p;            // v + off in [0, 2^29 + 2p)
+        return (r * w) % p;
+    }
+}
+
+// X from its residues: byte c of every modulus' 16-byte chunk; returns X as a double (one
+// rounding of the exact 128-bit value).
+template <int NM, int COL>
+__device__ __forceinline__ double crt_rebuild(const uint4 (&r)[NM])
+{
+    unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    uint32_t           s24 = 0;
+    crt_static_for<0, NM>([&](auto I) {
+        constexpr int     i  = decltype(I)::value;
+        constexpr CrtU128 Mi = crt_cofactor(NM, i);
+        const uint32_t    wd = (COL >> 2) == 0 ? r[i].x : (COL >> 2) == 1 ? r[i].y : (COL >> 2) == 2 ? r[i].z : r[i].w;
+        const uint32_t    y  = (wd >> (8 * (COL & 3))) & 0xFFu;
+        s24 += y * crt_recip24(i);
+        a0 += (unsigned long long)y * crt_limb(Mi, 0);
+        a1 += (unsigned long long)y * crt_limb(Mi, 1);
+        a2 += (unsigned long long)y * crt_limb(Mi, 2);
+        a3 += (unsigned long long)y * crt_limb(Mi, 3);
+    });
+    constexpr CrtU128 P = crt_product(NM);
+    const unsigned long long q = (s24 + (1u << 23)) >> 24; // rint(sum y_i / p_i)
+    long long d0 = (long long)a0 - (long long)(q * crt_limb(P, 0));
+    long long d1 = (long long)a1 - (long long)(q * crt_limb(P, 1));
+    long long d2 = (long long)a2 - (long long)(q * crt_limb(P, 2));
+    long long d3 = (long long)a3 - (long long)(q * crt_limb(P, 3));
+    // carries (arithmetic shifts), the value modulo 2^128 in two's complement
+    d1 += d0 >> 32;
+    d2 += d1 >> 32;
+    d3 += d2 >> 32;
+    const unsigned long long lo = ((unsigned long long)(uint32_t)d1 << 32) | (uint32_t)d0;
+    const unsigned long long hi = ((unsigned long long)(uint32_t)d3 << 32) | (uint32_t)d2;
+    const bool               neg = (long long)hi < 0;
+    const unsigned long long mlo = neg ? 0ull - lo : lo;
+    const unsigned long long mhi = neg ? ~hi + (lo == 0 ? 1ull : 0ull) : hi;
+    const double             mag = fma((double)mhi, 0x1p64, (double)mlo);
+    return neg ? -mag : mag;
+}
+
+template <int NM>
+__global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_constant__ CrtParams p)
+{
+    constexpr int kTileA = kOzBM * kCrtBK;  // 8 KB of P residues per stage
+    constexpr int kTileB = kCrtBN * kCrtBK; // 16 KB of Q residues
+    constexpr int kStage = kTileA + kTileB;
+    constexpr int64_t kModBytes = (int64_t)kCrtChunks * kOzBM * 16; // one modulus in a slot
+    extern __shared__ __align__(1024) unsigned char crt_smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(crt_smem_raw) + 1023) & ~uintptr_t(1023));
+    const int NS = p.stages;
+
+    __shared__ uint64_t full_bar[8], empty_bar[8], acc_full[2], acc_empty[2], slot_full[2],
+        slot_empty[2], mma_done;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int      abort_flag;
+    __shared__ int      issued, consumed; // K steps loaded / handed to the tensor cores
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nk       = p.nkc;
+    const int tiles_m  = p.M_pad / kOzBM;
+    const int tiles_n  = p.N_pad / kCrtBN;
+    const int tiles    = tiles_m * tiles_n;
+    const int my_tiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int items    = my_tiles * NM;
+    uint8_t*  slots    = p.scratch + (int64_t)blockIdx.x * 2 * kCrtSlotBytes;
+
+    if(threadIdx.x == 0)
+    {
+        for(int i = 0; i < NS; ++i)
+        {
+            mbar_init(&full_bar[i], 1);
+            mbar_init(&empty_bar[i], 1);
+        }
+        for(int b = 0; b < 2; ++b)
+        {
+            mbar_init(&acc_full[b], 1);    // tcgen05.commit
+            mbar_init(&acc_empty[b], 4);   // one arrival per residue warp
+            mbar_init(&slot_full[b], 128); // every residue thread, after its last modulus
+            mbar_init(&slot_empty[b], 128); // every reconstruction thread
+        }
+        mbar_init(&mma_done, 1);
+        abort_flag = 0;
+        issued     = 0;
+        consumed   = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if(warp == 1)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_sh;
+
+    if(warp == 0)
+    {
+        // ---------------- copy producer ----------------
+        if(lane == 0)
+        {
+            int  it = 0; // K steps issued over all items
+            bool ok = true;
+            for(int j = 0; j < items && ok; ++j)
+            {
+                const int jt = j / NM, i = j - jt * NM;
+                int       mt, nt;
+                oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+                const int8_t* srcP = p.resP + ((int64_t)i * nk * p.M_pad + mt * kOzBM) * kCrtBK;
+                const int8_t* srcQ = p.resQ + ((int64_t)i * nk * p.N_pad + nt * kCrtBN) * kCrtBK;
+                for(int kc = 0; kc < nk; ++kc, ++it)
+                {
+                    const int      st = it % NS;
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if(!crt_wait(&empty_bar[st], ph ^ 1, &abort_flag))
+                    {
+                        crt_fail(p.error, &abort_flag, 11);
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* base = smem + st * kStage;
+                    mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
+                    bulk_load(base, srcP + (int64_t)kc * p.M_pad * kCrtBK, kTileA, &full_bar[st]);
+                    bulk_load(base + kTileA, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kTileB, &full_bar[st]);
+                    *(volatile int*)&issued = it + 1;
+                }
+            }
+        }
+    }
+    else if(warp == 1)
+    {
+        // ---------------- MMA issuer ----------------
+        if(lane == 0)
+        {
+            const uint64_t desc_a0 = oz_smem_desc<kCrtBK>(smem_u32(smem));
+            const uint64_t desc_b0 = oz_smem_desc<kCrtBK>(smem_u32(smem) + kTileA);
+            constexpr uint32_t idesc = oz_idesc(kCrtBN);
+            int  it = 0;
+            bool ok = true;
+            for(int j = 0; j < items && ok; ++j)
+            {
+                const int buf = j & 1;
+                // the residue warps have drained this accumulator's previous item
+                if(!crt_wait(&acc_empty[buf], (uint32_t)(((j >> 1) & 1) ^ 1), &abort_flag))
+                {
+                    crt_fail(p.error, &abort_flag, 12);
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t dcol = tmem + (uint32_t)(buf * kCrtBN);
+                for(int kc = 0; kc < nk; ++kc, ++it)
+                {
+                    const int      st = it % NS;
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if(!crt_wait(&full_bar[st], ph, &abort_flag))
+                    {
+                        crt_fail(p.error, &abort_flag, 12);
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    *(volatile int*)&consumed = it + 1;
+                    const uint64_t soff = (uint64_t)((st * kStage) >> 4);
+#pragma unroll
+                    for(int kk = 0; kk < kCrtBK / kOzMmaK; ++kk)
+                    {
+                        const uint64_t kof = (uint64_t)((kk * kOzMmaK) >> 4);
+                        oz_mma(dcol, desc_a0 + soff + kof, desc_b0 + soff + kof, idesc,
+                               (kc > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    oz_commit(&empty_bar[st]);
+                }
+                oz_commit(&acc_full[buf]);
+            }
+            // every MMA issued has completed before TMEM is freed
+            oz_commit(&mma_done);
+            (void)mbar_wait_bounded(&mma_done, 0);
+        }
+    }
+    else if(warp < 6)
+    {
+        // ---------------- residue epilogue (warps 2..5) ----------------
+        const int      quarter   = warp & 3; // TMEM lane group this warp may access
+        const int      row       = quarter * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+        for(int j = 0; j < items; ++j)
+        {
+            const int jt = j / NM, i = j - jt * NM, buf = j & 1, slot = jt & 1;
+            bool      ok = true;
+            if(i == 0) // the reconstruction warps are done with this slot's previous tile
+                ok = crt_wait(&slot_empty[slot], (uint32_t)(((jt >> 1) & 1) ^ 1), &abort_flag);
+            ok = ok && crt_wait(&acc_full[buf], (uint32_t)((j >> 1) & 1), &abort_flag);
+            // warp-uniform outcome: the tcgen05.ld below needs the whole warp
+            if(!__all_sync(0xffffffffu, ok))
+            {
+                crt_fail(p.error, &abort_flag, 13);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            uint8_t* dst = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)i * kModBytes + (int64_t)row * 16;
+            crt_static_for<0, NM>([&](auto I) {
+                constexpr int ii = decltype(I)::value;
+                if(i != ii)
+                    return;
+#pragma unroll 1
+                for(int cc = 0; cc < kCrtBN / 32; ++cc)
+                {
+                    uint32_t v[32];
+                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)(buf * kCrtBN + cc * 32), v);
+                    uint32_t w[8];
+#pragma unroll
+                    for(int q = 0; q < 8; ++q)
+                        w[q] = crt_residue_of<NM, ii>(v[4 * q]) | (crt_residue_of<NM, ii>(v[4 * q + 1]) << 8)
+                               | (crt_residue_of<NM, ii>(v[4 * q + 2]) << 16)
+                               | (crt_residue_of<NM, ii>(v[4 * q + 3]) << 24);
+                    *reinterpret_cast<uint4*>(dst + (int64_t)(2 * cc) * kOzBM * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+                    *reinterpret_cast<uint4*>(dst + (int64_t)(2 * cc + 1) * kOzBM * 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+            });
+            // accumulator free for the item after next
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if(lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+            if(i == NM - 1) // this thread's residues of the tile are all in the slot
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_full[slot])) : "memory");
+        }
+    }
+    else
+    {
+        // ---------------- reconstruction (warps 6..9) ----------------
+        const int    row  = (warp - 6) * 32 + lane;
+        const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
+        const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
+        for(int jt = 0; jt < my_tiles; ++jt)
+        {
+            const int slot = jt & 1;
+            if(!crt_wait(&slot_full[slot], (uint32_t)((jt >> 1) & 1), &abort_flag))
+            {
+                crt_fail(p.error, &abort_flag, 14);
+                break;
+            }
+            int mt, nt;
+            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+            const int gr = mt * kOzBM + row;
+            int       er = gr < p.M ? p.exp_rows[gr] : 0;
+            if(er == kOzExpNone)
+                er = 0;
+            const uint8_t* src = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)row * 16;
+#pragma unroll 1
+            for(int ch = 0; ch < kCrtChunks; ++ch)
+            {
+                uint4 r[NM];
+#pragma unroll
+                for(int i = 0; i < NM; ++i)
+                    r[i] = *reinterpret_cast<const uint4*>(src + (int64_t)i * kModBytes + (int64_t)ch * kOzBM * 16);
+                const int c0 = nt * kCrtBN + ch * 16;
+                auto out = [&](double x, int c) {
+                    const int gc = c0 + c;
+                    if(gr >= p.M || gc >= p.N)
+                        return;
+                    const int ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
+                    const int E  = er + ec - p.shift;
+                    const double pq = (E >= -1022 && E <= 1023)
+                                          ? x * __longlong_as_double((long long)(1023 + E) << 52)
+                                          : ldexp(x, E);
+                    double* cp = p.C + gr + (int64_t)gc * p.ldc;
+                    double  o;
+                    if(zero)
+                        o = 0.0;
+                    else if(beta == 0.0)
+                        o = p.alpha * pq;
+                    else
+                        o = fma(p.alpha, pq, beta * (*cp));
+                    *cp = o;
+                };
+                crt_static_for<0, 16>([&](auto Cc) {
+                    constexpr int c = decltype(Cc)::value;
+                    out(crt_rebuild<NM, c>(r), c);
+                });
+            }
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_empty[slot])) : "memory");
+        }
+    }
+
+    // ---------------- teardown ----------------
+    __syncthreads();
+    if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
+    {
+        // let the copies that were issued but never consumed land before the CTA exits
+        for(int i = consumed; i < issued; ++i)
+            (void)mbar_wait_bounded(&full_bar[i % NS], (uint32_t)((i / NS) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if(warp == 1)
+    {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+}
+
+} // namespace rb200

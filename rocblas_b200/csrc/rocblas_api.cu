@@ -1433,7 +1433,7 @@ int* ensure_err(rocblas_handle h)
 rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_operation tb, int m,
                                 int n, int k, const double* alpha, const double* A, int lda,
                                 const double* B, int ldb, const double* beta, double* C, int ldc,
-                                int slices)
+                                int slices, int moduli = 0)
 {
     DeviceScope device_scope; // the caller's current device is restored on return
     if(!h)
@@ -1444,12 +1444,14 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
     };
     if(!okop(ta) || !okop(tb) || slices < 1 || slices > kOzMaxS)
         return rocblas_status_invalid_value;
+    if(moduli && !crt_moduli_supported(moduli))
+        return rocblas_status_invalid_value;
     const bool nA = ta == rocblas_operation_none, nB = tb == rocblas_operation_none;
     if(m < 0 || n < 0 || k < 0 || lda < (nA ? m : k) || ldb < (nB ? k : n) || ldc < m)
         return rocblas_status_invalid_size;
     if(!m || !n)
         return h->size_query ? rocblas_status_size_unchanged : rocblas_status_success;
-    const size_t ws_bytes = sliced_gemm_workspace_bytes(m, n, k, slices);
+    const size_t ws_bytes = update_workspace_bytes(m, n, k, slices, moduli, h->sm_count);
     if(h->size_query)
         return h->set_optimal_size(ws_bytes);
     if(!alpha || !beta || !C || (k && (!A || !B)))
@@ -1469,6 +1471,7 @@ rocblas_status gemm_sliced_impl(rocblas_handle h, rocblas_operation ta, rocblas_
     g.N = n;
     g.K = k;
     g.S = slices;
+    g.moduli = moduli;
     g.P = nA ? SliceOperand{A, 1, lda} : SliceOperand{A, lda, 1};
     g.Q = nB ? SliceOperand{B, ldb, 1} : SliceOperand{B, 1, ldb};
     g.C = C;
@@ -1573,6 +1576,7 @@ bool mixed_run(TrsmProblem<double> pr, int slices, const MixedPlan& plan, void* 
     pr.invA = inv;
     MixedRecursive rec{{pr, (int)pr.k(), (int)ceil_div(pr.k(), kInvNB)}};
     rec.S        = slices;
+    rec.moduli   = tuning().mixed_moduli;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + plan.inv_bytes;
     rec.err_dev  = err;
     if(plan.ch_bytes)
@@ -2075,7 +2079,8 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
     const int    nstep     = (int)ceil_div(nblk, DB);
     const bool   forward   = pr.oplower();
     const size_t inv_bytes = align256((size_t)kInvNB * k * sizeof(double));
-    const size_t sl_bytes  = sliced_gemm_workspace_bytes(std::min(k, DB * kInvNB), n, k, slices);
+    const size_t sl_bytes  = update_workspace_bytes(std::min(k, DB * kInvNB), n, k, slices,
+                                                    tuning().mixed_moduli, pr.sm_count);
     const size_t ch_bytes  = mixed_chain_workspace_bytes(pr);
     const size_t ws_bytes  = inv_bytes + (sl_bytes + 255) / 256 * 256 + (ch_bytes + 255) / 256 * 256;
     int*         err       = ensure_err(h);
@@ -2090,6 +2095,7 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
 
     MixedRecursive rec{{pr, k, nblk}};
     rec.S        = slices;
+    rec.moduli   = tuning().mixed_moduli;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
     rec.err_dev  = err;
     if(ch_bytes)
@@ -3158,6 +3164,24 @@ rocblas_status rocblas_b200_dgemm_sliced(rocblas_handle h, rocblas_operation tra
 try
 {
     return gemm_sliced_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices);
+}
+catch(...)
+{
+    return exception_status();
+}
+
+rocblas_status rocblas_b200_dgemm_crt(rocblas_handle h, rocblas_operation transA,
+                                      rocblas_operation transB, rocblas_int m, rocblas_int n,
+                                      rocblas_int k, const double* alpha, const double* A,
+                                      rocblas_int lda, const double* B, rocblas_int ldb,
+                                      const double* beta, double* C, rocblas_int ldc,
+                                      rocblas_int moduli)
+try
+{
+    if(!moduli)
+        moduli = kCrtMaxModuli;
+    return gemm_sliced_impl(h, transA, transB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 1,
+                            moduli);
 }
 catch(...)
 {

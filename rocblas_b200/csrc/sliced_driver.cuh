@@ -4,6 +4,7 @@
 #include <functional>
 #include <mutex>
 
+#include "crt_gemm.cuh"
 #include "ozaki_gemm.cuh"
 #include "trsm_driver.cuh"
 
@@ -53,6 +54,7 @@ struct SlicedGemm
     int           b_user;
     int           zero_guard;
     int           sms;        // SMs of the device (persistent grid)
+    int           moduli = 0; // > 0: the residue (CRT) engine with this many moduli, else slices
 };
 
 __global__ void oz_fill_kernel(int* p, int n, int v)
@@ -175,9 +177,136 @@ static void launch_oz_pass(const OzParams& p, int64_t Mp, int64_t Np, int sms, c
     launch_oz_kernel<BN, BK, 0>(p, Mp, Np, sms, s);
 }
 
+// ---- residue (CRT) engine ------------------------------------------------------------------
+// K range per set of row / column exponents (the tuning key shared with the slice engine).
+static int64_t crt_k_chunk()
+{
+    return std::max<int64_t>(64, std::min<int64_t>(kCrtKMax, tuning().sliced_k_chunk / 64 * 64));
+}
+
+static int64_t crt_grid(int64_t Mp, int64_t Np, int sms)
+{
+    const int64_t tiles = (Mp / kOzBM) * (Np / kCrtBN);
+    return std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(sms, 1)));
+}
+
+// Workspace for one residue-engine GEMM of M x N x K with nm moduli on sms SMs: the residue
+// panels of one K range, the exponents and two 512 KB reconstruction slots per CTA.
+static size_t crt_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int nm, int sms)
+{
+    const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()), kCrtBK);
+    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kCrtNPad);
+    return align256((size_t)nm * Mp * Kp) + align256((size_t)nm * Np * Kp) + align256(4 * Mp)
+           + align256(4 * Np) + align256((size_t)crt_grid(Mp, Np, sms) * 2 * kCrtSlotBytes);
+}
+
+static bool crt_moduli_supported(int nm)
+{
+    return nm == 14 || nm == 15 || nm == 16;
+}
+
+template <int NM>
+static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int* eP, int* eQ,
+                       int8_t* rP, int8_t* rQ, int64_t Mp, int64_t Np, int64_t Kp, CrtParams p,
+                       int sms, cudaStream_t s)
+{
+    const int bits = crt_bits(NM, K);
+    dim3      gP((unsigned)(Kp / kOzSliceTile), (unsigned)(Mp / kOzSliceTile));
+    crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.ptr, P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp);
+    count_launch();
+    dim3 gQ((unsigned)(Kp / kOzSliceTile), (unsigned)(Np / kOzSliceTile));
+    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.ptr, Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp);
+    count_launch();
+    p.shift = 2 * bits;
+    p.stages = std::min(8, (kCrtSmemBudget - 1024) / ((kOzBM + kCrtBN) * kCrtBK));
+    const size_t smem = (size_t)p.stages * (kOzBM + kCrtBN) * kCrtBK + 1024;
+    cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned grid = (unsigned)crt_grid(Mp, Np, sms);
+    // algorithmic work: int8 tensor operations of the NM residue products
+    TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)M * N * K);
+    crt_gemm_kernel<NM><<<grid, kCrtThreads, smem, s>>>(p);
+    count_launch();
+}
+
+// Runs the residue engine; ws must hold crt_gemm_workspace_bytes(M, N, K, moduli, sms).
+static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream_t s)
+{
+    if(g.M <= 0 || g.N <= 0)
+        return true;
+    if(!crt_moduli_supported(g.moduli))
+        return false;
+    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kCrtNPad);
+    const int64_t K  = std::max<int64_t>(g.K, 0);
+    const int64_t kchunk = crt_k_chunk();
+    for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kchunk)
+    {
+        const int64_t kc = std::min<int64_t>(kchunk, K - k0);
+        const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kCrtBK);
+        unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+        int8_t* rP = reinterpret_cast<int8_t*>(w);
+        w += align256((size_t)g.moduli * Mp * Kp);
+        int8_t* rQ = reinterpret_cast<int8_t*>(w);
+        w += align256((size_t)g.moduli * Np * Kp);
+        int* eP = reinterpret_cast<int*>(w);
+        w += align256(4 * Mp);
+        int* eQ = reinterpret_cast<int*>(w);
+        w += align256(4 * Np);
+        uint8_t* scratch = reinterpret_cast<uint8_t*>(w);
+
+        const SliceOperand P = g.P.shifted_k(k0), Q = g.Q.shifted_k(k0);
+        if(kc > 0)
+        {
+            launch_exponents(P, (int)g.M, (int)kc, eP, s);
+            launch_exponents(Q, (int)g.N, (int)kc, eQ, s);
+        }
+        else
+        {
+            cudaMemsetAsync(eP, 0, 4 * Mp, s);
+            cudaMemsetAsync(eQ, 0, 4 * Np, s);
+        }
+        CrtParams p{};
+        p.M = (int)g.M;
+        p.N = (int)g.N;
+        p.K = (int)std::max<int64_t>(kc, 1);
+        p.M_pad = (int)Mp;
+        p.N_pad = (int)Np;
+        p.nkc = (int)(Kp / kCrtBK);
+        p.resP = rP;
+        p.resQ = rQ;
+        p.exp_rows = eP;
+        p.exp_cols = eQ;
+        p.C = g.C;
+        p.ldc = g.ldc;
+        p.alpha = g.a;
+        const bool first = k0 == 0;
+        p.beta = first ? (g.b_user ? g.ualpha_host : g.b_imm) : 1.0;
+        p.beta_ptr = (first && g.b_user) ? g.ualpha_dev : nullptr;
+        p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
+        p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
+        p.scratch = scratch;
+        p.error = err_dev;
+        const int kk = (int)std::max<int64_t>(kc, 1);
+        switch(g.moduli)
+        {
+        case 14: launch_crt<14>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
+        case 15: launch_crt<15>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
+        default: launch_crt<16>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
+        }
+    }
+    return true;
+}
+
+// Workspace of one update on the engine the tuning table selects (moduli > 0: residues).
+static size_t update_workspace_bytes(int64_t M, int64_t N, int64_t K, int S, int moduli, int sms)
+{
+    return moduli > 0 ? crt_gemm_workspace_bytes(M, N, K, moduli, sms) : sliced_gemm_workspace_bytes(M, N, K, S);
+}
+
 // Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
 static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream_t s)
 {
+    if(g.moduli > 0)
+        return run_crt_gemm(g, ws, err_dev, s);
     if(g.M <= 0 || g.N <= 0)
         return true;
     const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kOzNPad);
@@ -278,6 +407,7 @@ static int mixed_chain_w()
 struct MixedRecursive : Recursive<double>
 {
     int   S;
+    int   moduli = 0; // > 0: updates on the residue (CRT) engine with this many moduli
     void* slice_ws;
     int*  err_dev;
     void* chain_ws = nullptr; // flags of the chain sub-solves (nullptr: recursion to the leaves)
@@ -321,6 +451,7 @@ struct MixedRecursive : Recursive<double>
             g.C = B + (int64_t)c_lo * q.ldb;
         }
         g.S = S;
+        g.moduli = moduli;
         g.ldc = q.ldb;
         g.a = -1.0;
         g.b_imm = 1.0;
@@ -391,8 +522,9 @@ static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S)
     const int64_t bm   = nblk / 2;
     const int64_t r_m  = std::min<int64_t>(bm * kInvNB, k);
     const int64_t big  = std::max(r_m, k - r_m);
-    return pr.side_left ? sliced_gemm_workspace_bytes(big, pr.n, big, S)
-                        : sliced_gemm_workspace_bytes(pr.m, big, big, S);
+    const int moduli = tuning().mixed_moduli;
+    return pr.side_left ? update_workspace_bytes(big, pr.n, big, S, moduli, pr.sm_count)
+                        : update_workspace_bytes(pr.m, big, big, S, moduli, pr.sm_count);
 }
 
 } // namespace rb200

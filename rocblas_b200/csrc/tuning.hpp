@@ -43,6 +43,8 @@ struct Tuning
                                      // right-hand sides, which runs beside the sliced solve
     int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
                                      // cycles (2^31: about a second), records error 4, returns
+    int mixed_moduli         = 0;    // precision form: 0 updates on the slice engine; 14..16 on
+                                     // the residue (CRT) engine with this many moduli
     int chain_first_item     = 0;    // failure injection for tests: uniform chain launches start
                                      // claiming items here, so the flags of the items before it
                                      // are never set and the waits on them run out (0: off)
@@ -75,6 +77,7 @@ static const TuningEntry kTuningEntries[] = {
     {"refine_check_sms", &Tuning::refine_check_sms, 1, 1024},
     {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
     {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
+    {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)
