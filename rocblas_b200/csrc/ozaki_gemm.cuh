@@ -68,11 +68,13 @@ struct OzParams
     int      nkc;              // K panels per slice (K_pad / BK)
     const int* exp_rows;       // e_r, M entries
     const int* exp_cols;       // f_c, N entries
-    double*  C;                // output (column-major, ldc)
+    void*    C;                // output (column-major, ldc): double, or float if c_f32
     int64_t  ldc;
     double   alpha, beta;      // C := beta C + alpha P Q ; beta == 0 => C not read
-    const double* beta_ptr;    // if set, beta := *beta_ptr (device pointer mode alpha of a trsm)
-    const double* ualpha_ptr;  // if set and *ualpha_ptr == 0: C := 0 (a trsm with alpha == 0)
+    const void* beta_ptr;      // if set, beta := *beta_ptr (device pointer mode alpha of a trsm;
+                               // the element type of C)
+    const void* ualpha_ptr;    // if set and *ualpha_ptr == 0: C := 0 (a trsm with alpha == 0)
+    int      c_f32;            // C, beta_ptr, ualpha_ptr are float (the FP32 trsm's updates)
     int      ualpha_zero;      // host-side form of the same condition
     int      stages;
     int      tmem_cols;        // power of two >= S * 64
@@ -162,6 +164,14 @@ __device__ __forceinline__ void oz_mma(uint32_t tmem_d, uint64_t adesc, uint64_t
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
                  "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// A scalar of C's element type from device memory, as a double (`dflt` when ptr is null).
+__device__ __forceinline__ double oz_read_scalar(const void* ptr, int f32, double dflt)
+{
+    if(!ptr)
+        return dflt;
+    return f32 ? (double)*static_cast<const float*>(ptr) : *static_cast<const double*>(ptr);
 }
 
 __device__ __forceinline__ void oz_commit(uint64_t* bar)
@@ -375,8 +385,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         const int      quarter   = warp & 3; // TMEM lane group this warp may access
         const int      row       = quarter * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
-        const double   beta      = p.beta_ptr ? *p.beta_ptr : p.beta;
-        const bool     zero      = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
+        const double   beta      = oz_read_scalar(p.beta_ptr, p.c_f32, p.beta);
+        const bool     zero      = p.ualpha_zero || (p.ualpha_ptr && oz_read_scalar(p.ualpha_ptr, p.c_f32, 1.0) == 0.0);
         int            tcount    = 0;
         for(int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++tcount)
         {
@@ -406,17 +416,22 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     const int gc = n0 + half * 32 + j;
                     if(gc < p.N)
                     {
-                        double*      cp = p.C + gr + (int64_t)gc * p.ldc;
-                        const int    ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
-                        const double pq = ldexp(h[j], er + ec - 14 - 7 * DLO);
-                        double       out;
+                        const int64_t ci = gr + (int64_t)gc * p.ldc;
+                        const int     ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
+                        const double  pq = ldexp(h[j], er + ec - 14 - 7 * DLO);
+                        double        out;
                         if(zero)
                             out = 0.0;
                         else if(beta == 0.0)
                             out = p.alpha * pq;
                         else
-                            out = fma(p.alpha, pq, beta * (*cp));
-                        *cp = out;
+                            out = fma(p.alpha, pq,
+                                      beta * (p.c_f32 ? (double)static_cast<float*>(p.C)[ci]
+                                                      : static_cast<double*>(p.C)[ci]));
+                        if(p.c_f32)
+                            static_cast<float*>(p.C)[ci] = (float)out;
+                        else
+                            static_cast<double*>(p.C)[ci] = out;
                     }
                 }
             };
@@ -496,7 +511,8 @@ __device__ __forceinline__ void oz_merge_exp(int* exps, int o, double mx)
 }
 
 // one warp per row o and K chunk; lanes stride over k (rows whose k is contiguous)
-__global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, int O, int K, int* exps)
+template <typename TIn>
+__global__ void oz_exponent_kernel(const TIn* src, int64_t so, int64_t sk, int O, int K, int* exps)
 {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     const int k0 = blockIdx.y * kOzExpChunk;
@@ -506,7 +522,7 @@ __global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, in
     const int kend = min(K, k0 + kOzExpChunk);
 #pragma unroll 8
     for(int k = k0 + lane; k < kend; k += 32)
-        mx = fmax(mx, fabs(src[(int64_t)w * so + (int64_t)k * sk]));
+        mx = fmax(mx, fabs((double)src[(int64_t)w * so + (int64_t)k * sk]));
 #pragma unroll
     for(int off = 16; off; off >>= 1)
         mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
@@ -519,7 +535,8 @@ __global__ void oz_exponent_kernel(const double* src, int64_t so, int64_t sk, in
 // that the grid has enough threads to keep HBM busy (rows are few, K is long).
 constexpr int kOzExpRowsChunk = 64;
 
-__global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, int K, int* exps)
+template <typename TIn>
+__global__ void oz_exponent_rows_kernel(const TIn* src, int64_t sk, int O, int K, int* exps)
 {
     const int o  = blockIdx.x * blockDim.x + threadIdx.x;
     const int k0 = blockIdx.y * kOzExpRowsChunk;
@@ -531,7 +548,7 @@ __global__ void oz_exponent_rows_kernel(const double* src, int64_t sk, int O, in
     const int kend = min(K, k0 + kOzExpRowsChunk);
 #pragma unroll 16
     for(int k = k0; k < kend; ++k)
-        mx = fmax(mx, fabs(src[o + (int64_t)k * sk]));
+        mx = fmax(mx, fabs((double)src[o + (int64_t)k * sk]));
     oz_merge_exp(exps, o, mx);
 }
 
@@ -553,9 +570,9 @@ __host__ __device__ constexpr int oz_swizzle_chunk(int o, int c)
     return BK == 64 ? (c ^ ((o >> 1) & 3)) : (c ^ ((o >> 2) & 1));
 }
 
-template <int BK>
+template <int BK, typename TIn>
 __global__ void __launch_bounds__(256, 4)
-    oz_slice_kernel(const double* src, int64_t so, int64_t sk, int O, int K, const int* exps, int S,
+    oz_slice_kernel(const TIn* src, int64_t so, int64_t sk, int O, int K, const int* exps, int S,
                     int8_t* dst, int O_pad, int K_pad)
 {
     __shared__ double tile[kOzSliceTile][kOzSliceTile + 1];
@@ -573,7 +590,7 @@ __global__ void __launch_bounds__(256, 4)
         const int oo  = o_fast ? idx % kOzSliceTile : idx / kOzSliceTile;
         const int kk  = o_fast ? idx / kOzSliceTile : idx % kOzSliceTile;
         const int o = o0 + oo, k = k0 + kk;
-        ld[it] = (o < O && k < K) ? src[(int64_t)o * so + (int64_t)k * sk] : 0.0;
+        ld[it] = (o < O && k < K) ? (double)src[(int64_t)o * so + (int64_t)k * sk] : 0.0;
     }
 #pragma unroll
     for(int it = 0; it < kLoads; ++it)

@@ -190,6 +190,8 @@ rocblas_status trsm_arg_check(rocblas_handle h, rocblas_side side, rocblas_fill 
     return rocblas_status_continue;
 }
 
+int* ensure_err(rocblas_handle h);
+
 // The body shared by all trsm entry points (rocblas_trsm_ex_impl,
 // library/src/blas3/rocblas_trsm_imp.hpp:55-272 and its batched / strided twins).
 template <typename T>
@@ -286,6 +288,8 @@ rocblas_status trsm_impl(rocblas_handle h, rocblas_side side, rocblas_fill uplo,
     if(have_invA)
         pr.invA = invA;
     pr.err_dev = h->err_dev;
+    if(!pr.err_dev && ws && strsm_slice_bytes(pr))
+        pr.err_dev = ensure_err(h); // the sliced FP32 updates' bounded waits report here
     trsm_run<T>(pr, ws, have_invA);
     st = launch_status();
     return st != rocblas_status_success ? st : perf;

@@ -11,12 +11,19 @@
 namespace rb200
 {
 
-// Element (o, k) of an operand at ptr[o * so + k * sk].
+// Element (o, k) of an operand at ptr[o * so + k * sk]: doubles, or floats if f32.
 struct SliceOperand
 {
-    const double* ptr;
-    int64_t       so, sk;
-    SliceOperand  shifted_k(int64_t k0) const { return {ptr + k0 * sk, so, sk}; }
+    const void* ptr;
+    int64_t     so, sk;
+    int         f32 = 0;
+    SliceOperand shifted_k(int64_t k0) const
+    {
+        const size_t es = f32 ? sizeof(float) : sizeof(double);
+        return {static_cast<const char*>(ptr) + k0 * sk * (int64_t)es, so, sk, f32};
+    }
+    const double* d() const { return static_cast<const double*>(ptr); }
+    const float*  f() const { return static_cast<const float*>(ptr); }
 };
 
 static inline int64_t round_up(int64_t a, int64_t b)
@@ -45,11 +52,12 @@ struct SlicedGemm
     int64_t       M, N, K;
     int           S;
     SliceOperand  P, Q;
-    double*       C;
+    void*         C;          // double, or float if c_f32 (then P and Q are float too)
+    int           c_f32;
     int64_t       ldc;
     double        a;
     double        b_imm;
-    const double* ualpha_dev; // device-mode alpha of the caller (or nullptr)
+    const void*   ualpha_dev; // device-mode alpha of the caller, C's element type (or nullptr)
     double        ualpha_host;
     int           b_user;
     int           zero_guard;
@@ -73,12 +81,18 @@ static void launch_exponents(SliceOperand X, int O, int K, int* exps, cudaStream
     {
         const unsigned rchunks = (unsigned)std::max<int64_t>(1, ceil_div(K, kOzExpRowsChunk));
         dim3 grid((unsigned)ceil_div(O, 128), rchunks);
-        oz_exponent_rows_kernel<<<grid, 128, 0, s>>>(X.ptr, X.sk, O, K, exps);
+        if(X.f32)
+            oz_exponent_rows_kernel<float><<<grid, 128, 0, s>>>(X.f(), X.sk, O, K, exps);
+        else
+            oz_exponent_rows_kernel<double><<<grid, 128, 0, s>>>(X.d(), X.sk, O, K, exps);
     }
     else
     {
         dim3 grid((unsigned)ceil_div((int64_t)O * 32, 256), kchunks);
-        oz_exponent_kernel<<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps);
+        if(X.f32)
+            oz_exponent_kernel<float><<<grid, 256, 0, s>>>(X.f(), X.so, X.sk, O, K, exps);
+        else
+            oz_exponent_kernel<double><<<grid, 256, 0, s>>>(X.d(), X.so, X.sk, O, K, exps);
     }
     count_launch();
 }
@@ -87,10 +101,20 @@ static void launch_slices(SliceOperand X, int O, int K, const int* exps, int S, 
                           int K_pad, int bk, cudaStream_t s)
 {
     dim3 grid((unsigned)(K_pad / kOzSliceTile), (unsigned)(O_pad / kOzSliceTile));
-    if(bk == 64)
-        oz_slice_kernel<64><<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    if(X.f32)
+    {
+        if(bk == 64)
+            oz_slice_kernel<64, float><<<grid, 256, 0, s>>>(X.f(), X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+        else
+            oz_slice_kernel<32, float><<<grid, 256, 0, s>>>(X.f(), X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    }
     else
-        oz_slice_kernel<32><<<grid, 256, 0, s>>>(X.ptr, X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    {
+        if(bk == 64)
+            oz_slice_kernel<64, double><<<grid, 256, 0, s>>>(X.d(), X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+        else
+            oz_slice_kernel<32, double><<<grid, 256, 0, s>>>(X.d(), X.so, X.sk, O, K, exps, S, dst, O_pad, K_pad);
+    }
     count_launch();
 }
 
@@ -212,10 +236,10 @@ static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int*
 {
     const int bits = crt_bits(NM, K);
     dim3      gP((unsigned)(Kp / kOzSliceTile), (unsigned)(Mp / kOzSliceTile));
-    crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.ptr, P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp);
+    crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.d(), P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp);
     count_launch();
     dim3 gQ((unsigned)(Kp / kOzSliceTile), (unsigned)(Np / kOzSliceTile));
-    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.ptr, Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp);
+    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp);
     count_launch();
     p.shift = 2 * bits;
     p.stages = std::min(8, (kCrtSmemBudget - 1024) / ((kOzBM + kCrtBN) * kCrtBK));
@@ -233,7 +257,7 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
 {
     if(g.M <= 0 || g.N <= 0)
         return true;
-    if(!crt_moduli_supported(g.moduli))
+    if(!crt_moduli_supported(g.moduli) || g.c_f32 || g.P.f32 || g.Q.f32)
         return false;
     const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kCrtNPad);
     const int64_t K  = std::max<int64_t>(g.K, 0);
@@ -275,13 +299,13 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         p.resQ = rQ;
         p.exp_rows = eP;
         p.exp_cols = eQ;
-        p.C = g.C;
+        p.C = static_cast<double*>(g.C);
         p.ldc = g.ldc;
         p.alpha = g.a;
         const bool first = k0 == 0;
         p.beta = first ? (g.b_user ? g.ualpha_host : g.b_imm) : 1.0;
-        p.beta_ptr = (first && g.b_user) ? g.ualpha_dev : nullptr;
-        p.ualpha_ptr = g.zero_guard ? g.ualpha_dev : nullptr;
+        p.beta_ptr = (first && g.b_user) ? static_cast<const double*>(g.ualpha_dev) : nullptr;
+        p.ualpha_ptr = g.zero_guard ? static_cast<const double*>(g.ualpha_dev) : nullptr;
         p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
         p.scratch = scratch;
         p.error = err_dev;
@@ -365,6 +389,7 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
             p.exp_rows = eP;
             p.exp_cols = eQ;
             p.C = g.C;
+            p.c_f32 = g.c_f32;
             p.ldc = g.ldc;
             p.alpha = g.a;
             const bool first = k0 == 0 && pi == 0;
@@ -393,6 +418,52 @@ static bool run_sliced_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStr
         }
     }
     return true;
+}
+
+// One trailing update of a recursive solve of one system on the integer engines:
+// C := C - op(A) X (side L) or C - X op(A) (side R), with the caller's alpha applied to C
+// (`first`) and alpha == 0 giving C := 0, the way Recursive::update does on the tiles.
+template <typename T>
+static bool sliced_trsm_update(const TrsmProblem<T>& q, int c_lo, int c_hi, int x_lo, int x_hi,
+                               int first, int S, int moduli, void* ws, int* err)
+{
+    static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value, "real types");
+    const int f32 = std::is_same<T, float>::value ? 1 : 0;
+    const T*  A   = q.A.base + q.A.offset;
+    T*        B   = q.B.base + q.B.offset;
+    SlicedGemm g{};
+    if(q.side_left)
+    {
+        g.M = c_hi - c_lo;
+        g.N = q.n;
+        g.K = x_hi - x_lo;
+        g.P = !q.trans ? SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda, f32}
+                       : SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1, f32};
+        g.Q = SliceOperand{B + x_lo, q.ldb, 1, f32};
+        g.C = B + c_lo;
+    }
+    else
+    {
+        g.M = q.m;
+        g.N = c_hi - c_lo;
+        g.K = x_hi - x_lo;
+        g.P = SliceOperand{B + (int64_t)x_lo * q.ldb, 1, q.ldb, f32};
+        g.Q = !q.trans ? SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1, f32}
+                       : SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda, f32};
+        g.C = B + (int64_t)c_lo * q.ldb;
+    }
+    g.c_f32 = f32;
+    g.S = S;
+    g.moduli = moduli;
+    g.ldc = q.ldb;
+    g.a = -1.0;
+    g.b_imm = 1.0;
+    g.b_user = first;
+    g.ualpha_dev = q.alpha.ptr;
+    g.ualpha_host = (double)q.alpha.val;
+    g.zero_guard = 1;
+    g.sms = q.sm_count;
+    return run_sliced_gemm(g, ws, err, q.stream);
 }
 
 static int mixed_chain_w()
@@ -426,41 +497,7 @@ struct MixedRecursive : Recursive<double>
             update(c_lo, c_hi, x_lo, x_hi, first);
             return;
         }
-        const TrsmProblem<double>& q = pr;
-        const double* A = q.A.base + q.A.offset;
-        double*       B = q.B.base + q.B.offset;
-        SlicedGemm g{};
-        if(q.side_left)
-        {
-            g.M = c_hi - c_lo;
-            g.N = q.n;
-            g.K = x_hi - x_lo;
-            g.P = !q.trans ? SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda}
-                           : SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1};
-            g.Q = SliceOperand{B + x_lo, q.ldb, 1};
-            g.C = B + c_lo;
-        }
-        else
-        {
-            g.M = q.m;
-            g.N = c_hi - c_lo;
-            g.K = x_hi - x_lo;
-            g.P = SliceOperand{B + (int64_t)x_lo * q.ldb, 1, q.ldb};
-            g.Q = !q.trans ? SliceOperand{A + x_lo + (int64_t)c_lo * q.lda, q.lda, 1}
-                           : SliceOperand{A + c_lo + (int64_t)x_lo * q.lda, 1, q.lda};
-            g.C = B + (int64_t)c_lo * q.ldb;
-        }
-        g.S = S;
-        g.moduli = moduli;
-        g.ldc = q.ldb;
-        g.a = -1.0;
-        g.b_imm = 1.0;
-        g.b_user = first;
-        g.ualpha_dev = q.alpha.ptr;
-        g.ualpha_host = q.alpha.val;
-        g.zero_guard = 1;
-        g.sms = q.sm_count;
-        ok = ok && run_sliced_gemm(g, slice_ws, err_dev, q.stream);
+        ok = ok && sliced_trsm_update<double>(pr, c_lo, c_hi, x_lo, x_hi, first, S, moduli, slice_ws, err_dev);
     }
 
     void solve_mixed(int b0, int b1, int first)

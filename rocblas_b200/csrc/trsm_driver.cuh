@@ -167,11 +167,21 @@ static void launch_block_solve(const TrsmProblem<T>& pr, int m, int n, BatchPtr<
 }
 
 // ---- recursive blocked solve --------------------------------------------------------------
+// The FP32 solve's trailing updates on the int8 slice engine (sliced_driver.cuh, later in this
+// translation unit): C := beta C - op(A) X (side L) or C - X op(A) (side R); false if not run.
+template <typename T>
+static bool sliced_trsm_update(const TrsmProblem<T>& q, int c_lo, int c_hi, int x_lo, int x_hi,
+                               int first, int S, int moduli, void* ws, int* err);
+static size_t sliced_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int S);
+
 template <typename T>
 struct Recursive
 {
     const TrsmProblem<T>& pr;
     int                   k, nblk;
+    // FP32: workspace of the trailing updates on the int8 slice engine (nullptr: FFMA tiles)
+    void*                 slice_ws = nullptr;
+    int                   slice_S  = 0;
 
     int row_of(int b) const { return std::min(b * kInvNB, k); }
 
@@ -232,6 +242,12 @@ struct Recursive
     // C := beta * C - X * opA(rows i0.., cols j0..)  (side R)
     void update(int c_lo, int c_hi, int x_lo, int x_hi, int first) const
     {
+        if constexpr(std::is_same<T, float>::value)
+        {
+            if(slice_ws && x_hi - x_lo >= tuning().strsm_sliced_min_k
+               && sliced_trsm_update<T>(pr, c_lo, c_hi, x_lo, x_hi, first, slice_S, 0, slice_ws, pr.err_dev))
+                return;
+        }
         GemmParams<T> g{};
         if(pr.side_left)
         {
@@ -408,12 +424,37 @@ static size_t trsm_invA_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
     return (size_t)kInvNB * (size_t)pr.k() * sizeof(T) * (size_t)pr.batch;
 }
 
+// The FP32 recursive solve's slice workspace: the largest trailing update (the top node's)
+// when its updates run on the int8 slice engine (strsm_slices > 0, one system, no chain).
+template <typename T>
+static size_t strsm_slice_bytes(const TrsmProblem<T>& pr)
+{
+    if constexpr(!std::is_same<T, float>::value)
+        return 0;
+    else
+    {
+        const Tuning& t = tuning();
+        if(t.strsm_slices <= 0 || pr.batch != 1 || choose_algo(pr) != Algo::recursive || use_chain(pr))
+            return 0;
+        const int64_t k    = pr.k();
+        const int64_t nblk = ceil_div(k, kInvNB);
+        const int64_t rm   = std::min<int64_t>(nblk / 2 * kInvNB, k);
+        const int64_t big  = std::max(rm, k - rm);
+        if(big < t.strsm_sliced_min_k)
+            return 0;
+        return pr.side_left ? sliced_gemm_workspace_bytes(big, pr.n, big, t.strsm_slices)
+                            : sliced_gemm_workspace_bytes(pr.m, big, big, t.strsm_slices);
+    }
+}
+
 template <typename T>
 static size_t trsm_workspace_bytes(const TrsmProblem<T>& pr, bool have_supplied_invA)
 {
     size_t b = trsm_invA_bytes(pr, have_supplied_invA);
     if(use_chain(pr))
         b = (b + 255) / 256 * 256 + chain_workspace_bytes(chain_shape_of(pr));
+    else if(const size_t sl = strsm_slice_bytes(pr))
+        b = (b + 255) / 256 * 256 + sl;
     return b;
 }
 
@@ -456,6 +497,11 @@ static void trsm_run(TrsmProblem<T> pr, void* ws, bool supplied_invA)
         }
     }
     Recursive<T> rec{pr, k, (int)ceil_div(k, kInvNB)};
+    if(ws && pr.err_dev && strsm_slice_bytes(pr))
+    {
+        rec.slice_ws = reinterpret_cast<char*>(ws) + (trsm_invA_bytes(pr, supplied_invA) + 255) / 256 * 256;
+        rec.slice_S  = tuning().strsm_slices;
+    }
     rec.solve(0, rec.nblk, 1);
 }
 

@@ -43,6 +43,9 @@ struct Tuning
                                      // right-hand sides, which runs beside the sliced solve
     int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
                                      // cycles (2^31: about a second), records error 4, returns
+    int strsm_slices         = 4;    // FP32 solve: slices of its trailing updates on the int8 slice
+                                     // engine (0: FFMA tiles)
+    int strsm_sliced_min_k   = 1024; // ... for updates with at least this inner dimension
     int mixed_moduli         = 0;    // precision form: 0 updates on the slice engine; 14..16 on
                                      // the residue (CRT) engine with this many moduli
     int chain_first_item     = 0;    // failure injection for tests: uniform chain launches start
@@ -78,6 +81,8 @@ static const TuningEntry kTuningEntries[] = {
     {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
     {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
     {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},
+    {"strsm_slices", &Tuning::strsm_slices, 0, 8},
+    {"strsm_sliced_min_k", &Tuning::strsm_sliced_min_k, 64, 1 << 30},
 };
 
 inline bool tuning_set(Tuning& t, const char* key, int value)
