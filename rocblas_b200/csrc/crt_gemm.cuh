@@ -11,17 +11,17 @@
 //     coprime moduli p_i <= 256 (crt_modulus): residues P'_i = P' mod p_i, Q'_i = Q' mod p_i in
 //     the symmetric range fit int8, and C_i = P'_i Q'_i is one tcgen05.mma kind::i8 GEMM whose
 //     int32 accumulation is exact (|C_i| <= K 128^2 <= 2^28 for K <= 16384);
-//   * X is rebuilt from its residues y_i = (C_i (P/p_i)^-1) mod p_i (P = prod p_i) as
-//     X = sum_i y_i (P/p_i) - q P with q = rint(sum_i y_i / p_i): the sum is taken modulo 2^128
-//     in four 32-bit limbs, which is exact because |X| < P / 8 by the choice of b
-//     (2b + log2 K <= log2 P - 3), and q from a 24-bit fixed-point sum whose error (< 2^-13) is
-//     far inside the 3/8 margin that bound leaves;
+//   * X is rebuilt from its residues r_i = C_i mod p_i (P = prod p_i, M_i = P / p_i,
+//     w_i = M_i^-1 mod p_i) as X = sum_i r_i (w_i M_i) - q P with q = rint(sum_i r_i w_i / p_i):
+//     the sum is taken modulo 2^128 in four 32-bit limbs, which is exact because |X| < P / 8 by
+//     the choice of b (2b + log2 K <= log2 P - 3), and q from a 20-bit fixed-point sum whose
+//     error (< 2^-9) is far inside the 3/8 margin that bound leaves;
 //   * P Q ~= 2^(e_r + f_c - 2b) X, rounded once to FP64 in the epilogue.
 // With 16 moduli (P ~ 2^125.4) and K <= 4096, b = 55: every entry keeps 55 bits relative to its
 // row's (column's) largest entry and the product of the truncated operands is exact, at 16 int8
 // GEMMs where the 7-bit slice form (ozaki_gemm.cuh) needs 36 slice-pair products for 56 bits.
 //
-// Kernel layout (persistent, one CTA per SM, 320 threads; output tiles 128 x 256; the tiles of
+// Kernel layout (persistent, one CTA per SM, 448 threads; output tiles 128 x 256; the tiles of
 // a CTA are t = blockIdx.x + j * gridDim.x in a grouped order, so the CTAs in flight work on
 // neighbouring tiles and, being in step, on the same modulus, and share its residue panels in L2):
 //   warp 0    copy producer: per work item (tile, modulus) and 64-deep K step, one bulk copy of
@@ -30,10 +30,11 @@
 //   warp 1    TMEM owner and MMA issuer: one 128 x 256 int32 accumulator per item, two
 //             accumulators (all 512 TMEM columns) so that an item's MMAs overlap the drain of the
 //             previous one;
-//   warps 2-5 residue epilogue: tcgen05.ld of the accumulator (lanes = rows), y_i as one byte
-//             per entry into the CTA's scratch slot in global memory (L2), two slots so that a
-//             tile's residues are written while the previous tile is rebuilt;
-//   warps 6-9 reconstruction: once all NM residues of a tile are in its slot, each thread takes
+//   warps 2-9 residue epilogue (two warps per TMEM lane group, half the columns each):
+//             tcgen05.ld of the accumulator (lanes = rows), r_i as one byte per entry into the
+//             CTA's scratch slot in global memory (L2), two slots so that a tile's residues are
+//             written while the previous tile is rebuilt;
+//   warps 10-13 reconstruction: once all NM residues of a tile are in its slot, each thread takes
 //             one row, rebuilds X for 16 columns at a time and writes beta C + alpha 2^s X.
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its in-flight
 // copies and MMAs (again bounded), frees TMEM and returns.
@@ -50,7 +51,7 @@ namespace rb200
 constexpr int kCrtMaxModuli = 16;
 constexpr int kCrtBN        = 256;  // output tile width: N of one MMA
 constexpr int kCrtBK        = 64;   // int8 K of one ring stage (SWIZZLE_64B rows)
-constexpr int kCrtThreads   = 320;  // 10 warps
+constexpr int kCrtThreads   = 448;  // 14 warps
 constexpr int kCrtKMax      = 16384; // |C_i| <= K 128^2 <= 2^28 keeps the residue step in int32
 constexpr int kCrtMaxBits   = 60;   // W < 2^60: three 20-bit fields in the residue kernel
 constexpr int kCrtNPad      = kCrtBN;
@@ -149,7 +150,7 @@ __host__ __device__ constexpr CrtU128 crt_product(int nm)
     return p;
 }
 
-// M_i = P / p_i, w_i = M_i^-1 mod p_i, R_i = round(2^24 / p_i)
+// M_i = P / p_i, w_i = M_i^-1 mod p_i
 __host__ __device__ constexpr CrtU128 crt_cofactor(int nm, int i)
 {
     return crt_div(crt_product(nm), crt_modulus(i));
@@ -160,9 +161,18 @@ __host__ __device__ constexpr uint32_t crt_weight(int nm, int i)
     return crt_inverse(crt_rem(crt_cofactor(nm, i), crt_modulus(i)), crt_modulus(i));
 }
 
-__host__ __device__ constexpr uint32_t crt_recip24(int i)
+// The reconstruction works on r_i = C_i mod p_i with the weights folded into its constants:
+// W_i = w_i M_i (< P, as w_i < p_i) is 1 modulo p_i and 0 modulo the others, so
+// X = sum_i r_i W_i - q P with q = rint(sum_i r_i w_i / p_i); R_i = round(2^20 w_i / p_i) gives
+// q from sum_i r_i R_i < 16 * 255 * 2^20 < 2^32 with an error below 16 * 128 / 2^20 = 2^-9.
+__host__ __device__ constexpr CrtU128 crt_folded(int nm, int i)
 {
-    return ((1u << 24) + crt_modulus(i) / 2) / crt_modulus(i);
+    return crt_mul(crt_cofactor(nm, i), crt_weight(nm, i));
+}
+
+__host__ __device__ constexpr uint32_t crt_recip20(int nm, int i)
+{
+    return (uint32_t)((((unsigned long long)crt_weight(nm, i) << 20) + crt_modulus(i) / 2) / crt_modulus(i));
 }
 
 // the largest symmetric residue kept as is (larger ones have p subtracted)
@@ -188,7 +198,7 @@ __host__ __device__ constexpr bool crt_tables_ok(int nm)
             if(a != 1)
                 return false; // not coprime
         }
-        if(crt_rem(crt_mul(crt_cofactor(nm, i), crt_weight(nm, i)), p) != 1)
+        if(crt_rem(crt_folded(nm, i), p) != 1)
             return false; // w_i is not the inverse of M_i
         for(int j = 0; j < nm; ++j)
             if(j != i && crt_rem(crt_cofactor(nm, i), crt_modulus(j)) != 0)
@@ -228,6 +238,21 @@ __host__ __device__ __forceinline__ void crt_static_for(F&& f)
         f(std::integral_constant<int, I0>{});
         crt_static_for<I0 + 1, I1>(f);
     }
+}
+
+// tcgen05.ld of 32 columns (lanes = rows) without the wait: several loads go out before one
+// tcgen05.wait::ld.
+__device__ __forceinline__ void tmem_ld_32x32b_x32_nowait(uint32_t taddr, uint32_t* v)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+                 "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                   "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                   "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                   "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                   "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                   "=r"(v[30]), "=r"(v[31])
+                 : "r"(taddr));
 }
 
 // ---- residues --------------------------------------------------------------------------------
@@ -364,42 +389,40 @@ __device__ __forceinline__ void crt_fail(int* error, int* abort_flag, int code)
     atomicExch(abort_flag, 1);
 }
 
-// y_i = (C_i w_i) mod p_i for the int32 accumulator value v (|v| <= 2^28)
-template <int NM, int I>
+// r_i = C_i mod p_i in [0, p_i) for the int32 accumulator value v (|v| <= 2^28)
+template <int I>
 __device__ __forceinline__ uint32_t crt_residue_of(uint32_t v)
 {
     constexpr uint32_t p = crt_modulus(I);
-    constexpr uint32_t w = crt_weight(NM, I);
     if constexpr(p == 256u)
-        return ((v & 255u) * w) & 255u;
+        return v & 255u;
     else
     {
         constexpr uint32_t off = p * ((1u << 28) / p + 1); // >= 2^28, a multiple of p
-        const uint32_t     r   = (v + off) % p;            // v + off in [0, 2^29 + 2p)
-        return (r * w) % p;
+        return (v + off) % p;                              // v + off in [0, 2^29 + 2p)
     }
 }
 
-// X from its residues: byte c of every modulus' 16-byte chunk; returns X as a double (one
-// rounding of the exact 128-bit value).
+// X from its residues r_i (byte COL of every modulus' 16-byte chunk); returns X as a double
+// (one rounding of the exact 128-bit value).
 template <int NM, int COL>
 __device__ __forceinline__ double crt_rebuild(const uint4 (&r)[NM])
 {
     unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    uint32_t           s24 = 0;
+    uint32_t           s20 = 0;
     crt_static_for<0, NM>([&](auto I) {
         constexpr int     i  = decltype(I)::value;
-        constexpr CrtU128 Mi = crt_cofactor(NM, i);
+        constexpr CrtU128 Wi = crt_folded(NM, i);
         const uint32_t    wd = (COL >> 2) == 0 ? r[i].x : (COL >> 2) == 1 ? r[i].y : (COL >> 2) == 2 ? r[i].z : r[i].w;
         const uint32_t    y  = (wd >> (8 * (COL & 3))) & 0xFFu;
-        s24 += y * crt_recip24(i);
-        a0 += (unsigned long long)y * crt_limb(Mi, 0);
-        a1 += (unsigned long long)y * crt_limb(Mi, 1);
-        a2 += (unsigned long long)y * crt_limb(Mi, 2);
-        a3 += (unsigned long long)y * crt_limb(Mi, 3);
+        s20 += y * crt_recip20(NM, i);
+        a0 += (unsigned long long)y * crt_limb(Wi, 0);
+        a1 += (unsigned long long)y * crt_limb(Wi, 1);
+        a2 += (unsigned long long)y * crt_limb(Wi, 2);
+        a3 += (unsigned long long)y * crt_limb(Wi, 3);
     });
     constexpr CrtU128 P = crt_product(NM);
-    const unsigned long long q = (s24 + (1u << 23)) >> 24; // rint(sum y_i / p_i)
+    const unsigned long long q = (s20 + (1u << 19)) >> 20; // rint(sum r_i w_i / p_i)
     long long d0 = (long long)a0 - (long long)(q * crt_limb(P, 0));
     long long d1 = (long long)a1 - (long long)(q * crt_limb(P, 1));
     long long d2 = (long long)a2 - (long long)(q * crt_limb(P, 2));
@@ -454,8 +477,8 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
         for(int b = 0; b < 2; ++b)
         {
             mbar_init(&acc_full[b], 1);    // tcgen05.commit
-            mbar_init(&acc_empty[b], 4);   // one arrival per residue warp
-            mbar_init(&slot_full[b], 128); // every residue thread, after its last modulus
+            mbar_init(&acc_empty[b], 8);   // one arrival per residue warp
+            mbar_init(&slot_full[b], 256); // every residue thread, after its last modulus
             mbar_init(&slot_empty[b], 128); // every reconstruction thread
         }
         mbar_init(&mma_done, 1);
@@ -559,10 +582,13 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             (void)mbar_wait_bounded(&mma_done, 0);
         }
     }
-    else if(warp < 6)
+    else if(warp < 10)
     {
-        // ---------------- residue epilogue (warps 2..5) ----------------
+        // ---------------- residue epilogue (warps 2..9) ----------------
+        // two warps per TMEM lane group (warp & 3): warps 2..5 take columns 0..127 of the
+        // accumulator, warps 6..9 columns 128..255
         const int      quarter   = warp & 3; // TMEM lane group this warp may access
+        const int      col0      = ((warp - 2) >> 2) * (kCrtBN / 2);
         const int      row       = quarter * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
         for(int j = 0; j < items; ++j)
@@ -585,18 +611,22 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 if(i != ii)
                     return;
 #pragma unroll 1
-                for(int cc = 0; cc < kCrtBN / 32; ++cc)
+                for(int cc = col0; cc < col0 + kCrtBN / 2; cc += 64)
                 {
-                    uint32_t v[32];
-                    tmem_ld_32x32b_x32(lane_addr + (uint32_t)(buf * kCrtBN + cc * 32), v);
-                    uint32_t w[8];
+                    // two loads in flight before the wait
+                    uint32_t v[64];
+                    tmem_ld_32x32b_x32_nowait(lane_addr + (uint32_t)(buf * kCrtBN + cc), v);
+                    tmem_ld_32x32b_x32_nowait(lane_addr + (uint32_t)(buf * kCrtBN + cc + 32), v + 32);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    uint32_t w[16];
 #pragma unroll
-                    for(int q = 0; q < 8; ++q)
-                        w[q] = crt_residue_of<NM, ii>(v[4 * q]) | (crt_residue_of<NM, ii>(v[4 * q + 1]) << 8)
-                               | (crt_residue_of<NM, ii>(v[4 * q + 2]) << 16)
-                               | (crt_residue_of<NM, ii>(v[4 * q + 3]) << 24);
-                    *reinterpret_cast<uint4*>(dst + (int64_t)(2 * cc) * kOzBM * 16) = make_uint4(w[0], w[1], w[2], w[3]);
-                    *reinterpret_cast<uint4*>(dst + (int64_t)(2 * cc + 1) * kOzBM * 16) = make_uint4(w[4], w[5], w[6], w[7]);
+                    for(int q = 0; q < 16; ++q)
+                        w[q] = crt_residue_of<ii>(v[4 * q]) | (crt_residue_of<ii>(v[4 * q + 1]) << 8)
+                               | (crt_residue_of<ii>(v[4 * q + 2]) << 16) | (crt_residue_of<ii>(v[4 * q + 3]) << 24);
+#pragma unroll
+                    for(int c = 0; c < 4; ++c)
+                        *reinterpret_cast<uint4*>(dst + (int64_t)(cc / 16 + c) * kOzBM * 16)
+                            = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
                 }
             });
             // accumulator free for the item after next
@@ -610,8 +640,8 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     }
     else
     {
-        // ---------------- reconstruction (warps 6..9) ----------------
-        const int    row  = (warp - 6) * 32 + lane;
+        // ---------------- reconstruction (warps 10..13) ----------------
+        const int    row  = (warp - 10) * 32 + lane;
         const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
         const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
         for(int jt = 0; jt < my_tiles; ++jt)
