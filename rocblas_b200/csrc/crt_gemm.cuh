@@ -35,7 +35,13 @@
 //             CTA's scratch slot in global memory (L2), two slots so that a tile's residues are
 //             written while the previous tile is rebuilt;
 //   warps 10-13 reconstruction: once all NM residues of a tile are in its slot, each thread takes
-//             one row, rebuilds X for 16 columns at a time and writes beta C + alpha 2^s X.
+//             one row, rebuilds X for 16 columns at a time and writes beta C + alpha 2^s X;
+//   warp 14   forwarder (CM x CN clusters): the A tile of a stage is shared by the CN CTAs of a
+//             cluster row, the B tile by the CM CTAs of a cluster column; each CTA fetches its
+//             1 / CN of A and 1 / CM of B from L2 and copies them into its peers' shared memory
+//             (cp.async.bulk shared::cta -> shared::cluster), so a 2 x 2 cluster reads half the
+//             operand bytes from L2 that four single CTAs would.  The MMA commits that free a
+//             stage arrive on the stage's barrier in every CTA that writes into it.
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its in-flight
 // copies and MMAs (again bounded), frees TMEM and returns.
 #pragma once
@@ -51,7 +57,11 @@ namespace rb200
 constexpr int kCrtMaxModuli = 16;
 constexpr int kCrtBN        = 256;  // output tile width: N of one MMA
 constexpr int kCrtBK        = 64;   // int8 K of one ring stage (SWIZZLE_64B rows)
-constexpr int kCrtThreads   = 448;  // 14 warps
+constexpr int kCrtThreads   = 480;  // 15 warps
+constexpr int kCrtResWarps  = 4;    // residue epilogue warps (warps 2 ..), a multiple of 4
+constexpr int kCrtRebWarps  = 8;    // reconstruction warps (after them), a multiple of 4
+constexpr int kCrtFwdWarp   = 2 + kCrtResWarps + kCrtRebWarps; // forwarder
+static_assert(kCrtFwdWarp < kCrtThreads / 32, "warp roles");
 constexpr int kCrtKMax      = 16384; // |C_i| <= K 128^2 <= 2^28 keeps the residue step in int32
 constexpr int kCrtMaxBits   = 60;   // W < 2^60: three 20-bit fields in the residue kernel
 constexpr int kCrtNPad      = kCrtBN;
@@ -440,46 +450,105 @@ __device__ __forceinline__ double crt_rebuild(const uint4 (&r)[NM])
     return neg ? -mag : mag;
 }
 
-template <int NM>
+// Cluster helpers (a CTA's peers share its A or B tiles through distributed shared memory).
+__device__ __forceinline__ uint32_t crt_cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t crt_mapa(uint32_t saddr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void crt_cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// shared::cta -> a peer's shared memory (both 16-byte aligned, bytes a multiple of 16), completing
+// `bytes` on the peer's mbarrier at the cluster address peer_bar
+__device__ __forceinline__ void crt_forward(uint32_t peer_dst, const void* src, uint32_t bytes, uint32_t peer_bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     peer_dst),
+                 "r"(smem_u32(src)), "r"(bytes), "r"(peer_bar)
+                 : "memory");
+}
+
+// tcgen05.commit arriving on the mbarrier at the same offset in every CTA of `mask`
+__device__ __forceinline__ void crt_commit_mc(uint64_t* bar, uint16_t mask)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                     smem_u32(bar)),
+                 "h"(mask)
+                 : "memory");
+}
+
+// CM x CN clusters: CTA rank r = b + CM a computes tile (CM smt + b, CN snt + a) of super-tile
+// (smt, snt); the CM CTAs of one column a share the B tile (each fetches 256 / CM of its rows),
+// the CN CTAs of one row b share the A tile (each fetches 128 / CN rows), and every CTA forwards
+// its part to those peers' shared memory.  CM = CN = 1: no cluster, no forwarding.
+template <int NM, int CM, int CN>
 __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_constant__ CrtParams p)
 {
     constexpr int kTileA = kOzBM * kCrtBK;  // 8 KB of P residues per stage
     constexpr int kTileB = kCrtBN * kCrtBK; // 16 KB of Q residues
     constexpr int kStage = kTileA + kTileB;
+    constexpr int kCS    = CM * CN;         // CTAs per cluster
+    constexpr int kPartA = kTileA / CN, kPartB = kTileB / CM; // bytes this CTA fetches
+    static_assert(kPartA % 512 == 0 && kPartB % 512 == 0, "parts of whole 8-row swizzle atoms");
     constexpr int64_t kModBytes = (int64_t)kCrtChunks * kOzBM * 16; // one modulus in a slot
     extern __shared__ __align__(1024) unsigned char crt_smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(crt_smem_raw) + 1023) & ~uintptr_t(1023));
     const int NS = p.stages;
 
-    __shared__ uint64_t full_bar[8], empty_bar[8], acc_full[2], acc_empty[2], slot_full[2],
-        slot_empty[2], mma_done;
+    __shared__ uint64_t full_bar[8], empty_bar[8], half_bar[8], acc_full[2], acc_empty[2],
+        slot_full[2], slot_empty[2], mma_done;
     __shared__ uint32_t tmem_base_sh;
     __shared__ int      abort_flag;
     __shared__ int      issued, consumed; // K steps loaded / handed to the tensor cores
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nk       = p.nkc;
-    const int tiles_m  = p.M_pad / kOzBM;
-    const int tiles_n  = p.N_pad / kCrtBN;
+    const int tiles_m  = p.M_pad / kOzBM / CM; // super-tiles (CM x CN tiles, one per cluster)
+    const int tiles_n  = p.N_pad / kCrtBN / CN;
     const int tiles    = tiles_m * tiles_n;
-    const int my_tiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int cid      = (int)blockIdx.x / kCS, nclu = (int)gridDim.x / kCS;
+    const int my_tiles = tiles > cid ? (tiles - 1 - cid) / nclu + 1 : 0;
     const int items    = my_tiles * NM;
+    const uint32_t crank = kCS > 1 ? crt_cluster_rank() : 0;
+    const int      cb = (int)crank % CM, ca = (int)crank / CM; // position in the cluster
+    // the CTA's tile of super-tile t
+    auto tile_of = [&](int t, int& mt, int& nt) {
+        oz_tile_coords(t, tiles_m, tiles_n, mt, nt);
+        mt = mt * CM + cb;
+        nt = nt * CN + ca;
+    };
     uint8_t*  slots    = p.scratch + (int64_t)blockIdx.x * 2 * kCrtSlotBytes;
 
     if(threadIdx.x == 0)
     {
         for(int i = 0; i < NS; ++i)
         {
-            mbar_init(&full_bar[i], 1);
-            mbar_init(&empty_bar[i], 1);
+            // with peers: the producer's expect_tx of the peers' bytes and the forwarder's
+            // arrival once this CTA's own parts have landed; freed by this CTA's MMAs and those
+            // of every peer it forwards to
+            mbar_init(&full_bar[i], kCS > 1 ? 2 : 1);
+            mbar_init(&empty_bar[i], kCS > 1 ? CM + CN - 1 : 1);
+            mbar_init(&half_bar[i], 1);
         }
         for(int b = 0; b < 2; ++b)
         {
             mbar_init(&acc_full[b], 1);    // tcgen05.commit
-            mbar_init(&acc_empty[b], 8);   // one arrival per residue warp
-            mbar_init(&slot_full[b], 256); // every residue thread, after its last modulus
-            mbar_init(&slot_empty[b], 128); // every reconstruction thread
+            mbar_init(&acc_empty[b], kCrtResWarps);       // one arrival per residue warp
+            mbar_init(&slot_full[b], 32 * kCrtResWarps);  // every residue thread, after its last modulus
+            mbar_init(&slot_empty[b], 32 * kCrtRebWarps); // every reconstruction thread
         }
         mbar_init(&mma_done, 1);
         abort_flag = 0;
@@ -496,6 +565,8 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
+    if constexpr(kCS > 1)
+        crt_cluster_sync(); // the peers' barriers are initialised before anything arrives on them
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
@@ -510,9 +581,10 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             {
                 const int jt = j / NM, i = j - jt * NM;
                 int       mt, nt;
-                oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
-                const int8_t* srcP = p.resP + ((int64_t)i * nk * p.M_pad + mt * kOzBM) * kCrtBK;
-                const int8_t* srcQ = p.resQ + ((int64_t)i * nk * p.N_pad + nt * kCrtBN) * kCrtBK;
+                tile_of(cid + jt * nclu, mt, nt);
+                // this CTA's parts: rows ca * 128 / CN.. of the A tile, cb * 256 / CM.. of the B tile
+                const int8_t* srcP = p.resP + ((int64_t)i * nk * p.M_pad + mt * kOzBM) * kCrtBK + ca * kPartA;
+                const int8_t* srcQ = p.resQ + ((int64_t)i * nk * p.N_pad + nt * kCrtBN) * kCrtBK + cb * kPartB;
                 for(int kc = 0; kc < nk; ++kc, ++it)
                 {
                     const int      st = it % NS;
@@ -524,9 +596,22 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                         break;
                     }
                     unsigned char* base = smem + st * kStage;
-                    mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
-                    bulk_load(base, srcP + (int64_t)kc * p.M_pad * kCrtBK, kTileA, &full_bar[st]);
-                    bulk_load(base + kTileA, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kTileB, &full_bar[st]);
+                    if constexpr(kCS == 1)
+                    {
+                        mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
+                        bulk_load(base, srcP + (int64_t)kc * p.M_pad * kCrtBK, kTileA, &full_bar[st]);
+                        bulk_load(base + kTileA, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kTileB, &full_bar[st]);
+                    }
+                    else
+                    {
+                        // the peers' parts arrive on full_bar, this CTA's own on half_bar (the
+                        // forwarder sends them on from there)
+                        mbar_expect_tx(&full_bar[st], (uint32_t)(kStage - kPartA - kPartB));
+                        mbar_expect_tx(&half_bar[st], (uint32_t)(kPartA + kPartB));
+                        bulk_load(base + ca * kPartA, srcP + (int64_t)kc * p.M_pad * kCrtBK, kPartA, &half_bar[st]);
+                        bulk_load(base + kTileA + cb * kPartB, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kPartB,
+                                  &half_bar[st]);
+                    }
                     *(volatile int*)&issued = it + 1;
                 }
             }
@@ -537,6 +622,11 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
         // ---------------- MMA issuer ----------------
         if(lane == 0)
         {
+            // this CTA and the peers it exchanges parts with: same b (A) or same a (B)
+            uint16_t peer_mask = 0;
+            for(int r = 0; r < kCS; ++r)
+                if(r % CM == cb || r / CM == ca)
+                    peer_mask |= (uint16_t)(1u << r);
             const uint64_t desc_a0 = oz_smem_desc<kCrtBK>(smem_u32(smem));
             const uint64_t desc_b0 = oz_smem_desc<kCrtBK>(smem_u32(smem) + kTileA);
             constexpr uint32_t idesc = oz_idesc(kCrtBN);
@@ -573,7 +663,10 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                         oz_mma(dcol, desc_a0 + soff + kof, desc_b0 + soff + kof, idesc,
                                (kc > 0 || kk > 0) ? 1u : 0u);
                     }
-                    oz_commit(&empty_bar[st]);
+                    if constexpr(kCS == 1)
+                        oz_commit(&empty_bar[st]);
+                    else
+                        crt_commit_mc(&empty_bar[st], peer_mask);
                 }
                 oz_commit(&acc_full[buf]);
             }
@@ -582,13 +675,14 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             (void)mbar_wait_bounded(&mma_done, 0);
         }
     }
-    else if(warp < 10)
+    else if(warp < 2 + kCrtResWarps)
     {
-        // ---------------- residue epilogue (warps 2..9) ----------------
-        // two warps per TMEM lane group (warp & 3): warps 2..5 take columns 0..127 of the
-        // accumulator, warps 6..9 columns 128..255
+        // ---------------- residue epilogue ----------------
+        // kCrtResWarps / 4 warps per TMEM lane group (warp & 3), each taking an equal share of
+        // the accumulator's columns
+        constexpr int  kCols     = kCrtBN / (kCrtResWarps / 4);
         const int      quarter   = warp & 3; // TMEM lane group this warp may access
-        const int      col0      = ((warp - 2) >> 2) * (kCrtBN / 2);
+        const int      col0      = ((warp - 2) >> 2) * kCols;
         const int      row       = quarter * 32 + lane;
         const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
         for(int j = 0; j < items; ++j)
@@ -611,7 +705,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 if(i != ii)
                     return;
 #pragma unroll 1
-                for(int cc = col0; cc < col0 + kCrtBN / 2; cc += 64)
+                for(int cc = col0; cc < col0 + kCols; cc += 64)
                 {
                     // two loads in flight before the wait
                     uint32_t v[64];
@@ -638,10 +732,53 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_full[slot])) : "memory");
         }
     }
-    else
+    else if(warp == kCrtFwdWarp)
     {
-        // ---------------- reconstruction (warps 10..13) ----------------
-        const int    row  = (warp - 10) * 32 + lane;
+        // ---------------- forwarder (clusters) ----------------
+        // once this CTA's own parts of a stage have landed, copy them into the same stage of
+        // the peers that share them (A part: same cluster row b; B part: same column a),
+        // completing on the peers' full barriers, and count the own parts in on full_bar
+        if constexpr(kCS > 1)
+        {
+            if(lane == 0)
+            {
+                const int total = items * nk;
+                for(int it = 0; it < total; ++it)
+                {
+                    const int      st = it % NS;
+                    const uint32_t ph = (uint32_t)((it / NS) & 1);
+                    if(!crt_wait(&half_bar[st], ph, &abort_flag))
+                    {
+                        crt_fail(p.error, &abort_flag, 15);
+                        break;
+                    }
+                    unsigned char* base   = smem + st * kStage;
+                    unsigned char* a_part = base + ca * kPartA;
+                    unsigned char* b_part = base + kTileA + cb * kPartB;
+#pragma unroll
+                    for(int r = 0; r < kCS; ++r)
+                    {
+                        if(r == (int)crank)
+                            continue;
+                        const uint32_t pbar = crt_mapa(smem_u32(&full_bar[st]), (uint32_t)r);
+                        if(r % CM == cb)
+                            crt_forward(crt_mapa(smem_u32(a_part), (uint32_t)r), a_part, kPartA, pbar);
+                        else if(r / CM == ca)
+                            crt_forward(crt_mapa(smem_u32(b_part), (uint32_t)r), b_part, kPartB, pbar);
+                    }
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_bar[st])) : "memory");
+                }
+            }
+        }
+    }
+    else if(warp < kCrtFwdWarp)
+    {
+        // ---------------- reconstruction ----------------
+        // thread t: row t % 128, the t / 128-th share of the tile's 16-column chunks
+        constexpr int kChunksPer = kCrtChunks / (kCrtRebWarps / 4);
+        const int    t    = (warp - 2 - kCrtResWarps) * 32 + lane;
+        const int    row  = t & (kOzBM - 1);
+        const int    ch0  = (t >> 7) * kChunksPer;
         const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
         const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
         for(int jt = 0; jt < my_tiles; ++jt)
@@ -653,14 +790,14 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 break;
             }
             int mt, nt;
-            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+            tile_of(cid + jt * nclu, mt, nt);
             const int gr = mt * kOzBM + row;
             int       er = gr < p.M ? p.exp_rows[gr] : 0;
             if(er == kOzExpNone)
                 er = 0;
             const uint8_t* src = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)row * 16;
 #pragma unroll 1
-            for(int ch = 0; ch < kCrtChunks; ++ch)
+            for(int ch = ch0; ch < ch0 + kChunksPer; ++ch)
             {
                 uint4 r[NM];
 #pragma unroll
@@ -697,7 +834,24 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
 
     // ---------------- teardown ----------------
     __syncthreads();
-    if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
+    if constexpr(kCS > 1)
+    {
+        // every CTA of the cluster is done issuing: in the normal course every part forwarded
+        // to this CTA has landed (it was consumed) and every peer's MMAs have completed
+        crt_cluster_sync();
+        if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
+        {
+            // after an abort, give the copies still in flight (own loads, peers' forwards) time
+            // to land before the shared memory is released
+            for(int i = consumed; i < issued; ++i)
+                (void)mbar_wait_bounded(&half_bar[i % NS], (uint32_t)((i / NS) & 1));
+            const long long t0 = clock64();
+            while(clock64() - t0 < (1ll << 20))
+            {
+            }
+        }
+    }
+    else if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
     {
         // let the copies that were issued but never consumed land before the CTA exits
         for(int i = consumed; i < issued; ++i)

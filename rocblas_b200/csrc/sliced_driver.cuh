@@ -208,6 +208,32 @@ static int64_t crt_k_chunk()
     return std::max<int64_t>(64, std::min<int64_t>(kCrtKMax, tuning().sliced_k_chunk / 64 * 64));
 }
 
+// Cluster shape of the residue GEMM (tuning key crt_cluster): 1 single CTAs; 2: pairs along M
+// sharing the B tile; 4: 2 x 2 clusters sharing A along N and B along M.
+struct CrtShape
+{
+    int cm, cn;
+};
+
+static CrtShape crt_shape(int nm)
+{
+    const int c = tuning().crt_cluster;
+    if(nm == 14 || c <= 1)
+        return {1, 1};
+    return c >= 4 ? CrtShape{2, 2} : CrtShape{2, 1};
+}
+
+static int64_t crt_m_pad(int64_t M, CrtShape c)
+{
+    return round_up(std::max<int64_t>(M, 1), (int64_t)kOzBM * c.cm);
+}
+
+static int64_t crt_n_pad(int64_t N, CrtShape c)
+{
+    return round_up(std::max<int64_t>(N, 1), (int64_t)kCrtNPad * c.cn);
+}
+
+// CTAs of the persistent grid: at most one per SM (an upper bound for the scratch slots)
 static int64_t crt_grid(int64_t Mp, int64_t Np, int sms)
 {
     const int64_t tiles = (Mp / kOzBM) * (Np / kCrtBN);
@@ -218,8 +244,9 @@ static int64_t crt_grid(int64_t Mp, int64_t Np, int sms)
 // panels of one K range, the exponents and two 512 KB reconstruction slots per CTA.
 static size_t crt_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int nm, int sms)
 {
-    const int64_t Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()), kCrtBK);
-    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kCrtNPad);
+    const CrtShape c  = crt_shape(nm);
+    const int64_t  Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()), kCrtBK);
+    const int64_t  Mp = crt_m_pad(M, c), Np = crt_n_pad(N, c);
     return align256((size_t)nm * Mp * Kp) + align256((size_t)nm * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np) + align256((size_t)crt_grid(Mp, Np, sms) * 2 * kCrtSlotBytes);
 }
@@ -227,6 +254,50 @@ static size_t crt_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int nm, 
 static bool crt_moduli_supported(int nm)
 {
     return nm == 14 || nm == 15 || nm == 16;
+}
+
+template <int NM, int CM, int CN>
+static void launch_crt_gemm(const CrtParams& p, int64_t Mp, int64_t Np, int sms, cudaStream_t s)
+{
+    constexpr int kCS  = CM * CN;
+    const size_t  smem = (size_t)p.stages * (kOzBM + kCrtBN) * kCrtBK + 1024;
+    const void*   fn   = (const void*)crt_gemm_kernel<NM, CM, CN>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int64_t supers = (Mp / kOzBM / CM) * (Np / kCrtBN / CN);
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    cfg.blockDim         = dim3(kCrtThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream           = s;
+    int64_t nclu         = std::max<int64_t>(1, std::min<int64_t>(supers, std::max(sms, 1) / kCS));
+    if constexpr(kCS > 1)
+    {
+        attr[0].id               = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kCS;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs                = attr;
+        cfg.numAttrs             = 1;
+        // clusters that can be resident at once (SMs of a GPC are taken in whole clusters)
+        static int max_clusters = 0;
+        if(!max_clusters)
+        {
+            cfg.gridDim = dim3((unsigned)(kCS * nclu));
+            int n = 0;
+            if(cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess || n < 1)
+            {
+                cudaGetLastError();
+                n = std::max(1, sms / kCS);
+            }
+            max_clusters = n;
+        }
+        nclu = std::min<int64_t>(nclu, max_clusters);
+    }
+    cfg.gridDim = dim3((unsigned)(kCS * nclu));
+    // algorithmic work: int8 tensor operations of the NM residue products
+    TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)p.M * p.N * p.K);
+    cudaLaunchKernelEx(&cfg, crt_gemm_kernel<NM, CM, CN>, p);
+    count_launch();
 }
 
 template <int NM>
@@ -241,15 +312,20 @@ static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int*
     dim3 gQ((unsigned)(Kp / kOzSliceTile), (unsigned)(Np / kOzSliceTile));
     crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp);
     count_launch();
-    p.shift = 2 * bits;
+    p.shift  = 2 * bits;
     p.stages = std::min(8, (kCrtSmemBudget - 1024) / ((kOzBM + kCrtBN) * kCrtBK));
-    const size_t smem = (size_t)p.stages * (kOzBM + kCrtBN) * kCrtBK + 1024;
-    cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const unsigned grid = (unsigned)crt_grid(Mp, Np, sms);
-    // algorithmic work: int8 tensor operations of the NM residue products
-    TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)M * N * K);
-    crt_gemm_kernel<NM><<<grid, kCrtThreads, smem, s>>>(p);
-    count_launch();
+    const CrtShape c = crt_shape(NM);
+    if constexpr(NM == 14)
+        launch_crt_gemm<NM, 1, 1>(p, Mp, Np, sms, s);
+    else
+    {
+        if(c.cm == 2 && c.cn == 2)
+            launch_crt_gemm<NM, 2, 2>(p, Mp, Np, sms, s);
+        else if(c.cm == 2)
+            launch_crt_gemm<NM, 2, 1>(p, Mp, Np, sms, s);
+        else
+            launch_crt_gemm<NM, 1, 1>(p, Mp, Np, sms, s);
+    }
 }
 
 // Runs the residue engine; ws must hold crt_gemm_workspace_bytes(M, N, K, moduli, sms).
@@ -259,9 +335,10 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         return true;
     if(!crt_moduli_supported(g.moduli) || g.c_f32 || g.P.f32 || g.Q.f32)
         return false;
-    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kCrtNPad);
-    const int64_t K  = std::max<int64_t>(g.K, 0);
-    const int64_t kchunk = crt_k_chunk();
+    const CrtShape cs = crt_shape(g.moduli);
+    const int64_t  Mp = crt_m_pad(g.M, cs), Np = crt_n_pad(g.N, cs);
+    const int64_t  K  = std::max<int64_t>(g.K, 0);
+    const int64_t  kchunk = crt_k_chunk();
     for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kchunk)
     {
         const int64_t kc = std::min<int64_t>(kchunk, K - k0);
