@@ -50,6 +50,8 @@ SLICED_TRAFFIC_PER_LAUNCH = 1.0795e9
 SLICED_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum of "
                          "`bench.py --no-extras --steps 2 --warmup 3`: 77 launches, mean per launch "
                          "(0.248 / 1.035 / 4.496 GB for the 4 / 2 / 1 launches of each solve)")
+CRT_TRAFFIC_PER_LAUNCH = None
+CRT_TRAFFIC_SOURCE = "not captured yet for the residue GEMM"
 CHAIN_TRAFFIC_PER_LAUNCH = 35.57e9
 CHAIN_TRAFFIC_SOURCE = ("same capture: the 8 plain-solve launches of trsm_chain_kernel (45.5 ms each); "
                         "A (1.07 GB) is streamed once per 64-column strip group")
@@ -159,6 +161,22 @@ def headline_slices(L, S):
     v = ctypes.c_int(0)
     assert L.rocblas_b200_get_tuning(b"mixed_slices", ctypes.byref(v)) == 0
     return v.value
+
+
+def headline_engine(L, S):
+    """The integer GEMM engine of the precision form's updates for a call with `S` (0: the
+    tuning table's engine, the residue GEMM with mixed_moduli moduli unless that is 0; 1..8: the
+    slice GEMM with S slices): {"engine", "moduli" | "slices", "kernel", "label"}."""
+    nm = ctypes.c_int(0)
+    assert L.rocblas_b200_get_tuning(b"mixed_moduli", ctypes.byref(nm)) == 0
+    if S == 0 and nm.value > 0:
+        return {"engine": "residue", "moduli": nm.value,
+                "kernel": f"crt_gemm_kernel<{nm.value}> (tcgen05 kind::i8, {nm.value} residue products)",
+                "label": f"int8 residue (CRT) tensor-core updates, {nm.value} moduli"}
+    S_used = headline_slices(L, S)
+    return {"engine": "slices", "slices": S_used,
+            "kernel": f"ozaki_gemm_kernel<64,64,{S_used}> (tcgen05 kind::i8, {S_used} slices)",
+            "label": f"int8-slice tensor-core updates, {S_used} slices"}
 
 
 def kernel_timing(L, cls):
@@ -773,7 +791,7 @@ def run_ours(args):
         e2e = {"value": FLOPS / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(a_h2d + B0.numel() * 8),
                "d2h_bytes_per_step": int(B0.numel() * 8), "ms_per_step": e2e_ms,
-               "form": f"precision form, {headline_slices(L, S)} slices, rocblas_b200_dtrsm_mixed_host on pinned host "
+               "form": f"precision form ({headline_engine(L, S)['label']}), rocblas_b200_dtrsm_mixed_host on pinned host "
                        "buffers (transfers of A's block rows, of B and of X overlap the left-looking solve)"}
         del A_host, B_host
 
@@ -799,25 +817,28 @@ def run_ours(args):
         cpu_tflops, cpu_s, _ = cpu_cblas_sample(A_host, B_host, N, threads)
         del A_host, B_host
         pk = measured_peaks()
-        # dominant kernel of the headline: the integer-slice GEMM (ozaki_gemm_kernel), work =
-        # int8 tensor operations of its slice pairs (2 * pairs * M * N * K per launch), timed
-        # per launch with CUDA events on the solve's stream inside the timed region.  The peak is
-        # the burst figure: the kernel is timed in short launches and the clocks stay at their
-        # maximum (the `clocks` record), not under the power cap the sustained figure saw.
+        # dominant kernel of the headline: the integer tensor-core GEMM of the updates (the
+        # residue GEMM crt_gemm_kernel, work = int8 tensor operations of its NM residue products,
+        # 2 * NM * M * N * K per launch; or the slice GEMM ozaki_gemm_kernel, 2 * pairs * M * N * K),
+        # timed per launch with CUDA events on the solve's stream inside the timed region.  The
+        # peak is the burst figure: the kernel is timed in short launches and the clocks stay at
+        # their maximum (the `clocks` record), not under the power cap the sustained figure saw.
         s_ms, s_ops, s_n = sliced_t
         achieved = s_ops / (s_ms * 1e-3) / 1e12 if s_ms > 0 else 0.0
         i8_peak = 2.0 * pk["bf16_tflops"]
-        S_used = headline_slices(L, S)
+        eng = headline_engine(L, S)
+        traffic, traffic_src = ((CRT_TRAFFIC_PER_LAUNCH, CRT_TRAFFIC_SOURCE) if eng["engine"] == "residue"
+                                else (SLICED_TRAFFIC_PER_LAUNCH, SLICED_TRAFFIC_SOURCE))
         roofline = {"bound": "tensor", "achieved": achieved, "peak": i8_peak, "unit": "TOP/s (int8)",
-                    "frac": achieved / i8_peak, "traffic": SLICED_TRAFFIC_PER_LAUNCH,
-                    "kernel": f"ozaki_gemm_kernel<64,64,{S_used}> (tcgen05 kind::i8, {S_used} slices)",
+                    "frac": achieved / i8_peak, "traffic": traffic,
+                    "kernel": eng["kernel"],
                     "launches": s_n, "kernel_ms_per_step": s_ms / args.steps,
                     "kernel_share_of_step": s_ms / total_ms,
                     "peak_source": "int8 dense = 2 x bf16_tflops (burst) of " + pk["source"]
                                    + " (B200's dense int8 rate is twice bf16)",
                     "frac_of_sustained": achieved / (2.0 * pk["bf16_tflops_sustained"]),
                     "sm_mhz_median": clocks.get("sm_mhz"),
-                    "traffic_source": SLICED_TRAFFIC_SOURCE,
+                    "traffic_source": traffic_src,
                     "fp64_equivalent": {"achieved": FLOPS / (med_ref * 1e-3) / 1e12, "peak": peak,
                                         "unit": "TFLOP/s", "what": "whole refined solve, m*n*k flops, "
                                         "against cuBLAS DGEMM 8192^3 measured in this run"}}
@@ -873,8 +894,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": workload_name(), "m": M, "n": N,
-                       "form": f"refined precision form: int8-slice tensor-core updates "
-                               f"({headline_slices(L, S)} slices), FP64 diagonal blocks; test: agreement to "
+                       "form": f"refined precision form: {headline_engine(L, S)['label']}, "
+                               f"FP64 diagonal blocks; test: agreement to "
                                f"1e-12 with the plain FP64 form on {args.check_columns or 8} right-hand sides "
                                "(solved on a second stream), FP64-residual corrections if it fails",
                        "l2": "inputs larger than L2 (A 2 GiB, B 512 MiB); no flush",

@@ -283,9 +283,11 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_cgemm(rocblas_handle               ha
 /* ---- precision form of dtrsm ----------------------------------------------------------------
  * Same contract as rocblas_dtrsm.  The blocked solve keeps the diagonal blocks in FP64
  * (inverted 128 x 128 blocks applied with FP64 tensor-core MMA) and runs every trailing
- * update with K >= sliced_min_k on the integer-slice tensor-core GEMM above with `slices`
- * slices (1..8; 0 = the tuning table's mixed_slices); shorter updates stay on FP64 DMMA.
- * Workspace: the invA blocks plus the slices of the largest update (size query supported). */
+ * update with K >= sliced_min_k on an integer tensor-core GEMM: slices = 0 takes the tuning
+ * table's engine (the residue GEMM rocblas_b200_dgemm_crt with mixed_moduli moduli, or, with
+ * mixed_moduli 0, the slice GEMM with mixed_slices slices); slices = 1..8 takes the slice GEMM
+ * rocblas_b200_dgemm_sliced with that many slices.  Shorter updates stay on FP64 DMMA.
+ * Workspace: the invA blocks plus the operands of the largest update (size query supported). */
 ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
                                                        rocblas_side      side,
                                                        rocblas_fill      uplo,
@@ -325,7 +327,8 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  * NULL. */
 typedef struct rocblas_b200_refine_options
 {
-    rocblas_int slices;         /* 0: the tuning table's mixed_slices */
+    rocblas_int slices;         /* 0: the tuning table's engine (mixed_moduli / mixed_slices);
+                                   1..8: the slice engine with that many slices */
     rocblas_int max_iterations; /* correction solves at most (negative: 10) */
     rocblas_int check_columns;  /* right-hand sides tested (0: 8; >= their count: all) */
     rocblas_int fallback;       /* 1: plain FP64 solve when the test never passes */
@@ -388,7 +391,9 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed_host(rocblas_handle    ha
  * to the library ("key value" lines, written by rocblas_b200/autotune.py); these two calls
  * read or change one entry in the running process.  Keys: block_max_k, block_always_k,
  * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices, dmma_force_tile,
- * dmma_big_bk.  Unknown keys or
+ * dmma_big_bk, oz_bn, oz_bk, chain_max_cols, chain_max_cols_f32, chain_w, mixed_chain_blocks,
+ * host_step_blocks, sliced_k_chunk, refine_check_sms, wait_cycles_log2, chain_first_item,
+ * mixed_moduli, strsm_slices, strsm_sliced_min_k.  Unknown keys or
  * out-of-range values return rocblas_status_invalid_value. */
 /* Per-launch timing of the main kernels with CUDA events on the launching stream, for
  * measuring one kernel's achieved rate inside a larger call.  enable != 0 starts recording

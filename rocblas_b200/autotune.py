@@ -128,8 +128,11 @@ def tune(quick=False, out_dir=HERE):
         Bt = B0.clone()
         return b.time(lambda: (Bt.copy_(B0), b.dtrsm(At, Bt, m, n, mixed_slices=S)))
 
+    # engines: the 7-bit slice engine with S slices (mixed_moduli 0) and the residue engine
+    # with NM moduli (mixed_moduli NM; the slice count is then unused)
     cands = {}
-    for S in (7, 8):
+    for engine, S, NM in (("slices", 7, 0), ("slices", 8, 0), ("moduli", 8, 15), ("moduli", 8, 16)):
+        set_tuning("mixed_moduli", NM)
         for chunk in (16384, 4096, 2048):
             set_tuning("sliced_k_chunk", chunk)
             worst = 0.0
@@ -138,13 +141,15 @@ def tune(quick=False, out_dir=HERE):
                 b.dtrsm(A_, Xm, m, nb, mixed_slices=S)
                 torch.cuda.synchronize()
                 worst = max(worst, float(torch.linalg.norm(Xm - Xp) / torch.linalg.norm(Xp)))
-            cands[f"{S},{chunk}"] = {"worst_band_error": worst, "ms": mixed_ms(S)}
+            cands[f"{S},{NM},{chunk}"] = {"engine": engine, "worst_band_error": worst, "ms": mixed_ms(S)}
     ok = {k: v for k, v in cands.items() if v["worst_band_error"] <= 1e-13}
-    pick = min(ok, key=lambda k: ok[k]["ms"]) if ok else "8,2048"
-    S_best, chunk_best = (int(x) for x in pick.split(","))
+    pick = min(ok, key=lambda k: ok[k]["ms"]) if ok else "8,0,2048"
+    S_best, NM_best, chunk_best = (int(x) for x in pick.split(","))
     set_tuning("mixed_slices", S_best)
+    set_tuning("mixed_moduli", NM_best)
     set_tuning("sliced_k_chunk", chunk_best)
-    report["entries"]["mixed_slices"] = {"chosen": S_best, "sliced_k_chunk": chunk_best, "candidates": cands,
+    report["entries"]["mixed_slices"] = {"chosen": S_best, "mixed_moduli": NM_best, "sliced_k_chunk": chunk_best,
+                                         "candidates": cands,
                                          "target": "worst band error <= 1e-13 (1e-12 with a 10x margin)",
                                          "shape": [m, n], "error_shape": [m, nb]}
     del bands, plain
@@ -159,6 +164,31 @@ def tune(quick=False, out_dir=HERE):
         set_tuning(key, _pick(res))
         report["entries"][key] = {"chosen": _pick(res), "ms": res, "shape": big}
     del data
+
+    # ---- FP32 solve: slices of the trailing updates and the smallest sliced update ---------
+    # 4 slices keep 28 bits of every entry (FP32 has 24); the error against the FFMA tiles is
+    # reported, the time of strsm at 8192 x 8192 picks the minimum inner dimension
+    k32 = 4096 if quick else 8192
+    At32, B32 = condition_band_lower_torch(k32, k32, 0, seed=32, device="cuda", dtype=torch.float32)
+    one32 = ctypes.c_float(1.0)
+
+    def strsm_ms():
+        Bt = B32.clone()
+        args = (b.h.value, 141, 122, 111, 131, k32, k32, ctypes.cast(ctypes.byref(one32), ctypes.c_void_p),
+                ctypes.c_void_p(At32.data_ptr()), k32, ctypes.c_void_p(Bt.data_ptr()), k32)
+        return b.time(lambda: (Bt.copy_(B32), lib().rocblas_strsm(*args)))
+
+    res = {}
+    set_tuning("strsm_slices", 0)
+    res["ffma"] = strsm_ms()
+    set_tuning("strsm_slices", 4)
+    for mk in (512, 1024, 2048):
+        set_tuning("strsm_sliced_min_k", mk)
+        res[mk] = strsm_ms()
+    best_mk = min((k for k in res if k != "ffma"), key=lambda k: res[k])
+    set_tuning("strsm_sliced_min_k", best_mk)
+    report["entries"]["strsm_sliced_min_k"] = {"chosen": best_mk, "strsm_slices": 4, "ms": res, "shape": [k32, k32]}
+    del At32, B32
 
     # ---- block solver vs the blocked paths for k in (128, 512] ------------------------------
     res = {}
@@ -175,7 +205,8 @@ def tune(quick=False, out_dir=HERE):
 
     keys = ["block_max_k", "block_always_k", "block_min_strips_pct", "sliced_min_k",
             "dmma_big_tile_pct", "mixed_slices", "oz_bn", "oz_bk", "chain_max_cols",
-            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks", "host_step_blocks", "sliced_k_chunk"]
+            "chain_max_cols_f32", "chain_w", "mixed_chain_blocks", "host_step_blocks", "sliced_k_chunk",
+            "mixed_moduli", "strsm_slices", "strsm_sliced_min_k"]
     with open(os.path.join(out_dir, "tuning.cfg"), "w") as f:
         f.write("# written by rocblas_b200/autotune.py on " + report["device"] + "\n")
         for k in keys:

@@ -21,27 +21,24 @@
 // row's (column's) largest entry and the product of the truncated operands is exact, at 16 int8
 // GEMMs where the 7-bit slice form (ozaki_gemm.cuh) needs 36 slice-pair products for 56 bits.
 //
-// Kernel layout (persistent, one CTA per SM, 448 threads; output tiles 128 x 256; the tiles of
+// Kernel layout (persistent, one CTA per SM, 480 threads; output tiles 128 x 256; the tiles of
 // a CTA are t = blockIdx.x + j * gridDim.x in a grouped order, so the CTAs in flight work on
 // neighbouring tiles and, being in step, on the same modulus, and share its residue panels in L2):
-//   warp 0    copy producer: per work item (tile, modulus) and 64-deep K step, one bulk copy of
-//             the 128 x 64 P residue tile and one of the 256 x 64 Q tile into a ring stage; the
-//             residue kernel writes the panels in the tensor cores' SWIZZLE_64B order;
+//   warps 0, 14 copy producers (one thread each, alternate stages): per work item (tile,
+//             modulus) and 128-deep K stage (two 64-deep panels), one bulk copy of the 2 x 128 x 64
+//             P residues and one of the 2 x 256 x 64 Q residues into a 48 KB ring stage (4
+//             stages); the residue kernel writes each row tile's panels back to back in the
+//             tensor cores' SWIZZLE_64B order.  A single thread issues a stage in a few hundred
+//             cycles whatever its size, so stages are large and two threads issue them;
 //   warp 1    TMEM owner and MMA issuer: one 128 x 256 int32 accumulator per item, two
 //             accumulators (all 512 TMEM columns) so that an item's MMAs overlap the drain of the
 //             previous one;
-//   warps 2-9 residue epilogue (two warps per TMEM lane group, half the columns each):
-//             tcgen05.ld of the accumulator (lanes = rows), r_i as one byte per entry into the
-//             CTA's scratch slot in global memory (L2), two slots so that a tile's residues are
-//             written while the previous tile is rebuilt;
-//   warps 10-13 reconstruction: once all NM residues of a tile are in its slot, each thread takes
-//             one row, rebuilds X for 16 columns at a time and writes beta C + alpha 2^s X;
-//   warp 14   forwarder (CM x CN clusters): the A tile of a stage is shared by the CN CTAs of a
-//             cluster row, the B tile by the CM CTAs of a cluster column; each CTA fetches its
-//             1 / CN of A and 1 / CM of B from L2 and copies them into its peers' shared memory
-//             (cp.async.bulk shared::cta -> shared::cluster), so a 2 x 2 cluster reads half the
-//             operand bytes from L2 that four single CTAs would.  The MMA commits that free a
-//             stage arrive on the stage's barrier in every CTA that writes into it.
+//   warps 2-5 residue epilogue: tcgen05.ld of the accumulator (lanes = rows), r_i as one byte per
+//             entry into the CTA's scratch slot in global memory (L2), two slots so that a tile's
+//             residues are written while the previous tile is rebuilt;
+//   warps 6-13 reconstruction: once all NM residues of a tile are in its slot, each thread takes
+//             one row and half the columns, rebuilds X for 16 columns at a time and writes
+//             beta C + alpha 2^s X.
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its in-flight
 // copies and MMAs (again bounded), frees TMEM and returns.
 #pragma once
@@ -60,8 +57,8 @@ constexpr int kCrtBK        = 64;   // int8 K of one ring stage (SWIZZLE_64B row
 constexpr int kCrtThreads   = 480;  // 15 warps
 constexpr int kCrtResWarps  = 4;    // residue epilogue warps (warps 2 ..), a multiple of 4
 constexpr int kCrtRebWarps  = 8;    // reconstruction warps (after them), a multiple of 4
-constexpr int kCrtFwdWarp   = 2 + kCrtResWarps + kCrtRebWarps; // forwarder
-static_assert(kCrtFwdWarp < kCrtThreads / 32, "warp roles");
+constexpr int kCrtProdWarp2 = 2 + kCrtResWarps + kCrtRebWarps; // second copy producer
+static_assert(kCrtProdWarp2 < kCrtThreads / 32, "warp roles");
 constexpr int kCrtKMax      = 16384; // |C_i| <= K 128^2 <= 2^28 keeps the residue step in int32
 constexpr int kCrtMaxBits   = 60;   // W < 2^60: three 20-bit fields in the residue kernel
 constexpr int kCrtNPad      = kCrtBN;
@@ -267,11 +264,13 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32_nowait(uint32_t taddr, uint32
 
 // ---- residues --------------------------------------------------------------------------------
 // Operand element (o, k) at src[o * so + k * sk]; exps[o] from launch_exponents (1 + exponent of
-// the row's largest |x|; kOzExpNone for an all-zero row, whose residues are 0).  The residue
+// the row's largest |x|; kOzExpNone for an all-zero row, whose residues are 0).  The rows are
+// cut into row tiles of TR rows (the GEMM's tile height: 128 for P, 256 for Q); the residue
 // modulo p_i of row o, column k lives in the K panel kc = k / 64 as
-// dst[((i * K_pad / 64 + kc) * O_pad + o) * 64 + swizzled(k % 64)], the layout of the slice
-// panels (ozaki_gemm.cuh): every panel is the row-major image of O_pad rows of 64 bytes with the
-// 16-byte chunks of a row permuted for SWIZZLE_64B.  Rows o >= O and columns k >= K are zero.
+// dst[(((i * O_pad / TR + o / TR) * K_pad / 64 + kc) * TR + o % TR) * 64 + swizzled(k % 64)]:
+// every (row tile, panel) block is the row-major image of TR rows of 64 bytes with the 16-byte
+// chunks of a row permuted for SWIZZLE_64B, and a row tile's panels follow one another, so a
+// run of K panels of one tile is one contiguous block.  Rows o >= O and columns k >= K are zero.
 //
 // Per entry: W = trunc(|x| 2^(bits - e)) < 2^bits (one exact power-of-two scaling and a 64-bit
 // conversion), split into three 20-bit fields W = a 2^40 + m 2^20 + c, so that
@@ -279,7 +278,7 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32_nowait(uint32_t taddr, uint32
 template <int NM>
 __global__ void __launch_bounds__(256, 2)
     crt_residue_kernel(const double* src, int64_t so, int64_t sk, int O, int K, const int* exps,
-                       int bits, int8_t* dst, int O_pad, int K_pad)
+                       int bits, int8_t* dst, int O_pad, int K_pad, int TR)
 {
     __shared__ double tile[kOzSliceTile][kOzSliceTile + 1];
     const int  o0 = blockIdx.y * kOzSliceTile, k0 = blockIdx.x * kOzSliceTile;
@@ -333,7 +332,9 @@ __global__ void __launch_bounds__(256, 2)
     }
     const int     kc  = k / kCrtBK, c = (k % kCrtBK) / 16;
     const int64_t nkc = K_pad / kCrtBK;
-    int8_t* out = dst + (int64_t)kc * O_pad * kCrtBK + (int64_t)o * kCrtBK + oz_swizzle_chunk<kCrtBK>(o, c) * 16;
+    const int64_t tiles = O_pad / TR;
+    int8_t* out = dst + ((int64_t)(o / TR) * nkc + kc) * TR * kCrtBK + (int64_t)(o % TR) * kCrtBK
+                  + oz_swizzle_chunk<kCrtBK>(o, c) * 16;
     crt_static_for<0, NM>([&](auto I) {
         constexpr int      i    = decltype(I)::value;
         constexpr uint32_t p    = crt_modulus(i);
@@ -351,7 +352,7 @@ __global__ void __launch_bounds__(256, 2)
                 s = -s; // -(-128) = 128 for p = 256: the same byte, the same residue
             words[j >> 2] |= ((uint32_t)s & 0xFFu) << (8 * (j & 3));
         }
-        *reinterpret_cast<uint4*>(out + (int64_t)i * nkc * O_pad * kCrtBK)
+        *reinterpret_cast<uint4*>(out + (int64_t)i * tiles * nkc * TR * kCrtBK)
             = make_uint4(words[0], words[1], words[2], words[3]);
     });
 }
@@ -361,9 +362,9 @@ struct CrtParams
 {
     int           M, N, K;       // logical sizes (K <= kCrtKMax)
     int           M_pad, N_pad;  // residue-panel rows (multiples of 128 and 256)
-    int           nkc;           // 64-deep K panels per modulus
-    const int8_t* resP;          // [NM][nkc][M_pad][64], swizzled rows
-    const int8_t* resQ;          // [NM][nkc][N_pad][64]
+    int           nkc;           // 64-deep K panels per modulus (a multiple of kCrtKS)
+    const int8_t* resP;          // [NM][M_pad / 128][nkc][128][64], swizzled rows
+    const int8_t* resQ;          // [NM][N_pad / 256][nkc][256][64]
     const int*    exp_rows;      // e_r, M entries
     const int*    exp_cols;      // f_c, N entries
     int           shift;         // 2b: P Q ~= 2^(e_r + f_c - shift) X
@@ -374,7 +375,6 @@ struct CrtParams
     const double* ualpha_ptr;    // if set and *ualpha_ptr == 0: C := 0 (a trsm with alpha == 0)
     int           ualpha_zero;   // host-side form of the same condition
     uint8_t*      scratch;       // two slots of kCrtSlotBytes per CTA
-    int           stages;
     int*          error;         // set to a nonzero code if a wait timed out
 };
 
@@ -450,109 +450,58 @@ __device__ __forceinline__ double crt_rebuild(const uint4 (&r)[NM])
     return neg ? -mag : mag;
 }
 
-// Cluster helpers (a CTA's peers share its A or B tiles through distributed shared memory).
-__device__ __forceinline__ uint32_t crt_cluster_rank()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
+// Stage of the copy ring: kCrtKS consecutive 64-deep K panels of one (tile, modulus) item,
+// the P tile (128 x 64 per panel) then the Q tile (256 x 64 per panel); the residue kernel
+// lays a row tile's K panels out back to back, so each operand of a stage is one bulk copy.
+constexpr int kCrtKS     = 2;
+constexpr int kCrtStages = 4;
 
-__device__ __forceinline__ uint32_t crt_mapa(uint32_t saddr, uint32_t rank)
-{
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
-    return r;
-}
-
-__device__ __forceinline__ void crt_cluster_sync()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-// shared::cta -> a peer's shared memory (both 16-byte aligned, bytes a multiple of 16), completing
-// `bytes` on the peer's mbarrier at the cluster address peer_bar
-__device__ __forceinline__ void crt_forward(uint32_t peer_dst, const void* src, uint32_t bytes, uint32_t peer_bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     peer_dst),
-                 "r"(smem_u32(src)), "r"(bytes), "r"(peer_bar)
-                 : "memory");
-}
-
-// tcgen05.commit arriving on the mbarrier at the same offset in every CTA of `mask`
-__device__ __forceinline__ void crt_commit_mc(uint64_t* bar, uint16_t mask)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-                     smem_u32(bar)),
-                 "h"(mask)
-                 : "memory");
-}
-
-// CM x CN clusters: CTA rank r = b + CM a computes tile (CM smt + b, CN snt + a) of super-tile
-// (smt, snt); the CM CTAs of one column a share the B tile (each fetches 256 / CM of its rows),
-// the CN CTAs of one row b share the A tile (each fetches 128 / CN rows), and every CTA forwards
-// its part to those peers' shared memory.  CM = CN = 1: no cluster, no forwarding.
-template <int NM, int CM, int CN>
+template <int NM>
 __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_constant__ CrtParams p)
 {
-    constexpr int kTileA = kOzBM * kCrtBK;  // 8 KB of P residues per stage
-    constexpr int kTileB = kCrtBN * kCrtBK; // 16 KB of Q residues
-    constexpr int kStage = kTileA + kTileB;
-    constexpr int kCS    = CM * CN;         // CTAs per cluster
-    constexpr int kPartA = kTileA / CN, kPartB = kTileB / CM; // bytes this CTA fetches
-    static_assert(kPartA % 512 == 0 && kPartB % 512 == 0, "parts of whole 8-row swizzle atoms");
+    constexpr int kPanelA = kOzBM * kCrtBK;  // 8 KB of P residues per K panel
+    constexpr int kPanelB = kCrtBN * kCrtBK; // 16 KB of Q residues
+    constexpr int kStageA = kCrtKS * kPanelA;
+    constexpr int kStage  = kCrtKS * (kPanelA + kPanelB);
+    constexpr int NS      = kCrtStages;
     constexpr int64_t kModBytes = (int64_t)kCrtChunks * kOzBM * 16; // one modulus in a slot
     extern __shared__ __align__(1024) unsigned char crt_smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(crt_smem_raw) + 1023) & ~uintptr_t(1023));
-    const int NS = p.stages;
 
-    __shared__ uint64_t full_bar[8], empty_bar[8], half_bar[8], acc_full[2], acc_empty[2],
-        slot_full[2], slot_empty[2], mma_done;
+    __shared__ uint64_t full_bar[NS], empty_bar[NS], acc_full[2], acc_empty[2], slot_full[2],
+        slot_empty[2], mma_done;
     __shared__ uint32_t tmem_base_sh;
     __shared__ int      abort_flag;
-    __shared__ int      issued, consumed; // K steps loaded / handed to the tensor cores
+    __shared__ int      issued[2], consumed; // stages loaded by each producer / handed to the MMAs
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nk       = p.nkc;
-    const int tiles_m  = p.M_pad / kOzBM / CM; // super-tiles (CM x CN tiles, one per cluster)
-    const int tiles_n  = p.N_pad / kCrtBN / CN;
+    const int nks      = p.nkc / kCrtKS; // stages per item
+    const int tiles_m  = p.M_pad / kOzBM;
+    const int tiles_n  = p.N_pad / kCrtBN;
     const int tiles    = tiles_m * tiles_n;
-    const int cid      = (int)blockIdx.x / kCS, nclu = (int)gridDim.x / kCS;
-    const int my_tiles = tiles > cid ? (tiles - 1 - cid) / nclu + 1 : 0;
+    const int my_tiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int items    = my_tiles * NM;
-    const uint32_t crank = kCS > 1 ? crt_cluster_rank() : 0;
-    const int      cb = (int)crank % CM, ca = (int)crank / CM; // position in the cluster
-    // the CTA's tile of super-tile t
-    auto tile_of = [&](int t, int& mt, int& nt) {
-        oz_tile_coords(t, tiles_m, tiles_n, mt, nt);
-        mt = mt * CM + cb;
-        nt = nt * CN + ca;
-    };
+    const int total    = items * nks; // stage uses of the whole CTA
     uint8_t*  slots    = p.scratch + (int64_t)blockIdx.x * 2 * kCrtSlotBytes;
 
     if(threadIdx.x == 0)
     {
         for(int i = 0; i < NS; ++i)
         {
-            // with peers: the producer's expect_tx of the peers' bytes and the forwarder's
-            // arrival once this CTA's own parts have landed; freed by this CTA's MMAs and those
-            // of every peer it forwards to
-            mbar_init(&full_bar[i], kCS > 1 ? 2 : 1);
-            mbar_init(&empty_bar[i], kCS > 1 ? CM + CN - 1 : 1);
-            mbar_init(&half_bar[i], 1);
+            mbar_init(&full_bar[i], 1);
+            mbar_init(&empty_bar[i], 1);
         }
         for(int b = 0; b < 2; ++b)
         {
-            mbar_init(&acc_full[b], 1);    // tcgen05.commit
+            mbar_init(&acc_full[b], 1);                   // tcgen05.commit
             mbar_init(&acc_empty[b], kCrtResWarps);       // one arrival per residue warp
             mbar_init(&slot_full[b], 32 * kCrtResWarps);  // every residue thread, after its last modulus
             mbar_init(&slot_empty[b], 32 * kCrtRebWarps); // every reconstruction thread
         }
         mbar_init(&mma_done, 1);
         abort_flag = 0;
-        issued     = 0;
+        issued[0] = issued[1] = 0;
         consumed   = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -565,56 +514,36 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if constexpr(kCS > 1)
-        crt_cluster_sync(); // the peers' barriers are initialised before anything arrives on them
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
-    if(warp == 0)
+    if(warp == 0 || warp == kCrtProdWarp2)
     {
-        // ---------------- copy producer ----------------
-        if(lane == 0)
+        // ---------------- copy producers ----------------
+        // lane 0 of two warps takes alternate stage uses (one thread issues a stage in a few
+        // hundred cycles whatever its size, less than the tensor cores need for it at full
+        // rate); the whole warps enter this branch so that no lane reaches another role
+        const int who = warp == 0 ? 0 : 1;
+        for(int it = who; it < total && lane == 0; it += 2)
         {
-            int  it = 0; // K steps issued over all items
-            bool ok = true;
-            for(int j = 0; j < items && ok; ++j)
+            const int      st = it % NS;
+            const uint32_t ph = (uint32_t)((it / NS) & 1);
+            const int      j  = it / nks, ks = it - j * nks;
+            const int      jt = j / NM, i = j - jt * NM;
+            if(!crt_wait(&empty_bar[st], ph ^ 1, &abort_flag))
             {
-                const int jt = j / NM, i = j - jt * NM;
-                int       mt, nt;
-                tile_of(cid + jt * nclu, mt, nt);
-                // this CTA's parts: rows ca * 128 / CN.. of the A tile, cb * 256 / CM.. of the B tile
-                const int8_t* srcP = p.resP + ((int64_t)i * nk * p.M_pad + mt * kOzBM) * kCrtBK + ca * kPartA;
-                const int8_t* srcQ = p.resQ + ((int64_t)i * nk * p.N_pad + nt * kCrtBN) * kCrtBK + cb * kPartB;
-                for(int kc = 0; kc < nk; ++kc, ++it)
-                {
-                    const int      st = it % NS;
-                    const uint32_t ph = (uint32_t)((it / NS) & 1);
-                    if(!crt_wait(&empty_bar[st], ph ^ 1, &abort_flag))
-                    {
-                        crt_fail(p.error, &abort_flag, 11);
-                        ok = false;
-                        break;
-                    }
-                    unsigned char* base = smem + st * kStage;
-                    if constexpr(kCS == 1)
-                    {
-                        mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
-                        bulk_load(base, srcP + (int64_t)kc * p.M_pad * kCrtBK, kTileA, &full_bar[st]);
-                        bulk_load(base + kTileA, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kTileB, &full_bar[st]);
-                    }
-                    else
-                    {
-                        // the peers' parts arrive on full_bar, this CTA's own on half_bar (the
-                        // forwarder sends them on from there)
-                        mbar_expect_tx(&full_bar[st], (uint32_t)(kStage - kPartA - kPartB));
-                        mbar_expect_tx(&half_bar[st], (uint32_t)(kPartA + kPartB));
-                        bulk_load(base + ca * kPartA, srcP + (int64_t)kc * p.M_pad * kCrtBK, kPartA, &half_bar[st]);
-                        bulk_load(base + kTileA + cb * kPartB, srcQ + (int64_t)kc * p.N_pad * kCrtBK, kPartB,
-                                  &half_bar[st]);
-                    }
-                    *(volatile int*)&issued = it + 1;
-                }
+                crt_fail(p.error, &abort_flag, 11);
+                break;
             }
+            int mt, nt;
+            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+            const int8_t*  srcP = p.resP + (((int64_t)i * tiles_m + mt) * p.nkc + ks * kCrtKS) * kPanelA;
+            const int8_t*  srcQ = p.resQ + (((int64_t)i * tiles_n + nt) * p.nkc + ks * kCrtKS) * kPanelB;
+            unsigned char* base = smem + st * kStage;
+            mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
+            bulk_load(base, srcP, kStageA, &full_bar[st]);
+            bulk_load(base + kStageA, srcQ, kCrtKS * kPanelB, &full_bar[st]);
+            *(volatile int*)&issued[who] = it + 1;
         }
     }
     else if(warp == 1)
@@ -622,13 +551,8 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
         // ---------------- MMA issuer ----------------
         if(lane == 0)
         {
-            // this CTA and the peers it exchanges parts with: same b (A) or same a (B)
-            uint16_t peer_mask = 0;
-            for(int r = 0; r < kCS; ++r)
-                if(r % CM == cb || r / CM == ca)
-                    peer_mask |= (uint16_t)(1u << r);
             const uint64_t desc_a0 = oz_smem_desc<kCrtBK>(smem_u32(smem));
-            const uint64_t desc_b0 = oz_smem_desc<kCrtBK>(smem_u32(smem) + kTileA);
+            const uint64_t desc_b0 = oz_smem_desc<kCrtBK>(smem_u32(smem) + kStageA);
             constexpr uint32_t idesc = oz_idesc(kCrtBN);
             int  it = 0;
             bool ok = true;
@@ -643,7 +567,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t dcol = tmem + (uint32_t)(buf * kCrtBN);
-                for(int kc = 0; kc < nk; ++kc, ++it)
+                for(int ks = 0; ks < nks; ++ks, ++it)
                 {
                     const int      st = it % NS;
                     const uint32_t ph = (uint32_t)((it / NS) & 1);
@@ -657,16 +581,16 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                     *(volatile int*)&consumed = it + 1;
                     const uint64_t soff = (uint64_t)((st * kStage) >> 4);
 #pragma unroll
-                    for(int kk = 0; kk < kCrtBK / kOzMmaK; ++kk)
-                    {
-                        const uint64_t kof = (uint64_t)((kk * kOzMmaK) >> 4);
-                        oz_mma(dcol, desc_a0 + soff + kof, desc_b0 + soff + kof, idesc,
-                               (kc > 0 || kk > 0) ? 1u : 0u);
-                    }
-                    if constexpr(kCS == 1)
-                        oz_commit(&empty_bar[st]);
-                    else
-                        crt_commit_mc(&empty_bar[st], peer_mask);
+                    for(int q = 0; q < kCrtKS; ++q)
+#pragma unroll
+                        for(int kk = 0; kk < kCrtBK / kOzMmaK; ++kk)
+                        {
+                            const uint64_t aof = (uint64_t)((q * kPanelA + kk * kOzMmaK) >> 4);
+                            const uint64_t bof = (uint64_t)((q * kPanelB + kk * kOzMmaK) >> 4);
+                            oz_mma(dcol, desc_a0 + soff + aof, desc_b0 + soff + bof, idesc,
+                                   (ks > 0 || q > 0 || kk > 0) ? 1u : 0u);
+                        }
+                    oz_commit(&empty_bar[st]);
                 }
                 oz_commit(&acc_full[buf]);
             }
@@ -732,46 +656,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_full[slot])) : "memory");
         }
     }
-    else if(warp == kCrtFwdWarp)
-    {
-        // ---------------- forwarder (clusters) ----------------
-        // once this CTA's own parts of a stage have landed, copy them into the same stage of
-        // the peers that share them (A part: same cluster row b; B part: same column a),
-        // completing on the peers' full barriers, and count the own parts in on full_bar
-        if constexpr(kCS > 1)
-        {
-            if(lane == 0)
-            {
-                const int total = items * nk;
-                for(int it = 0; it < total; ++it)
-                {
-                    const int      st = it % NS;
-                    const uint32_t ph = (uint32_t)((it / NS) & 1);
-                    if(!crt_wait(&half_bar[st], ph, &abort_flag))
-                    {
-                        crt_fail(p.error, &abort_flag, 15);
-                        break;
-                    }
-                    unsigned char* base   = smem + st * kStage;
-                    unsigned char* a_part = base + ca * kPartA;
-                    unsigned char* b_part = base + kTileA + cb * kPartB;
-#pragma unroll
-                    for(int r = 0; r < kCS; ++r)
-                    {
-                        if(r == (int)crank)
-                            continue;
-                        const uint32_t pbar = crt_mapa(smem_u32(&full_bar[st]), (uint32_t)r);
-                        if(r % CM == cb)
-                            crt_forward(crt_mapa(smem_u32(a_part), (uint32_t)r), a_part, kPartA, pbar);
-                        else if(r / CM == ca)
-                            crt_forward(crt_mapa(smem_u32(b_part), (uint32_t)r), b_part, kPartB, pbar);
-                    }
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full_bar[st])) : "memory");
-                }
-            }
-        }
-    }
-    else if(warp < kCrtFwdWarp)
+    else if(warp < 2 + kCrtResWarps + kCrtRebWarps)
     {
         // ---------------- reconstruction ----------------
         // thread t: row t % 128, the t / 128-th share of the tile's 16-column chunks
@@ -790,7 +675,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 break;
             }
             int mt, nt;
-            tile_of(cid + jt * nclu, mt, nt);
+            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
             const int gr = mt * kOzBM + row;
             int       er = gr < p.M ? p.exp_rows[gr] : 0;
             if(er == kOzExpNone)
@@ -834,28 +719,12 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
 
     // ---------------- teardown ----------------
     __syncthreads();
-    if constexpr(kCS > 1)
-    {
-        // every CTA of the cluster is done issuing: in the normal course every part forwarded
-        // to this CTA has landed (it was consumed) and every peer's MMAs have completed
-        crt_cluster_sync();
-        if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
-        {
-            // after an abort, give the copies still in flight (own loads, peers' forwards) time
-            // to land before the shared memory is released
-            for(int i = consumed; i < issued; ++i)
-                (void)mbar_wait_bounded(&half_bar[i % NS], (uint32_t)((i / NS) & 1));
-            const long long t0 = clock64();
-            while(clock64() - t0 < (1ll << 20))
-            {
-            }
-        }
-    }
-    else if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
+    if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
     {
         // let the copies that were issued but never consumed land before the CTA exits
-        for(int i = consumed; i < issued; ++i)
-            (void)mbar_wait_bounded(&full_bar[i % NS], (uint32_t)((i / NS) & 1));
+        for(int it = consumed; it < max(issued[0], issued[1]); ++it)
+            if(it < issued[it & 1])
+                (void)mbar_wait_bounded(&full_bar[it % NS], (uint32_t)((it / NS) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();

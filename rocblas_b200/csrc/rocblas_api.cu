@@ -1548,14 +1548,14 @@ struct MixedPlan
     size_t inv_bytes = 0, sl_bytes = 0, ch_bytes = 0, total = 0;
 };
 
-MixedPlan mixed_plan(const TrsmProblem<double>& pr, int slices)
+MixedPlan mixed_plan(const TrsmProblem<double>& pr, int slices, int moduli)
 {
     MixedPlan p;
     p.recursive = choose_algo(pr) == Algo::recursive;
     if(!p.recursive)
         return p;
     p.inv_bytes = align256((size_t)kInvNB * pr.k() * sizeof(double));
-    p.sl_bytes  = mixed_slice_workspace_bytes(pr, slices);
+    p.sl_bytes  = mixed_slice_workspace_bytes(pr, slices, moduli);
     p.ch_bytes  = mixed_chain_workspace_bytes(pr);
     p.total     = p.inv_bytes + align256(p.sl_bytes) + align256(p.ch_bytes);
     return p;
@@ -1564,7 +1564,8 @@ MixedPlan mixed_plan(const TrsmProblem<double>& pr, int slices)
 // The precision-form solve of pr (alpha, A, B as set there) on the workspace laid out by
 // mixed_plan.  invA is built into the workspace when build_inv, else the blocks already there
 // (from an earlier solve with the same A) are used.  false if the GPU lacks the tensor path.
-bool mixed_run(TrsmProblem<double> pr, int slices, const MixedPlan& plan, void* ws, int* err, bool build_inv)
+bool mixed_run(TrsmProblem<double> pr, int slices, int moduli, const MixedPlan& plan, void* ws, int* err,
+               bool build_inv)
 {
     if(!plan.recursive)
     {
@@ -1580,7 +1581,7 @@ bool mixed_run(TrsmProblem<double> pr, int slices, const MixedPlan& plan, void* 
     pr.invA = inv;
     MixedRecursive rec{{pr, (int)pr.k(), (int)ceil_div(pr.k(), kInvNB)}};
     rec.S        = slices;
-    rec.moduli   = tuning().mixed_moduli;
+    rec.moduli   = moduli;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + plan.inv_bytes;
     rec.err_dev  = err;
     if(plan.ch_bytes)
@@ -1601,6 +1602,9 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
         = trsm_arg_check<double>(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb, 1);
     if(st != rocblas_status_continue)
         return st;
+    // slices 0: the tuning table's engine (the residue engine with mixed_moduli moduli, or
+    // mixed_slices slices); 1..8: the slice engine with that many slices
+    const int moduli = slices == 0 ? tuning().mixed_moduli : 0;
     if(slices == 0)
         slices = tuning().mixed_slices;
     if(slices < 1 || slices > kOzMaxS)
@@ -1628,7 +1632,7 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     pr.ldb = ldb;
     pr.stream   = h->stream;
     pr.sm_count = h->sm_count;
-    const MixedPlan plan = mixed_plan(pr, slices);
+    const MixedPlan plan = mixed_plan(pr, slices, moduli);
     if(h->size_query)
         return plan.total ? h->set_optimal_size(plan.total) : rocblas_status_size_unchanged;
     if((st = device_ready(h)) != rocblas_status_success)
@@ -1641,7 +1645,7 @@ rocblas_status trsm_mixed_impl(rocblas_handle h, rocblas_side side, rocblas_fill
     void* ws  = plan.total ? h->borrow(plan.total) : nullptr;
     if(plan.recursive && (!ws || !err))
         return rocblas_status_memory_error;
-    if(!mixed_run(pr, slices, plan, ws, err, true))
+    if(!mixed_run(pr, slices, moduli, plan, ws, err, true))
         return rocblas_status_arch_mismatch;
     return launch_status();
 }
@@ -1799,7 +1803,8 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     }
     if(h->pointer_mode != rocblas_pointer_mode_host)
         return rocblas_status_not_implemented;
-    const int S = opt && opt->slices ? opt->slices : tuning().mixed_slices;
+    const int S      = opt && opt->slices ? opt->slices : tuning().mixed_slices;
+    const int moduli = opt && opt->slices ? 0 : tuning().mixed_moduli; // an explicit slice count: slices
     if(S < 1 || S > kOzMaxS || (opt && (opt->check_columns < 0 || opt->tolerance < 0.0)))
         return rocblas_status_invalid_value;
     const bool   left     = side == rocblas_side_left;
@@ -1851,7 +1856,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     ps.sm_count         = std::max(1, std::min(tuning().refine_check_sms, h->sm_count / 4));
     // workspace: the precision form's | B0 (m x n) | R (m x n) | the tested right-hand sides |
     // their chain flags | the test's maxima
-    const MixedPlan plan  = mixed_plan(pr, S);
+    const MixedPlan plan  = mixed_plan(pr, S, moduli);
     const size_t    mn    = (size_t)m * n * sizeof(double);
     const size_t    smp   = (size_t)srows * scols * sizeof(double);
     const size_t    fl    = ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, 32)) : 0;
@@ -1914,7 +1919,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
 
     TrsmProblem<double> pr1 = pr; // the first solve shares the GPU with the reference solve
     pr1.sm_count            = std::max(1, h->sm_count - ps.sm_count);
-    if(!mixed_run(pr1, S, plan, ws, err, false))
+    if(!mixed_run(pr1, S, moduli, plan, ws, err, false))
         return rocblas_status_arch_mismatch;
     cudaStreamWaitEvent(s, ev_ref, 0);
 
@@ -1955,7 +1960,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
         // R := alpha B0 - op(A) X in FP64, D := the precision-form solve of op(A) D = R, X += D
         refine_prep(pr, B0, m, m, n, 0, nrhs, *alpha, pr.unit, R, m, nullptr);
         refine_product(pr, B, ldb, R, m, m, n);
-        if(!mixed_run(prc, S, plan, ws, err, false))
+        if(!mixed_run(prc, S, moduli, plan, ws, err, false))
             return rocblas_status_arch_mismatch;
         const dim3 grid((unsigned)ceil_div(m, 256), (unsigned)std::min(n, 65535));
         refine_update_kernel<<<grid, 256, 0, s>>>(B, ldb, R, m, m, n);
@@ -2005,6 +2010,7 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
     h->pointer_mode = mode;
     if(st != rocblas_status_continue)
         return st;
+    const int moduli = slices == 0 ? tuning().mixed_moduli : 0; // 0: the tuned engine
     if(slices == 0)
         slices = tuning().mixed_slices;
     if(slices < 1 || slices > kOzMaxS)
@@ -2083,8 +2089,8 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
     const int    nstep     = (int)ceil_div(nblk, DB);
     const bool   forward   = pr.oplower();
     const size_t inv_bytes = align256((size_t)kInvNB * k * sizeof(double));
-    const size_t sl_bytes  = update_workspace_bytes(std::min(k, DB * kInvNB), n, k, slices,
-                                                    tuning().mixed_moduli, pr.sm_count);
+    const size_t sl_bytes  = update_workspace_bytes(std::min(k, DB * kInvNB), n, k, slices, moduli,
+                                                    pr.sm_count);
     const size_t ch_bytes  = mixed_chain_workspace_bytes(pr);
     const size_t ws_bytes  = inv_bytes + (sl_bytes + 255) / 256 * 256 + (ch_bytes + 255) / 256 * 256;
     int*         err       = ensure_err(h);
@@ -2099,7 +2105,7 @@ rocblas_status trsm_mixed_host_impl(rocblas_handle h, rocblas_side side, rocblas
 
     MixedRecursive rec{{pr, k, nblk}};
     rec.S        = slices;
-    rec.moduli   = tuning().mixed_moduli;
+    rec.moduli   = moduli;
     rec.slice_ws = reinterpret_cast<unsigned char*>(ws) + inv_bytes;
     rec.err_dev  = err;
     if(ch_bytes)

@@ -208,45 +208,25 @@ static int64_t crt_k_chunk()
     return std::max<int64_t>(64, std::min<int64_t>(kCrtKMax, tuning().sliced_k_chunk / 64 * 64));
 }
 
-// Cluster shape of the residue GEMM (tuning key crt_cluster): 1 single CTAs; 2: pairs along M
-// sharing the B tile; 4: 2 x 2 clusters sharing A along N and B along M.
-struct CrtShape
-{
-    int cm, cn;
-};
-
-static CrtShape crt_shape(int nm)
-{
-    const int c = tuning().crt_cluster;
-    if(nm == 14 || c <= 1)
-        return {1, 1};
-    return c >= 4 ? CrtShape{2, 2} : CrtShape{2, 1};
-}
-
-static int64_t crt_m_pad(int64_t M, CrtShape c)
-{
-    return round_up(std::max<int64_t>(M, 1), (int64_t)kOzBM * c.cm);
-}
-
-static int64_t crt_n_pad(int64_t N, CrtShape c)
-{
-    return round_up(std::max<int64_t>(N, 1), (int64_t)kCrtNPad * c.cn);
-}
-
-// CTAs of the persistent grid: at most one per SM (an upper bound for the scratch slots)
+// CTAs of the persistent grid: at most one per SM
 static int64_t crt_grid(int64_t Mp, int64_t Np, int sms)
 {
     const int64_t tiles = (Mp / kOzBM) * (Np / kCrtBN);
     return std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(sms, 1)));
 }
 
+// K padded to whole ring stages (kCrtKS panels of 64)
+static int64_t crt_k_pad(int64_t K)
+{
+    return round_up(std::max<int64_t>(K, 1), (int64_t)kCrtKS * kCrtBK);
+}
+
 // Workspace for one residue-engine GEMM of M x N x K with nm moduli on sms SMs: the residue
 // panels of one K range, the exponents and two 512 KB reconstruction slots per CTA.
 static size_t crt_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int nm, int sms)
 {
-    const CrtShape c  = crt_shape(nm);
-    const int64_t  Kp = round_up(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()), kCrtBK);
-    const int64_t  Mp = crt_m_pad(M, c), Np = crt_n_pad(N, c);
+    const int64_t Kp = crt_k_pad(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()));
+    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kCrtNPad);
     return align256((size_t)nm * Mp * Kp) + align256((size_t)nm * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np) + align256((size_t)crt_grid(Mp, Np, sms) * 2 * kCrtSlotBytes);
 }
@@ -256,50 +236,6 @@ static bool crt_moduli_supported(int nm)
     return nm == 14 || nm == 15 || nm == 16;
 }
 
-template <int NM, int CM, int CN>
-static void launch_crt_gemm(const CrtParams& p, int64_t Mp, int64_t Np, int sms, cudaStream_t s)
-{
-    constexpr int kCS  = CM * CN;
-    const size_t  smem = (size_t)p.stages * (kOzBM + kCrtBN) * kCrtBK + 1024;
-    const void*   fn   = (const void*)crt_gemm_kernel<NM, CM, CN>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int64_t supers = (Mp / kOzBM / CM) * (Np / kCrtBN / CN);
-    cudaLaunchConfig_t cfg{};
-    cudaLaunchAttribute attr[1];
-    cfg.blockDim         = dim3(kCrtThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream           = s;
-    int64_t nclu         = std::max<int64_t>(1, std::min<int64_t>(supers, std::max(sms, 1) / kCS));
-    if constexpr(kCS > 1)
-    {
-        attr[0].id               = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kCS;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs                = attr;
-        cfg.numAttrs             = 1;
-        // clusters that can be resident at once (SMs of a GPC are taken in whole clusters)
-        static int max_clusters = 0;
-        if(!max_clusters)
-        {
-            cfg.gridDim = dim3((unsigned)(kCS * nclu));
-            int n = 0;
-            if(cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess || n < 1)
-            {
-                cudaGetLastError();
-                n = std::max(1, sms / kCS);
-            }
-            max_clusters = n;
-        }
-        nclu = std::min<int64_t>(nclu, max_clusters);
-    }
-    cfg.gridDim = dim3((unsigned)(kCS * nclu));
-    // algorithmic work: int8 tensor operations of the NM residue products
-    TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)p.M * p.N * p.K);
-    cudaLaunchKernelEx(&cfg, crt_gemm_kernel<NM, CM, CN>, p);
-    count_launch();
-}
-
 template <int NM>
 static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int* eP, int* eQ,
                        int8_t* rP, int8_t* rQ, int64_t Mp, int64_t Np, int64_t Kp, CrtParams p,
@@ -307,25 +243,19 @@ static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int*
 {
     const int bits = crt_bits(NM, K);
     dim3      gP((unsigned)(Kp / kOzSliceTile), (unsigned)(Mp / kOzSliceTile));
-    crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.d(), P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp);
+    crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.d(), P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp, kOzBM);
     count_launch();
     dim3 gQ((unsigned)(Kp / kOzSliceTile), (unsigned)(Np / kOzSliceTile));
-    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp);
+    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp, kCrtBN);
     count_launch();
-    p.shift  = 2 * bits;
-    p.stages = std::min(8, (kCrtSmemBudget - 1024) / ((kOzBM + kCrtBN) * kCrtBK));
-    const CrtShape c = crt_shape(NM);
-    if constexpr(NM == 14)
-        launch_crt_gemm<NM, 1, 1>(p, Mp, Np, sms, s);
-    else
-    {
-        if(c.cm == 2 && c.cn == 2)
-            launch_crt_gemm<NM, 2, 2>(p, Mp, Np, sms, s);
-        else if(c.cm == 2)
-            launch_crt_gemm<NM, 2, 1>(p, Mp, Np, sms, s);
-        else
-            launch_crt_gemm<NM, 1, 1>(p, Mp, Np, sms, s);
-    }
+    p.shift = 2 * bits;
+    const size_t smem = (size_t)kCrtStages * kCrtKS * (kOzBM + kCrtBN) * kCrtBK + 1024;
+    cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned grid = (unsigned)crt_grid(Mp, Np, sms);
+    // algorithmic work: int8 tensor operations of the NM residue products
+    TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)M * N * K);
+    crt_gemm_kernel<NM><<<grid, kCrtThreads, smem, s>>>(p);
+    count_launch();
 }
 
 // Runs the residue engine; ws must hold crt_gemm_workspace_bytes(M, N, K, moduli, sms).
@@ -335,14 +265,13 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         return true;
     if(!crt_moduli_supported(g.moduli) || g.c_f32 || g.P.f32 || g.Q.f32)
         return false;
-    const CrtShape cs = crt_shape(g.moduli);
-    const int64_t  Mp = crt_m_pad(g.M, cs), Np = crt_n_pad(g.N, cs);
-    const int64_t  K  = std::max<int64_t>(g.K, 0);
-    const int64_t  kchunk = crt_k_chunk();
+    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kCrtNPad);
+    const int64_t K  = std::max<int64_t>(g.K, 0);
+    const int64_t kchunk = crt_k_chunk();
     for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kchunk)
     {
         const int64_t kc = std::min<int64_t>(kchunk, K - k0);
-        const int64_t Kp = round_up(std::max<int64_t>(kc, 1), kCrtBK);
+        const int64_t Kp = crt_k_pad(kc);
         unsigned char* w = reinterpret_cast<unsigned char*>(ws);
         int8_t* rP = reinterpret_cast<int8_t*>(w);
         w += align256((size_t)g.moduli * Mp * Kp);
@@ -397,10 +326,12 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
     return true;
 }
 
-// Workspace of one update on the engine the tuning table selects (moduli > 0: residues).
+// Workspace of one update on the engine the tuning table selects (moduli > 0: residues, or
+// slices for updates with too few residue tiles, see sliced_trsm_update).
 static size_t update_workspace_bytes(int64_t M, int64_t N, int64_t K, int S, int moduli, int sms)
 {
-    return moduli > 0 ? crt_gemm_workspace_bytes(M, N, K, moduli, sms) : sliced_gemm_workspace_bytes(M, N, K, S);
+    const size_t sl = sliced_gemm_workspace_bytes(M, N, K, S);
+    return moduli > 0 ? std::max(crt_gemm_workspace_bytes(M, N, K, moduli, sms), sl) : sl;
 }
 
 // Runs the sliced GEMM; ws must hold sliced_gemm_workspace_bytes(M, N, min(K, kOzKMax), S).
@@ -531,7 +462,9 @@ static bool sliced_trsm_update(const TrsmProblem<T>& q, int c_lo, int c_hi, int 
     }
     g.c_f32 = f32;
     g.S = S;
-    g.moduli = moduli;
+    // the residue engine's 128 x 256 tiles leave SMs idle on updates with fewer tiles than SMs
+    // (the host-buffer path's 512-row block rows); the slice engine's 128 x 64 tiles do not
+    g.moduli = (int64_t)ceil_div(g.M, kOzBM) * ceil_div(g.N, kCrtBN) >= q.sm_count ? moduli : 0;
     g.ldc = q.ldb;
     g.a = -1.0;
     g.b_imm = 1.0;
@@ -627,7 +560,7 @@ static size_t mixed_chain_workspace_bytes(const TrsmProblem<double>& pr)
 }
 
 // Largest sliced update of the recursion (the top node's off-diagonal block).
-static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S)
+static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S, int moduli)
 {
     const int64_t k = pr.k();
     if(k <= kInvNB)
@@ -636,7 +569,6 @@ static size_t mixed_slice_workspace_bytes(const TrsmProblem<double>& pr, int S)
     const int64_t bm   = nblk / 2;
     const int64_t r_m  = std::min<int64_t>(bm * kInvNB, k);
     const int64_t big  = std::max(r_m, k - r_m);
-    const int moduli = tuning().mixed_moduli;
     return pr.side_left ? update_workspace_bytes(big, pr.n, big, S, moduli, pr.sm_count)
                         : update_workspace_bytes(pr.m, big, big, S, moduli, pr.sm_count);
 }

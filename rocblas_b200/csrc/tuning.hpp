@@ -46,8 +46,7 @@ struct Tuning
     int strsm_slices         = 4;    // FP32 solve: slices of its trailing updates on the int8 slice
                                      // engine (0: FFMA tiles)
     int strsm_sliced_min_k   = 1024; // ... for updates with at least this inner dimension
-    int mixed_moduli         = 0;
-    int crt_cluster          = 4;    // residue GEMM: CTAs sharing operand tiles (1, 2 or 4)    // precision form: 0 updates on the slice engine; 14..16 on
+    int mixed_moduli         = 16;   // precision form: 0 updates on the slice engine; 14..16 on
                                      // the residue (CRT) engine with this many moduli
     int chain_first_item     = 0;    // failure injection for tests: uniform chain launches start
                                      // claiming items here, so the flags of the items before it
@@ -82,7 +81,6 @@ static const TuningEntry kTuningEntries[] = {
     {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
     {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
     {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},
-    {"crt_cluster", &Tuning::crt_cluster, 1, 4},
     {"strsm_slices", &Tuning::strsm_slices, 0, 8},
     {"strsm_sliced_min_k", &Tuning::strsm_sliced_min_k, 64, 1 << 30},
 };

@@ -85,32 +85,6 @@ def test_crt_gemm_fp64_accuracy(handle, m, n, k):
     assert err < 2e-15, err
 
 
-@pytest.mark.parametrize("cluster", [1, 2, 4])
-@pytest.mark.parametrize("nm", [15, 16])
-def test_crt_gemm_clusters(handle, cluster, nm):
-    """Single CTAs, pairs sharing the B tile and 2 x 2 clusters sharing A and B through
-    distributed shared memory give the same result bit for bit (the products are exact)."""
-    rng = np.random.default_rng(21)
-    m, n, k = 700, 1100, 1500
-    A = np.asfortranarray(rng.standard_normal((m, k)))
-    B = np.asfortranarray(rng.standard_normal((k, n)))
-    C = np.asfortranarray(rng.standard_normal((m, n)))
-    L = rb.lib()
-    old = ctypes.c_int(-1)
-    assert L.rocblas_b200_get_tuning(b"crt_cluster", ctypes.byref(old)) == 0
-    try:
-        assert L.rocblas_b200_set_tuning(b"crt_cluster", 1) == 0
-        single = crt_gemm(handle, "N", "N", A, B, C, -1.0, 0.5, nm)
-        assert L.rocblas_b200_set_tuning(b"crt_cluster", cluster) == 0
-        got = crt_gemm(handle, "N", "N", A, B, C, -1.0, 0.5, nm)
-    finally:
-        L.rocblas_b200_set_tuning(b"crt_cluster", old.value)
-    assert np.array_equal(got, single)
-    ref = 0.5 * C.astype(np.longdouble) - A.astype(np.longdouble) @ B.astype(np.longdouble)
-    scale = np.abs(A) @ np.abs(B) + 0.5 * np.abs(C)
-    assert np.max(np.abs(got - ref.astype(np.float64)) / scale) < (2e-15 if nm == 16 else 2e-14)
-
-
 def test_crt_gemm_bits_per_modulus(handle):
     """Fewer moduli keep fewer bits: 14 < 15 < 16 in accuracy; 16 at the 8-slice level."""
     rng = np.random.default_rng(3)
