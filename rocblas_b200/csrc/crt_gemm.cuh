@@ -376,6 +376,7 @@ struct CrtParams
     int           ualpha_zero;   // host-side form of the same condition
     uint8_t*      scratch;       // two slots of kCrtSlotBytes per CTA
     int*          error;         // set to a nonzero code if a wait timed out
+    int           group_m;       // tile order: group_m row tiles side by side, then the next columns
 };
 
 // Bounded wait that also gives up once another role has aborted.
@@ -448,6 +449,17 @@ __device__ __forceinline__ double crt_rebuild(const uint4 (&r)[NM])
     const unsigned long long mhi = neg ? ~hi + (lo == 0 ? 1ull : 0ull) : hi;
     const double             mag = fma((double)mhi, 0x1p64, (double)mlo);
     return neg ? -mag : mag;
+}
+
+// Tile t of the persistent order: groups of g row tiles, within a group row-fastest, so the tiles
+// in flight share the residue panels of g row tiles and of a run of column tiles in L2.
+__device__ __forceinline__ void crt_tile_coords(int t, int tiles_m, int tiles_n, int g, int& mt, int& nt)
+{
+    const int per_group = g * tiles_n;
+    const int grp = t / per_group, r = t - grp * per_group;
+    const int gm  = min(g, tiles_m - grp * g); // rows in this group
+    mt = grp * g + r % gm;
+    nt = r / gm;
 }
 
 // Stage of the copy ring: kCrtKS consecutive 64-deep K panels of one (tile, modulus) item,
@@ -536,7 +548,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 break;
             }
             int mt, nt;
-            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+            crt_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, p.group_m, mt, nt);
             const int8_t*  srcP = p.resP + (((int64_t)i * tiles_m + mt) * p.nkc + ks * kCrtKS) * kPanelA;
             const int8_t*  srcQ = p.resQ + (((int64_t)i * tiles_n + nt) * p.nkc + ks * kCrtKS) * kPanelB;
             unsigned char* base = smem + st * kStage;
@@ -675,7 +687,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 break;
             }
             int mt, nt;
-            oz_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, mt, nt);
+            crt_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, p.group_m, mt, nt);
             const int gr = mt * kOzBM + row;
             int       er = gr < p.M ? p.exp_rows[gr] : 0;
             if(er == kOzExpNone)

@@ -315,6 +315,7 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         p.ualpha_zero = g.zero_guard && !g.ualpha_dev && g.ualpha_host == 0.0;
         p.scratch = scratch;
         p.error = err_dev;
+        p.group_m = std::max(1, tuning().crt_group_m);
         const int kk = (int)std::max<int64_t>(kc, 1);
         switch(g.moduli)
         {
