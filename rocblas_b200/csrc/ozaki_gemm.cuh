@@ -2,9 +2,12 @@
 //
 //     C := beta * C + alpha * P * Q            (P: M x K, Q: K x N, C: M x N, FP64)
 //
-// Used by the precision form of the TRSM for the trailing updates of the blocked solve (the
-// refinement's FP64 residuals run on the DMMA tiles, gemm_dmma.cuh).  The reference computes these updates with FP64 GEMMs
-// (rocblas_internal_gemm -> Tensile, library/src/blas3/Tensile/gemm_templates.cpp:41-181).
+// Used for the trailing updates of the blocked solve: by the precision form of the dtrsm when
+// a slice count is asked for, or for updates with fewer output tiles than SMs (the residue
+// engine of crt_gemm.cuh takes the others), and by the FP32 trsm with FP32 operands and C (4
+// slices); the refinement's FP64 residuals run on the DMMA tiles, gemm_dmma.cuh.  The reference
+// computes these updates with FP64 / FP32 GEMMs (rocblas_internal_gemm -> Tensile,
+// library/src/blas3/Tensile/gemm_templates.cpp:41-181).
 //
 // Method (a multi-limb split in the style of Ozaki's error-free matrix product):
 //   * every row r of P is scaled by 2^-e_r (e_r = exponent of its largest entry) and cut into
