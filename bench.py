@@ -569,15 +569,18 @@ def bench_complex(torch, L, h, dev, fp64_peak, m=8192, n=2048, steps=5):
     return out
 
 
-def bench_serving(torch, dev, n_requests, rate, seed=7):
+def bench_serving(torch, dev, n_requests, rate, seed=7, payload_on_host=False):
     """The serving workload: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
     60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
-    budget.  The native server loop (rocblas_b200_server_run) serves the list; returns p50 /
-    p99 latency, solves/s over the server's own wall time, and its batching statistics."""
+    (120e9 bytes) budget.  The native server loop (rocblas_b200_server_run) serves the list;
+    returns p50 / p99 latency, solves/s over the server's own wall time, and its batching
+    statistics.  payload_on_host: each request's B and fresh A are read from pinned host memory
+    across PCIe by the server's gather launch, inside the measured latency."""
     from rocblas_b200 import serving
 
     rng = np.random.default_rng(seed)
-    srv = serving.TrsmServer(device=dev, hbm_budget=120 << 30, n_streams=2, window_us=200.0)
+    srv = serving.TrsmServer(device=dev, hbm_budget=120_000_000_000, n_streams=2, window_us=200.0,
+                             payload_on_host=payload_on_host)
     sizes = {}
     for key in range(256):
         m = int(round(np.exp(rng.uniform(np.log(64), np.log(8192)))))
@@ -597,7 +600,13 @@ def bench_serving(torch, dev, n_requests, rate, seed=7):
             "collections": st["collections"], "largest_collection": st["largest_collection"],
             "peak_arena_gb": st["peak_bytes"] / 1e9, "gpu_launches": st["kernel_launches"],
             "fp64_fraction": float(np.mean([q.dtype == "d" for q in reqs])),
-            "reuse_fraction": float(np.mean([q.a_key is not None for q in reqs]))}
+            "reuse_fraction": float(np.mean([q.a_key is not None for q in reqs])),
+            "budget_bytes": 120_000_000_000,
+            "payload": ("pinned host memory, read across PCIe by the gather launch inside each request's "
+                        "latency" if payload_on_host else "device pools (copied device to device)"),
+            "payload_bytes": int(sum(q.m * q.n * (8 if q.dtype == "d" else 4)
+                                     + (0 if q.a_key is not None else q.m * (q.m + 1) // 2 * (8 if q.dtype == "d" else 4))
+                                     for q in reqs))}
 
 
 ERROR_COLUMNS = 64  # right-hand sides per band checked against the extended-precision X*
@@ -888,6 +897,11 @@ def run_ours(args):
         extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
         extra["complex"] = bench_complex(torch, L, h, dev, peak)
         extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
+        # the same stream with its payloads arriving from pinned host memory, on a bounded
+        # sample of the requests (the fresh A matrices make the payload several MB per request
+        # on average; the total is in payload_bytes)
+        extra["serving_host_payload"] = bench_serving(torch, dev, max(1000, args.serving_requests // 10),
+                                                      50000.0, payload_on_host=True)
 
     if rank == 0:
         line = {

@@ -71,8 +71,8 @@ class Resident:
 
 
 class TrsmServer:
-    def __init__(self, device="cuda", hbm_budget=120 << 30, n_streams=2, window_us=200.0,
-                 max_batch=4096, keep_resident_copies=False):
+    def __init__(self, device="cuda", hbm_budget=120_000_000_000, n_streams=2, window_us=200.0,
+                 max_batch=4096, keep_resident_copies=False, payload_on_host=False):
         self.dev = torch.device(device)
         if self.dev.index is None:
             self.dev = torch.device("cuda", torch.cuda.current_device())
@@ -87,7 +87,10 @@ class TrsmServer:
         # request payloads are cut from fixed pools (a stand-in for data that arrives with the
         # request): B from U(-1,1) values; a fresh A is a principal submatrix of a lower
         # triangle built by the drop-in recipe (off-diagonals U(-1,1)/FRESH_MAX, diagonal
-        # 1.5 + U(-1,1)/FRESH_MAX), at an offset given by the request's seed
+        # 1.5 + U(-1,1)/FRESH_MAX), at an offset given by the request's seed.  With
+        # payload_on_host the pools are pinned host memory: the server's gather launch then
+        # reads each request's B and fresh A across PCIe (mapped host memory), inside the
+        # request's measured latency, as data arriving from the host would be.
         g = torch.Generator(device=self.dev)
         g.manual_seed(12345)
         self.pool = {"d": torch.rand((1 << 27) + 4096, generator=g, device=self.dev,
@@ -97,6 +100,10 @@ class TrsmServer:
         F *= 1.0 / FRESH_MAX
         F.diagonal().add_(1.5)
         self.fresh = {"d": F, "s": F.to(torch.float32)}  # (col, row) storage: column-major ld FRESH_MAX
+        self.payload_on_host = payload_on_host
+        if payload_on_host:
+            self.pool = {k: v.cpu().pin_memory() for k, v in self.pool.items()}
+            self.fresh = {k: v.cpu().pin_memory() for k, v in self.fresh.items()}
         torch.cuda.synchronize(self.dev)
 
     # ---- resident matrices ------------------------------------------------------------

@@ -77,3 +77,23 @@ def test_serving_rejects_bad_requests():
     with pytest.raises(serving.RocblasError):
         srv.run([q])
     srv.close()
+
+
+def test_serving_host_payloads_equal_device_payloads():
+    """Payloads read from pinned host memory across PCIe by the gather launch give the same
+    results, bit for bit, as the same payloads in device memory."""
+    reqs = _requests(120, 20000.0, 9)
+    dev_srv = _server()
+    dev_srv.run(reqs, keep_results=True)
+    ref = {q.rid: q.B.clone() for q in reqs}
+    dev_srv.close()
+    host_srv = serving.TrsmServer(hbm_budget=8 << 30, n_streams=2, window_us=100.0,
+                                  keep_resident_copies=True, payload_on_host=True)
+    for key, m in RESIDENT.items():
+        host_srv.add_resident(key, m, kband=key % 3 * 2, seed=10 + key)
+    assert not host_srv.pool["d"].is_cuda and host_srv.pool["d"].is_pinned()
+    lat = host_srv.run(reqs, keep_results=True)
+    assert np.all(lat > 0)
+    for q in reqs:
+        assert torch.equal(q.B, ref[q.rid]), (q.rid, q.m, q.n, q.dtype)
+    host_srv.close()
