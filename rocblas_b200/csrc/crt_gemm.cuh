@@ -182,12 +182,6 @@ __host__ __device__ constexpr uint32_t crt_recip20(int nm, int i)
     return (uint32_t)((((unsigned long long)crt_weight(nm, i) << 20) + crt_modulus(i) / 2) / crt_modulus(i));
 }
 
-// the largest symmetric residue kept as is (larger ones have p subtracted)
-__host__ __device__ constexpr uint32_t crt_half(int i)
-{
-    return crt_modulus(i) == 256u ? 127u : (crt_modulus(i) - 1) / 2;
-}
-
 __host__ __device__ constexpr bool crt_tables_ok(int nm)
 {
     for(int i = 0; i < nm; ++i)
@@ -316,19 +310,20 @@ __global__ void __launch_bounds__(256, 2)
     const int    se     = bits - e;
     const bool   direct = se <= 1023; // 2^se is a normal double (se >= bits - 1025 > -1022)
     const double scale  = direct ? __longlong_as_double((long long)(1023 + se) << 52) : 0.0;
-    uint32_t     fa[16], fm[16], fc[16];
-    uint32_t     negmask = 0;
+    // the signed integer Ws = +-trunc(|x| 2^se) as a 2^40 (signed) + m 2^20 + c (m, c in [0, 2^20))
+    int32_t  fa[16];
+    uint32_t fm[16], fc[16];
 #pragma unroll
     for(int j = 0; j < 16; ++j)
     {
         const double x = tile[oo][kq + j];
         // exact scaling; |w| < 2^bits <= 2^60
-        const double             w = direct ? x * scale : ldexp(x, se);
-        const unsigned long long W = __double2ull_rz(fabs(w));
-        fa[j] = (uint32_t)(W >> 40);
-        fm[j] = (uint32_t)(W >> 20) & 0xFFFFFu;
-        fc[j] = (uint32_t)W & 0xFFFFFu;
-        negmask |= (signbit(x) ? 1u : 0u) << j;
+        const double    w  = direct ? x * scale : ldexp(x, se);
+        const long long W  = (long long)__double2ull_rz(fabs(w));
+        const long long Ws = signbit(x) ? -W : W;
+        fa[j] = (int32_t)(Ws >> 40); // arithmetic shift: in [-2^20, 2^20)
+        fm[j] = (uint32_t)(Ws >> 20) & 0xFFFFFu;
+        fc[j] = (uint32_t)Ws & 0xFFFFFu;
     }
     const int     kc  = k / kCrtBK, c = (k % kCrtBK) / 16;
     const int64_t nkc = K_pad / kCrtBK;
@@ -338,19 +333,28 @@ __global__ void __launch_bounds__(256, 2)
     crt_static_for<0, NM>([&](auto I) {
         constexpr int      i    = decltype(I)::value;
         constexpr uint32_t p    = crt_modulus(i);
-        constexpr uint32_t k40  = (uint32_t)((1ull << 40) % p);
+        constexpr int32_t  k40  = (int32_t)((1ull << 40) % p);
         constexpr uint32_t k20  = (uint32_t)((1ull << 20) % p);
-        constexpr uint32_t half = crt_half(i);
-        uint32_t           words[4] = {0u, 0u, 0u, 0u};
+        // the symmetric residue of t is ((t + half) mod p) - half for half = (p - 1) / 2 (odd p)
+        // or 128 (p = 256); off (>= 2^28, a multiple of p) makes t + half non-negative
+        constexpr uint32_t half = p == 256u ? 128u : (p - 1) / 2;
+        constexpr uint32_t add  = p * ((1u << 28) / p + 1) + half;
+        uint32_t           r[16];
 #pragma unroll
         for(int j = 0; j < 16; ++j)
         {
-            const uint32_t t = fa[j] * k40 + fm[j] * k20 + fc[j]; // < 2^29
-            const uint32_t r = t % p;
-            int            s = r > half ? (int)r - (int)p : (int)r;
-            if((negmask >> j) & 1u)
-                s = -s; // -(-128) = 128 for p = 256: the same byte, the same residue
-            words[j >> 2] |= ((uint32_t)s & 0xFFu) << (8 * (j & 3));
+            // in [0, 2^30): |fa k40| < 2^28, fm k20 + fc < 2^28 + 2^20, add < 2^29
+            const uint32_t t = (uint32_t)(fa[j] * k40) + fm[j] * k20 + (fc[j] + add);
+            r[j] = t % p;
+        }
+        // bytes r_j - half, four to a word: pack, then one bytewise subtract (wraps mod 256)
+        uint32_t words[4];
+#pragma unroll
+        for(int q = 0; q < 4; ++q)
+        {
+            const uint32_t lo = __byte_perm(r[4 * q], r[4 * q + 1], 0x0040);
+            const uint32_t hi = __byte_perm(r[4 * q + 2], r[4 * q + 3], 0x0040);
+            words[q] = __vsub4(__byte_perm(lo, hi, 0x5410), half * 0x01010101u);
         }
         *reinterpret_cast<uint4*>(out + (int64_t)i * tiles * nkc * TR * kCrtBK)
             = make_uint4(words[0], words[1], words[2], words[3]);
