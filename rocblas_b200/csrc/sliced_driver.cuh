@@ -465,7 +465,10 @@ static bool sliced_trsm_update(const TrsmProblem<T>& q, int c_lo, int c_hi, int 
     g.S = S;
     // the residue engine's 128 x 256 tiles leave SMs idle on updates with fewer tiles than SMs
     // (the host-buffer path's 512-row block rows); the slice engine's 128 x 64 tiles do not
-    g.moduli = (int64_t)ceil_div(g.M, kOzBM) * ceil_div(g.N, kCrtBN) >= q.sm_count ? moduli : 0;
+    g.moduli = (int64_t)ceil_div(g.M, kOzBM) * ceil_div(g.N, kCrtBN) * 100
+                       >= (int64_t)q.sm_count * tuning().crt_min_tiles_pct
+                   ? moduli
+                   : 0;
     g.ldc = q.ldb;
     g.a = -1.0;
     g.b_imm = 1.0;

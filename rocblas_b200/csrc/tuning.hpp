@@ -44,6 +44,8 @@ struct Tuning
     int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
                                      // cycles (2^31: about a second), records error 4, returns
     int crt_group_m          = 8;    // residue GEMM tile order: row tiles per group
+    int crt_min_tiles_pct    = 100;  // precision form: residue engine for updates with at least
+                                     // SMs * pct / 100 output tiles of 128 x 256, else slices
     int strsm_slices         = 4;    // FP32 solve: slices of its trailing updates on the int8 slice
                                      // engine (0: FFMA tiles)
     int strsm_sliced_min_k   = 1024; // ... for updates with at least this inner dimension
@@ -84,6 +86,7 @@ static const TuningEntry kTuningEntries[] = {
     {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},
     {"strsm_slices", &Tuning::strsm_slices, 0, 8},
     {"crt_group_m", &Tuning::crt_group_m, 1, 1024},
+    {"crt_min_tiles_pct", &Tuning::crt_min_tiles_pct, 0, 100000},
     {"strsm_sliced_min_k", &Tuning::strsm_sliced_min_k, 64, 1 << 30},
 };
 
