@@ -569,6 +569,40 @@ def bench_complex(torch, L, h, dev, fp64_peak, m=8192, n=2048, steps=5):
     return out
 
 
+def bench_trsv(torch, L, h, dev, hbm_gbs):
+    """rocblas_?trsv of one vector (the memory-bound flag-synchronised solve) at n = 4096 ..
+    32768, lower, no-trans: median of 7 event-timed calls, reported as GB/s of A's triangle
+    (n (n + 1) / 2 elements, the solve's algorithmic bytes) and as a fraction of the measured
+    HBM copy bandwidth."""
+    import rocblas_b200 as rb
+    from rocblas_b200 import workloads
+
+    rb_fill_lower, rb_op_none, rb_diag_non_unit = rb.fill_lower, rb.operation_none, rb.diagonal_non_unit
+    out = {}
+    for dt, tdt, es, fn in (("d", torch.float64, 8, L.rocblas_dtrsv), ("s", torch.float32, 4, L.rocblas_strsv)):
+        for n in (4096, 16384, 32768):
+            At, x0 = workloads.condition_band_lower_torch(n, 1, 0, seed=3, device=dev, dtype=tdt)
+            x = x0.clone()
+            args = (h.value, rb_fill_lower, rb_op_none, rb_diag_non_unit, n, ctypes.c_void_p(At.data_ptr()), n,
+                    ctypes.c_void_p(x.data_ptr()), 1)
+            ts = []
+            for it in range(9):
+                x.copy_(x0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                st = fn(*args)
+                e1.record()
+                e1.synchronize()
+                assert st == 0, st
+                if it >= 2:
+                    ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            gbs = n * (n + 1) / 2 * es / (ms * 1e-3) / 1e9
+            out[f"{dt}trsv_{n}"] = {"us": ms * 1e3, "GBps": gbs, "hbm_frac": gbs / hbm_gbs}
+            del At, x0, x
+    return out
+
+
 def bench_serving(torch, dev, n_requests, rate, seed=7, payload_on_host=False):
     """The serving workload: Poisson arrivals, m log-uniform [64, 8192], n log-uniform [1, 512], 70% FP64,
     60% of requests on one of 256 resident A (condition-band recipe, k in {0, 2, 4}), 120 GB
@@ -896,6 +930,7 @@ def run_ours(args):
         extra["sweep"] = bench_sweep(torch, rb, L, h, dev)
         extra["batched"] = bench_batched(torch, rb, L, h, dev, hbm)
         extra["complex"] = bench_complex(torch, L, h, dev, peak)
+        extra["trsv"] = bench_trsv(torch, L, h, dev, hbm)
         extra["serving"] = bench_serving(torch, dev, args.serving_requests, 50000.0)
         # the same stream with its payloads arriving from pinned host memory, on a bounded
         # sample of the requests (the fresh A matrices make the payload several MB per request

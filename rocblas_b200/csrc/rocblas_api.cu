@@ -20,6 +20,7 @@
 #include "layer_log.hpp"
 #include "refine.cuh"
 #include "sliced_driver.cuh"
+#include "trsv_flag.cuh"
 #include "trsm_driver.cuh"
 #include "server.cuh"
 #include "vbatched.cuh"
@@ -517,6 +518,59 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
     rocblas_status ast = trsv_arg_check(h, uplo, trans, diag, n, Aptr, lda, xptr, incx, batch);
     if(ast != rocblas_status_continue)
         return ast;
+    // one real vector with a positive increment: the memory-bound flag-synchronised solve
+    if constexpr(!is_cplx<T>::value)
+    {
+        if(batch == 1 && incx > 0 && n >= tuning().trsv_flag_min_n)
+        {
+            const int    nblk  = (int)ceil_div(n, kTvNB);
+            const size_t bytes = (size_t)nblk * sizeof(int);
+            if(h->size_query)
+                return h->set_optimal_size(bytes);
+            rocblas_status st;
+            if((st = device_ready(h)) != rocblas_status_success)
+                return st;
+            int*  err = ensure_err(h);
+            void* ws  = h->borrow(bytes);
+            if(err && ws)
+            {
+                cudaMemsetAsync(ws, 0, bytes, h->stream);
+                TrsvParams<T> p{};
+                p.A     = A.base + A.offset;
+                p.lda   = lda;
+                p.x     = x.base + x.offset;
+                p.incx  = incx;
+                p.n     = n;
+                const bool lower = uplo == rocblas_fill_lower;
+                p.trans = trans != rocblas_operation_none;
+                p.rev   = lower == p.trans; // op(A) upper: the solve starts at the last row
+                p.unit  = diag == rocblas_diagonal_unit;
+                p.flags = reinterpret_cast<int*>(ws);
+                p.error = err;
+                p.wait_cycles = 1ll << tuning().wait_cycles_log2;
+                constexpr size_t smem = trsv_flag_smem_bytes<T>();
+                static int per_sm = 0;
+                if(!per_sm)
+                {
+                    cudaFuncSetAttribute((const void*)trsv_flag_kernel<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flag_kernel<T>, kTvThreads, smem)
+                           != cudaSuccess
+                       || per_sm < 1)
+                    {
+                        cudaGetLastError();
+                        per_sm = 1;
+                    }
+                }
+                // persistent: every CTA resident at once, so that no block waits on one not started
+                const int grid = std::min(nblk, h->sm_count * per_sm);
+                trsv_flag_kernel<T><<<grid, kTvThreads, smem, h->stream>>>(p);
+                count_launch();
+                return launch_status();
+            }
+            // no workspace: the blocked path below needs none
+        }
+    }
     // op(A) x = b is x^T op(A)^T = b^T: op(A)^T is A^T for N, A for T, conj(A) for C
     const rocblas_operation flip
         = trans == rocblas_operation_none ? rocblas_operation_transpose : rocblas_operation_none;
