@@ -507,6 +507,29 @@ inline rocblas_status trsv_arg_check(rocblas_handle h, rocblas_fill uplo, rocbla
     return rocblas_status_continue;
 }
 
+// The flag-synchronised single-vector solve (trsv_flag.cuh): a persistent grid, every CTA
+// resident at once, so that no block waits on one that has not started.
+template <typename T, int NB>
+void launch_trsv_flag(const TrsvParams<T>& p, int nblk, int sms, cudaStream_t s)
+{
+    constexpr size_t smem = trsv_flag_smem_bytes<T, NB>();
+    static int per_sm = 0;
+    if(!per_sm)
+    {
+        cudaFuncSetAttribute((const void*)trsv_flag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flag_kernel<T, NB>, kTvThreads, smem)
+               != cudaSuccess
+           || per_sm < 1)
+        {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+    }
+    const int grid = std::min(nblk, sms * per_sm);
+    trsv_flag_kernel<T, NB><<<grid, kTvThreads, smem, s>>>(p);
+}
+
 template <typename T>
 rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation trans,
                          rocblas_diagonal diag, int n, const void* Aptr, BatchPtr<T> A, int64_t lda,
@@ -523,7 +546,8 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
     {
         if(batch == 1 && incx > 0 && n >= tuning().trsv_flag_min_n)
         {
-            const int    nblk  = (int)ceil_div(n, kTvNB);
+            const int    NB    = tuning().trsv_flag_nb == 128 ? 128 : 64;
+            const int    nblk  = (int)ceil_div(n, NB);
             const size_t bytes = (size_t)nblk * sizeof(int);
             if(h->size_query)
                 return h->set_optimal_size(bytes);
@@ -548,23 +572,10 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
                 p.flags = reinterpret_cast<int*>(ws);
                 p.error = err;
                 p.wait_cycles = 1ll << tuning().wait_cycles_log2;
-                constexpr size_t smem = trsv_flag_smem_bytes<T>();
-                static int per_sm = 0;
-                if(!per_sm)
-                {
-                    cudaFuncSetAttribute((const void*)trsv_flag_kernel<T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flag_kernel<T>, kTvThreads, smem)
-                           != cudaSuccess
-                       || per_sm < 1)
-                    {
-                        cudaGetLastError();
-                        per_sm = 1;
-                    }
-                }
-                // persistent: every CTA resident at once, so that no block waits on one not started
-                const int grid = std::min(nblk, h->sm_count * per_sm);
-                trsv_flag_kernel<T><<<grid, kTvThreads, smem, h->stream>>>(p);
+                if(NB == 128)
+                    launch_trsv_flag<T, 128>(p, nblk, h->sm_count, h->stream);
+                else
+                    launch_trsv_flag<T, 64>(p, nblk, h->sm_count, h->stream);
                 count_launch();
                 return launch_status();
             }

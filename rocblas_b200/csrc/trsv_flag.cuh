@@ -29,7 +29,7 @@
 namespace rb200
 {
 
-constexpr int kTvNB      = 64;  // rows per block
+constexpr int kTvNB      = 64;  // rows per 64-row block (the inverse is built from blocks of this)
 constexpr int kTvThreads = 256; // 8 warps
 constexpr int kTvWarps   = kTvThreads / 32;
 
@@ -79,139 +79,210 @@ __device__ __forceinline__ bool tv_wait_flag(const int* flag, long long limit)
     }
 }
 
-template <typename T>
+// Dynamic shared memory of the NB-row kernel: the diagonal block (NB x NB + 1; for NB = 128 its
+// inverse in place) and 64 x 65 scratch blocks for the inverses of its 64-row halves (one for
+// NB = 64, where it holds the inverse, two for NB = 128).
+template <typename T, int NB>
 constexpr size_t trsv_flag_smem_bytes()
 {
-    return 2 * sizeof(T) * kTvNB * (kTvNB + 1);
+    return sizeof(T) * ((size_t)NB * (NB + 1) + (NB / kTvNB) * kTvNB * (kTvNB + 1));
 }
 
+// inverse of the lower-triangular 64 x 64 block S (stride ls) into D (stride ld), zero above the
+// diagonal: thread c < 64 of the calling group solves S z = e_c by forward substitution
 template <typename T>
+__device__ __forceinline__ void tv_invert64(const T* S, int ls, T* D, int ld, int c)
+{
+    for(int r = 0; r < c; ++r)
+        D[r * ld + c] = T(0);
+    D[c * ld + c] = T(1) / S[c * ls + c];
+    for(int r = c + 1; r < kTvNB; ++r)
+    {
+        T acc = T(0);
+        for(int k = c; k < r; ++k)
+            acc += S[r * ls + k] * D[k * ld + c];
+        D[r * ld + c] = -acc / S[r * ls + r];
+    }
+}
+
+template <typename T, int NB>
 __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<T> p)
 {
-    // the diagonal block and its inverse in dynamic shared memory (trsv_flag_smem_bytes)
+    static_assert(NB == 64 || NB == 128, "block rows");
+    constexpr int RPL = NB / 32;          // no-trans: rows per lane
+    constexpr int CPW = kTvNB / kTvWarps; // columns per warp in a 64-column half tile
+    constexpr int RPW = NB / kTvWarps;    // trans: rows per warp
+    constexpr int LD  = NB + 1;
     extern __shared__ __align__(16) unsigned char tv_smem[];
-    T(*diag)[kTvNB + 1] = reinterpret_cast<T(*)[kTvNB + 1]>(tv_smem);
-    T(*inv)[kTvNB + 1]  = reinterpret_cast<T(*)[kTvNB + 1]>(tv_smem + sizeof(T) * kTvNB * (kTvNB + 1));
-    __shared__ T   part[kTvWarps][kTvNB];
-    __shared__ T   ysh[kTvNB];
+    T* dg = reinterpret_cast<T*>(tv_smem); // diagonal block, then its inverse in place
+    T* s1 = dg + NB * LD;                  // NB = 128: inverses of the two 64-row halves
+    T* s2 = s1 + kTvNB * (kTvNB + 1);
+    __shared__ T   part[kTvWarps][NB];
+    __shared__ T   ysh[NB];
     __shared__ int stop;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nblk = (p.n + kTvNB - 1) / kTvNB;
+    const int nblk = (p.n + NB - 1) / NB;
     if(threadIdx.x == 0)
         stop = 0;
     __syncthreads();
     for(int b = blockIdx.x; b < nblk; b += gridDim.x)
     {
-        const int r0 = b * kTvNB, rows = min(kTvNB, p.n - r0);
+        const int r0 = b * NB, rows = min(NB, p.n - r0);
         // the diagonal block, staged before any wait (zero outside the triangle; rows past the
-        // matrix get a unit diagonal so that the inverse below stays finite)
-        for(int e = threadIdx.x; e < kTvNB * kTvNB; e += kTvThreads)
+        // matrix get a unit diagonal so that the inverse stays finite)
+        for(int e = threadIdx.x; e < NB * NB; e += kTvThreads)
         {
-            const int rr = e % kTvNB, cc = e / kTvNB;
+            const int rr = e % NB, cc = e / NB;
             T v = (rr < rows && cc <= rr) ? tv_load(p, r0 + rr, r0 + cc) : T(0);
             if(rr == cc && (p.unit || rr >= rows))
                 v = T(1);
-            diag[rr][cc] = v;
-        }
-        __syncthreads();
-        // its inverse, also before any wait (the wait on the block before is the critical path,
-        // and after it only a product with the inverse remains): thread c < 64 solves
-        // diag z = e_c by forward substitution (column c of the inverse; zero above the diagonal)
-        if(threadIdx.x < kTvNB)
-        {
-            const int c = threadIdx.x;
-            for(int r = 0; r < c; ++r)
-                inv[r][c] = T(0);
-            const T zc = T(1) / diag[c][c];
-            inv[c][c]  = zc;
-            for(int r = c + 1; r < kTvNB; ++r)
-            {
-                T s = T(0);
-                for(int k = c; k < r; ++k)
-                    s += diag[r][k] * inv[k][c];
-                inv[r][c] = -s / diag[r][r];
-            }
+            dg[rr * LD + cc] = v;
         }
         // this block's right-hand side, read before any wait (no other block writes it)
         const T xb = threadIdx.x < rows ? *tv_x(p, r0 + threadIdx.x) : T(0);
-        // the tiles j < b: no-trans maps lanes to rows (2 each, columns warp, warp + 8, ..),
-        // trans maps lanes to columns (2 each) and warps to rows (8 each)
-        T    acc[8];
+        __syncthreads();
+        // its inverse, also before any wait: after the wait on the block before (the critical
+        // path) only a product with it remains
+        if constexpr(NB == 64)
+        {
+            if(threadIdx.x < kTvNB)
+                tv_invert64(dg, LD, s1, kTvNB + 1, threadIdx.x);
+        }
+        else
+        {
+            // [[L11, 0], [L21, L22]]^-1 = [[I11, 0], [-I22 L21 I11, I22]] with I = inverses of the
+            // 64-row halves: threads 0..63 invert L11 into s1, threads 64..127 L22 into s2
+            if(threadIdx.x < kTvNB)
+                tv_invert64(dg, LD, s1, kTvNB + 1, threadIdx.x);
+            else if(threadIdx.x < 2 * kTvNB)
+                tv_invert64(dg + kTvNB * LD + kTvNB, LD, s2, kTvNB + 1, threadIdx.x - kTvNB);
+            __syncthreads();
+            // W = L21 I11 (64 x 64, 16 entries per thread), written over L21
+            T w[16];
 #pragma unroll
-        for(int q = 0; q < 8; ++q)
+            for(int q = 0; q < 16; ++q)
+            {
+                const int e = threadIdx.x + q * kTvThreads, rr = e % kTvNB, cc = e / kTvNB;
+                T         acc = T(0);
+                for(int k = cc; k < kTvNB; ++k)
+                    acc += dg[(kTvNB + rr) * LD + k] * s1[k * (kTvNB + 1) + cc];
+                w[q] = acc;
+            }
+            __syncthreads();
+#pragma unroll
+            for(int q = 0; q < 16; ++q)
+            {
+                const int e = threadIdx.x + q * kTvThreads, rr = e % kTvNB, cc = e / kTvNB;
+                dg[(kTvNB + rr) * LD + cc] = w[q];
+            }
+            __syncthreads();
+            // -I22 W over the lower-left block, then the half inverses on the diagonal
+#pragma unroll
+            for(int q = 0; q < 16; ++q)
+            {
+                const int e = threadIdx.x + q * kTvThreads, rr = e % kTvNB, cc = e / kTvNB;
+                T         acc = T(0);
+                for(int k = 0; k <= rr; ++k)
+                    acc += s2[rr * (kTvNB + 1) + k] * dg[(kTvNB + k) * LD + cc];
+                w[q] = -acc;
+            }
+            __syncthreads();
+#pragma unroll
+            for(int q = 0; q < 16; ++q)
+            {
+                const int e = threadIdx.x + q * kTvThreads, rr = e % kTvNB, cc = e / kTvNB;
+                dg[(kTvNB + rr) * LD + cc] = w[q];
+                dg[rr * LD + cc]                   = s1[rr * (kTvNB + 1) + cc];
+                dg[(kTvNB + rr) * LD + kTvNB + cc] = s2[rr * (kTvNB + 1) + cc];
+                dg[rr * LD + kTvNB + cc]           = T(0);
+            }
+        }
+        // the tiles j < b, in 64-column halves: no-trans maps lanes to rows (RPL each) and warps
+        // to columns (8 of each half), trans maps lanes to columns (2 of each half) and warps to
+        // rows (RPW each)
+        T    acc[RPL > RPW ? RPL : RPW];
+#pragma unroll
+        for(int q = 0; q < (RPL > RPW ? RPL : RPW); ++q)
             acc[q] = T(0);
         bool ok = true;
         for(int j = 0; j < b && ok; ++j)
         {
-            const int c0 = j * kTvNB; // a full block: j < b
-            T         a[16];
-            if(!p.trans)
+            for(int hf = 0; hf < NB / kTvNB; ++hf)
             {
-#pragma unroll
-                for(int q = 0; q < 8; ++q)
+                const int c0 = j * NB + hf * kTvNB; // a full block: j < b
+                constexpr int kAv = RPL * CPW > 2 * RPW ? RPL * CPW : 2 * RPW;
+                T             av[kAv];
+                if(!p.trans)
                 {
-                    const int cc = c0 + warp + q * kTvWarps;
-                    a[2 * q]     = lane < rows ? tv_load(p, r0 + lane, cc) : T(0);
-                    a[2 * q + 1] = lane + 32 < rows ? tv_load(p, r0 + lane + 32, cc) : T(0);
-                }
-            }
-            else
-            {
 #pragma unroll
-                for(int q = 0; q < 8; ++q)
+                    for(int q = 0; q < CPW; ++q)
+#pragma unroll
+                        for(int t = 0; t < RPL; ++t)
+                        {
+                            const int rr = lane + 32 * t;
+                            av[q * RPL + t] = rr < rows ? tv_load(p, r0 + rr, c0 + warp + q * kTvWarps) : T(0);
+                        }
+                }
+                else
                 {
-                    const int rr = warp + q * kTvWarps;
-                    a[2 * q]     = rr < rows ? tv_load(p, r0 + rr, c0 + lane) : T(0);
-                    a[2 * q + 1] = rr < rows ? tv_load(p, r0 + rr, c0 + lane + 32) : T(0);
-                }
-            }
-            // x_j is final once block j's flag is set
-            int bad = 0;
-            if(lane == 0)
-                bad = (*(volatile int*)&stop) || !tv_wait_flag(p.flags + j, p.wait_cycles);
-            bad = __shfl_sync(0xffffffffu, bad, 0);
-            __syncwarp(); // lane 0's acquire orders the whole warp's reads of x_j below
-            if(bad)
-            {
-                ok = false;
-                break;
-            }
-            if(!p.trans)
-            {
 #pragma unroll
-                for(int q = 0; q < 8; ++q)
+                    for(int q = 0; q < RPW; ++q)
+                    {
+                        const int rr = warp + q * kTvWarps;
+                        av[2 * q]     = rr < rows ? tv_load(p, r0 + rr, c0 + lane) : T(0);
+                        av[2 * q + 1] = rr < rows ? tv_load(p, r0 + rr, c0 + lane + 32) : T(0);
+                    }
+                }
+                if(hf == 0)
                 {
-                    const T xv = __ldcg(tv_x(p, c0 + warp + q * kTvWarps));
-                    acc[0] += a[2 * q] * xv;
-                    acc[1] += a[2 * q + 1] * xv;
+                    // x_j is final once block j's flag is set
+                    int bad = 0;
+                    if(lane == 0)
+                        bad = (*(volatile int*)&stop) || !tv_wait_flag(p.flags + j, p.wait_cycles);
+                    bad = __shfl_sync(0xffffffffu, bad, 0);
+                    __syncwarp(); // lane 0's acquire orders the whole warp's reads of x_j below
+                    if(bad)
+                    {
+                        ok = false;
+                        break;
+                    }
                 }
-            }
-            else
-            {
-                const T x0 = __ldcg(tv_x(p, c0 + lane)), x1 = __ldcg(tv_x(p, c0 + lane + 32));
+                if(!p.trans)
+                {
 #pragma unroll
-                for(int q = 0; q < 8; ++q)
-                    acc[q] += a[2 * q] * x0 + a[2 * q + 1] * x1;
+                    for(int q = 0; q < CPW; ++q)
+                    {
+                        const T xv = __ldcg(tv_x(p, c0 + warp + q * kTvWarps));
+#pragma unroll
+                        for(int t = 0; t < RPL; ++t)
+                            acc[t] += av[q * RPL + t] * xv;
+                    }
+                }
+                else
+                {
+                    const T x0 = __ldcg(tv_x(p, c0 + lane)), x1 = __ldcg(tv_x(p, c0 + lane + 32));
+#pragma unroll
+                    for(int q = 0; q < RPW; ++q)
+                        acc[q] += av[2 * q] * x0 + av[2 * q + 1] * x1;
+                }
             }
         }
-        if(!ok)
+        if(!ok && lane == 0)
         {
-            if(lane == 0)
-            {
-                atomicCAS(p.error, 0, 5);
-                atomicExch(&stop, 1);
-            }
+            atomicCAS(p.error, 0, 5);
+            atomicExch(&stop, 1);
         }
         // partial sums of the 8 warps into part[warp][row]
         if(!p.trans)
         {
-            part[warp][lane]      = acc[0];
-            part[warp][lane + 32] = acc[1];
+#pragma unroll
+            for(int t = 0; t < RPL; ++t)
+                part[warp][lane + 32 * t] = acc[t];
         }
         else
         {
 #pragma unroll
-            for(int q = 0; q < 8; ++q)
+            for(int q = 0; q < RPW; ++q)
             {
                 T v = acc[q];
 #pragma unroll
@@ -229,28 +300,31 @@ __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<
         __syncthreads();
         if(*(volatile int*)&stop)
             break;
-        // y = b - sum, then x_b = inv y, by the first 64 threads (named barrier 1 between them:
-        // the other warps go on to stage the CTA's next block once the barrier below lets them)
-        if(threadIdx.x < kTvNB)
+        // y = b - sum, then x_b = inv y, by the first NB threads (named barrier 1 between them;
+        // the other warps wait at the CTA barrier below before the next block reuses the buffers)
+        if(threadIdx.x < NB)
         {
             const int rr = threadIdx.x;
-            T         s  = T(0);
+            T         sum = T(0);
 #pragma unroll
             for(int w = 0; w < kTvWarps; ++w)
-                s += part[w][rr];
-            ysh[rr] = xb - s;
-            asm volatile("bar.sync 1, %0;" ::"n"(kTvNB) : "memory");
+                sum += part[w][rr];
+            ysh[rr] = xb - sum;
+            asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
+            // the inverse: s1 (stride 65) for NB = 64, the block itself for NB = 128
+            const T* inv = NB == 64 ? s1 : dg;
+            const int li = NB == 64 ? kTvNB + 1 : LD;
             T v = T(0);
             for(int cc = 0; cc <= rr; ++cc)
-                v += inv[rr][cc] * ysh[cc];
+                v += inv[rr * li + cc] * ysh[cc];
             if(rr < rows)
                 *tv_x(p, r0 + rr) = v;
             __threadfence();
-            asm volatile("bar.sync 1, %0;" ::"n"(kTvNB) : "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
             if(rr == 0)
                 asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p.flags + b), "r"(1) : "memory");
         }
-        __syncthreads(); // diag and part are reused by the CTA's next block
+        __syncthreads(); // the buffers are reused by the CTA's next block
     }
 }
 

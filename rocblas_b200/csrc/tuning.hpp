@@ -45,6 +45,7 @@ struct Tuning
                                      // cycles (2^31: about a second), records error 4, returns
     int trsv_flag_min_n      = 256;  // trsv of one real vector: the flag-synchronised solve from
                                      // this order up
+    int trsv_flag_nb         = 128;  // ... its block rows (64 or 128)
     int crt_group_m          = 8;    // residue GEMM tile order: row tiles per group
     int crt_min_tiles_pct    = 100;  // precision form: residue engine for updates with at least
                                      // SMs * pct / 100 output tiles of 128 x 256, else slices
@@ -89,6 +90,7 @@ static const TuningEntry kTuningEntries[] = {
     {"strsm_slices", &Tuning::strsm_slices, 0, 8},
     {"crt_group_m", &Tuning::crt_group_m, 1, 1024},
     {"trsv_flag_min_n", &Tuning::trsv_flag_min_n, 1, 1 << 30},
+    {"trsv_flag_nb", &Tuning::trsv_flag_nb, 64, 128},
     {"crt_min_tiles_pct", &Tuning::crt_min_tiles_pct, 0, 100000},
     {"strsm_sliced_min_k", &Tuning::strsm_sliced_min_k, 64, 1 << 30},
 };

@@ -1,8 +1,9 @@
 """The memory-bound single-vector solve (rocblas_?trsv with one vector and a positive increment,
 order >= trsv_flag_min_n): flag-synchronised row blocks of 64 over a persistent grid.
 
-* every uplo / transA / diag combination, FP64 and FP32, orders that are and are not
-  multiples of the block, increments 1 and 3, against the oracle at the rocblas-test gate;
+* every uplo / transA / diag combination, FP64 and FP32, blocks of 64 and 128 rows, orders that
+  are and are not multiples of the block, increments 1 and 3, against the oracle at the
+  rocblas-test gate;
 * the same solve through the blocked trsm path (trsv_flag_min_n above the order) agrees;
 * a large order against a GPU residual, and bitwise repeatability.
 """
@@ -60,11 +61,12 @@ def _trsv(h, dt, uplo, trans, diag, n, A, b, incx):
     return out[0:(n - 1) * incx + 1:incx].copy()
 
 
+@pytest.mark.parametrize("nb", [64, 128])
 @pytest.mark.parametrize("dt", ["d", "s"])
 @pytest.mark.parametrize("uplo,trans,diag", COMBOS)
-def test_trsv_flag_combos(dt, uplo, trans, diag):
+def test_trsv_flag_combos(dt, uplo, trans, diag, nb):
     npdt, _ = DT[dt]
-    with rb.Handle() as h:
+    with rb.Handle() as h, tuning(trsv_flag_nb=nb):
         for i, (n, incx) in enumerate([(256, 1), (1000, 3), (4097, 1)]):
             A, B = oracle.nan_triangle_problem(900 + i, "L", uplo, trans, diag, n, 1, n + 2, n, npdt)
             b = B[:, 0].copy()
