@@ -979,7 +979,8 @@ def run_case(args):
     with --moduli moduli; dmma: rocblas_b200_dgemm m x n x k;
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
     m x n (the chain solve); strsm: rocblas_strsm L/L/N/N m x n (FP32: the recursive solve with
-    FFMA tile updates above 512 columns); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
+    FFMA tile updates above 512 columns); trsv: rocblas_dtrsv lower, no-trans, order m (the flag
+    solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
     variable-size batch recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
     trtri: rocblas_dtrtri_strided_batched, --count lower m x m blocks."""
     import torch
@@ -1013,6 +1014,13 @@ def run_case(args):
             st = L.rocblas_strsm(h.value, rb.side_left, rb.fill_lower, rb.operation_none,
                                  rb.diagonal_non_unit, m, n, ctypes.cast(ctypes.byref(one_f), ctypes.c_void_p),
                                  ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(Bt.data_ptr()), m)
+            assert st == 0, st
+    elif args.case == "trsv":
+        At, xt = workloads.condition_band_lower_torch(m, 1, 0, seed=5, device=dev)
+
+        def run():
+            st = L.rocblas_dtrsv(h.value, rb.fill_lower, rb.operation_none, rb.diagonal_non_unit, m,
+                                 ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(xt.data_ptr()), 1)
             assert st == 0, st
     elif args.case == "vbatched":
         w = vbatched_workload(torch, dev, args.count, 2024, "d")
@@ -1102,8 +1110,8 @@ def main():
     ap.add_argument("--check-columns", type=int, default=0,
                     help="right-hand sides the refined form's test uses (0: its default, 8)")
     ap.add_argument("--moduli", type=int, default=16, help="moduli of a --case crt GEMM")
-    ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "vbatched", "strided",
-                                       "trtri"],
+    ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "trsv", "vbatched",
+                                       "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,
