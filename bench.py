@@ -980,7 +980,8 @@ def run_case(args):
     zgemm: rocblas_b200_zgemm m x n x k (the complex DMMA tiles); chain: rocblas_dtrsm L/L/N/N
     m x n (the chain solve); strsm: rocblas_strsm L/L/N/N m x n (FP32: the recursive solve with
     FFMA tile updates above 512 columns); trsv: rocblas_dtrsv lower, no-trans, order m (the flag
-    solve); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
+    solve); serving: the serving loop over --count requests (m up to 2048, 16 resident A; its
+    gather launch, variable-size batched solves and their chain solves); vbatched: rocblas_b200_dtrsm_vbatched over --count systems of the
     variable-size batch recipe; strided: rocblas_dtrsm_strided_batched, --count systems of m x n (L/L/N/N);
     trtri: rocblas_dtrtri_strided_batched, --count lower m x m blocks."""
     import torch
@@ -990,6 +991,9 @@ def run_case(args):
 
     rb.build()
     L = rb.lib()
+    for kv in args.tuning:
+        key, val = kv.split("=")
+        assert L.rocblas_b200_set_tuning(key.encode(), int(val)) == 0, kv
     h = rb.Handle()
     dev = torch.device("cuda", 0)
     m, n, k = args.m, args.n, args.k
@@ -1022,6 +1026,19 @@ def run_case(args):
             st = L.rocblas_dtrsv(h.value, rb.fill_lower, rb.operation_none, rb.diagonal_non_unit, m,
                                  ctypes.c_void_p(At.data_ptr()), m, ctypes.c_void_p(xt.data_ptr()), 1)
             assert st == 0, st
+    elif args.case == "serving":
+        from rocblas_b200 import serving
+
+        rng = np.random.default_rng(7)
+        srv = serving.TrsmServer(device=dev, hbm_budget=8 << 30, n_streams=2, window_us=200.0)
+        sizes = {}
+        for key in range(16):
+            sizes[key] = int(round(np.exp(rng.uniform(np.log(64), np.log(2048)))))
+            srv.add_resident(key, sizes[key], kband=0, seed=1000 + key)
+        reqs = serving.make_requests(args.count, 50000.0, 7, sizes, m_range=(64, 2048))
+
+        def run():
+            srv.run(reqs)
     elif args.case == "vbatched":
         w = vbatched_workload(torch, dev, args.count, 2024, "d")
         one_d = ctypes.c_double(1.0)
@@ -1110,8 +1127,10 @@ def main():
     ap.add_argument("--check-columns", type=int, default=0,
                     help="right-hand sides the refined form's test uses (0: its default, 8)")
     ap.add_argument("--moduli", type=int, default=16, help="moduli of a --case crt GEMM")
-    ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "trsv", "vbatched",
-                                       "strided", "trtri"],
+    ap.add_argument("--tuning", action="append", default=[],
+                    help="key=value tuning-table entry for a --case run (repeatable)")
+    ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "trsv", "serving",
+                                       "vbatched", "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")
     ap.add_argument("--k", type=int, default=4096, help="inner dimension of a --case GEMM")
     ap.add_argument("--count", type=int, default=4000,
