@@ -687,6 +687,13 @@ def band_errors(torch, dev, Ab, Bb, solve_plain, solve_refined, threads):
     }
 
 
+def apply_tuning(L, args):
+    """The --tuning key=value entries, set in the library's tuning table before any call."""
+    for kv in args.tuning:
+        key, val = kv.split("=")
+        assert L.rocblas_b200_set_tuning(key.encode(), int(val)) == 0, kv
+
+
 def run_ours(args):
     import torch
 
@@ -706,6 +713,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     rb.build()
     L = rb.lib()
+    apply_tuning(L, args)
     S = args.slices
 
     At, B0 = workloads.condition_band_lower_torch(M, N, 0, seed=1234 + rank, device=dev)
@@ -991,9 +999,7 @@ def run_case(args):
 
     rb.build()
     L = rb.lib()
-    for kv in args.tuning:
-        key, val = kv.split("=")
-        assert L.rocblas_b200_set_tuning(key.encode(), int(val)) == 0, kv
+    apply_tuning(L, args)
     h = rb.Handle()
     dev = torch.device("cuda", 0)
     m, n, k = args.m, args.n, args.k
@@ -1128,7 +1134,7 @@ def main():
                     help="right-hand sides the refined form's test uses (0: its default, 8)")
     ap.add_argument("--moduli", type=int, default=16, help="moduli of a --case crt GEMM")
     ap.add_argument("--tuning", action="append", default=[],
-                    help="key=value tuning-table entry for a --case run (repeatable)")
+                    help="key=value tuning-table entry set before the run (repeatable)")
     ap.add_argument("--case", choices=["sliced", "crt", "dmma", "zgemm", "chain", "strsm", "trsv", "serving",
                                        "vbatched", "strided", "trtri"],
                     help="run one kernel on one shape (--m --n --k), --steps times, for ncu captures")

@@ -42,6 +42,8 @@
 // Every mbarrier wait is bounded; on timeout the kernel records the error, drains its in-flight
 // copies and MMAs (again bounded), frees TMEM and returns.
 #pragma once
+#include <cuda.h> // CUtensorMap (the maps are encoded through the runtime's driver entry point)
+
 #include <algorithm>
 #include <cstdint>
 #include <type_traits>
@@ -364,11 +366,12 @@ __global__ void __launch_bounds__(256, 2)
 // ---- GEMM over the residues ------------------------------------------------------------------
 struct CrtParams
 {
+    CUtensorMap   mapP, mapQ;    // CTA-pair form: the residue arrays as 2-D byte arrays [rows][64]
     int           M, N, K;       // logical sizes (K <= kCrtKMax)
-    int           M_pad, N_pad;  // residue-panel rows (multiples of 128 and 256)
+    int           M_pad, N_pad;  // residue-panel rows (multiples of 128 (pair: 256) and 256)
     int           nkc;           // 64-deep K panels per modulus (a multiple of kCrtKS)
     const int8_t* resP;          // [NM][M_pad / 128][nkc][128][64], swizzled rows
-    const int8_t* resQ;          // [NM][N_pad / 256][nkc][256][64]
+    const int8_t* resQ;          // [NM][N_pad / 256][nkc][256][64] (pair: [NM][N_pad / 128][nkc][128][64])
     const int*    exp_rows;      // e_r, M entries
     const int*    exp_cols;      // f_c, N entries
     int           shift;         // 2b: P Q ~= 2^(e_r + f_c - shift) X
@@ -402,6 +405,108 @@ __device__ __forceinline__ void crt_fail(int* error, int* abort_flag, int code)
     if(!*(volatile int*)abort_flag)
         atomicCAS(error, 0, code);
     atomicExch(abort_flag, 1);
+}
+
+// ---- CTA-pair (cta_group::2) helpers -------------------------------------------------------
+__device__ __forceinline__ uint32_t crt_cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t crt_peer_addr(const void* ptr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(ptr)), "r"(rank));
+    return r;
+}
+
+// every thread of both CTAs
+__device__ __forceinline__ void crt_cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void crt_arrive_cluster(uint32_t caddr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(caddr) : "memory");
+}
+
+// try_wait with cluster-scope acquire: the barrier receives arrivals from the peer CTA
+__device__ __forceinline__ bool crt_try_wait_cluster(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+template <bool PAIR>
+__device__ __forceinline__ bool crt_wait_t(uint64_t* bar, uint32_t parity, const int* abort_flag)
+{
+    if constexpr(!PAIR)
+        return crt_wait(bar, parity, abort_flag);
+    const long long t0 = clock64();
+    while(!crt_try_wait_cluster(bar, parity))
+    {
+        if(*(volatile const int*)abort_flag)
+            return false;
+        if(clock64() - t0 > (1ll << 31))
+            return false;
+    }
+    return true;
+}
+
+// One 256-row x 64-byte box of a residue array (2-D tensor map, no swizzle: the rows are stored
+// pre-swizzled) into this CTA's shared memory, its bytes counted on the barrier at shared::cluster
+// address mbar (the pair's first CTA).  No multicast: each CTA loads its own half of the pair's
+// operands from this GPU's memory.
+__device__ __forceinline__ void crt_tma_pair(void* dst, const CUtensorMap* map, int y, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(mbar)
+                 : "memory");
+}
+
+// M = 256 x N MMA of the pair, issued by one thread of the first CTA: A rows 0-127 and B rows
+// (N) 0 .. N/2-1 from its shared memory, the other halves from the peer's at the same offsets;
+// D rows 0-127 in its TMEM, 128-255 in the peer's.
+__device__ __forceinline__ void crt_mma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+                 "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// arrive on the barrier at this offset in both CTAs once the pair's MMAs so far are done
+__device__ __forceinline__ void crt_commit_pair(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                     smem_u32(bar)),
+                 "h"((uint16_t)3)
+                 : "memory");
+}
+
+// the same, on this CTA's barrier only
+__device__ __forceinline__ void crt_commit_pair_local(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// instruction descriptor of the pair's M = 256 MMA
+__host__ __device__ constexpr uint32_t crt_idesc_pair(int n)
+{
+    return (oz_idesc(n) & ~(0x1Fu << 24)) | ((uint32_t)(256 >> 4) << 24);
 }
 
 // r_i = C_i mod p_i in [0, p_i) for the int32 accumulator value v (|v| <= 2^28)
@@ -467,19 +572,37 @@ __device__ __forceinline__ void crt_tile_coords(int t, int tiles_m, int tiles_n,
 }
 
 // Stage of the copy ring: kCrtKS consecutive 64-deep K panels of one (tile, modulus) item,
-// the P tile (128 x 64 per panel) then the Q tile (256 x 64 per panel); the residue kernel
-// lays a row tile's K panels out back to back, so each operand of a stage is one bulk copy.
-constexpr int kCrtKS     = 2;
-constexpr int kCrtStages = 4;
+// the P tile (128 x 64 per panel) then the Q tile (256 x 64 per panel; the pair form: this CTA's
+// 128 columns); the residue kernel lays a row tile's K panels out back to back, so each operand
+// of a stage is one copy.
+constexpr int kCrtKS         = 2;
+constexpr int kCrtStages     = 4; // 48 KB stages
+constexpr int kCrtPairStages = 6; // 32 KB stages of the pair form
 
-template <int NM>
+// Dynamic shared memory of the kernel (stages + 1 KB for the 1024-byte alignment)
+__host__ __device__ constexpr size_t crt_smem_bytes(bool pair)
+{
+    return pair ? (size_t)kCrtPairStages * kCrtKS * (kOzBM + kCrtBN / 2) * kCrtBK + 1024
+                : (size_t)kCrtStages * kCrtKS * (kOzBM + kCrtBN) * kCrtBK + 1024;
+}
+
+// PAIR: cta_group::2 form, launched as clusters of two CTAs (the pair) on 256 x 256 output
+// tiles.  The pair's first CTA issues M = 256 MMAs whose A rows and B columns come half from
+// each CTA's shared memory, so that a CTA streams 32 KB per 128-deep stage where the one-CTA
+// form streams 48 KB for the same tensor work on its SM.  Each CTA's producers load its own
+// halves by 2-D TMA and count the bytes on the first CTA's full barrier (which that CTA's
+// producer arms with both halves); the MMAs' commits arrive on both CTAs' empty and
+// accumulator barriers (multicast commit); each CTA drains and rebuilds its own 128 rows, and
+// its residue warps free the accumulator on the first CTA's barrier.
+template <int NM, bool PAIR>
 __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_constant__ CrtParams p)
 {
-    constexpr int kPanelA = kOzBM * kCrtBK;  // 8 KB of P residues per K panel
-    constexpr int kPanelB = kCrtBN * kCrtBK; // 16 KB of Q residues
+    constexpr int kPanelA = kOzBM * kCrtBK;                          // 8 KB of P residues per K panel
+    constexpr int kPanelB = (PAIR ? kCrtBN / 2 : kCrtBN) * kCrtBK;   // 8 / 16 KB of Q residues
     constexpr int kStageA = kCrtKS * kPanelA;
     constexpr int kStage  = kCrtKS * (kPanelA + kPanelB);
-    constexpr int NS      = kCrtStages;
+    constexpr int NS      = PAIR ? kCrtPairStages : kCrtStages;
+    constexpr int kTileRows = PAIR ? 2 * kOzBM : kOzBM;              // output tile height
     constexpr int64_t kModBytes = (int64_t)kCrtChunks * kOzBM * 16; // one modulus in a slot
     extern __shared__ __align__(1024) unsigned char crt_smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -491,12 +614,15 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     __shared__ int      abort_flag;
     __shared__ int      issued[2], consumed; // stages loaded by each producer / handed to the MMAs
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank  = PAIR ? crt_cluster_rank() : 0u;          // CTA in the pair
+    const int      unit  = PAIR ? (int)blockIdx.x >> 1 : (int)blockIdx.x;
+    const int      units = PAIR ? (int)gridDim.x >> 1 : (int)gridDim.x;
     const int nks      = p.nkc / kCrtKS; // stages per item
-    const int tiles_m  = p.M_pad / kOzBM;
+    const int tiles_m  = p.M_pad / kTileRows;
     const int tiles_n  = p.N_pad / kCrtBN;
     const int tiles    = tiles_m * tiles_n;
-    const int my_tiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int my_tiles = tiles > unit ? (tiles - 1 - unit) / units + 1 : 0;
     const int items    = my_tiles * NM;
     const int total    = items * nks; // stage uses of the whole CTA
     uint8_t*  slots    = p.scratch + (int64_t)blockIdx.x * 2 * kCrtSlotBytes;
@@ -505,13 +631,13 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     {
         for(int i = 0; i < NS; ++i)
         {
-            mbar_init(&full_bar[i], 1);
-            mbar_init(&empty_bar[i], 1);
+            mbar_init(&full_bar[i], 1);  // the producer's expect_tx (pair: the first CTA's)
+            mbar_init(&empty_bar[i], 1); // tcgen05.commit
         }
         for(int b = 0; b < 2; ++b)
         {
-            mbar_init(&acc_full[b], 1);                   // tcgen05.commit
-            mbar_init(&acc_empty[b], kCrtResWarps);       // one arrival per residue warp
+            mbar_init(&acc_full[b], 1);                                  // tcgen05.commit
+            mbar_init(&acc_empty[b], (PAIR ? 2 : 1) * kCrtResWarps);     // one arrival per residue warp
             mbar_init(&slot_full[b], 32 * kCrtResWarps);  // every residue thread, after its last modulus
             mbar_init(&slot_empty[b], 32 * kCrtRebWarps); // every reconstruction thread
         }
@@ -523,13 +649,26 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     }
     if(warp == 1)
     {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(&tmem_base_sh)),
-                     "r"(512));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        if constexpr(PAIR)
+        {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(&tmem_base_sh)),
+                         "r"(512));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+        }
+        else
+        {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(&tmem_base_sh)),
+                         "r"(512));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    if constexpr(PAIR)
+        crt_cluster_sync(); // both CTAs' barriers initialised and TMEM allocated
+    else
+        __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
@@ -546,37 +685,51 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             const uint32_t ph = (uint32_t)((it / NS) & 1);
             const int      j  = it / nks, ks = it - j * nks;
             const int      jt = j / NM, i = j - jt * NM;
-            if(!crt_wait(&empty_bar[st], ph ^ 1, &abort_flag))
+            if(!crt_wait_t<PAIR>(&empty_bar[st], ph ^ 1, &abort_flag))
             {
                 crt_fail(p.error, &abort_flag, 11);
                 break;
             }
             int mt, nt;
-            crt_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, p.group_m, mt, nt);
-            const int8_t*  srcP = p.resP + (((int64_t)i * tiles_m + mt) * p.nkc + ks * kCrtKS) * kPanelA;
-            const int8_t*  srcQ = p.resQ + (((int64_t)i * tiles_n + nt) * p.nkc + ks * kCrtKS) * kPanelB;
+            crt_tile_coords(unit + jt * units, tiles_m, tiles_n, p.group_m, mt, nt);
             unsigned char* base = smem + st * kStage;
-            mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
-            bulk_load(base, srcP, kStageA, &full_bar[st]);
-            bulk_load(base + kStageA, srcQ, kCrtKS * kPanelB, &full_bar[st]);
+            if constexpr(PAIR)
+            {
+                // this CTA's 128-row P tile and 128-column Q tile, rows of the 2-D maps
+                const int64_t yP = (((int64_t)i * (p.M_pad / kOzBM) + 2 * mt + rank) * p.nkc + ks * kCrtKS) * kOzBM;
+                const int64_t yQ = (((int64_t)i * (p.N_pad / kOzBM) + 2 * nt + rank) * p.nkc + ks * kCrtKS) * kOzBM;
+                if(rank == 0)
+                    mbar_expect_tx(&full_bar[st], 2u * (uint32_t)kStage); // both CTAs' bytes
+                const uint32_t fb = crt_peer_addr(&full_bar[st], 0);
+                crt_tma_pair(base, &p.mapP, (int)yP, fb);
+                crt_tma_pair(base + kStageA, &p.mapQ, (int)yQ, fb);
+            }
+            else
+            {
+                const int8_t* srcP = p.resP + (((int64_t)i * tiles_m + mt) * p.nkc + ks * kCrtKS) * kPanelA;
+                const int8_t* srcQ = p.resQ + (((int64_t)i * tiles_n + nt) * p.nkc + ks * kCrtKS) * kPanelB;
+                mbar_expect_tx(&full_bar[st], (uint32_t)kStage);
+                bulk_load(base, srcP, kStageA, &full_bar[st]);
+                bulk_load(base + kStageA, srcQ, kCrtKS * kPanelB, &full_bar[st]);
+            }
             *(volatile int*)&issued[who] = it + 1;
         }
     }
     else if(warp == 1)
     {
-        // ---------------- MMA issuer ----------------
-        if(lane == 0)
+        // ---------------- MMA issuer (pair: the first CTA's) ----------------
+        if(lane == 0 && rank == 0)
         {
             const uint64_t desc_a0 = oz_smem_desc<kCrtBK>(smem_u32(smem));
             const uint64_t desc_b0 = oz_smem_desc<kCrtBK>(smem_u32(smem) + kStageA);
-            constexpr uint32_t idesc = oz_idesc(kCrtBN);
+            constexpr uint32_t idesc = PAIR ? crt_idesc_pair(kCrtBN) : oz_idesc(kCrtBN);
             int  it = 0;
             bool ok = true;
             for(int j = 0; j < items && ok; ++j)
             {
                 const int buf = j & 1;
-                // the residue warps have drained this accumulator's previous item
-                if(!crt_wait(&acc_empty[buf], (uint32_t)(((j >> 1) & 1) ^ 1), &abort_flag))
+                // the residue warps (pair: of both CTAs) have drained this accumulator's previous item
+                if(!crt_wait_t<PAIR>(&acc_empty[buf], (uint32_t)(((j >> 1) & 1) ^ 1), &abort_flag))
                 {
                     crt_fail(p.error, &abort_flag, 12);
                     break;
@@ -587,7 +740,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                 {
                     const int      st = it % NS;
                     const uint32_t ph = (uint32_t)((it / NS) & 1);
-                    if(!crt_wait(&full_bar[st], ph, &abort_flag))
+                    if(!crt_wait_t<PAIR>(&full_bar[st], ph, &abort_flag))
                     {
                         crt_fail(p.error, &abort_flag, 12);
                         ok = false;
@@ -603,15 +756,27 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
                         {
                             const uint64_t aof = (uint64_t)((q * kPanelA + kk * kOzMmaK) >> 4);
                             const uint64_t bof = (uint64_t)((q * kPanelB + kk * kOzMmaK) >> 4);
-                            oz_mma(dcol, desc_a0 + soff + aof, desc_b0 + soff + bof, idesc,
-                                   (ks > 0 || q > 0 || kk > 0) ? 1u : 0u);
+                            const uint32_t acc = (ks > 0 || q > 0 || kk > 0) ? 1u : 0u;
+                            if constexpr(PAIR)
+                                crt_mma_pair(dcol, desc_a0 + soff + aof, desc_b0 + soff + bof, idesc, acc);
+                            else
+                                oz_mma(dcol, desc_a0 + soff + aof, desc_b0 + soff + bof, idesc, acc);
                         }
-                    oz_commit(&empty_bar[st]);
+                    if constexpr(PAIR)
+                        crt_commit_pair(&empty_bar[st]);
+                    else
+                        oz_commit(&empty_bar[st]);
                 }
-                oz_commit(&acc_full[buf]);
+                if constexpr(PAIR)
+                    crt_commit_pair(&acc_full[buf]);
+                else
+                    oz_commit(&acc_full[buf]);
             }
             // every MMA issued has completed before TMEM is freed
-            oz_commit(&mma_done);
+            if constexpr(PAIR)
+                crt_commit_pair_local(&mma_done);
+            else
+                oz_commit(&mma_done);
             (void)mbar_wait_bounded(&mma_done, 0);
         }
     }
@@ -631,7 +796,7 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             bool      ok = true;
             if(i == 0) // the reconstruction warps are done with this slot's previous tile
                 ok = crt_wait(&slot_empty[slot], (uint32_t)(((jt >> 1) & 1) ^ 1), &abort_flag);
-            ok = ok && crt_wait(&acc_full[buf], (uint32_t)((j >> 1) & 1), &abort_flag);
+            ok = ok && crt_wait_t<PAIR>(&acc_full[buf], (uint32_t)((j >> 1) & 1), &abort_flag);
             // warp-uniform outcome: the tcgen05.ld below needs the whole warp
             if(!__all_sync(0xffffffffu, ok))
             {
@@ -667,7 +832,12 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncwarp();
             if(lane == 0)
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+            {
+                if constexpr(PAIR)
+                    crt_arrive_cluster(crt_peer_addr(&acc_empty[buf], 0)); // the MMA issuer's barrier
+                else
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+            }
             if(i == NM - 1) // this thread's residues of the tile are all in the slot
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_full[slot])) : "memory");
         }
@@ -685,44 +855,58 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
         for(int jt = 0; jt < my_tiles; ++jt)
         {
             const int slot = jt & 1;
-            if(!crt_wait(&slot_full[slot], (uint32_t)((jt >> 1) & 1), &abort_flag))
+            // warp-uniform outcome: the shuffles below need the whole warp
+            if(!__all_sync(0xffffffffu, crt_wait(&slot_full[slot], (uint32_t)((jt >> 1) & 1), &abort_flag)))
             {
                 crt_fail(p.error, &abort_flag, 14);
                 break;
             }
             int mt, nt;
-            crt_tile_coords((int)blockIdx.x + jt * (int)gridDim.x, tiles_m, tiles_n, p.group_m, mt, nt);
-            const int gr = mt * kOzBM + row;
+            crt_tile_coords(unit + jt * units, tiles_m, tiles_n, p.group_m, mt, nt);
+            const int gr = mt * kTileRows + (int)rank * kOzBM + row;
             int       er = gr < p.M ? p.exp_rows[gr] : 0;
             if(er == kOzExpNone)
                 er = 0;
             const uint8_t* src = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)row * 16;
+            const bool read_c = !zero && beta != 0.0;
 #pragma unroll 1
             for(int ch = ch0; ch < ch0 + kChunksPer; ++ch)
             {
+                const int c0 = nt * kCrtBN + ch * 16;
+                // the chunk's 16 entries of C are loaded before the rebuild, together with the
+                // residues, so that their latency (C is usually in DRAM) is paid once per chunk
+                // instead of once per entry
+                double cin[16];
+#pragma unroll
+                for(int c = 0; c < 16; ++c)
+                {
+                    const int gc = c0 + c;
+                    cin[c] = gr < p.M && gc < p.N && read_c ? p.C[gr + (int64_t)gc * p.ldc] : 0.0;
+                }
+                // lane l holds the exponent of column c0 + (l & 15), read before any store to C
+                int ecl = c0 + (lane & 15) < p.N ? p.exp_cols[c0 + (lane & 15)] : 0;
+                ecl     = ecl == kOzExpNone ? 0 : ecl;
                 uint4 r[NM];
 #pragma unroll
                 for(int i = 0; i < NM; ++i)
                     r[i] = *reinterpret_cast<const uint4*>(src + (int64_t)i * kModBytes + (int64_t)ch * kOzBM * 16);
-                const int c0 = nt * kCrtBN + ch * 16;
                 auto out = [&](double x, int c) {
-                    const int gc = c0 + c;
+                    const int gc   = c0 + c;
+                    const int ecol = __shfl_sync(0xffffffffu, ecl, c); // every lane, before the bounds test
                     if(gr >= p.M || gc >= p.N)
                         return;
-                    const int ec = p.exp_cols[gc] == kOzExpNone ? 0 : p.exp_cols[gc];
-                    const int E  = er + ec - p.shift;
+                    const int    E    = er + ecol - p.shift;
                     const double pq = (E >= -1022 && E <= 1023)
                                           ? x * __longlong_as_double((long long)(1023 + E) << 52)
                                           : ldexp(x, E);
-                    double* cp = p.C + gr + (int64_t)gc * p.ldc;
-                    double  o;
+                    double o;
                     if(zero)
                         o = 0.0;
                     else if(beta == 0.0)
                         o = p.alpha * pq;
                     else
-                        o = fma(p.alpha, pq, beta * (*cp));
-                    *cp = o;
+                        o = fma(p.alpha, pq, beta * cin[c]);
+                    p.C[gr + (int64_t)gc * p.ldc] = o;
                 };
                 crt_static_for<0, 16>([&](auto Cc) {
                     constexpr int c = decltype(Cc)::value;
@@ -737,17 +921,34 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     __syncthreads();
     if(warp == 0 && lane == 0 && *(volatile int*)&abort_flag)
     {
-        // let the copies that were issued but never consumed land before the CTA exits
-        for(int it = consumed; it < max(issued[0], issued[1]); ++it)
-            if(it < issued[it & 1])
-                (void)mbar_wait_bounded(&full_bar[it % NS], (uint32_t)((it / NS) & 1));
+        if constexpr(PAIR)
+        {
+            // the copies count on the first CTA's barrier, which this CTA cannot always watch:
+            // give the ones still in flight (a few microseconds each) time to land
+            const long long t0 = clock64();
+            while(clock64() - t0 < 200000)
+                __nanosleep(1000);
+        }
+        else
+        {
+            // let the copies that were issued but never consumed land before the CTA exits
+            for(int it = consumed; it < max(issued[0], issued[1]); ++it)
+                if(it < issued[it & 1])
+                    (void)mbar_wait_bounded(&full_bar[it % NS], (uint32_t)((it / NS) & 1));
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    if constexpr(PAIR)
+        crt_cluster_sync(); // neither CTA leaves while the pair's MMAs or arrivals may touch it
+    else
+        __syncthreads();
     if(warp == 1)
     {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+        if constexpr(PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
     }
 }
 

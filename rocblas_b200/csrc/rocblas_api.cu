@@ -507,18 +507,19 @@ inline rocblas_status trsv_arg_check(rocblas_handle h, rocblas_fill uplo, rocbla
     return rocblas_status_continue;
 }
 
-// The flag-synchronised single-vector solve (trsv_flag.cuh): a persistent grid, every CTA
-// resident at once, so that no block waits on one that has not started.
-template <typename T, int NB>
-void launch_trsv_flag(const TrsvParams<T>& p, int nblk, int sms, cudaStream_t s)
+// The flag-synchronised solve (trsv_flag.cuh) with NR right-hand sides: a persistent grid of at
+// most `sms` SMs' worth of CTAs, each taking its row blocks in increasing order, so that a block
+// only waits on blocks that are done or in progress.
+template <typename T, int NB, int NR, int TR = -1>
+void launch_trsv_flag_nr(const TrsvParams<T>& p, int nblk, int sms, cudaStream_t s)
 {
-    constexpr size_t smem = trsv_flag_smem_bytes<T, NB>();
+    constexpr size_t smem = trsv_flag_smem_bytes<T, NB, NR>();
     static int per_sm = 0;
     if(!per_sm)
     {
-        cudaFuncSetAttribute((const void*)trsv_flag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flag_kernel<T, NB>, kTvThreads, smem)
+        cudaFuncSetAttribute((const void*)trsv_flag_kernel<T, NB, NR, TR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_flag_kernel<T, NB, NR, TR>, kTvThreads, smem)
                != cudaSuccess
            || per_sm < 1)
         {
@@ -527,7 +528,14 @@ void launch_trsv_flag(const TrsvParams<T>& p, int nblk, int sms, cudaStream_t s)
         }
     }
     const int grid = std::min(nblk, sms * per_sm);
-    trsv_flag_kernel<T, NB><<<grid, kTvThreads, smem, s>>>(p);
+    trsv_flag_kernel<T, NB, NR, TR><<<grid, kTvThreads, smem, s>>>(p);
+}
+
+// one vector (rocblas_?trsv)
+template <typename T, int NB>
+void launch_trsv_flag(const TrsvParams<T>& p, int nblk, int sms, cudaStream_t s)
+{
+    launch_trsv_flag_nr<T, NB, 1>(p, nblk, sms, s);
 }
 
 template <typename T>
@@ -564,6 +572,8 @@ rocblas_status trsv_impl(rocblas_handle h, rocblas_fill uplo, rocblas_operation 
                 p.lda   = lda;
                 p.x     = x.base + x.offset;
                 p.incx  = incx;
+                p.nrhs  = 1;
+                p.alpha = T(1);
                 p.n     = n;
                 const bool lower = uplo == rocblas_fill_lower;
                 p.trans = trans != rocblas_operation_none;
@@ -1919,12 +1929,18 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     ps.ldb = srows;
     const bool ps_chain = use_chain(ps);
     ps.sm_count         = std::max(1, std::min(tuning().refine_check_sms, h->sm_count / 4));
+    // up to 8 tested right-hand sides: the memory-bound flag-synchronised solve (one pass over
+    // A's triangle for all of them), else the chain
+    const bool ps_flag = c <= 8 && tuning().refine_check_flag != 0;
+    const int  nb_flag = (int)ceil_div(left ? m : n, 128);
     // workspace: the precision form's | B0 (m x n) | R (m x n) | the tested right-hand sides |
     // their chain flags | the test's maxima
     const MixedPlan plan  = mixed_plan(pr, S, moduli);
     const size_t    mn    = (size_t)m * n * sizeof(double);
     const size_t    smp   = (size_t)srows * scols * sizeof(double);
-    const size_t    fl    = ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, 32)) : 0;
+    const size_t    fl    = ps_flag    ? (size_t)nb_flag * 2 * sizeof(int)
+                            : ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, 32))
+                                       : 0;
     const size_t    o_b0  = align256(plan.total), o_r = o_b0 + align256(mn);
     const size_t    o_xs  = o_r + (max_it > 0 ? align256(mn) : 0), o_fl = o_xs + align256(smp);
     const size_t    o_mx  = o_fl + align256(fl);
@@ -1976,7 +1992,34 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     cudaStreamWaitEvent(res.tri, ev_inv, 0);
     ps.B      = strided<double>(Xs, 0);
     ps.stream = res.tri;
-    if(ps_chain && plan.recursive)
+    if(ps_flag)
+    {
+        // side L: op(A) x_v = alpha b_v, x_v a column of Xs (m x c); side R: x_v op(A) = alpha b_v
+        // is op(A)^T x_v^T = alpha b_v^T, x_v a row of Xs (c x n)
+        TrsvParams<double> tp{};
+        const bool tr = left ? pr.trans : !pr.trans;
+        tp.A           = A;
+        tp.lda         = lda;
+        tp.x           = Xs;
+        tp.incx        = left ? 1 : srows;
+        tp.ldx         = left ? srows : 1;
+        tp.nrhs        = c;
+        tp.alpha       = *alpha;
+        tp.n           = left ? m : n;
+        tp.trans       = tr ? 1 : 0;
+        tp.rev         = pr.upper != tr ? 1 : 0; // op(A) (side R: its transpose) upper
+        tp.unit        = pr.unit ? 1 : 0;
+        tp.flags       = reinterpret_cast<int*>(ws + o_fl);
+        tp.error       = err;
+        tp.wait_cycles = 1ll << tuning().wait_cycles_log2;
+        cudaMemsetAsync(tp.flags, 0, (size_t)nb_flag * 2 * sizeof(int), res.tri);
+        if(tr)
+            launch_trsv_flag_nr<double, 64, 8, 1>(tp, (int)ceil_div(tp.n, 64), ps.sm_count, res.tri);
+        else
+            launch_trsv_flag_nr<double, 128, 8, 0>(tp, nb_flag, ps.sm_count, res.tri);
+        count_launch();
+    }
+    else if(ps_chain && plan.recursive)
         launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, 32, ws + o_fl);
     else
         trsm_run<double>(ps, nullptr, false);

@@ -1,6 +1,7 @@
 // Host side of the sliced (integer-slice, tensor-core) FP64 GEMM and of the precision form
 // of the TRSM that uses it for its trailing updates.
 #pragma once
+#include <climits>
 #include <functional>
 #include <mutex>
 
@@ -208,11 +209,57 @@ static int64_t crt_k_chunk()
     return std::max<int64_t>(64, std::min<int64_t>(kCrtKMax, tuning().sliced_k_chunk / 64 * 64));
 }
 
-// CTAs of the persistent grid: at most one per SM
-static int64_t crt_grid(int64_t Mp, int64_t Np, int sms)
+// CTAs of the persistent grid: at most one per SM; the pair form has 256-row tiles and an even
+// number of CTAs
+static int64_t crt_grid(int64_t Mp, int64_t Np, int sms, bool pair = false)
 {
+    if(pair)
+    {
+        const int64_t tiles = (Mp / (2 * kOzBM)) * (Np / kCrtBN);
+        return 2 * std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(sms, 2) / 2));
+    }
     const int64_t tiles = (Mp / kOzBM) * (Np / kCrtBN);
     return std::max<int64_t>(1, std::min<int64_t>(tiles, std::max(sms, 1)));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not link
+// libcuda); null if the driver does not provide it
+using CrtEncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                    CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                    CUtensorMapFloatOOBfill);
+static CrtEncodeTiled crt_encode_fn()
+{
+    static CrtEncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess
+           && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CrtEncodeTiled>(f);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// A residue array of `rows` rows of 64 bytes as a 2-D tensor map with 256-row boxes (no swizzle:
+// the rows are stored in the MMA's swizzled order already).  The pair kernel's row coordinates
+// are int32, so rows must stay below 2^31.
+static bool crt_encode_map(CUtensorMap* m, const void* base, int64_t rows)
+{
+    const CrtEncodeTiled fn = crt_encode_fn();
+    if(!fn || rows <= 0 || rows >= ((int64_t)1 << 31) || (reinterpret_cast<uintptr_t>(base) & 15))
+        return false;
+    const cuuint64_t dims[2]    = {(cuuint64_t)kCrtBK, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kCrtBK};
+    const cuuint32_t box[2]     = {(cuuint32_t)kCrtBK, (cuuint32_t)(kCrtKS * kOzBM)};
+    const cuuint32_t estr[2]    = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+           == CUDA_SUCCESS;
 }
 
 // K padded to whole ring stages (kCrtKS panels of 64)
@@ -226,7 +273,8 @@ static int64_t crt_k_pad(int64_t K)
 static size_t crt_gemm_workspace_bytes(int64_t M, int64_t N, int64_t K, int nm, int sms)
 {
     const int64_t Kp = crt_k_pad(std::min<int64_t>(std::max<int64_t>(K, 1), crt_k_chunk()));
-    const int64_t Mp = round_up(std::max<int64_t>(M, 1), kOzBM), Np = round_up(std::max<int64_t>(N, 1), kCrtNPad);
+    // rows padded for either form (the pair form's tiles are 256 rows high)
+    const int64_t Mp = round_up(std::max<int64_t>(M, 1), 2 * kOzBM), Np = round_up(std::max<int64_t>(N, 1), kCrtNPad);
     return align256((size_t)nm * Mp * Kp) + align256((size_t)nm * Np * Kp) + align256(4 * Mp)
            + align256(4 * Np) + align256((size_t)crt_grid(Mp, Np, sms) * 2 * kCrtSlotBytes);
 }
@@ -236,25 +284,49 @@ static bool crt_moduli_supported(int nm)
     return nm == 14 || nm == 15 || nm == 16;
 }
 
+// pair: the cta_group::2 form (Mp a multiple of 256; the Q residues in 128-column tiles)
 template <int NM>
 static void launch_crt(SliceOperand P, SliceOperand Q, int M, int N, int K, int* eP, int* eQ,
                        int8_t* rP, int8_t* rQ, int64_t Mp, int64_t Np, int64_t Kp, CrtParams p,
-                       int sms, cudaStream_t s)
+                       int sms, bool pair, cudaStream_t s)
 {
     const int bits = crt_bits(NM, K);
     dim3      gP((unsigned)(Kp / kOzSliceTile), (unsigned)(Mp / kOzSliceTile));
     crt_residue_kernel<NM><<<gP, 256, 0, s>>>(P.d(), P.so, P.sk, M, K, eP, bits, rP, (int)Mp, (int)Kp, kOzBM);
     count_launch();
     dim3 gQ((unsigned)(Kp / kOzSliceTile), (unsigned)(Np / kOzSliceTile));
-    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp, kCrtBN);
+    crt_residue_kernel<NM><<<gQ, 256, 0, s>>>(Q.d(), Q.so, Q.sk, N, K, eQ, bits, rQ, (int)Np, (int)Kp,
+                                              pair ? kOzBM : kCrtBN);
     count_launch();
     p.shift = 2 * bits;
-    const size_t smem = (size_t)kCrtStages * kCrtKS * (kOzBM + kCrtBN) * kCrtBK + 1024;
-    cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const unsigned grid = (unsigned)crt_grid(Mp, Np, sms);
+    const size_t   smem = crt_smem_bytes(pair);
+    const unsigned grid = (unsigned)crt_grid(Mp, Np, sms, pair);
     // algorithmic work: int8 tensor operations of the NM residue products
     TimedLaunch tl(KernelClass::sliced, s, 2.0 * NM * (double)M * N * K);
-    crt_gemm_kernel<NM><<<grid, kCrtThreads, smem, s>>>(p);
+    if(pair)
+    {
+        cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim          = dim3(grid);
+        cfg.blockDim         = dim3(kCrtThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream           = s;
+        cudaLaunchAttribute at[1];
+        at[0].id               = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs    = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, crt_gemm_kernel<NM, true>, p);
+    }
+    else
+    {
+        cudaFuncSetAttribute((const void*)crt_gemm_kernel<NM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        crt_gemm_kernel<NM, false><<<grid, kCrtThreads, smem, s>>>(p);
+    }
     count_launch();
 }
 
@@ -265,9 +337,23 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         return true;
     if(!crt_moduli_supported(g.moduli) || g.c_f32 || g.P.f32 || g.Q.f32)
         return false;
-    const int64_t Mp = round_up(g.M, kOzBM), Np = round_up(g.N, kCrtNPad);
-    const int64_t K  = std::max<int64_t>(g.K, 0);
+    // the pair form: clusters of two CTAs on 256 x 256 tiles (its 2-D maps take int32 rows),
+    // only for a GEMM that has every SM of the device: beside another kernel (the refined form's
+    // test solve) SM pairs may be split, and a cluster that cannot be placed waits for it
     const int64_t kchunk = crt_k_chunk();
+    int           dev = 0, dev_sms = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess
+       || cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    {
+        cudaGetLastError();
+        dev_sms = INT_MAX;
+    }
+    const bool    pair   = tuning().crt_pair != 0 && g.sms >= 2 && g.sms >= dev_sms && crt_encode_fn() != nullptr
+                      && (int64_t)g.moduli * round_up(std::max<int64_t>(g.M, g.N), 2 * kOzBM)
+                                 * (crt_k_pad(std::min<int64_t>(std::max<int64_t>(g.K, 1), kchunk)) / kCrtBK)
+                             < ((int64_t)1 << 31);
+    const int64_t Mp = round_up(g.M, pair ? 2 * kOzBM : kOzBM), Np = round_up(g.N, kCrtNPad);
+    const int64_t K  = std::max<int64_t>(g.K, 0);
     for(int64_t k0 = 0; k0 < std::max<int64_t>(K, 1); k0 += kchunk)
     {
         const int64_t kc = std::min<int64_t>(kchunk, K - k0);
@@ -317,11 +403,15 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         p.error = err_dev;
         p.group_m = std::max(1, tuning().crt_group_m);
         const int kk = (int)std::max<int64_t>(kc, 1);
+        if(pair
+           && !(crt_encode_map(&p.mapP, rP, (int64_t)g.moduli * Mp * (Kp / kCrtBK))
+                && crt_encode_map(&p.mapQ, rQ, (int64_t)g.moduli * Np * (Kp / kCrtBK))))
+            return false;
         switch(g.moduli)
         {
-        case 14: launch_crt<14>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
-        case 15: launch_crt<15>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
-        default: launch_crt<16>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, s); break;
+        case 14: launch_crt<14>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, pair, s); break;
+        case 15: launch_crt<15>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, pair, s); break;
+        default: launch_crt<16>(P, Q, (int)g.M, (int)g.N, kk, eP, eQ, rP, rQ, Mp, Np, Kp, p, g.sms, pair, s); break;
         }
     }
     return true;

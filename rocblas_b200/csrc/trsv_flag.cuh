@@ -40,6 +40,9 @@ struct TrsvParams
     int64_t   lda;
     T*        x;
     int64_t   incx; // > 0
+    int64_t   ldx;  // distance between the right-hand sides (nrhs > 1)
+    int       nrhs; // right-hand sides, 1 .. the kernel's NR
+    T         alpha; // op(A) x_v = alpha b_v (1 for trsv)
     int       n;
     int       rev;   // op(A) is upper: the solve runs from the last row
     int       trans; // op(A) = A^T (A^H reads the same for real types)
@@ -57,10 +60,10 @@ __device__ __forceinline__ T tv_load(const TrsvParams<T>& p, int rl, int cl)
 }
 
 template <typename T>
-__device__ __forceinline__ T* tv_x(const TrsvParams<T>& p, int rl)
+__device__ __forceinline__ T* tv_x(const TrsvParams<T>& p, int rl, int v = 0)
 {
     const int r = p.rev ? p.n - 1 - rl : rl;
-    return p.x + (int64_t)r * p.incx;
+    return p.x + (int64_t)v * p.ldx + (int64_t)r * p.incx;
 }
 
 // bounded wait for block j's flag (acquire); false when it ran out
@@ -79,13 +82,15 @@ __device__ __forceinline__ bool tv_wait_flag(const int* flag, long long limit)
     }
 }
 
-// Dynamic shared memory of the NB-row kernel: the diagonal block (NB x NB + 1; for NB = 128 its
-// inverse in place) and 64 x 65 scratch blocks for the inverses of its 64-row halves (one for
-// NB = 64, where it holds the inverse, two for NB = 128).
-template <typename T, int NB>
+// Dynamic shared memory of the NB-row kernel with NR right-hand sides: the diagonal block
+// (NB x NB + 1; for NB = 128 its inverse in place), 64 x 65 scratch blocks for the inverses of its
+// 64-row halves (one for NB = 64, where it holds the inverse, two for NB = 128) and the 8 warps'
+// partial sums (8 x NR x NB; for NB = 128 over the two scratch blocks, free by then).
+template <typename T, int NB, int NR = 1>
 constexpr size_t trsv_flag_smem_bytes()
 {
-    return sizeof(T) * ((size_t)NB * (NB + 1) + (NB / kTvNB) * kTvNB * (kTvNB + 1));
+    return sizeof(T) * ((size_t)NB * (NB + 1) + (NB / kTvNB) * kTvNB * (kTvNB + 1)
+                        + (NB == 64 ? (size_t)kTvWarps * NR * NB : 0));
 }
 
 // inverse of the lower-triangular 64 x 64 block S (stride ls) into D (stride ld), zero above the
@@ -105,23 +110,34 @@ __device__ __forceinline__ void tv_invert64(const T* S, int ls, T* D, int ld, in
     }
 }
 
-template <typename T, int NB>
+// TR: -1 takes op(A)'s transposition from p.trans; 0 / 1 fix it at compile time (fewer
+// registers: the accumulators of one layout only).
+template <typename T, int NB, int NR = 1, int TR = -1>
 __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<T> p)
 {
     static_assert(NB == 64 || NB == 128, "block rows");
+    static_assert(NR >= 1 && NR <= 8, "right-hand sides");
+    static_assert(NB == 64 || kTvWarps * NR * NB <= 2 * kTvNB * (kTvNB + 1), "partial sums fit the scratch");
     constexpr int RPL = NB / 32;          // no-trans: rows per lane
     constexpr int CPW = kTvNB / kTvWarps; // columns per warp in a 64-column half tile
     constexpr int RPW = NB / kTvWarps;    // trans: rows per warp
     constexpr int LD  = NB + 1;
+    constexpr int NACC = TR == 0 ? RPL : TR == 1 ? RPW : (RPL > RPW ? RPL : RPW);
+    const bool    trans = TR < 0 ? p.trans != 0 : TR == 1;
+    constexpr int G    = kTvThreads / NB;   // right-hand-side groups of the final product
+    constexpr int VPT  = (NR + G - 1) / G;  // right-hand sides per thread in it
     extern __shared__ __align__(16) unsigned char tv_smem[];
     T* dg = reinterpret_cast<T*>(tv_smem); // diagonal block, then its inverse in place
     T* s1 = dg + NB * LD;                  // NB = 128: inverses of the two 64-row halves
     T* s2 = s1 + kTvNB * (kTvNB + 1);
-    __shared__ T   part[kTvWarps][NB];
-    __shared__ T   ysh[NB];
+    // partial sums [warp][v][row]: NB = 128 over s1 / s2 (dead once the inverse is assembled),
+    // NB = 64 after s1
+    T* part = NB == 128 ? s1 : s1 + kTvNB * (kTvNB + 1);
+    __shared__ T   ysh[NR][NB];
     __shared__ int stop;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nblk = (p.n + NB - 1) / NB;
+    const int fr = threadIdx.x % NB, fg = threadIdx.x / NB; // final product: row, group
     if(threadIdx.x == 0)
         stop = 0;
     __syncthreads();
@@ -138,8 +154,14 @@ __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<
                 v = T(1);
             dg[rr * LD + cc] = v;
         }
-        // this block's right-hand side, read before any wait (no other block writes it)
-        const T xb = threadIdx.x < rows ? *tv_x(p, r0 + threadIdx.x) : T(0);
+        // this block's right-hand sides, read before any wait (no other block writes them)
+        T xb[VPT];
+#pragma unroll
+        for(int i = 0; i < VPT; ++i)
+        {
+            const int v = fg + G * i;
+            xb[i] = (fr < rows && v < NR && v < p.nrhs) ? *tv_x(p, r0 + fr, v) : T(0);
+        }
         __syncthreads();
         // its inverse, also before any wait: after the wait on the block before (the critical
         // path) only a product with it remains
@@ -200,37 +222,45 @@ __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<
         // the tiles j < b, in 64-column halves: no-trans maps lanes to rows (RPL each) and warps
         // to columns (8 of each half), trans maps lanes to columns (2 of each half) and warps to
         // rows (RPW each)
-        T    acc[RPL > RPW ? RPL : RPW];
+        T acc[NR][NACC];
 #pragma unroll
-        for(int q = 0; q < (RPL > RPW ? RPL : RPW); ++q)
-            acc[q] = T(0);
+        for(int v = 0; v < NR; ++v)
+#pragma unroll
+            for(int q = 0; q < NACC; ++q)
+                acc[v][q] = T(0);
         bool ok = true;
         for(int j = 0; j < b && ok; ++j)
         {
             for(int hf = 0; hf < NB / kTvNB; ++hf)
             {
                 const int c0 = j * NB + hf * kTvNB; // a full block: j < b
-                constexpr int kAv = RPL * CPW > 2 * RPW ? RPL * CPW : 2 * RPW;
+                constexpr int kAv = TR == 0 ? RPL * CPW : TR == 1 ? 2 * RPW : (RPL * CPW > 2 * RPW ? RPL * CPW : 2 * RPW);
                 T             av[kAv];
-                if(!p.trans)
+                if(!trans)
                 {
+                    if constexpr(TR != 1)
+                    {
 #pragma unroll
-                    for(int q = 0; q < CPW; ++q)
+                        for(int q = 0; q < CPW; ++q)
 #pragma unroll
-                        for(int t = 0; t < RPL; ++t)
-                        {
-                            const int rr = lane + 32 * t;
-                            av[q * RPL + t] = rr < rows ? tv_load(p, r0 + rr, c0 + warp + q * kTvWarps) : T(0);
-                        }
+                            for(int t = 0; t < RPL; ++t)
+                            {
+                                const int rr = lane + 32 * t;
+                                av[q * RPL + t] = rr < rows ? tv_load(p, r0 + rr, c0 + warp + q * kTvWarps) : T(0);
+                            }
+                    }
                 }
                 else
                 {
-#pragma unroll
-                    for(int q = 0; q < RPW; ++q)
+                    if constexpr(TR != 0)
                     {
-                        const int rr = warp + q * kTvWarps;
-                        av[2 * q]     = rr < rows ? tv_load(p, r0 + rr, c0 + lane) : T(0);
-                        av[2 * q + 1] = rr < rows ? tv_load(p, r0 + rr, c0 + lane + 32) : T(0);
+#pragma unroll
+                        for(int q = 0; q < RPW; ++q)
+                        {
+                            const int rr = warp + q * kTvWarps;
+                            av[2 * q]     = rr < rows ? tv_load(p, r0 + rr, c0 + lane) : T(0);
+                            av[2 * q + 1] = rr < rows ? tv_load(p, r0 + rr, c0 + lane + 32) : T(0);
+                        }
                     }
                 }
                 if(hf == 0)
@@ -247,23 +277,37 @@ __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<
                         break;
                     }
                 }
-                if(!p.trans)
+                if(!trans)
                 {
-#pragma unroll
-                    for(int q = 0; q < CPW; ++q)
+                    if constexpr(TR != 1)
                     {
-                        const T xv = __ldcg(tv_x(p, c0 + warp + q * kTvWarps));
 #pragma unroll
-                        for(int t = 0; t < RPL; ++t)
-                            acc[t] += av[q * RPL + t] * xv;
+                        for(int q = 0; q < CPW; ++q)
+#pragma unroll
+                            for(int v = 0; v < NR; ++v)
+                            {
+                                const T xv = v < p.nrhs ? __ldcg(tv_x(p, c0 + warp + q * kTvWarps, v)) : T(0);
+#pragma unroll
+                                for(int t = 0; t < RPL; ++t)
+                                    acc[v][t] += av[q * RPL + t] * xv;
+                            }
                     }
                 }
                 else
                 {
-                    const T x0 = __ldcg(tv_x(p, c0 + lane)), x1 = __ldcg(tv_x(p, c0 + lane + 32));
+                    if constexpr(TR != 0)
+                    {
 #pragma unroll
-                    for(int q = 0; q < RPW; ++q)
-                        acc[q] += av[2 * q] * x0 + av[2 * q + 1] * x1;
+                        for(int v = 0; v < NR; ++v)
+                        {
+                            const bool live = v < p.nrhs;
+                            const T    x0   = live ? __ldcg(tv_x(p, c0 + lane, v)) : T(0);
+                            const T    x1   = live ? __ldcg(tv_x(p, c0 + lane + 32, v)) : T(0);
+#pragma unroll
+                            for(int q = 0; q < RPW; ++q)
+                                acc[v][q] += av[2 * q] * x0 + av[2 * q + 1] * x1;
+                        }
+                    }
                 }
             }
         }
@@ -272,58 +316,85 @@ __global__ void __launch_bounds__(kTvThreads) trsv_flag_kernel(const TrsvParams<
             atomicCAS(p.error, 0, 5);
             atomicExch(&stop, 1);
         }
-        // partial sums of the 8 warps into part[warp][row]
-        if(!p.trans)
+        __syncthreads(); // NB = 128: the partial sums reuse the inverse's scratch
+        // partial sums into part[warp][v][row] (trans: only warp 0's slots, one warp owns a row)
+        if(!trans)
         {
+            if constexpr(TR != 1)
+            {
 #pragma unroll
-            for(int t = 0; t < RPL; ++t)
-                part[warp][lane + 32 * t] = acc[t];
+                for(int v = 0; v < NR; ++v)
+#pragma unroll
+                    for(int t = 0; t < RPL; ++t)
+                        part[(warp * NR + v) * NB + lane + 32 * t] = acc[v][t];
+            }
         }
         else
         {
-#pragma unroll
-            for(int q = 0; q < RPW; ++q)
+            if constexpr(TR != 0)
             {
-                T v = acc[q];
 #pragma unroll
-                for(int off = 16; off; off >>= 1)
-                    v += __shfl_xor_sync(0xffffffffu, v, off);
-                if(lane == 0)
-                {
-                    // row warp + 8 q: one warp owns each row, the others contribute zero
-                    const int rr = warp + q * kTvWarps;
-                    for(int w = 0; w < kTvWarps; ++w)
-                        part[w][rr] = w == warp ? v : T(0);
-                }
+                for(int v = 0; v < NR; ++v)
+#pragma unroll
+                    for(int q = 0; q < RPW; ++q)
+                    {
+                        T s = acc[v][q];
+#pragma unroll
+                        for(int off = 16; off; off >>= 1)
+                            s += __shfl_xor_sync(0xffffffffu, s, off);
+                        if(lane == 0)
+                            part[v * NB + warp + q * kTvWarps] = s;
+                    }
             }
         }
         __syncthreads();
         if(*(volatile int*)&stop)
             break;
-        // y = b - sum, then x_b = inv y, by the first NB threads (named barrier 1 between them;
-        // the other warps wait at the CTA barrier below before the next block reuses the buffers)
-        if(threadIdx.x < NB)
-        {
-            const int rr = threadIdx.x;
-            T         sum = T(0);
+        // y = alpha b - sum, then x_b = inv y: thread (row fr, group fg) takes the right-hand
+        // sides fg, fg + G, ...
+        const int nw = trans ? 1 : kTvWarps;
 #pragma unroll
-            for(int w = 0; w < kTvWarps; ++w)
-                sum += part[w][rr];
-            ysh[rr] = xb - sum;
-            asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
-            // the inverse: s1 (stride 65) for NB = 64, the block itself for NB = 128
-            const T* inv = NB == 64 ? s1 : dg;
-            const int li = NB == 64 ? kTvNB + 1 : LD;
-            T v = T(0);
-            for(int cc = 0; cc <= rr; ++cc)
-                v += inv[rr * li + cc] * ysh[cc];
-            if(rr < rows)
-                *tv_x(p, r0 + rr) = v;
-            __threadfence();
-            asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
-            if(rr == 0)
-                asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p.flags + b), "r"(1) : "memory");
+        for(int i = 0; i < VPT; ++i)
+        {
+            const int v = fg + G * i;
+            if(v < NR)
+            {
+                T sum = T(0);
+                for(int w = 0; w < nw; ++w)
+                    sum += part[(w * NR + v) * NB + fr];
+                ysh[v][fr] = p.alpha * xb[i] - sum;
+            }
         }
+        __syncthreads();
+        {
+            // the inverse: s1 (stride 65) for NB = 64, the block itself for NB = 128
+            const T*  inv = NB == 64 ? s1 : dg;
+            const int li  = NB == 64 ? kTvNB + 1 : LD;
+            T         out[VPT];
+#pragma unroll
+            for(int i = 0; i < VPT; ++i)
+                out[i] = T(0);
+            if(fg < NR)
+                for(int cc = 0; cc <= fr; ++cc)
+                {
+                    const T a = inv[fr * li + cc];
+#pragma unroll
+                    for(int i = 0; i < VPT; ++i)
+                        if(fg + G * i < NR)
+                            out[i] += a * ysh[fg + G * i][cc];
+                }
+#pragma unroll
+            for(int i = 0; i < VPT; ++i)
+            {
+                const int v = fg + G * i;
+                if(fr < rows && v < NR && v < p.nrhs)
+                    *tv_x(p, r0 + fr, v) = out[i];
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if(threadIdx.x == 0)
+            asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p.flags + b), "r"(1) : "memory");
         __syncthreads(); // the buffers are reused by the CTA's next block
     }
 }

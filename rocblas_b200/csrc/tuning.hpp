@@ -41,12 +41,16 @@ struct Tuning
                                       // more bits of entries far below their row's maximum
     int refine_check_sms     = 4;    // refined form: SMs of the FP64 solve of the tested
                                      // right-hand sides, which runs beside the sliced solve
+    int refine_check_flag    = 0;    // refined form: that solve as the memory-bound flag
+                                     // solve (up to 8 right-hand sides; 0: the chain)
     int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
                                      // cycles (2^31: about a second), records error 4, returns
     int trsv_flag_min_n      = 256;  // trsv of one real vector: the flag-synchronised solve from
                                      // this order up
     int trsv_flag_nb         = 128;  // ... its block rows (64 or 128)
     int crt_group_m          = 8;    // residue GEMM tile order: row tiles per group
+    int crt_pair             = 1;    // residue GEMM as CTA pairs (cta_group::2, 256 x 256 tiles)
+                                     // when it has every SM of the device
     int crt_min_tiles_pct    = 100;  // precision form: residue engine for updates with at least
                                      // SMs * pct / 100 output tiles of 128 x 256, else slices
     int strsm_slices         = 4;    // FP32 solve: slices of its trailing updates on the int8 slice
@@ -84,11 +88,13 @@ static const TuningEntry kTuningEntries[] = {
     {"host_step_blocks", &Tuning::host_step_blocks, 1, 1 << 20},
     {"sliced_k_chunk", &Tuning::sliced_k_chunk, 64, 16384},
     {"refine_check_sms", &Tuning::refine_check_sms, 1, 1024},
+    {"refine_check_flag", &Tuning::refine_check_flag, 0, 1},
     {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
     {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
     {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},
     {"strsm_slices", &Tuning::strsm_slices, 0, 8},
     {"crt_group_m", &Tuning::crt_group_m, 1, 1024},
+    {"crt_pair", &Tuning::crt_pair, 0, 1},
     {"trsv_flag_min_n", &Tuning::trsv_flag_min_n, 1, 1 << 30},
     {"trsv_flag_nb", &Tuning::trsv_flag_nb, 64, 128},
     {"crt_min_tiles_pct", &Tuning::crt_min_tiles_pct, 0, 100000},

@@ -58,8 +58,19 @@ def handle():
     h.close()
 
 
+@pytest.fixture(params=[0, 1], ids=["cta", "pair"])
+def form(request):
+    """The one-CTA kernel (128 x 256 tiles) and the CTA-pair kernel (cta_group::2, 256 x 256)."""
+    L = rb.lib()
+    old = ctypes.c_int(-1)
+    assert L.rocblas_b200_get_tuning(b"crt_pair", ctypes.byref(old)) == 0
+    assert L.rocblas_b200_set_tuning(b"crt_pair", request.param) == 0
+    yield request.param
+    L.rocblas_b200_set_tuning(b"crt_pair", old.value)
+
+
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
-def test_crt_gemm_integer_exact(handle, ta, tb):
+def test_crt_gemm_integer_exact(handle, form, ta, tb):
     rng = np.random.default_rng(11)
     m, n, k = 300, 270, 1000
     Ai = rng.integers(-(1 << 15), 1 << 15, size=(m, k))
@@ -73,7 +84,7 @@ def test_crt_gemm_integer_exact(handle, ta, tb):
 
 @pytest.mark.parametrize("m,n,k", [(128, 256, 64), (300, 200, 777), (1, 1, 1), (129, 65, 5000),
                                    (64, 300, 20000), (1000, 513, 4096)])
-def test_crt_gemm_fp64_accuracy(handle, m, n, k):
+def test_crt_gemm_fp64_accuracy(handle, form, m, n, k):
     rng = np.random.default_rng(m + n + k)
     A = np.asfortranarray(rng.standard_normal((m, k)) * np.exp(rng.uniform(-5, 5, size=(m, 1))))
     B = np.asfortranarray(rng.standard_normal((k, n)))
@@ -85,7 +96,7 @@ def test_crt_gemm_fp64_accuracy(handle, m, n, k):
     assert err < 2e-15, err
 
 
-def test_crt_gemm_bits_per_modulus(handle):
+def test_crt_gemm_bits_per_modulus(handle, form):
     """Fewer moduli keep fewer bits: 14 < 15 < 16 in accuracy; 16 at the 8-slice level."""
     rng = np.random.default_rng(3)
     m, n, k = 256, 512, 2048
@@ -101,7 +112,7 @@ def test_crt_gemm_bits_per_modulus(handle):
     assert errs[14] < 2.0 ** -40, errs
 
 
-def test_crt_gemm_zero_rows_and_columns(handle):
+def test_crt_gemm_zero_rows_and_columns(handle, form):
     rng = np.random.default_rng(4)
     m, n, k = 257, 300, 700
     A = np.asfortranarray(rng.standard_normal((m, k)))
@@ -162,7 +173,7 @@ def _mixed(h, side, uplo, trans, diag, m, n, alpha, A, B):
 
 
 @pytest.mark.parametrize("side,uplo,trans,diag", COMBOS)
-def test_mixed_trsm_crt_all_combos(handle, side, uplo, trans, diag):
+def test_mixed_trsm_crt_all_combos(handle, form, side, uplo, trans, diag):
     m, n = (2100, 300) if side == "L" else (300, 2100)
     k = m if side == "L" else n
     A, B = oracle.nan_triangle_problem(37, side, uplo, trans, diag, m, n, k + 3, m + 1, np.float64)
@@ -175,7 +186,7 @@ def test_mixed_trsm_crt_all_combos(handle, side, uplo, trans, diag):
 
 
 @pytest.mark.parametrize("kband", [0, 2, 4, 6])
-def test_mixed_trsm_crt_condition_bands(handle, kband):
+def test_mixed_trsm_crt_condition_bands(handle, form, kband):
     """Normwise forward error against the float128 oracle on the graded-singular-value bands
     (kappa_2 = 10^kband): the residue engine at the FP64 oracle's own level."""
     m, n = 1536, 24
