@@ -1105,12 +1105,28 @@ def run_case(args):
             else:
                 st = L.rocblas_b200_dgemm(*gemm_args)
             assert st == 0, st
+    if args.case in ("sliced", "crt"):
+        # one untimed call, then the steps with the library's kernel timer (the integer GEMM
+        # kernel alone) and CUDA events around the whole calls
+        run()
+        torch.cuda.synchronize()
+        L.rocblas_b200_kernel_timing_enable(1)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
     for _ in range(max(args.steps, 1)):
         run()
     torch.cuda.synchronize()
+    timing = ""
+    if args.case in ("sliced", "crt"):
+        ev1.record()
+        ev1.synchronize()
+        k_ms, _, k_n = kernel_timing(L, "sliced")
+        L.rocblas_b200_kernel_timing_enable(0)
+        timing = (f"; GEMM kernel {1000 * k_ms / max(k_n, 1):.0f} us per launch, whole call "
+                  f"{1000 * ev0.elapsed_time(ev1) / max(args.steps, 1):.0f} us")
     code = ctypes.c_int(-1)
     assert L.rocblas_b200_get_device_error(h.value, ctypes.byref(code)) == 0 and code.value == 0
-    print(f"case {args.case} m={m} n={n} k={k}: {args.steps} launches ok", flush=True)
+    print(f"case {args.case} m={m} n={n} k={k}: {args.steps} launches ok{timing}", flush=True)
     h.close()
 
 

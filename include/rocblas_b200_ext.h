@@ -392,8 +392,9 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed_host(rocblas_handle    ha
  * read or change one entry in the running process.  Keys: block_max_k, block_always_k,
  * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices, dmma_force_tile,
  * dmma_big_bk, oz_bn, oz_bk, chain_max_cols, chain_max_cols_f32, chain_w, mixed_chain_blocks,
- * host_step_blocks, sliced_k_chunk, refine_check_sms, wait_cycles_log2, chain_first_item,
- * mixed_moduli, strsm_slices, strsm_sliced_min_k.  Unknown keys or
+ * host_step_blocks, sliced_k_chunk, refine_check_sms, refine_check_flag, wait_cycles_log2,
+ * chain_first_item, mixed_moduli, crt_group_m, crt_min_tiles_pct, crt_pair, strsm_slices,
+ * strsm_sliced_min_k, trsv_flag_min_n, trsv_flag_nb.  Unknown keys or
  * out-of-range values return rocblas_status_invalid_value. */
 /* Per-launch timing of the main kernels with CUDA events on the launching stream, for
  * measuring one kernel's achieved rate inside a larger call.  enable != 0 starts recording
