@@ -1938,8 +1938,10 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     const MixedPlan plan  = mixed_plan(pr, S, moduli);
     const size_t    mn    = (size_t)m * n * sizeof(double);
     const size_t    smp   = (size_t)srows * scols * sizeof(double);
+    // the chain's strip width: 16 wastes half as much DMMA work on up to 8 tested columns
+    const int       ps_w  = tuning().refine_check_w == 16 && c <= 16 ? 16 : 32;
     const size_t    fl    = ps_flag    ? (size_t)nb_flag * 2 * sizeof(int)
-                            : ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, 32))
+                            : ps_chain ? chain_workspace_bytes(chain_shape(ps.k(), c, 1, ps_w))
                                        : 0;
     const size_t    o_b0  = align256(plan.total), o_r = o_b0 + align256(mn);
     const size_t    o_xs  = o_r + (max_it > 0 ? align256(mn) : 0), o_fl = o_xs + align256(smp);
@@ -2020,7 +2022,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
         count_launch();
     }
     else if(ps_chain && plan.recursive)
-        launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, 32, ws + o_fl);
+        launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, ps_w, ws + o_fl);
     else
         trsm_run<double>(ps, nullptr, false);
     cudaEventRecord(ev_ref, res.tri);

@@ -406,7 +406,9 @@ static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first
     // KCP: M's column index (K) is contiguous in memory when M(r, c) = A(c, r)
     const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
     const bool kcq = pr.side_left != 0;
-    if(w == 32)
+    if(w == 16)
+        launch_chain_w<T, 16, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+    else if(w == 32)
         launch_chain_w<T, 32, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
     else
         launch_chain_w<T, 64, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);

@@ -77,15 +77,20 @@ def _plain(h, side, uplo, trans, diag, m, n, alpha, A, B):
     return dm.to_host(dB)
 
 
-@pytest.mark.parametrize("check", [1, 0], ids=["flag-check", "chain-check"])
+CHECK_FORMS = {"flag-check": dict(refine_check_flag=1), "chain32-check": dict(refine_check_flag=0, refine_check_w=32),
+               "chain16-check": dict(refine_check_flag=0, refine_check_w=16)}
+
+
+@pytest.mark.parametrize("check", list(CHECK_FORMS))
 @pytest.mark.parametrize("side,uplo,trans,diag", COMBOS)
 def test_refined_all_combos(handle, side, uplo, trans, diag, check):
-    """Both forms of the test's FP64 solve of the sampled right-hand sides (the memory-bound
-    flag solve, the chain) agree with the precision form's first solve to the tolerance."""
+    """Every form of the test's FP64 solve of the sampled right-hand sides (the memory-bound
+    flag solve, the chain with 32- or 16-column strips) agrees with the precision form's first
+    solve to the tolerance."""
     m, n = (900, 120) if side == "L" else (120, 900)
     k = m if side == "L" else n
     A, B = oracle.nan_triangle_problem(41, side, uplo, trans, diag, m, n, k + 3, m + 2, np.float64)
-    with tuning(refine_check_flag=check, **SLICED_SMALL):
+    with tuning(**CHECK_FORMS[check], **SLICED_SMALL):
         out, info = _refined(handle, side, uplo, trans, diag, m, n, -0.75, A, B)
     assert info["error_estimate_first"] <= info["tolerance"], info
     X = oracle.trsm(side, uplo, trans, diag, -0.75, A, np.asfortranarray(B[:m]))
