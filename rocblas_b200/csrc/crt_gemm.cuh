@@ -571,6 +571,73 @@ __device__ __forceinline__ void crt_tile_coords(int t, int tiles_m, int tiles_n,
     nt = r / gm;
 }
 
+// x 2^E for an integer-valued x (|x| >= 1 or 0) by exact power-of-two factors: one factor when
+// 2^E is a normal double; else x 2^E1 (E1 clamped to the normal range, exact because |x| >= 1)
+// times 2^(E - E1), whose single rounding is the one of x 2^E; products below the smallest
+// subnormal become zero and above the largest double infinity, as for ldexp.
+__device__ __forceinline__ double crt_scale2(double x, int E)
+{
+    auto p2 = [](int e) { return __longlong_as_double((long long)(1023 + e) << 52); };
+    if(E >= -1022 && E <= 1023)
+        return x * p2(E);
+    const int E1 = E < 0 ? -1022 : 1023;
+    const int E2 = E - E1;
+    if(E2 < -1022)
+        return x * 0.0;
+    return (x * p2(E1)) * p2(E2 > 1023 ? 1023 : E2);
+}
+
+// Reconstruction of row `row`'s 16-column chunk ch of output tile (mt, nt) from the residues in
+// scratch slot `slot` (called by whole warps whose lanes take 32 consecutive rows of one chunk):
+// X rebuilt per entry, scaled by 2^(e_r + f_c - shift) and written as beta C + alpha X.
+template <int NM, int kTileRows>
+__device__ __forceinline__ void crt_rebuild_chunk(const CrtParams& p, const uint8_t* slots, int slot, int mt,
+                                                  int nt, int row, int ch, uint32_t rank, int lane,
+                                                  double beta, bool zero)
+{
+    constexpr int64_t kModBytes = (int64_t)kCrtChunks * kOzBM * 16; // one modulus in a slot
+    const int gr = mt * kTileRows + (int)rank * kOzBM + row;
+    int       er = gr < p.M ? p.exp_rows[gr] : 0;
+    if(er == kOzExpNone)
+        er = 0;
+    const uint8_t* src    = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)row * 16;
+    const bool     read_c = !zero && beta != 0.0;
+    const int      c0     = nt * kCrtBN + ch * 16;
+    // the chunk's 16 entries of C are loaded before the rebuild, together with the residues, so
+    // that their latency (C is usually in DRAM) is paid once per chunk instead of once per entry
+    double cin[16];
+#pragma unroll
+    for(int c = 0; c < 16; ++c)
+    {
+        const int gc = c0 + c;
+        cin[c] = gr < p.M && gc < p.N && read_c ? p.C[gr + (int64_t)gc * p.ldc] : 0.0;
+    }
+    // lane l holds the exponent of column c0 + (l & 15), read before any store to C
+    int ecl = c0 + (lane & 15) < p.N ? p.exp_cols[c0 + (lane & 15)] : 0;
+    ecl     = ecl == kOzExpNone ? 0 : ecl;
+    uint4 r[NM];
+#pragma unroll
+    for(int i = 0; i < NM; ++i)
+        r[i] = *reinterpret_cast<const uint4*>(src + (int64_t)i * kModBytes + (int64_t)ch * kOzBM * 16);
+    crt_static_for<0, 16>([&](auto Cc) {
+        constexpr int c    = decltype(Cc)::value;
+        const double  x    = crt_rebuild<NM, c>(r);
+        const int     gc   = c0 + c;
+        const int     ecol = __shfl_sync(0xffffffffu, ecl, c); // every lane, before the bounds test
+        if(gr >= p.M || gc >= p.N)
+            return;
+        const double pq = crt_scale2(x, er + ecol - p.shift);
+        double o;
+        if(zero)
+            o = 0.0;
+        else if(beta == 0.0)
+            o = p.alpha * pq;
+        else
+            o = fma(p.alpha, pq, beta * cin[c]);
+        p.C[gr + (int64_t)gc * p.ldc] = o;
+    });
+}
+
 // Stage of the copy ring: kCrtKS consecutive 64-deep K panels of one (tile, modulus) item,
 // the P tile (128 x 64 per panel) then the Q tile (256 x 64 per panel; the pair form: this CTA's
 // 128 columns); the residue kernel lays a row tile's K panels out back to back, so each operand
@@ -672,6 +739,8 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
+    const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
+    const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
     if(warp == 0 || warp == kCrtProdWarp2)
     {
         // ---------------- copy producers ----------------
@@ -845,17 +914,16 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
     else if(warp < 2 + kCrtResWarps + kCrtRebWarps)
     {
         // ---------------- reconstruction ----------------
-        // thread t: row t % 128, the t / 128-th share of the tile's 16-column chunks
+        // thread t: row t % 128, the t / 128-th share of the tile's 16-column chunks; the
+        // CTA's last tile is rebuilt by every warp of the CTA (below)
         constexpr int kChunksPer = kCrtChunks / (kCrtRebWarps / 4);
-        const int    t    = (warp - 2 - kCrtResWarps) * 32 + lane;
-        const int    row  = t & (kOzBM - 1);
-        const int    ch0  = (t >> 7) * kChunksPer;
-        const double beta = p.beta_ptr ? *p.beta_ptr : p.beta;
-        const bool   zero = p.ualpha_zero || (p.ualpha_ptr && *p.ualpha_ptr == 0.0);
-        for(int jt = 0; jt < my_tiles; ++jt)
+        const int     t   = (warp - 2 - kCrtResWarps) * 32 + lane;
+        const int     row = t & (kOzBM - 1);
+        const int     ch0 = (t >> 7) * kChunksPer;
+        for(int jt = 0; jt + 1 < my_tiles; ++jt)
         {
             const int slot = jt & 1;
-            // warp-uniform outcome: the shuffles below need the whole warp
+            // warp-uniform outcome: the shuffles of the rebuild need the whole warp
             if(!__all_sync(0xffffffffu, crt_wait(&slot_full[slot], (uint32_t)((jt >> 1) & 1), &abort_flag)))
             {
                 crt_fail(p.error, &abort_flag, 14);
@@ -863,58 +931,40 @@ __global__ void __launch_bounds__(kCrtThreads, 1) crt_gemm_kernel(const __grid_c
             }
             int mt, nt;
             crt_tile_coords(unit + jt * units, tiles_m, tiles_n, p.group_m, mt, nt);
-            const int gr = mt * kTileRows + (int)rank * kOzBM + row;
-            int       er = gr < p.M ? p.exp_rows[gr] : 0;
-            if(er == kOzExpNone)
-                er = 0;
-            const uint8_t* src = slots + (int64_t)slot * kCrtSlotBytes + (int64_t)row * 16;
-            const bool read_c = !zero && beta != 0.0;
 #pragma unroll 1
             for(int ch = ch0; ch < ch0 + kChunksPer; ++ch)
-            {
-                const int c0 = nt * kCrtBN + ch * 16;
-                // the chunk's 16 entries of C are loaded before the rebuild, together with the
-                // residues, so that their latency (C is usually in DRAM) is paid once per chunk
-                // instead of once per entry
-                double cin[16];
-#pragma unroll
-                for(int c = 0; c < 16; ++c)
-                {
-                    const int gc = c0 + c;
-                    cin[c] = gr < p.M && gc < p.N && read_c ? p.C[gr + (int64_t)gc * p.ldc] : 0.0;
-                }
-                // lane l holds the exponent of column c0 + (l & 15), read before any store to C
-                int ecl = c0 + (lane & 15) < p.N ? p.exp_cols[c0 + (lane & 15)] : 0;
-                ecl     = ecl == kOzExpNone ? 0 : ecl;
-                uint4 r[NM];
-#pragma unroll
-                for(int i = 0; i < NM; ++i)
-                    r[i] = *reinterpret_cast<const uint4*>(src + (int64_t)i * kModBytes + (int64_t)ch * kOzBM * 16);
-                auto out = [&](double x, int c) {
-                    const int gc   = c0 + c;
-                    const int ecol = __shfl_sync(0xffffffffu, ecl, c); // every lane, before the bounds test
-                    if(gr >= p.M || gc >= p.N)
-                        return;
-                    const int    E    = er + ecol - p.shift;
-                    const double pq = (E >= -1022 && E <= 1023)
-                                          ? x * __longlong_as_double((long long)(1023 + E) << 52)
-                                          : ldexp(x, E);
-                    double o;
-                    if(zero)
-                        o = 0.0;
-                    else if(beta == 0.0)
-                        o = p.alpha * pq;
-                    else
-                        o = fma(p.alpha, pq, beta * cin[c]);
-                    p.C[gr + (int64_t)gc * p.ldc] = o;
-                };
-                crt_static_for<0, 16>([&](auto Cc) {
-                    constexpr int c = decltype(Cc)::value;
-                    out(crt_rebuild<NM, c>(r), c);
-                });
-            }
+                crt_rebuild_chunk<NM, kTileRows>(p, slots, slot, mt, nt, row, ch, rank, lane, beta, zero);
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&slot_empty[slot])) : "memory");
         }
+    }
+
+    // ---------------- the last tile: every warp rebuilds ----------------
+    // After its last MMA nothing else is left for the CTA, so the producer, MMA and residue warps
+    // join the reconstruction warps on the last tile's 128 x 16 (row, chunk) units: unit u goes to
+    // helper thread u mod (helpers), and the 32 consecutive units of a warp are 32 rows of one
+    // chunk.  Each helper reaches this point when at most a few items of the last tile are left
+    // (the copies run a few stages ahead of the MMAs, the MMAs two items ahead of the residue
+    // warps), so its parity wait cannot see the slot's phase of two tiles before.  The pair's
+    // second CTA issues no MMAs: its warp 1 would arrive at the start and stays out.
+    __syncwarp(); // the producer and MMA warps' idle lanes wait for their lane 0
+    const bool idle_warp = PAIR && rank != 0 && warp == 1;
+    if(my_tiles > 0 && !idle_warp)
+    {
+        const int helpers = kCrtThreads - (PAIR && rank != 0 ? 32 : 0);
+        const int hid     = (int)threadIdx.x - (PAIR && rank != 0 && warp > 1 ? 32 : 0);
+        const int jt      = my_tiles - 1;
+        const int slot    = jt & 1;
+        if(__all_sync(0xffffffffu, crt_wait(&slot_full[slot], (uint32_t)((jt >> 1) & 1), &abort_flag)))
+        {
+            int mt, nt;
+            crt_tile_coords(unit + jt * units, tiles_m, tiles_n, p.group_m, mt, nt);
+#pragma unroll 1
+            for(int u = hid; u < kOzBM * kCrtChunks; u += helpers)
+                crt_rebuild_chunk<NM, kTileRows>(p, slots, slot, mt, nt, u & (kOzBM - 1), u / kOzBM, rank, lane,
+                                                 beta, zero);
+        }
+        else
+            crt_fail(p.error, &abort_flag, 15);
     }
 
     // ---------------- teardown ----------------
