@@ -1929,6 +1929,10 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     ps.ldb = srows;
     const bool ps_chain = use_chain(ps);
     ps.sm_count         = std::max(1, std::min(tuning().refine_check_sms, h->sm_count / 4));
+    // the test solve's chain in clusters of two CTAs (refine_check_pairs, an even SM count):
+    // it then holds whole SM pairs and the precision-form solve may use the CTA-pair GEMM
+    const bool ps_pairs = tuning().refine_check_pairs != 0 && ps.sm_count % 2 == 0
+                          && tuning().refine_check_flag == 0 && (h->sm_count - ps.sm_count) % 2 == 0;
     // up to 8 tested right-hand sides: the memory-bound flag-synchronised solve (one pass over
     // A's triangle for all of them), else the chain
     const bool ps_flag = c <= 8 && tuning().refine_check_flag != 0;
@@ -1994,6 +1998,7 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
     cudaStreamWaitEvent(res.tri, ev_inv, 0);
     ps.B      = strided<double>(Xs, 0);
     ps.stream = res.tri;
+    bool check_in_pairs = false;
     if(ps_flag)
     {
         // side L: op(A) x_v = alpha b_v, x_v a column of Xs (m x c); side R: x_v op(A) = alpha b_v
@@ -2022,13 +2027,17 @@ rocblas_status trsm_refined_impl(rocblas_handle h, rocblas_side side, rocblas_fi
         count_launch();
     }
     else if(ps_chain && plan.recursive)
-        launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, ps_w, ws + o_fl);
+    {
+        launch_chain_sub<double>(ps, 0, (int)ceil_div(ps.k(), kInvNB), 1, ps_w, ws + o_fl, ps_pairs);
+        check_in_pairs = ps_pairs;
+    }
     else
         trsm_run<double>(ps, nullptr, false);
     cudaEventRecord(ev_ref, res.tri);
 
     TrsmProblem<double> pr1 = pr; // the first solve shares the GPU with the reference solve
     pr1.sm_count            = std::max(1, h->sm_count - ps.sm_count);
+    pr1.crt_pair_ok         = check_in_pairs ? 1 : 0; // the test solve holds whole SM pairs
     if(!mixed_run(pr1, S, moduli, plan, ws, err, false))
         return rocblas_status_arch_mismatch;
     cudaStreamWaitEvent(s, ev_ref, 0);

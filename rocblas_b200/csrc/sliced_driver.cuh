@@ -64,6 +64,7 @@ struct SlicedGemm
     int           zero_guard;
     int           sms;        // SMs of the device (persistent grid)
     int           moduli = 0; // > 0: the residue (CRT) engine with this many moduli, else slices
+    int           pair_ok = 0; // the sms SMs are whole SM pairs although fewer than the device's
 };
 
 __global__ void oz_fill_kernel(int* p, int n, int v)
@@ -348,7 +349,8 @@ static bool run_crt_gemm(const SlicedGemm& g, void* ws, int* err_dev, cudaStream
         cudaGetLastError();
         dev_sms = INT_MAX;
     }
-    const bool    pair   = tuning().crt_pair != 0 && g.sms >= 2 && g.sms >= dev_sms && crt_encode_fn() != nullptr
+    const bool    pair   = tuning().crt_pair != 0 && g.sms >= 2 && (g.sms >= dev_sms || g.pair_ok)
+                      && crt_encode_fn() != nullptr
                       && (int64_t)g.moduli * round_up(std::max<int64_t>(g.M, g.N), 2 * kOzBM)
                                  * (crt_k_pad(std::min<int64_t>(std::max<int64_t>(g.K, 1), kchunk)) / kCrtBK)
                              < ((int64_t)1 << 31);
@@ -567,6 +569,7 @@ static bool sliced_trsm_update(const TrsmProblem<T>& q, int c_lo, int c_hi, int 
     g.ualpha_host = (double)q.alpha.val;
     g.zero_guard = 1;
     g.sms = q.sm_count;
+    g.pair_ok = q.crt_pair_ok;
     return run_sliced_gemm(g, ws, err, q.stream);
 }
 

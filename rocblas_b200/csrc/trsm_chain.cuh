@@ -546,8 +546,11 @@ inline size_t chain_workspace_bytes(const ChainShape& c)
     return chain_flags_bytes(c.items);
 }
 
+// cluster2: the grid as clusters of two CTAs (placement only; the kernel uses no cluster
+// feature), for an even grid
 template <typename T, int W, bool KCP, bool KCQ, bool VB>
-static void launch_chain_cfg(const ChainParams<T>& p, int sms, int64_t max_items, cudaStream_t s)
+static void launch_chain_cfg(const ChainParams<T>& p, int sms, int64_t max_items, cudaStream_t s,
+                             bool cluster2 = false)
 {
     using Cfg = ChainCfg<T, W, KCP, KCQ, VB>;
     auto kern = trsm_chain_kernel<T, W, KCP, KCQ, VB>;
@@ -558,21 +561,38 @@ static void launch_chain_cfg(const ChainParams<T>& p, int sms, int64_t max_items
     // algorithmic work (uniform batch): k * k * ncols per system, the trsm flop count
     const double work = VB ? 0.0 : (double)p.systems * p.k * (double)p.k * p.ncols;
     TimedLaunch tl(KernelClass::chain, s, work);
-    kern<<<(unsigned)grid, kChainThreads, Cfg::kSmem, s>>>(p);
+    if(cluster2 && grid % 2 == 0)
+    {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim          = dim3((unsigned)grid);
+        cfg.blockDim         = dim3(kChainThreads);
+        cfg.dynamicSmemBytes = Cfg::kSmem;
+        cfg.stream           = s;
+        cudaLaunchAttribute at[1];
+        at[0].id               = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs    = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kern, p);
+    }
+    else
+        kern<<<(unsigned)grid, kChainThreads, Cfg::kSmem, s>>>(p);
 }
 
 template <typename T, int W, bool VB>
 static void launch_chain_w(const ChainParams<T>& p, bool kcp, bool kcq, int sms, int64_t max_items,
-                           cudaStream_t s)
+                           cudaStream_t s, bool cluster2 = false)
 {
     if(kcp && kcq)
-        launch_chain_cfg<T, W, true, true, VB>(p, sms, max_items, s);
+        launch_chain_cfg<T, W, true, true, VB>(p, sms, max_items, s, cluster2);
     else if(kcp)
-        launch_chain_cfg<T, W, true, false, VB>(p, sms, max_items, s);
+        launch_chain_cfg<T, W, true, false, VB>(p, sms, max_items, s, cluster2);
     else if(kcq)
-        launch_chain_cfg<T, W, false, true, VB>(p, sms, max_items, s);
+        launch_chain_cfg<T, W, false, true, VB>(p, sms, max_items, s, cluster2);
     else
-        launch_chain_cfg<T, W, false, false, VB>(p, sms, max_items, s);
+        launch_chain_cfg<T, W, false, false, VB>(p, sms, max_items, s, cluster2);
 }
 
 } // namespace rb200

@@ -63,6 +63,8 @@ struct TrsmProblem
     cudaStream_t stream;
     int         sm_count;
     int*        err_dev;  // device error word of the bounded waits (or nullptr)
+    int         crt_pair_ok = 0; // the residue GEMM may run as CTA pairs on sm_count SMs that
+                                 // are whole SM pairs (set beside a kernel placed in pairs)
     int         k() const { return side_left ? m : n; }
     // op(A) lower?
     int oplower() const { return (!upper) != (trans != 0); }
@@ -366,7 +368,10 @@ __global__ void chain_set_counter_kernel(int* counter, int v)
 // Chain solve of the diagonal blocks [b0, b1) of pr (all of it: 0, nblk) with invA available:
 // `first` as in Recursive::solve; `ws` holds chain_workspace_bytes of the sub-problem.
 template <typename T>
-static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first, int w, void* ws)
+// cluster2: launch the CTAs as clusters of two (placement only: each pair takes both SMs of an SM
+// pair, so that a CTA-pair kernel beside it finds the other SMs in whole pairs)
+static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first, int w, void* ws,
+                             bool cluster2 = false)
 {
     const int        r0    = b0 * kInvNB;
     const int        kk    = std::min(b1 * kInvNB, pr.k()) - r0;
@@ -407,11 +412,11 @@ static void launch_chain_sub(const TrsmProblem<T>& pr, int b0, int b1, int first
     const bool tM  = pr.trans != (pr.side_left ? 0 : 1);
     const bool kcq = pr.side_left != 0;
     if(w == 16)
-        launch_chain_w<T, 16, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+        launch_chain_w<T, 16, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream, cluster2);
     else if(w == 32)
-        launch_chain_w<T, 32, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+        launch_chain_w<T, 32, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream, cluster2);
     else
-        launch_chain_w<T, 64, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream);
+        launch_chain_w<T, 64, false>(c, tM, kcq, pr.sm_count, cs.items, pr.stream, cluster2);
     count_launch();
 }
 

@@ -39,9 +39,11 @@ struct Tuning
     int sliced_k_chunk       = 16384; // sliced GEMM: K range per set of row / column exponents
                                       // (multiple of 64, at most 16384); shorter ranges keep
                                       // more bits of entries far below their row's maximum
-    int refine_check_sms     = 4;    // refined form: SMs of the FP64 solve of the tested
+    int refine_check_sms     = 6;    // refined form: SMs of the FP64 solve of the tested
                                      // right-hand sides, which runs beside the sliced solve
     int refine_check_w       = 32;   // refined form: strip width of that solve's chain (16, 32)
+    int refine_check_pairs   = 1;    // refined form: that chain in clusters of two CTAs, so the
+                                     // sliced solve beside it may run CTA-pair GEMMs
     int refine_check_flag    = 0;    // refined form: that solve as the memory-bound flag
                                      // solve (up to 8 right-hand sides; 0: the chain)
     int wait_cycles_log2     = 31;   // chain solve: a flag wait gives up after 2^this clock
@@ -91,6 +93,7 @@ static const TuningEntry kTuningEntries[] = {
     {"refine_check_sms", &Tuning::refine_check_sms, 1, 1024},
     {"refine_check_flag", &Tuning::refine_check_flag, 0, 1},
     {"refine_check_w", &Tuning::refine_check_w, 16, 32},
+    {"refine_check_pairs", &Tuning::refine_check_pairs, 0, 1},
     {"wait_cycles_log2", &Tuning::wait_cycles_log2, 10, 40},
     {"chain_first_item", &Tuning::chain_first_item, 0, 1 << 30},
     {"mixed_moduli", &Tuning::mixed_moduli, 0, 16},

@@ -77,8 +77,10 @@ def _plain(h, side, uplo, trans, diag, m, n, alpha, A, B):
     return dm.to_host(dB)
 
 
-CHECK_FORMS = {"flag-check": dict(refine_check_flag=1), "chain32-check": dict(refine_check_flag=0, refine_check_w=32),
-               "chain16-check": dict(refine_check_flag=0, refine_check_w=16)}
+CHECK_FORMS = {"flag-check": dict(refine_check_flag=1),
+               "chain32-check": dict(refine_check_flag=0, refine_check_w=32, refine_check_pairs=0),
+               "chain16-check": dict(refine_check_flag=0, refine_check_w=16, refine_check_pairs=0),
+               "paired-check": dict(refine_check_flag=0, refine_check_pairs=1)}
 
 
 @pytest.mark.parametrize("check", list(CHECK_FORMS))
