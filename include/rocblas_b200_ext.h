@@ -310,8 +310,9 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed(rocblas_handle    handle,
  *   X := precision-form solve of op(A) X = alpha B (or X op(A) = alpha B);
  *   test: `check_columns` evenly spaced right-hand sides (columns of B for side left, rows for
  *         side right) are also solved by the plain FP64 form, on a second stream and a few SMs
- *         of their own (tuning key refine_check_sms) while the precision-form solve runs on
- *         the others; the test passes when, for each of them,
+ *         of their own (tuning keys refine_check_sms, refine_check_pairs: 6 SMs held as SM
+ *         pairs) while the precision-form solve runs on the others; the test passes when, for
+ *         each of them,
  *         ||x - x_fp64||_inf <= tolerance * ||x_fp64||_inf;
  *   while the test fails and fewer than max_iterations corrections were made:
  *         R := alpha B - op(A) X in FP64 over all right-hand sides (DMMA tiles);
@@ -392,7 +393,8 @@ ROCBLAS_EXPORT rocblas_status rocblas_b200_dtrsm_mixed_host(rocblas_handle    ha
  * read or change one entry in the running process.  Keys: block_max_k, block_always_k,
  * block_min_strips_pct, sliced_min_k, dmma_big_tile_pct, mixed_slices, dmma_force_tile,
  * dmma_big_bk, oz_bn, oz_bk, chain_max_cols, chain_max_cols_f32, chain_w, mixed_chain_blocks,
- * host_step_blocks, sliced_k_chunk, refine_check_sms, refine_check_flag, wait_cycles_log2,
+ * host_step_blocks, sliced_k_chunk, refine_check_sms, refine_check_flag, refine_check_w,
+ * refine_check_pairs, wait_cycles_log2,
  * chain_first_item, mixed_moduli, crt_group_m, crt_min_tiles_pct, crt_pair, strsm_slices,
  * strsm_sliced_min_k, trsv_flag_min_n, trsv_flag_nb.  Unknown keys or
  * out-of-range values return rocblas_status_invalid_value. */
