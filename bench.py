@@ -50,11 +50,11 @@ SLICED_TRAFFIC_PER_LAUNCH = 1.0795e9
 SLICED_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum of "
                          "`bench.py --no-extras --steps 2 --warmup 3`: 77 launches, mean per launch "
                          "(0.248 / 1.035 / 4.496 GB for the 4 / 2 / 1 launches of each solve)")
-CRT_TRAFFIC_PER_LAUNCH = 2.08e9
+CRT_TRAFFIC_PER_LAUNCH = 1.91e9
 CRT_TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --case crt "
-                      "--moduli 16` at the solve's three update shapes (8192x4096x8192: 7.31 GB, 4096^3: "
-                      "2.19 GB, 2048x4096x2048: 0.72 GB per launch), weighted by their 1 / 2 / 4 launches "
-                      "per solve (16384-deep exponent chunks)")
+                      "--moduli 16` (CTA-pair form) at the solve's three update shapes (8192x4096x8192: "
+                      "6.74 GB, 4096^3: 2.03 GB, 2048x4096x2048: 0.64 GB per launch), weighted by their "
+                      "1 / 2 / 4 launches per solve (16384-deep exponent chunks)")
 CHAIN_TRAFFIC_PER_LAUNCH = 35.57e9
 CHAIN_TRAFFIC_SOURCE = ("same capture: the 8 plain-solve launches of trsm_chain_kernel (45.5 ms each); "
                         "A (1.07 GB) is streamed once per 64-column strip group")
