@@ -1,6 +1,7 @@
-// Single right-hand side triangular solve, op(A) x = b (rocblas_?trsv with one vector), as a
-// memory-bound kernel: the work is one read of A's triangle (n^2 / 2 elements) and the bound is
-// HBM bandwidth, not arithmetic.
+// Triangular solve of one or a few right-hand sides, op(A) x_v = alpha b_v (rocblas_?trsv with
+// one vector; up to 8 vectors for the refined form's test solve), as a memory-bound kernel: the
+// work is one read of A's triangle (n^2 / 2 elements) for all of them and the bound is HBM
+// bandwidth, not arithmetic.
 //
 // The reference solves it with its own flag-synchronised substitution
 // (library/src/blas2/rocblas_trsv_kernels.cpp:461-775).  Here:
@@ -14,10 +15,11 @@
 //     waits (bounded) for block j's flag, then reads x_j (bypassing L1) and accumulates; the
 //     tiles of finished blocks stream at full speed and only the last ones wait;
 //   * before any wait the CTA stages its diagonal block in shared memory and inverts it (64
-//     threads, one column each); after the tiles, the partial sums of the 8 warps meet in shared
-//     memory and x_b = inv(M_bb) (b_b - sum) is one 64 x 64 product, so that the critical path
-//     from one block's flag to the next is a tile product, a reduction and that product; the
-//     CTA writes x_b, fences, and sets block b's flag.
+//     threads per 64-row half, one column each); after the tiles, the partial sums of the 8
+//     warps meet in shared memory and x_b = inv(M_bb) (alpha b_b - sum) is one product with the
+//     inverse per right-hand side, so that the critical path from one block's flag to the next
+//     is a tile product, a reduction and that product; the CTA writes x_b, fences, and sets
+//     block b's flag.
 // A wait that runs out records error 5 in the handle's error word and the CTA stops; the
 // blocks after it then stop too (their waits run out), and the call reports the error through
 // rocblas_b200_get_device_error.
